@@ -1,0 +1,292 @@
+"""Initial data for the SPB 6+1-equation two-phase solver.
+
+Every case is a dict of solver settings (the fields of ``spb6g_config`` in
+``include/spb6g.h``) plus the initial conservative state ``U`` as a float64
+array of shape (ny, nx, 8) in the reference variable order
+alpha1, m1, m2, rho*u, rho*v, eps1, eps2, E (src/spb6_physics_omp.h:27-28).
+
+Two families:
+
+* reference cases (``reference_case``): a few of the reference's own
+  ``test_setup``/``test_state`` entries (src/spb6_physics_omp.h:1017-1157),
+  restated with the same arithmetic so the states are bitwise identical to the
+  reference's ``u_initialization`` for SUBCELL = 1;
+* seeded synthetic workloads (``water_air_tube``, ``bubble_field``,
+  ``shock_bubble``, ``riemann_batch``, ``lowmach_bubbles``) used by the bench
+  and the parity tests.  They are generated from ``numpy.random.default_rng``
+  with a recorded seed.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+NUM_VARS = 8
+IA1, IM1, IM2, IMU, IMV, IE1, IE2, IEN = range(8)
+BC_TRANS, BC_WALL, BC_PERIODIC, BC_PRES = 0, 1, 2, 3
+
+WATER_SG = dict(g=4.4, pinf=6e8, q=0.0, qp=0.0, cv=1000.0, b=0.0)
+AIR_SG = dict(g=1.4, pinf=0.0, q=0.0, qp=0.0, cv=1000.0, b=0.0)
+
+
+def default_settings() -> dict:
+    """Solver settings with the reference's defaults (src/SPB6_PC_IMEX_omp.cpp:55-95)."""
+    return dict(
+        nx=100, ny=1, x0=0.0, x1=1.0, y0=0.0, y1=1.0,
+        bc=[BC_TRANS] * 4, bcu=[0.0] * 4, bcp=[0.0] * 4,
+        phases=[dict(WATER_SG), dict(AIR_SG)],
+        rk=2, cfl=0.2, cfl_ac=0.4, ramp=1, dtfix=0.0, rus_local=1, limiter=1,
+        acdt=0, newton_tol=1e-13, newton_iter=60, bicg_tol=1e-13, bicg_iter=4000,
+        share_mode=0, tend=1.0,
+    )
+
+
+def eps_amp(ph: dict, a, m, p):
+    """Phase internal energy per unit volume (SG/NASG), src/spb6_physics_omp.h:71-73."""
+    return (p + ph["g"] * ph["pinf"]) * (a - m * ph["b"]) / (ph["g"] - 1.0) + m * ph["q"]
+
+
+def prim2cell(phases, a1, r1, r2, u, v, p1, p2):
+    """Primitive -> conservative, src/spb6_physics_omp.h:904-909 (vectorised, same op order)."""
+    a1 = np.asarray(a1, dtype=np.float64)
+    a2 = 1 - a1
+    m1 = a1 * r1
+    m2 = a2 * r2
+    rho = m1 + m2
+    out = np.empty(np.broadcast(a1, r1, r2, u, v, p1, p2).shape + (NUM_VARS,))
+    out[..., IA1] = a1
+    out[..., IM1] = m1
+    out[..., IM2] = m2
+    out[..., IMU] = rho * u
+    out[..., IMV] = rho * v
+    out[..., IE1] = eps_amp(phases[0], a1, m1, p1)
+    out[..., IE2] = eps_amp(phases[1], a2, m2, p2)
+    out[..., IEN] = out[..., IE1] + out[..., IE2] + 0.5 * rho * (u * u + v * v)
+    return out
+
+
+def cell_centres(cfg: dict):
+    nx, ny = cfg["nx"], cfg["ny"]
+    dx = (cfg["x1"] - cfg["x0"]) / nx
+    dy = (cfg["y1"] - cfg["y0"]) / ny
+    x = cfg["x0"] + (np.arange(nx) + 0.5) * dx
+    y = cfg["y0"] + (np.arange(ny) + 0.5) * dy
+    return x, y, dx, dy
+
+
+# --------------------------------------------------------------------------------------------
+# Reference cases (test_setup / test_state, src/spb6_physics_omp.h:1017-1157)
+# --------------------------------------------------------------------------------------------
+def reference_case(case: int, nx: int | None = None) -> dict:
+    """A subset of the reference's 1D SG cases: 4 (interface advection), 5 (SPB 4.3.1
+    water-air), 80-88 (Schropff 2026 Riemann problems)."""
+    c = default_settings()
+    air, water = dict(AIR_SG), dict(WATER_SG)
+    if case == 4:
+        c.update(phases=[water, air], tend=2.79e-3, nx=200)
+    elif case == 5:
+        c.update(phases=[water, air], tend=240e-6, nx=1000)
+    elif case in (80, 82, 83, 84):
+        c.update(phases=[dict(air), dict(air)], nx=1000,
+                 tend={80: 0.5, 82: 0.14, 83: 2.5e-6, 84: 0.15}[case])
+    elif case in (81, 85):
+        c.update(phases=[dict(water), dict(water)], nx=1000, tend=1e-4 if case == 81 else 0.15e-3)
+    elif case in (86, 87):
+        c.update(phases=[water, air], nx=1000, tend=0.25 if case == 86 else 241e-6)
+    elif case == 88:
+        c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=1000, tend=30e-6)
+    else:
+        raise ValueError(f"reference case {case} is not restated here")
+    if nx is not None:
+        c["nx"] = nx
+    c["case"] = case
+    x, _, _, _ = cell_centres(c)
+    ph = c["phases"]
+    if case == 4:
+        L = x < 0.5
+        U = prim2cell(ph, np.where(L, 1 - 1e-8, 1e-8), 1000.0, 10.0, 100.0, 0.0, 1e5, 1e5)
+    elif case == 5:
+        L = x < 0.75
+        pl = np.where(L, 1e9, 1e5)
+        U = prim2cell(ph, np.where(L, 1 - 1e-6, 1e-6), 1000.0, 1.0, 0.0, 0.0, pl, pl)
+    elif case in (80, 81, 82, 83, 84, 85):
+        xi, rL, uL, pL, rR, uR, pR = {
+            80: (0.25, 1000, 1, 1e5, 0.01, 1, 1e5),
+            81: (0.5, 1000, 0, 1e8, 1000, 15, 0.98e8),
+            82: (0.5, 0.445, 0.698, 3.528, 0.5, 0, 0.571),
+            83: (0.5, 1, 0, 1e10, 0.125, 0, 0.1),
+            84: (0.5, 1, -1, 0.4, 1, 1, 0.4),
+            85: (0.5, 1000, 0, 1e6, 1000, 0, 1e5),
+        }[case]
+        L = x < xi
+        r = np.where(L, float(rL), float(rR))
+        u = np.where(L, float(uL), float(uR))
+        p = np.where(L, float(pL), float(pR))
+        U = prim2cell(ph, np.full_like(x, 1 - 1e-8), r, r, u, 0.0, p, p)
+    elif case in (86, 87):
+        adv = case == 86
+        L = x < (0.25 if adv else 0.7)
+        p = np.full_like(x, 1e5) if adv else np.where(L, 1e9, 1e5)
+        U = prim2cell(ph, np.where(L, 1 - 1e-7, 1e-7), 1000.0, 0.01 if adv else 50.0, 1.0 if adv else 0.0, 0.0, p, p)
+    else:  # 88
+        p = np.where(x < 0.6, 1e10, 1e5)
+        U = prim2cell(ph, np.full_like(x, 0.5954), 1185.0, 3622.0, 0.0, 0.0, p, p)
+    c["U"] = U.reshape(1, c["nx"], NUM_VARS)
+    return c
+
+
+# --------------------------------------------------------------------------------------------
+# Synthetic workloads
+# --------------------------------------------------------------------------------------------
+def water_air_tube(nx: int = 1000) -> dict:
+    """1D water-air shock tube: water SG (4.4, 6e8) | air (1.4, 0) on [0, 1] m, interface 0.7,
+    alpha_w 1-1e-6 | 1e-6, rho_w 1000, rho_a 50, p 1e9 | 1e5, u = 0; transmissive; material
+    CFL 0.5; Newton tol 1e-10, BiCGStab tol 1e-12; t_end 240 us."""
+    c = default_settings()
+    c.update(nx=nx, ny=1, phases=[dict(WATER_SG), dict(AIR_SG)], cfl=0.5, newton_tol=1e-10,
+             bicg_tol=1e-12, tend=240e-6)
+    x, _, _, _ = cell_centres(c)
+    L = x < 0.7
+    p = np.where(L, 1e9, 1e5)
+    c["U"] = prim2cell(c["phases"], np.where(L, 1 - 1e-6, 1e-6), 1000.0, 50.0, 0.0, 0.0, p, p).reshape(1, nx, 8)
+    c["workload"] = f"water-air shock tube 1D, {nx} cells"
+    return c
+
+
+def _place_bubbles(rng, n, rmin, rmax, dx, lo=0.0, hi=1.0, ylo=0.0, yhi=1.0, tries=100000):
+    """Rejection-sample n non-overlapping discs: radius U[rmin, rmax], centre uniform in
+    [R, 1-R]^2, |c_i - c_j| > R_i + R_j + 4 dx."""
+    out = []
+    for _ in range(tries):
+        if len(out) == n:
+            break
+        R = rng.uniform(rmin, rmax)
+        cx = rng.uniform(lo + R, hi - R)
+        cy = rng.uniform(ylo + R, yhi - R)
+        if all(math.hypot(cx - qx, cy - qy) > R + qR + 4 * dx for qx, qy, qR in out):
+            out.append((cx, cy, R))
+    if len(out) < n:
+        raise RuntimeError("could not place the requested bubbles")
+    return out
+
+
+def _bubble_blend(x, y, bubbles, dx):
+    """f = 1/2 (1 + tanh((r - R)/(2 dx))), 0 inside a bubble and 1 in the liquid; the nearest
+    bubble (minimum of f over the non-overlapping bubbles) decides."""
+    X, Y = np.meshgrid(x, y)
+    f = np.ones_like(X)
+    for cx, cy, R in bubbles:
+        r = np.hypot(X - cx, Y - cy)
+        f = np.minimum(f, 0.5 * (1.0 + np.tanh((r - R) / (2.0 * dx))))
+    return f
+
+
+def bubble_field(n: int = 1024, seed: int = 0, nbub: int = 8, steps: int = 200) -> dict:
+    """Water at rest (SG 4.4/6e8, rho 1000, p 1e7) with `nbub` air bubbles (alpha_w 1e-6,
+    rho_a 1, p 1e5) on an n x n grid over [0, 1]^2; radii U[0.03, 0.08]; tanh profile over
+    2 cells; transmissive; material CFL 0.5; Newton tol 1e-10, BiCGStab tol 1e-12."""
+    c = default_settings()
+    c.update(nx=n, ny=n, phases=[dict(WATER_SG), dict(AIR_SG)], cfl=0.5, newton_tol=1e-10,
+             bicg_tol=1e-12, tend=1.0)
+    x, y, dx, _ = cell_centres(c)
+    rng = np.random.default_rng(seed)
+    bubbles = _place_bubbles(rng, nbub, 0.03, 0.08, dx)
+    f = _bubble_blend(x, y, bubbles, dx)
+    a1 = 1e-6 + (1 - 1e-6 - 1e-6) * f
+    p = 1e5 + (1e7 - 1e5) * f
+    c["U"] = prim2cell(c["phases"], a1, 1000.0, 1.0, 0.0, 0.0, p, p)
+    c["seed"], c["bubbles"], c["steps"] = seed, bubbles, steps
+    c["workload"] = f"water with {nbub} air bubbles 2D, {n}x{n} cells"
+    return c
+
+
+def shock_bubble(nx: int = 2048, ny: int = 1024) -> dict:
+    """Mach-1.5 planar shock in air (1.4, 0; 1.29 kg/m3, 101325 Pa) moving left onto a light-gas
+    bubble (1.67, 0; rho 0.167, R 0.1 at (0.35, 0.5)) on [0, 2] x [0, 1] m; post-shock state from
+    the ideal-gas Rankine-Hugoniot relations as in the reference's case 70
+    (src/spb6_physics_omp.h:1098-1104); shock front at x = 0.5."""
+    c = default_settings()
+    c.update(nx=nx, ny=ny, x0=0.0, x1=2.0, y0=0.0, y1=1.0,
+             phases=[dict(AIR_SG), dict(AIR_SG, g=1.67)], tend=1.0)
+    x, y, dx, _ = cell_centres(c)
+    g, Ms, p0, r0 = 1.4, 1.5, 101325.0, 1.29
+    c0 = math.sqrt(g * p0 / r0)
+    p1 = p0 * (1 + 2 * g / (g + 1) * (Ms * Ms - 1))
+    r1 = r0 * (g + 1) * Ms * Ms / ((g - 1) * Ms * Ms + 2)
+    u1 = -Ms * c0 * (1 - r0 / r1)
+    X, Y = np.meshgrid(x, y)
+    inside = (X - 0.35) ** 2 + (Y - 0.5) ** 2 < 0.1 * 0.1
+    post = X > 0.5
+    a1 = np.where(post, 1 - 1e-6, np.where(inside, 1e-6, 1 - 1e-6))
+    r_air = np.where(post, r1, r0)
+    u = np.where(post, u1, 0.0)
+    p = np.where(post, p1, p0)
+    c["U"] = prim2cell(c["phases"], a1, r_air, 0.167, u, 0.0, p, p)
+    c["workload"] = f"Mach-1.5 shock on a light-gas bubble 2D, {nx}x{ny} cells"
+    return c
+
+
+def lowmach_bubbles(n: int = 2048, seed: int = 0, nbub: int = 16, amp: float = 15.0) -> dict:
+    """Low-Mach water field (p 1e5, rho 1000) with a seeded divergence-free velocity of max
+    amplitude `amp` m/s from a stream function of Fourier modes 1 <= |k| <= 4, differenced at
+    cell centres (discrete divergence zero, as the reference's wellprep,
+    src/SPB6_PC_IMEX_omp.cpp:1260-1272), and `nbub` air bubbles (rho 1, p 1e5, radii
+    U[0.01, 0.04]); periodic; material CFL 0.8; Newton tol 1e-10, BiCGStab tol 1e-10."""
+    c = default_settings()
+    c.update(nx=n, ny=n, bc=[BC_PERIODIC] * 4, phases=[dict(WATER_SG), dict(AIR_SG)], cfl=0.8,
+             newton_tol=1e-10, bicg_tol=1e-10, tend=1.0)
+    x, y, dx, dy = cell_centres(c)
+    rng = np.random.default_rng(seed)
+    modes = [(kx, ky) for kx in range(-4, 5) for ky in range(-4, 5) if 1 <= math.hypot(kx, ky) <= 4]
+    coef = rng.normal(size=(len(modes), 2))
+
+    def psi(X, Y):
+        s = np.zeros_like(X)
+        for (kx, ky), (a, b) in zip(modes, coef):
+            ph = 2 * math.pi * (kx * X + ky * Y)
+            s += a * np.sin(ph) + b * np.cos(ph)
+        return s
+    X, Y = np.meshgrid(x, y)
+    u = (psi(X, Y + dy) - psi(X, Y - dy)) / (2 * dy)
+    v = -(psi(X + dx, Y) - psi(X - dx, Y)) / (2 * dx)
+    scale = amp / max(np.abs(u).max(), np.abs(v).max())
+    u, v = u * scale, v * scale
+    bubbles = _place_bubbles(rng, nbub, 0.01, 0.04, dx)
+    f = _bubble_blend(x, y, bubbles, dx)
+    a1 = 1e-6 + (1 - 1e-6 - 1e-6) * f
+    c["U"] = prim2cell(c["phases"], a1, 1000.0, 1.0, u, v, 1e5, 1e5)
+    c["seed"], c["bubbles"] = seed, bubbles
+    c["workload"] = f"low-Mach water with {nbub} bubbles 2D periodic, {n}x{n} cells"
+    return c
+
+
+NASG_LIQ = dict(g=2.35, pinf=4e8, q=0.0, qp=0.0, cv=1000.0, b=7.5e-4)
+NASG_VAP = dict(g=1.025, pinf=0.0, q=0.0, qp=0.0, cv=1000.0, b=0.0)
+
+
+def riemann_batch(count: int = 512, seed: int = 0, nmin: int = 256, nmax: int = 4096, steps: int = 200):
+    """`count` independent 1D two-phase Riemann problems: cells U{nmin..nmax}, p_L log-U[1e6, 1e9],
+    p_R log-U[1e4, 1e6], interface U[0.3, 0.7], alpha 1-1e-6 | 1e-6, phase pair water/air SG
+    (rho 1000 / 50) or NASG liquid/vapour (rho 500 / 2) with probability 1/2; q = 0,
+    c_v = 1000; `steps` steps each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.integers(nmin, nmax + 1))
+        pL = float(np.exp(rng.uniform(np.log(1e6), np.log(1e9))))
+        pR = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+        x0 = float(rng.uniform(0.3, 0.7))
+        nasg = bool(rng.random() < 0.5)
+        c = default_settings()
+        ph = [dict(NASG_LIQ), dict(NASG_VAP)] if nasg else [dict(WATER_SG), dict(AIR_SG)]
+        rl, rv = (500.0, 2.0) if nasg else (1000.0, 50.0)
+        c.update(nx=n, ny=1, phases=ph, cfl=0.5, newton_tol=1e-10, bicg_tol=1e-12, tend=1.0)
+        x, _, _, _ = cell_centres(c)
+        L = x < x0
+        p = np.where(L, pL, pR)
+        c["U"] = prim2cell(ph, np.where(L, 1 - 1e-6, 1e-6), rl, rv, 0.0, 0.0, p, p).reshape(1, n, 8)
+        c.update(steps=steps, instance=k, nasg=nasg)
+        out.append(c)
+    return out

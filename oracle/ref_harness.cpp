@@ -1,0 +1,316 @@
+// Test infrastructure only -- never part of the product.
+//
+// Builds the UNMODIFIED reference solver (src/SPB6_PC_IMEX_omp.cpp with
+// src/spb6_physics_omp.h, compiled in place from the reference tree by
+// oracle/Makefile) into a command-line oracle that runs caller-supplied
+// initial data.  The reference has no API beyond main(); this translation unit
+// includes its sources and
+//   * renames its main() to ref_main() (still callable: "--main key=value ..."),
+//   * hooks cell_diag() (src/spb6_physics_omp.h:1161) to capture the final
+//     conservative state that write_profile() prints,
+//   * re-states main()'s set-up (src/SPB6_PC_IMEX_omp.cpp:1222-1315) and one
+//     iteration of its time loop (:1316-1384) over the reference's own stage
+//     functions (TVDReconstruction, Update, PressureSubsystem, caldt,
+//     bound_cond_u), so that a case file can inject any initial state,
+//     boundary set and tolerance (GMREStol has no command-line key, :84).
+// The "--main" path runs the reference main() itself; tests check that both
+// paths agree bitwise on the reference's own cases, which pins this loop.
+//
+// Usage:  spb6_ref case.bin result.bin
+//         spb6_ref --main result.bin case=87 N=200 ...
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <vector>
+#include <omp.h>
+
+static std::vector<double> g_capture;  // cells captured by the cell_diag hook
+
+#define cell_diag ref_cell_diag_orig
+#include "spb6_physics_omp.h"
+#undef cell_diag
+static void harness_cell_diag(const double* Q, double* o) {
+    g_capture.insert(g_capture.end(), Q, Q + NUM_VARS);
+    ref_cell_diag_orig(Q, o);
+}
+#define cell_diag harness_cell_diag
+#define main ref_main
+#include "SPB6_PC_IMEX_omp.cpp"
+#undef main
+#undef cell_diag
+
+#include "spb6_case.h"
+
+namespace {
+
+struct Harness {
+    std::unique_ptr<Grid> u_con, u_con_n, Qe, Qs, wxL, wxR, wyL, wyR, Ust;
+    std::unique_ptr<Array> phx, phy, a2s, ubx, uby;
+    std::unique_ptr<Tensor> Hs;
+    PField P, Pst;
+    double dtprev = -1;
+    bool startup = true;
+    double Ae[3][3], Ai[3][3];
+};
+
+void set_tab(Harness& H, int rk) {  // main's set_tab lambda, :1281-1303
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) H.Ae[a][b] = H.Ai[a][b] = 0;
+    if (rk == 1) {
+        H.Ai[0][0] = 1.0;
+    } else if (rk == 2) {
+        double bb = 1.0 - 1.0 / sqrt(2.0);
+        double cc = 1.0 / (2.0 * bb);
+        H.Ae[1][0] = cc;
+        H.Ai[0][0] = bb;
+        H.Ai[1][0] = 1 - bb;
+        H.Ai[1][1] = bb;
+    } else if (rk == 3) {
+        double r12 = 0.5, r13 = 1.0 / 3.0, r14 = 1.0 / 4.0;
+        H.Ae[1][0] = r12;
+        H.Ae[2][0] = r12;
+        H.Ae[2][1] = r12;
+        H.Ai[0][0] = r14;
+        H.Ai[1][1] = r14;
+        H.Ai[2][0] = r13;
+        H.Ai[2][1] = r13;
+        H.Ai[2][2] = r13;
+    }
+}
+
+// main() :1222-1315 for an injected state (cell values, not test_state()).
+void setup(Harness& H, const spb6_case& c, const double* U0) {
+    nxCells = c.nx;
+    nyCells = c.ny;
+    for (int k = 0; k < 2; k++) {
+        PH[k] = Phase{};
+        PH[k].g = c.g[k]; PH[k].pi = c.pinf[k]; PH[k].q = c.q[k];
+        PH[k].qp = c.qp[k]; PH[k].cv = c.cv[k]; PH[k].b = c.b[k];
+        PH[k].kind = 0;
+    }
+    RELAX_LEVEL = 0;
+    theta_rate = 0.0;
+    nu_rate = 0.0;
+    SHARE_MODE = c.share_mode;
+    RKs = c.rk;
+    CFL = c.cfl;
+    CFL_ac = c.cfl_ac;
+    RAMP = c.ramp;
+    DTFIX = c.dtfix;
+    NewtonTol = c.newton_tol;
+    NewtonIter = c.newton_iter;
+    GMREStol = c.bicg_tol;
+    GMRESiter = c.bicg_iter;
+    RUS_LOCAL = c.rus_local;
+    LIMITER = c.limiter;
+    recon = Minmod;
+    SpaceOrder = 2;
+    caltimestep = c.acdt ? Fullydt : IMEXdt;
+    JREUSE = 0;
+    x_0 = c.x0; x_1 = c.x1; y_0 = c.y0; y_1 = c.y1;
+    time_stop = c.tend;
+    // apply_bc_setup (physics :974-979) with the per-side codes given directly
+    x_bc = c.bc[0] == SPB6_BC_PERIODIC ? x_Periodic : (c.bc[0] == SPB6_BC_WALL ? x_Reflective : x_Transmissive);
+    y_bc = c.bc[2] == SPB6_BC_PERIODIC ? y_Periodic : (c.bc[2] == SPB6_BC_WALL ? y_Reflective : y_Transmissive);
+    for (int q = 0; q < 4; q++) { BCS[q] = c.bc[q]; BCU[q] = c.bcu[q]; BCP[q] = c.bcp[q]; }
+    SUBCELL = 1;
+    dx = (x_1 - x_0) / nxCells;
+    dy = (y_1 - y_0) / nyCells;
+    st_steps = st_reject = st_newton_it = st_stage = st_rk1 = st_floor = 0;
+    st_maxres = 0;
+    st_cl_fail = 0;
+
+    t = 0; dt = 0; timestep = 0;
+    const int nx = nxCells, ny = nyCells;
+    H.u_con.reset(new Grid(nx, ny)); H.u_con_n.reset(new Grid(nx, ny));
+    H.Qe.reset(new Grid(nx, ny)); H.Qs.reset(new Grid(nx, ny));
+    H.wxL.reset(new Grid(nx, ny)); H.wxR.reset(new Grid(nx, ny));
+    H.wyL.reset(new Grid(nx, ny)); H.wyR.reset(new Grid(nx, ny));
+    H.Ust.reset(new Grid(nx, ny));
+    H.phx.reset(new Array(nx, ny)); H.phy.reset(new Array(nx, ny));
+    H.a2s.reset(new Array(nx, ny)); H.ubx.reset(new Array(nx, ny)); H.uby.reset(new Array(nx, ny));
+    H.Hs.reset(new Tensor(3, nx, ny));
+    phi_x = H.phx.get(); phi_y = H.phy.get(); a2_star = H.a2s.get(); ube_x = H.ubx.get(); ube_y = H.uby.get();
+    wxL_g = H.wxL.get(); wxR_g = H.wxR.get(); wyL_g = H.wyL.get(); wyR_g = H.wyR.get();
+    Grid& u = *H.u_con;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+            for (int k = 0; k < NUM_VARS; k++) u(IG(i), IG(j), k) = U0[((size_t)j * nx + i) * NUM_VARS + k];
+    bound_cond_u(u);
+    H.P = PField{nx, ny, std::vector<double>((size_t)nx * ny, 0.0)};
+    P_REF = INF;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) P_REF = std::min(P_REF, pbar_of(u.cell(IG(i), IG(j))));
+    if (!std::isfinite(P_REF)) P_REF = 0.0;
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) H.P.at(i, j) = pbar_of(u.cell(IG(i), IG(j))) - P_REF;
+    H.dtprev = -1;
+    H.startup = true;
+    H.Pst = H.P;
+}
+
+// One iteration of main()'s do-while loop, :1316-1384.  Returns 0 ok, 2 failed.
+int step(Harness& H) {
+    Grid &u_con = *H.u_con, &u_con_n = *H.u_con_n, &Qe = *H.Qe, &Qs = *H.Qs, &Ust = *H.Ust;
+    Grid &w_xL = *H.wxL, &w_xR = *H.wxR, &w_yL = *H.wyL, &w_yR = *H.wyR;
+    Tensor& Hs = *H.Hs;
+    bool ramping = false;
+    if (DTFIX > 0) dt = DTFIX;
+    else {
+        dt = CFL * caldt(u_con, caltimestep == Fullydt);
+        if (RAMP) {
+            if (H.dtprev < 0) H.dtprev = CFL_ac * caldt(u_con, true) / ramp_factor;
+            if (dt > ramp_factor * H.dtprev) { dt = ramp_factor * H.dtprev; ramping = true; }
+        }
+        if (!std::isfinite(dt)) dt = CFL_ac * caldt(u_con, true);
+    }
+    dt = std::min(dt, time_stop - t);
+    if (!(dt > 1e-12 * time_stop)) return 2;
+    bool done = false;
+    for (int attempt = 0; attempt < 30 && !done; attempt++) {
+        const bool first_order = RAMP && ramping && H.startup;
+        const int rk = first_order ? 1 : RKs;
+        if (rk == 1) st_rk1++;
+        set_tab(H, rk);
+        copy(u_con_n, u_con);
+        H.Pst = H.P;
+        bool ok = true;
+        for (int rks = 0; rks < rk && ok; rks++) {
+            copy(Qe, u_con_n);
+            copy(Qs, u_con_n);
+            for (int r = 0; r < rks; r++) {
+#pragma omp parallel for collapse(2) schedule(static)
+                for (int i = ghost_cells; i < nxCells + ghost_cells; i++)
+                    for (int j = ghost_cells; j < nyCells + ghost_cells; j++)
+                        for (int k = 0; k < NUM_VARS; k++) {
+                            Qe(i, j, k) = Qe(i, j, k) + H.Ae[rks][r] * dt * Hs(r, i, j, k);
+                            Qs(i, j, k) = Qs(i, j, k) + H.Ai[rks][r] * dt * Hs(r, i, j, k);
+                        }
+            }
+            bound_cond_u(Qe);
+            bound_cond_u(Qs);
+            adt = H.Ai[rks][rks] * dt;
+            TVDReconstruction(Qe, w_xL, w_xR, w_yL, w_yR);
+            ok = Update(Ust, Qe, Qs, w_xL, w_xR, w_yL, w_yR);
+            ok = ok && PressureSubsystem(Ust, Qs, Qe, H.Pst, adt, rks);
+            if (ok) {
+#pragma omp parallel for collapse(2) schedule(static)
+                for (int i = ghost_cells; i < nxCells + ghost_cells; i++)
+                    for (int j = ghost_cells; j < nyCells + ghost_cells; j++)
+                        for (int k = 0; k < NUM_VARS; k++) Hs(rks, i, j, k) = (Ust(i, j, k) - Qs(i, j, k)) / adt;
+            }
+        }
+        if (ok) { copy(u_con, Ust); H.P = H.Pst; done = true; }
+        if (!done) { st_reject++; dt *= 0.5; }
+    }
+    if (!done) return 2;
+    t = t + dt; H.dtprev = dt; st_steps++; timestep++;
+    if (!ramping) H.startup = false;
+    return 0;
+}
+
+// Stage 0 of the first attempt with a given dt: the explicit predictor and the
+// implicit solve, for kernel-level parity dumps.
+int stage_dump(Harness& H, double dt_in, std::vector<double>& extra) {
+    Grid &u_con = *H.u_con, &Qe = *H.Qe, &Qs = *H.Qs, &Ust = *H.Ust;
+    dt = dt_in;
+    set_tab(H, RKs);
+    copy(Qe, u_con);
+    copy(Qs, u_con);
+    bound_cond_u(Qe);
+    bound_cond_u(Qs);
+    adt = H.Ai[0][0] * dt;
+    H.Pst = H.P;
+    TVDReconstruction(Qe, *H.wxL, *H.wxR, *H.wyL, *H.wyR);
+    bool ok = Update(Ust, Qe, Qs, *H.wxL, *H.wxR, *H.wyL, *H.wyR);
+    const int nx = nxCells, ny = nyCells, g = ghost_cells;
+    extra.clear();
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+            for (int k = 0; k < NUM_VARS; k++) extra.push_back(Ust(i + g, j + g, k));
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) extra.push_back((*a2_star)(i + g, j + g));
+    for (int j = 0; j < ny; j++)
+        for (int i = -1; i < nx; i++) extra.push_back((*ube_x)(i + g, j + g));
+    for (int j = -1; j < ny; j++)
+        for (int i = 0; i < nx; i++) extra.push_back(ny > 1 ? (*ube_y)(i + g, j + g) : 0.0);
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) extra.push_back((*phi_x)(i + g, j + g));
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) extra.push_back((*phi_y)(i + g, j + g));
+    ok = ok && PressureSubsystem(Ust, Qs, Qe, H.Pst, adt, 0);
+    if (!ok) return 2;
+    copy(u_con, Ust);
+    H.P = H.Pst;
+    return 0;
+}
+
+void totals(Grid& U, double M[3]) { conserved_totals(U, M); }
+
+int write_result(const char* path, const spb6_result& r, const std::vector<const std::vector<double>*>& blocks) {
+    FILE* f = fopen(path, "wb");
+    if (!f) return 1;
+    fwrite(&r, sizeof r, 1, f);
+    for (auto* b : blocks)
+        if (!b->empty()) fwrite(b->data(), sizeof(double), b->size(), f);
+    fclose(f);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc >= 3 && std::string(argv[1]) == "--main") {
+        // The reference main() itself; the final state is captured through cell_diag.
+        std::vector<char*> av;
+        av.push_back(argv[0]);
+        for (int a = 3; a < argc; a++) av.push_back(argv[a]);
+        static char outarg[] = "out=/dev/null";
+        av.push_back(outarg);
+        g_capture.clear();
+        const int rc = ref_main((int)av.size(), av.data());
+        spb6_result r{};
+        r.magic = SPB6_CASE_MAGIC; r.status = rc; r.nx = nxCells; r.ny = nyCells;
+        r.steps = st_steps; r.rejects = st_reject; r.rk1 = st_rk1; r.stages = st_stage;
+        r.newton_it = st_newton_it; r.floor_count = st_floor; r.t = t; r.dt = dt; r.maxres = st_maxres; r.p_ref = P_REF;
+        return write_result(argv[2], r, {&g_capture});
+    }
+    if (argc != 3) { fprintf(stderr, "usage: %s case.bin result.bin | --main result.bin key=value...\n", argv[0]); return 1; }
+    FILE* f = fopen(argv[1], "rb");
+    if (!f) { perror(argv[1]); return 1; }
+    spb6_case c;
+    if (fread(&c, sizeof c, 1, f) != 1 || c.magic != SPB6_CASE_MAGIC || c.version != SPB6_CASE_VERSION) {
+        fprintf(stderr, "bad case file\n");
+        return 1;
+    }
+    std::vector<double> U0((size_t)c.nx * c.ny * NUM_VARS);
+    if (fread(U0.data(), sizeof(double), U0.size(), f) != U0.size()) { fprintf(stderr, "short case file\n"); return 1; }
+    fclose(f);
+    if (c.threads > 0) omp_set_num_threads(c.threads);
+    Harness H;
+    setup(H, c, U0.data());
+    double M0[3]; totals(*H.u_con, M0);
+    spb6_result r{};
+    r.magic = SPB6_CASE_MAGIC; r.nx = c.nx; r.ny = c.ny;
+    std::vector<double> extra;
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = 0;
+    if (c.mode == SPB6_MODE_STAGE) {
+        rc = stage_dump(H, c.dtfix, extra);
+    } else if (c.mode == SPB6_MODE_STEPS) {
+        for (int s = 0; s < c.nsteps && rc == 0 && t < time_stop * (1 - 1e-12); s++) rc = step(H);
+    } else {
+        do { rc = step(H); } while (rc == 0 && t < time_stop * (1 - 1e-12));
+    }
+    r.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    double M1[3]; totals(*H.u_con, M1);
+    for (int q = 0; q < 3; q++) r.dM[q] = (M1[q] - M0[q]) / M0[q];
+    r.status = rc; r.steps = st_steps; r.rejects = st_reject; r.rk1 = st_rk1; r.stages = st_stage;
+    r.newton_it = st_newton_it; r.floor_count = st_floor; r.closure_fails = st_cl_fail;
+    r.t = t; r.dt = dt; r.maxres = st_maxres; r.p_ref = P_REF;
+    std::vector<double> U, P(H.P.P);
+    for (int j = 0; j < c.ny; j++)
+        for (int i = 0; i < c.nx; i++)
+            for (int k = 0; k < NUM_VARS; k++) U.push_back((*H.u_con)(IG(i), IG(j), k));
+    return write_result(argv[2], r, {&U, &P, &extra});
+}

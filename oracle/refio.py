@@ -1,0 +1,131 @@
+"""Test infrastructure: read/write the oracle case and result records (oracle/spb6_case.h)
+and run the two CPU oracles
+
+* ``run_ref``   -- oracle/_ref/spb6_ref, the reference solver compiled from its own sources;
+* ``run_port``  -- oracle/_build/libspb6_oracle.so, the C restatement (spb6_oracle.c).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(HERE, "_ref", "spb6_ref")
+PORT_LIB = os.path.join(HERE, "_build", "libspb6_oracle.so")
+MAGIC = 0x36425053
+MODE_STEPS, MODE_TEND, MODE_STAGE = 0, 1, 2
+
+CASE_DT = np.dtype([
+    ("magic", "<u4"), ("version", "<i4"), ("nx", "<i4"), ("ny", "<i4"), ("bc", "<i4", 4),
+    ("rk", "<i4"), ("ramp", "<i4"), ("rus_local", "<i4"), ("limiter", "<i4"), ("acdt", "<i4"),
+    ("newton_iter", "<i4"), ("bicg_iter", "<i4"), ("share_mode", "<i4"), ("mode", "<i4"), ("nsteps", "<i4"),
+    ("threads", "<i4"), ("pad", "<i4"),
+    ("x0", "<f8"), ("x1", "<f8"), ("y0", "<f8"), ("y1", "<f8"), ("bcu", "<f8", 4), ("bcp", "<f8", 4),
+    ("g", "<f8", 2), ("pinf", "<f8", 2), ("q", "<f8", 2), ("qp", "<f8", 2), ("cv", "<f8", 2), ("b", "<f8", 2),
+    ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
+])
+RESULT_DT = np.dtype([
+    ("magic", "<u4"), ("status", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
+    ("steps", "<i8"), ("rejects", "<i8"), ("rk1", "<i8"), ("stages", "<i8"), ("newton_it", "<i8"),
+    ("floor_count", "<i8"), ("bicg_it", "<i8"), ("closure_fails", "<i8"),
+    ("t", "<f8"), ("dt", "<f8"), ("maxres", "<f8"), ("p_ref", "<f8"), ("wall_s", "<f8"), ("dM", "<f8", 3),
+])
+
+
+def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0) -> np.ndarray:
+    r = np.zeros((), CASE_DT)
+    r["magic"], r["version"] = MAGIC, 1
+    for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
+        r[k] = int(cfg[k])
+    r["bc"] = cfg["bc"]
+    r["mode"], r["nsteps"], r["threads"] = mode, nsteps, threads
+    for k in ("x0", "x1", "y0", "y1", "cfl", "cfl_ac", "dtfix", "newton_tol", "bicg_tol", "tend"):
+        r[k] = float(cfg[k])
+    r["bcu"], r["bcp"] = cfg["bcu"], cfg["bcp"]
+    for f in ("g", "pinf", "q", "qp", "cv", "b"):
+        r[f] = [cfg["phases"][0][f], cfg["phases"][1][f]]
+    return r
+
+
+def parse_result(buf: bytes, nx: int, ny: int, mode: int) -> dict:
+    res = np.frombuffer(buf[:RESULT_DT.itemsize], RESULT_DT)[0]
+    arr = np.frombuffer(buf[RESULT_DT.itemsize:], "<f8")
+    n = nx * ny
+    out = {k: res[k].item() if res[k].ndim == 0 else np.array(res[k]) for k in RESULT_DT.names}
+    o = 0
+    out["U"] = arr[o:o + n * 8].reshape(ny, nx, 8).copy(); o += n * 8
+    out["P"] = arr[o:o + n].reshape(ny, nx).copy() if arr.size >= o + n else None; o += n
+    if mode == MODE_STAGE and arr.size > o:
+        out["Xs"] = arr[o:o + n * 8].reshape(ny, nx, 8).copy(); o += n * 8
+        out["a2s"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
+        out["ube_x"] = arr[o:o + (nx + 1) * ny].reshape(ny, nx + 1).copy(); o += (nx + 1) * ny
+        out["ube_y"] = arr[o:o + nx * (ny + 1)].reshape(ny + 1, nx).copy(); o += nx * (ny + 1)
+        out["phi_x"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
+        out["phi_y"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
+    return out
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def run_ref(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, timeout: float = 3600) -> dict:
+    """Run the reference solver (compiled from its sources) on cfg['U']."""
+    U = np.ascontiguousarray(cfg["U"], dtype="<f8")
+    with tempfile.TemporaryDirectory() as d:
+        ci, co = os.path.join(d, "case.bin"), os.path.join(d, "out.bin")
+        with open(ci, "wb") as f:
+            f.write(case_record(cfg, mode, nsteps, threads).tobytes())
+            f.write(U.tobytes())
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        subprocess.run([REF_BIN, ci, co], check=True, timeout=timeout, env=env)
+        with open(co, "rb") as f:
+            return parse_result(f.read(), cfg["nx"], cfg["ny"], mode)
+
+
+def run_ref_main(args: list[str], nx: int, ny: int = 1, timeout: float = 3600) -> dict:
+    """Run the reference's own main() (key=value arguments) and return its final state."""
+    with tempfile.TemporaryDirectory() as d:
+        co = os.path.join(d, "out.bin")
+        subprocess.run([REF_BIN, "--main", co, *args], check=True, timeout=timeout,
+                       stdout=subprocess.DEVNULL)
+        with open(co, "rb") as f:
+            return parse_result(f.read(), nx, ny, MODE_STEPS)
+
+
+_port = None
+
+
+def _port_lib():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            subprocess.run(["make", "-C", HERE, "oracle"], check=True, stdout=subprocess.DEVNULL)
+        lib = ctypes.CDLL(PORT_LIB)
+        lib.spb6_oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
+        lib.spb6_oracle_run.restype = ctypes.c_int
+        _port = lib
+    return _port
+
+
+def run_port(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 1) -> dict:
+    """Run the C restatement on cfg['U'] (same record format as run_ref)."""
+    lib = _port_lib()
+    rec = case_record(cfg, mode, nsteps, threads)
+    U = np.ascontiguousarray(cfg["U"], dtype="<f8")
+    nx, ny = cfg["nx"], cfg["ny"]
+    n = nx * ny
+    cap = RESULT_DT.itemsize + 8 * (n * 8 + n + n * 8 + n + (nx + 1) * ny + nx * (ny + 1) + 2 * n)
+    out = np.zeros(cap, np.uint8)
+    size = lib.spb6_oracle_run(rec.ctypes.data, U.ctypes.data, out.ctypes.data, cap)
+    if size <= 0:
+        raise RuntimeError(f"oracle port rejected the case ({size})")
+    return parse_result(out[:size].tobytes(), nx, ny, mode)

@@ -1,0 +1,51 @@
+/* Test infrastructure (oracle side): the binary case / result records shared by
+ * the reference harness (oracle/ref_harness.cpp, built into oracle/_ref/) and
+ * the C restatement (oracle/spb6_oracle.c).  Nothing in the product includes
+ * this file.
+ *
+ * A case file is one spb6_case record followed by the initial conservative
+ * state: nx*ny cells x 8 doubles, interior cells only, row-major (j outer,
+ * i inner), variables innermost in the reference order
+ * alpha1, m1, m2, rho*u, rho*v, eps1, eps2, E (src/spb6_physics_omp.h:27-28).
+ *
+ * A result file is one spb6_result record followed by U (same layout) and the
+ * pressure unknown P (nx*ny doubles, P - P_REF as in src/SPB6_PC_IMEX_omp.cpp:
+ * 1307-1312).  In stage-dump mode it is followed by the explicit predictor
+ * X* (nx*ny*8), alpha2* (nx*ny), the x-face velocities ube_x ((nx+1)*ny,
+ * faces i-1/2 .. nx-1/2 of interior rows), the y-face velocities ube_y
+ * (nx*(ny+1)), and the limiter factors phi_x, phi_y (nx*ny each).
+ */
+#ifndef SPB6_CASE_H
+#define SPB6_CASE_H
+#include <stdint.h>
+
+#define SPB6_CASE_MAGIC 0x36425053u /* "SPB6" */
+#define SPB6_CASE_VERSION 1
+
+enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2 };
+enum { SPB6_BC_TRANS = 0, SPB6_BC_WALL = 1, SPB6_BC_PERIODIC = 2, SPB6_BC_PRES = 3 };
+
+typedef struct {
+    uint32_t magic;
+    int32_t version;
+    int32_t nx, ny;
+    int32_t bc[4]; /* left, right, bottom, top */
+    int32_t rk, ramp, rus_local, limiter, acdt, newton_iter, bicg_iter, share_mode;
+    int32_t mode, nsteps;
+    int32_t threads, pad;
+    double x0, x1, y0, y1;
+    double bcu[4], bcp[4];
+    double g[2], pinf[2], q[2], qp[2], cv[2], b[2];
+    double cfl, cfl_ac, dtfix, newton_tol, bicg_tol, tend;
+} spb6_case;
+
+typedef struct {
+    uint32_t magic;
+    int32_t status; /* 0 ok, 1 bad input, 2 solver failure (as the reference's exit code 2) */
+    int32_t nx, ny;
+    int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it, closure_fails;
+    double t, dt, maxres, p_ref, wall_s;
+    double dM[3];
+} spb6_result;
+
+#endif
