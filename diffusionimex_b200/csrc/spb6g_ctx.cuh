@@ -1,0 +1,90 @@
+// Device views of one solver's buffers, passed by value to every kernel of the
+// stage pipeline, and the launchers the host driver calls.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "spb6g_common.cuh"
+
+namespace spb6g {
+
+// Device-resident scalars of one BiCGStab solve (GMRES_Solver, src/SPB6_PC_IMEX_omp.cpp:752-794).
+struct BicgScalars {
+    double rho, alpha, omega, bn, Einv, cb, r0A1, cc, cs, rr, r0r, ts, tt, ss;
+    double tol;
+    int maxit, iters, status, pad;
+};
+enum { BICG_RUNNING = 0, BICG_CONV = 1, BICG_FAIL = 2, BICG_CONV_HALF = 3 };
+
+// Reduction results read back by the host after a Newton decision point.
+struct NewtonScalars {
+    double res;    // residual max-norm of the last evaluation
+    double sn;     // Newton step criterion
+    double pmin;   // min pbar (P_REF) / caldt rates
+    double rate_x, rate_y;
+    double E, sumb, bb;  // Jacobian sums for the BiCGStab set-up
+    int fail;            // a residual / closure evaluation failed
+    int err;             // inadmissible state in the explicit part or stage prep
+    int nstrong;         // strong-shock worklist length
+    int pad;
+};
+
+struct Ctx {
+    Phys phy;
+    Geom g;
+    int n;
+    double tau, rx, ry, p_ref, adt;
+    // explicit stage
+    CState Qe, Qs;
+    State Xs;
+    double* a2s;
+    double *ube_x, *ube_y;                   // (nx+1)*ny, nx*(ny+1)
+    double *phiv_x, *phis_x, *slu_x, *slv_x;  // (nx+2)*ny
+    double *phiv_y, *phis_y, *slu_y, *slv_y;  // nx*(ny+2)
+    // stage data
+    double *ust, *vst, *kw, *qph0, *qph1;
+    double *fx_ubs, *fx_kp, *fx_wl, *fx_pv;
+    double *fy_ubs, *fy_kp, *fy_wl, *fy_pv;
+    int* strong_list;
+    // Newton
+    double *P, *Pn, *G, *Gn, *sc, *scn, *dP;
+    double *aC, *aW, *aE, *aS, *aN, *A1, *dinv;
+    double *br, *br0, *bp, *bv, *bq, *bs, *bu, *bt;
+    double *tcp, *tdp;
+    // final state
+    State Ust;
+    double* H;  // 8*n, this stage's derivative (U_s - Qs)/adt
+    // reductions
+    double* partials;
+    unsigned* counters;  // [16]
+    NewtonScalars* ns;
+    BicgScalars* bs_;
+};
+
+SPB6G_DEV size_t fxi(const Geom& g, int i, int j) { return (size_t)(i + 1) + (size_t)j * (g.nx + 1); }
+SPB6G_DEV size_t fyi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(j + 1) * g.nx; }
+SPB6G_DEV size_t rxi(const Geom& g, int i, int j) { return (size_t)(i + 1) + (size_t)j * (g.nx + 2); }
+SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(j + 1) * g.nx; }
+
+// ------------------------------------------------------------ launchers (spb6g_kernels.cu)
+int red_blocks(int n);
+void launch_combine(const Ctx& c, cudaStream_t st, const double* const* U, const double* Hs, int nH,
+                    const double* ae, const double* ai, double dt, double* const* Qe, double* const* Qs);
+void launch_recon(const Ctx& c, cudaStream_t st);
+void launch_update(const Ctx& c, cudaStream_t st);
+void launch_prep(const Ctx& c, cudaStream_t st);
+void launch_shock(const Ctx& c, cudaStream_t st);
+// mode 0: evaluate at P (writes G, sc);  mode 1: at Pn = P + lam dP (writes Pn, Gn, scn)
+void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam);
+void launch_jacobian(const Ctx& c, cudaStream_t st);
+void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit);
+void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity);
+void launch_thomas(const Ctx& c, cudaStream_t st);
+void launch_stepnorm(const Ctx& c, cudaStream_t st);
+void launch_apply_step(const Ctx& c, cudaStream_t st);
+void launch_floor(const Ctx& c, cudaStream_t st, double tol);
+void launch_final(const Ctx& c, cudaStream_t st);
+void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic);
+void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U);
+void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P);
+
+}  // namespace spb6g

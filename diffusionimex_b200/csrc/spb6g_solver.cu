@@ -1,0 +1,633 @@
+// Host driver of the B200 SPB6 IMEX solver and the C ABI of include/spb6g.h.
+//
+// The time loop, attempt/halving logic, stage combination and Newton control
+// follow main() (src/SPB6_PC_IMEX_omp.cpp:1316-1384) and Newton_Solver
+// (:799-904) decision for decision.  All field data stays on the device; the
+// host reads back only the scalars a decision needs (residual norm, step
+// criterion, BiCGStab status), through one pinned record per sync point.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/spb6g.h"
+#include "spb6g_ctx.cuh"
+
+using namespace spb6g;
+
+namespace {
+
+enum TimerGroup { TG_EXPLICIT = 0, TG_PREP, TG_SHOCK, TG_RESIDUAL, TG_JACOBIAN, TG_LINEAR, TG_FINAL, TG_CALDT, TG_COUNT };
+const char* kTimerNames[TG_COUNT] = {"explicit", "prep", "shock", "residual", "jacobian", "linear", "final", "caldt"};
+
+struct Pinned {
+    NewtonScalars ns;
+    BicgScalars bs;
+};
+
+}  // namespace
+
+struct spb6g_solver {
+    spb6g_config cfg;
+    Phys P;
+    Geom g;
+    int n = 0;
+    cudaStream_t st = nullptr;
+    std::vector<void*> allocs;
+    // state
+    double *U[NV], *Ust[NV], *Qe[NV], *Qs[NV], *Xs[NV];
+    double* Hs = nullptr;  // 3 stages x 8 x n
+    double* Pbuf[3] = {nullptr, nullptr, nullptr};
+    double* Pmain = nullptr;  // accepted pressure unknown; the other two buffers hold the Newton iterate and trial
+    Ctx c{};
+    Pinned* pin = nullptr;
+    // time state
+    double t = 0, dt = 0, dtprev = -1, p_ref = 0;
+    bool startup = true;
+    spb6g_stats stats{};
+    int bicg_parity = 0;
+    // timing
+    bool timing = false;
+    cudaEvent_t ev[2 * TG_COUNT];
+    double tms[TG_COUNT] = {};
+    int64_t tcnt[TG_COUNT] = {};
+    int open_group = -1;
+    int err = SPB6G_OK;
+};
+
+namespace {
+
+#define CK(x)                                                                                        \
+    do {                                                                                             \
+        cudaError_t e_ = (x);                                                                        \
+        if (e_ != cudaSuccess) {                                                                     \
+            fprintf(stderr, "spb6g: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return SPB6G_CUDA_ERROR;                                                                 \
+        }                                                                                            \
+    } while (0)
+
+double* dalloc(spb6g_solver* s, size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, (count ? count : 1) * sizeof(double)) != cudaSuccess) return nullptr;
+    cudaMemsetAsync(p, 0, (count ? count : 1) * sizeof(double), s->st);
+    s->allocs.push_back(p);
+    return (double*)p;
+}
+
+void tbegin(spb6g_solver* s, int g) {
+    if (!s->timing) return;
+    cudaEventRecord(s->ev[2 * g], s->st);
+    s->open_group = g;
+}
+void tend_(spb6g_solver* s, int g) {
+    if (!s->timing) return;
+    cudaEventRecord(s->ev[2 * g + 1], s->st);
+    cudaEventSynchronize(s->ev[2 * g + 1]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev[2 * g], s->ev[2 * g + 1]);
+    s->tms[g] += ms;
+    s->tcnt[g] += 1;
+    s->open_group = -1;
+}
+
+int sync_read(spb6g_solver* s, bool bicg) {
+    CK(cudaMemcpyAsync(&s->pin->ns, s->c.ns, sizeof(NewtonScalars), cudaMemcpyDeviceToHost, s->st));
+    if (bicg) CK(cudaMemcpyAsync(&s->pin->bs, s->c.bs_, sizeof(BicgScalars), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return SPB6G_OK;
+}
+int reset_flags(spb6g_solver* s) {
+    // fail, err, nstrong are contiguous ints at the end of NewtonScalars
+    CK(cudaMemsetAsync(&s->c.ns->fail, 0, 3 * sizeof(int), s->st));
+    return SPB6G_OK;
+}
+int reset_fail(spb6g_solver* s) {
+    CK(cudaMemsetAsync(&s->c.ns->fail, 0, sizeof(int), s->st));
+    return SPB6G_OK;
+}
+
+// Newton iterate and line-search trial live in the two buffers that are not Pmain.
+int begin_attempt_pressure(spb6g_solver* s) {
+    double* other[2];
+    int k = 0;
+    for (int b = 0; b < 3; b++)
+        if (s->Pbuf[b] != s->Pmain) other[k++] = s->Pbuf[b];
+    CK(cudaMemcpyAsync(other[0], s->Pmain, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    s->c.P = other[0];
+    s->c.Pn = other[1];
+    return SPB6G_OK;
+}
+
+void set_tab(int rk, double Ae[3][3], double Ai[3][3]) {  // main's set_tab, :1281-1303
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) Ae[a][b] = Ai[a][b] = 0;
+    if (rk == 1) {
+        Ai[0][0] = 1.0;
+    } else if (rk == 2) {
+        const double bb = 1.0 - 1.0 / std::sqrt(2.0), cc = 1.0 / (2.0 * bb);
+        Ae[1][0] = cc;
+        Ai[0][0] = bb;
+        Ai[1][0] = 1 - bb;
+        Ai[1][1] = bb;
+    } else if (rk == 3) {
+        const double r12 = 0.5, r13 = 1.0 / 3.0, r14 = 1.0 / 4.0;
+        Ae[1][0] = r12; Ae[2][0] = r12; Ae[2][1] = r12;
+        Ai[0][0] = r14; Ai[1][1] = r14; Ai[2][0] = r13; Ai[2][1] = r13; Ai[2][2] = r13;
+    }
+}
+
+int caldt(spb6g_solver* s, bool acoustic, double& inv) {
+    CState u;
+    for (int k = 0; k < NV; k++) u.v[k] = s->U[k];
+    tbegin(s, TG_CALDT);
+    launch_caldt(s->c, s->st, u, acoustic ? 1 : 0);
+    tend_(s, TG_CALDT);
+    int rc = sync_read(s, false);
+    if (rc) return rc;
+    const double rate = s->pin->ns.rate_x / s->g.dx + (s->g.ny > 1 ? s->pin->ns.rate_y / s->g.dy : 0.0);
+    inv = rate > 0 ? 1.0 / rate : INFINITY;
+    return SPB6G_OK;
+}
+
+// Newton_Solver (:799-904), jreuse = 0.  P lives in s->c.P (the stage pressure).
+int newton(spb6g_solver* s, double& resfinal) {
+    Ctx& c = s->c;
+    const bool tri = s->g.ny == 1 && s->g.bcs[0] != BC_PERIODIC;
+    const double tol = s->cfg.newton_tol;
+    if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+    tbegin(s, TG_RESIDUAL);
+    launch_residual(c, s->st, 0, 0.0);
+    tend_(s, TG_RESIDUAL);
+    if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+    if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
+    if (s->pin->ns.fail) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
+    double res = s->pin->ns.res;
+    for (int it = 0; it < s->cfg.newton_iter; it++) {
+        resfinal = res;
+        if (res < tol) return SPB6G_OK;
+        if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+        tbegin(s, TG_JACOBIAN);
+        launch_jacobian(c, s->st);
+        tend_(s, TG_JACOBIAN);
+        tbegin(s, TG_LINEAR);
+        if (tri) {
+            launch_thomas(c, s->st);
+            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            if (s->pin->ns.fail) { tend_(s, TG_LINEAR); return SPB6G_NEWTON_FAIL; }
+        } else {
+            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            if (s->pin->ns.fail) { tend_(s, TG_LINEAR); return SPB6G_NEWTON_FAIL; }
+            launch_bicg_init(c, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter);
+            s->bicg_parity = 0;
+            int chunk = 4;
+            for (;;) {
+                launch_bicg_iters(c, s->st, chunk, s->bicg_parity);
+                if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
+                if (s->pin->bs.status != BICG_RUNNING) break;
+                if (chunk < 32) chunk *= 2;
+            }
+            s->stats.bicg_it += s->pin->bs.iters;
+            if (s->pin->bs.status == BICG_FAIL) { tend_(s, TG_LINEAR); return SPB6G_LINEAR_FAIL; }
+        }
+        tend_(s, TG_LINEAR);
+        // step criterion (:870-879) and the first line-search trial (lam = 1) in one sync
+        if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+        tbegin(s, TG_RESIDUAL);
+        launch_stepnorm(c, s->st);
+        launch_residual(c, s->st, 1, 1.0);
+        tend_(s, TG_RESIDUAL);
+        if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+        if (s->pin->ns.sn < tol) {
+            launch_apply_step(c, s->st);
+            s->stats.newton_it++;
+            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+            tbegin(s, TG_RESIDUAL);
+            launch_residual(c, s->st, 0, 0.0);
+            tend_(s, TG_RESIDUAL);
+            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            if (s->pin->ns.fail) return SPB6G_NEWTON_FAIL;
+            resfinal = s->pin->ns.res;
+            return SPB6G_OK;
+        }
+        double lam = 1.0;
+        bool acc = false;
+        for (int ls = 0; ls < 40; ls++) {
+            if (ls > 0) {
+                if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+                tbegin(s, TG_RESIDUAL);
+                launch_residual(c, s->st, 1, lam);
+                tend_(s, TG_RESIDUAL);
+                if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            }
+            if (!s->pin->ns.fail) {
+                const double rn = s->pin->ns.res;
+                if (rn < res * (1.0 - 1e-4 * lam) || rn < tol) { acc = true; res = rn; break; }
+            }
+            lam *= 0.5;
+        }
+        if (!acc) {  // round-off floor acceptance (:890-899)
+            resfinal = res;
+            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+            launch_floor(c, s->st, tol);
+            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            if (s->pin->ns.fail) return SPB6G_NEWTON_FAIL;
+            s->stats.floor_count++;
+            return SPB6G_OK;
+        }
+        std::swap(c.P, c.Pn);
+        std::swap(c.G, c.Gn);
+        std::swap(c.sc, c.scn);
+        s->stats.newton_it++;
+    }
+    resfinal = res;
+    return res < tol ? SPB6G_OK : SPB6G_NEWTON_FAIL;
+}
+
+// One stage: combination, explicit predictor, stage data, Newton, final state and H_s.
+int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double dt) {
+    Ctx& c = s->c;
+    tbegin(s, TG_EXPLICIT);
+    if (rks == 0) {
+        for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->U[k]; c.Qs.v[k] = s->U[k]; }
+    } else {
+        const double ae[2] = {Ae[rks][0], Ae[rks][1]}, ai[2] = {Ai[rks][0], Ai[rks][1]};
+        launch_combine(c, s->st, s->U, s->Hs, rks, ae, ai, dt, s->Qe, s->Qs);
+        for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->Qe[k]; c.Qs.v[k] = s->Qs[k]; }
+    }
+    c.adt = Ai[rks][rks] * dt;
+    c.tau = c.adt;
+    c.rx = c.tau / s->g.dx;
+    c.ry = c.tau / s->g.dy;
+    c.H = s->Hs + (size_t)rks * NV * s->n;
+    if (reset_flags(s)) return SPB6G_CUDA_ERROR;
+    launch_recon(c, s->st);
+    launch_update(c, s->st);
+    tend_(s, TG_EXPLICIT);
+    tbegin(s, TG_PREP);
+    launch_prep(c, s->st);
+    tend_(s, TG_PREP);
+    tbegin(s, TG_SHOCK);
+    launch_shock(c, s->st);
+    tend_(s, TG_SHOCK);
+    double res = 0;
+    const int rc = newton(s, res);
+    if (rc != SPB6G_OK) return rc;
+    if (res > s->stats.maxres) s->stats.maxres = res;
+    if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+    tbegin(s, TG_FINAL);
+    launch_final(c, s->st);
+    tend_(s, TG_FINAL);
+    if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+    if (s->pin->ns.fail) return SPB6G_NEWTON_FAIL;
+    s->stats.stages++;
+    return SPB6G_OK;
+}
+
+// main()'s loop body (:1316-1384).
+int do_step(spb6g_solver* s) {
+    const spb6g_config& cf = s->cfg;
+    bool ramping = false;
+    double inv;
+    int rc;
+    if (cf.dtfix > 0) s->dt = cf.dtfix;
+    else {
+        if ((rc = caldt(s, cf.acdt != 0, inv))) return rc;
+        s->dt = cf.cfl * inv;
+        if (cf.ramp) {
+            if (s->dtprev < 0) {
+                if ((rc = caldt(s, true, inv))) return rc;
+                s->dtprev = cf.cfl_ac * inv / 1.2;
+            }
+            if (s->dt > 1.2 * s->dtprev) { s->dt = 1.2 * s->dtprev; ramping = true; }
+        }
+        if (!std::isfinite(s->dt)) {
+            if ((rc = caldt(s, true, inv))) return rc;
+            s->dt = cf.cfl_ac * inv;
+        }
+    }
+    s->dt = SMIN(s->dt, cf.tend - s->t);
+    if (!(s->dt > 1e-12 * cf.tend)) return SPB6G_DT_UNDERFLOW;
+    bool done = false;
+    double Ae[3][3], Ai[3][3];
+    for (int attempt = 0; attempt < 30 && !done; attempt++) {
+        const bool first_order = cf.ramp && ramping && s->startup;
+        const int rk = first_order ? 1 : cf.rk;
+        if (rk == 1) s->stats.rk1++;
+        set_tab(rk, Ae, Ai);
+        if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
+        bool ok = true;
+        for (int rks = 0; rks < rk && ok; rks++) {
+            rc = run_stage(s, rks, Ae, Ai, s->dt);
+            if (rc == SPB6G_CUDA_ERROR) return rc;
+            ok = rc == SPB6G_OK;
+        }
+        if (ok) {
+            for (int k = 0; k < NV; k++) std::swap(s->U[k], s->Ust[k]);
+            s->Pmain = s->c.P;  // the converged stage pressure becomes P (main :1374)
+            done = true;
+        }
+        if (!done) { s->stats.rejects++; s->dt *= 0.5; }
+    }
+    if (!done) return SPB6G_STEP_FAILED;
+    s->t = s->t + s->dt;
+    s->dtprev = s->dt;
+    s->stats.steps++;
+    if (!ramping) s->startup = false;
+    return SPB6G_OK;
+}
+
+}  // namespace
+
+// ============================================================ C ABI
+extern "C" {
+
+void spb6g_default_config(spb6g_config* cfg) {
+    if (!cfg) return;
+    memset(cfg, 0, sizeof *cfg);
+    cfg->nx = 1000; cfg->ny = 1;
+    cfg->x0 = 0; cfg->x1 = 1; cfg->y0 = 0; cfg->y1 = 1;
+    cfg->gamma[0] = 4.4; cfg->pinf[0] = 6e8; cfg->gamma[1] = 1.4; cfg->pinf[1] = 0;
+    cfg->cv[0] = cfg->cv[1] = 1000.0;
+    cfg->rk = 2; cfg->cfl = 0.2; cfg->cfl_ac = 0.4; cfg->ramp = 1; cfg->rus_local = 1; cfg->limiter = 1;
+    cfg->newton_tol = 1e-13; cfg->newton_iter = 60; cfg->bicg_tol = 1e-13; cfg->bicg_iter = 4000;
+    cfg->tend = 240e-6;
+}
+
+int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
+    if (!cfg || !out) return SPB6G_BAD_ARG;
+    *out = nullptr;
+    if (cfg->nx < 1 || cfg->ny < 1 || cfg->rk < 1 || cfg->rk > 3 || !(cfg->x1 > cfg->x0) || !(cfg->y1 > cfg->y0))
+        return SPB6G_BAD_ARG;
+    for (int q = 0; q < 4; q++)
+        if (cfg->bc[q] < 0 || cfg->bc[q] > 3) return SPB6G_BAD_ARG;
+    if ((cfg->bc[0] == SPB6G_BC_PERIODIC) != (cfg->bc[1] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
+    if ((cfg->bc[2] == SPB6G_BC_PERIODIC) != (cfg->bc[3] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
+    if (cfg->rus_local != 1) return SPB6G_UNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return SPB6G_NO_DEVICE;
+    spb6g_solver* s = new (std::nothrow) spb6g_solver();
+    if (!s) return SPB6G_BAD_ARG;
+    s->cfg = *cfg;
+    for (int k = 0; k < 2; k++) {
+        s->P.ph[k].g = cfg->gamma[k]; s->P.ph[k].pi = cfg->pinf[k]; s->P.ph[k].q = cfg->q[k];
+        s->P.ph[k].qp = cfg->qp[k]; s->P.ph[k].cv = cfg->cv[k]; s->P.ph[k].b = cfg->b[k];
+    }
+    s->P.share_mode = cfg->share_mode;
+    s->P.limiter = cfg->limiter;
+    s->P.rus_local = cfg->rus_local;
+    s->g.nx = cfg->nx; s->g.ny = cfg->ny;
+    for (int q = 0; q < 4; q++) { s->g.bcs[q] = cfg->bc[q]; s->g.bcu[q] = cfg->bcu[q]; s->g.bcp[q] = cfg->bcp[q]; }
+    s->g.dx = (cfg->x1 - cfg->x0) / cfg->nx;
+    s->g.dy = (cfg->y1 - cfg->y0) / cfg->ny;
+    const int nx = cfg->nx, ny = cfg->ny;
+    const size_t n = (size_t)nx * ny;
+    s->n = (int)n;
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { delete s; return SPB6G_CUDA_ERROR; }
+    bool ok = true;
+    auto A = [&](size_t cnt) { double* p = dalloc(s, cnt); if (!p) ok = false; return p; };
+    for (int k = 0; k < NV; k++) { s->U[k] = A(n); s->Ust[k] = A(n); s->Qe[k] = A(n); s->Qs[k] = A(n); s->Xs[k] = A(n); }
+    s->Hs = A(3 * NV * n);
+    for (int b = 0; b < 3; b++) s->Pbuf[b] = A(n);
+    s->Pmain = s->Pbuf[0];
+    Ctx& c = s->c;
+    c.P = s->Pbuf[1];
+    c.Pn = s->Pbuf[2];
+    c.g = s->g;
+    c.phy = s->P;
+    c.n = (int)n;
+    for (int k = 0; k < NV; k++) c.Xs.v[k] = s->Xs[k];
+    c.a2s = A(n);
+    c.ube_x = A((size_t)(nx + 1) * ny); c.ube_y = A((size_t)nx * (ny + 1));
+    const size_t nrx = (size_t)(nx + 2) * ny, nry = (size_t)nx * (ny + 2);
+    c.phiv_x = A(nrx); c.phis_x = A(nrx); c.slu_x = A(nrx); c.slv_x = A(nrx);
+    c.phiv_y = A(nry); c.phis_y = A(nry); c.slu_y = A(nry); c.slv_y = A(nry);
+    c.ust = A(n); c.vst = A(n); c.kw = A(n); c.qph0 = A(n); c.qph1 = A(n);
+    const size_t nfx = (size_t)(nx + 1) * ny, nfy = (size_t)nx * (ny + 1);
+    c.fx_ubs = A(nfx); c.fx_kp = A(nfx); c.fx_wl = A(nfx); c.fx_pv = A(nfx);
+    c.fy_ubs = A(nfy); c.fy_kp = A(nfy); c.fy_wl = A(nfy); c.fy_pv = A(nfy);
+    c.strong_list = (int*)A(n / 2 + 1);
+    c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
+    c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
+    c.br = A(n); c.br0 = A(n); c.bp = A(n); c.bv = A(n); c.bq = A(n); c.bs = A(n); c.bu = A(n); c.bt = A(n);
+    c.tcp = A(n); c.tdp = A(n);
+    for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];
+    c.partials = A((size_t)red_blocks((int)n) * MAXQ);
+    c.counters = (unsigned*)A(16);
+    c.ns = (NewtonScalars*)A(sizeof(NewtonScalars) / sizeof(double) + 1);
+    c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
+    if (ok && cudaMallocHost((void**)&s->pin, sizeof(Pinned)) != cudaSuccess) ok = false;
+    if (ok)
+        for (int e = 0; e < 2 * TG_COUNT; e++)
+            if (cudaEventCreate(&s->ev[e]) != cudaSuccess) ok = false;
+    c.p_ref = 0;
+    if (!ok || cudaStreamSynchronize(s->st) != cudaSuccess) { spb6g_destroy(s); return SPB6G_CUDA_ERROR; }
+    *out = s;
+    return SPB6G_OK;
+}
+
+int spb6g_destroy(spb6g_solver* s) {
+    if (!s) return SPB6G_BAD_ARG;
+    if (s->st) cudaStreamSynchronize(s->st);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->pin) cudaFreeHost(s->pin);
+    for (int e = 0; e < 2 * TG_COUNT; e++)
+        if (s->ev[e]) cudaEventDestroy(s->ev[e]);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return SPB6G_OK;
+}
+
+static int copy_state(spb6g_solver* s, double* const* dev, double* host_dst, const double* host_src, int layout) {
+    const int n = s->n;
+    std::vector<double> tmp;
+    if (layout != SPB6G_LAYOUT_AOS && layout != SPB6G_LAYOUT_SOA) return SPB6G_BAD_ARG;
+    if (host_src) {
+        if (layout == SPB6G_LAYOUT_SOA) {
+            for (int k = 0; k < NV; k++)
+                CK(cudaMemcpyAsync(dev[k], host_src + (size_t)k * n, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+        } else {
+            tmp.resize((size_t)n * NV);
+            for (int x = 0; x < n; x++)
+                for (int k = 0; k < NV; k++) tmp[(size_t)k * n + x] = host_src[(size_t)x * NV + k];
+            for (int k = 0; k < NV; k++)
+                CK(cudaMemcpyAsync(dev[k], tmp.data() + (size_t)k * n, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+        }
+        CK(cudaStreamSynchronize(s->st));
+    } else {
+        if (layout == SPB6G_LAYOUT_SOA) {
+            for (int k = 0; k < NV; k++)
+                CK(cudaMemcpyAsync(host_dst + (size_t)k * n, dev[k], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+        } else {
+            tmp.resize((size_t)n * NV);
+            for (int k = 0; k < NV; k++)
+                CK(cudaMemcpyAsync(tmp.data() + (size_t)k * n, dev[k], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            for (int x = 0; x < n; x++)
+                for (int k = 0; k < NV; k++) host_dst[(size_t)x * NV + k] = tmp[(size_t)k * n + x];
+        }
+    }
+    return SPB6G_OK;
+}
+
+int spb6g_upload_state(spb6g_solver* s, const double* U, int layout) {
+    if (!s || !U) return SPB6G_BAD_ARG;
+    return copy_state(s, s->U, nullptr, U, layout);
+}
+int spb6g_download_state(spb6g_solver* s, double* U, int layout) {
+    if (!s || !U) return SPB6G_BAD_ARG;
+    return copy_state(s, s->U, U, nullptr, layout);
+}
+
+int spb6g_init_pressure(spb6g_solver* s) {
+    if (!s) return SPB6G_BAD_ARG;
+    CState u;
+    for (int k = 0; k < NV; k++) u.v[k] = s->U[k];
+    launch_pbar_min(s->c, s->st, u);
+    if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+    double pr = s->pin->ns.pmin;
+    if (!std::isfinite(pr)) pr = 0.0;
+    s->p_ref = pr;
+    s->c.p_ref = pr;
+    s->stats.p_ref = pr;
+    launch_pbar_init(s->c, s->st, u, pr, s->Pmain);
+    CK(cudaStreamSynchronize(s->st));
+    s->t = 0; s->dt = 0; s->dtprev = -1; s->startup = true;
+    return SPB6G_OK;
+}
+int spb6g_set_pressure(spb6g_solver* s, const double* P, double p_ref) {
+    if (!s || !P) return SPB6G_BAD_ARG;
+    CK(cudaMemcpyAsync(s->Pmain, P, (size_t)s->n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->p_ref = p_ref; s->c.p_ref = p_ref; s->stats.p_ref = p_ref;
+    return SPB6G_OK;
+}
+int spb6g_get_pressure(spb6g_solver* s, double* P, double* p_ref) {
+    if (!s) return SPB6G_BAD_ARG;
+    if (P) {
+        CK(cudaMemcpyAsync(P, s->Pmain, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    if (p_ref) *p_ref = s->p_ref;
+    return SPB6G_OK;
+}
+int spb6g_caldt(spb6g_solver* s, int acoustic, double* inv_rate) {
+    if (!s || !inv_rate) return SPB6G_BAD_ARG;
+    return caldt(s, acoustic != 0, *inv_rate);
+}
+int spb6g_step(spb6g_solver* s) {
+    if (!s) return SPB6G_BAD_ARG;
+    const int rc = do_step(s);
+    s->stats.t = s->t;
+    s->stats.dt = s->dt;
+    return rc;
+}
+int spb6g_advance(spb6g_solver* s, int nsteps) {
+    if (!s) return SPB6G_BAD_ARG;
+    int rc = SPB6G_OK;
+    for (int k = 0; (nsteps <= 0 || k < nsteps) && s->t < s->cfg.tend * (1 - 1e-12); k++) {
+        rc = spb6g_step(s);
+        if (rc != SPB6G_OK) break;
+    }
+    return rc;
+}
+int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double* ube_x, double* ube_y, double* phi_x,
+                     double* phi_y) {
+    if (!s || !(dt > 0)) return SPB6G_BAD_ARG;
+    const int nx = s->g.nx, ny = s->g.ny, n = s->n;
+    double Ae[3][3], Ai[3][3];
+    set_tab(s->cfg.rk, Ae, Ai);
+    s->dt = dt;
+    if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
+    // explicit predictor, then the outputs, then the implicit part
+    Ctx& c = s->c;
+    for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->U[k]; c.Qs.v[k] = s->U[k]; }
+    c.adt = Ai[0][0] * dt; c.tau = c.adt; c.rx = c.tau / s->g.dx; c.ry = c.tau / s->g.dy;
+    c.H = s->Hs;
+    if (reset_flags(s)) return SPB6G_CUDA_ERROR;
+    launch_recon(c, s->st);
+    launch_update(c, s->st);
+    CK(cudaStreamSynchronize(s->st));
+    if (Xs) {
+        if (copy_state(s, s->Xs, Xs, nullptr, SPB6G_LAYOUT_AOS)) return SPB6G_CUDA_ERROR;
+    }
+    if (a2s) CK(cudaMemcpy(a2s, c.a2s, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ube_x) CK(cudaMemcpy(ube_x, c.ube_x, (size_t)(nx + 1) * ny * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ube_y) {
+        if (ny > 1) CK(cudaMemcpy(ube_y, c.ube_y, (size_t)nx * (ny + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+        else memset(ube_y, 0, (size_t)nx * (ny + 1) * sizeof(double));
+    }
+    if (phi_x || phi_y) {
+        std::vector<double> tx((size_t)(nx + 2) * ny), ty((size_t)nx * (ny + 2));
+        CK(cudaMemcpy(tx.data(), c.phis_x, tx.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        if (ny > 1) CK(cudaMemcpy(ty.data(), c.phis_y, ty.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                if (phi_x) phi_x[(size_t)j * nx + i] = tx[(size_t)(i + 1) + (size_t)j * (nx + 2)];
+                if (phi_y) phi_y[(size_t)j * nx + i] = ny > 1 ? ty[(size_t)i + (size_t)(j + 1) * nx] : 0.0;
+            }
+    }
+    launch_prep(c, s->st);
+    launch_shock(c, s->st);
+    double res;
+    int rc = newton(s, res);
+    if (rc != SPB6G_OK) return rc;
+    if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+    launch_final(c, s->st);
+    if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+    if (s->pin->ns.fail) return SPB6G_NEWTON_FAIL;
+    for (int k = 0; k < NV; k++) std::swap(s->U[k], s->Ust[k]);
+    c.Ust = State{};
+    for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];
+    s->Pmain = c.P;
+    return SPB6G_OK;
+}
+int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st) {
+    if (!s || !st) return SPB6G_BAD_ARG;
+    *st = s->stats;
+    st->t = s->t;
+    st->dt = s->dt;
+    st->p_ref = s->p_ref;
+    return SPB6G_OK;
+}
+int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup) {
+    if (!s) return SPB6G_BAD_ARG;
+    s->t = t; s->dtprev = dtprev; s->startup = startup != 0;
+    return SPB6G_OK;
+}
+int spb6g_timing_enable(spb6g_solver* s, int on) {
+    if (!s) return SPB6G_BAD_ARG;
+    s->timing = on != 0;
+    for (int g = 0; g < TG_COUNT; g++) { s->tms[g] = 0; s->tcnt[g] = 0; }
+    return SPB6G_OK;
+}
+int spb6g_timing_get(spb6g_solver* s, double* ms, int64_t* launches, int max_groups, int* n_groups) {
+    if (!s) return SPB6G_BAD_ARG;
+    for (int g = 0; g < TG_COUNT && g < max_groups; g++) {
+        if (ms) ms[g] = s->tms[g];
+        if (launches) launches[g] = s->tcnt[g];
+    }
+    if (n_groups) *n_groups = TG_COUNT;
+    return SPB6G_OK;
+}
+const char* spb6g_timing_name(int group) { return (group >= 0 && group < TG_COUNT) ? kTimerNames[group] : "?"; }
+
+const char* spb6g_status_string(int status) {
+    switch (status) {
+        case SPB6G_OK: return "ok";
+        case SPB6G_INADMISSIBLE: return "inadmissible state";
+        case SPB6G_NEWTON_FAIL: return "Newton failed";
+        case SPB6G_LINEAR_FAIL: return "BiCGStab failed";
+        case SPB6G_STEP_FAILED: return "step failed after 30 halvings";
+        case SPB6G_DT_UNDERFLOW: return "time step underflow";
+        case SPB6G_CUDA_ERROR: return "CUDA error";
+        case SPB6G_BAD_ARG: return "bad argument";
+        case SPB6G_UNSUPPORTED: return "unsupported configuration";
+        case SPB6G_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown";
+}
+
+}  // extern "C"

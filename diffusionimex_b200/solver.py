@@ -1,0 +1,218 @@
+"""Python host layer over the C ABI (include/spb6g.h).
+
+Mirrors the reference driver's interface (src/SPB6_PC_IMEX_omp.cpp): a solver
+object holds what main() keeps in globals and local grids; ``caldt``,
+``step``, ``advance`` and the stage-level ``stage_dump`` correspond to caldt
+(:502), one iteration of the time loop (:1316-1384), the loop itself, and
+TVDReconstruction + Update + PressureSubsystem (:369, :264, :908).
+Failures are reported as the reference does (a step that cannot be completed
+after 30 halvings, a time-step underflow) by raising ``SolverError`` with the
+library's status code.
+
+The CUDA library must exist (``python -m diffusionimex_b200.build``); there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .build import LIB
+
+NV = 8
+
+STATUS = {
+    0: "ok", 1: "inadmissible state", 2: "Newton failed", 3: "BiCGStab failed", 4: "step failed after 30 halvings",
+    5: "time step underflow", 6: "CUDA error", 7: "bad argument", 8: "unsupported configuration", 9: "no CUDA device",
+}
+
+
+class SolverError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        super().__init__(f"{where}: {STATUS.get(status, status)} (status {status})")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+        ("x0", ctypes.c_double), ("x1", ctypes.c_double), ("y0", ctypes.c_double), ("y1", ctypes.c_double),
+        ("bc", ctypes.c_int32 * 4), ("bcu", ctypes.c_double * 4), ("bcp", ctypes.c_double * 4),
+        ("gamma", ctypes.c_double * 2), ("pinf", ctypes.c_double * 2), ("q", ctypes.c_double * 2),
+        ("qp", ctypes.c_double * 2), ("cv", ctypes.c_double * 2), ("b", ctypes.c_double * 2),
+        ("rk", ctypes.c_int32), ("cfl", ctypes.c_double), ("cfl_ac", ctypes.c_double), ("ramp", ctypes.c_int32),
+        ("dtfix", ctypes.c_double), ("rus_local", ctypes.c_int32), ("limiter", ctypes.c_int32), ("acdt", ctypes.c_int32),
+        ("newton_tol", ctypes.c_double), ("newton_iter", ctypes.c_int32), ("bicg_tol", ctypes.c_double),
+        ("bicg_iter", ctypes.c_int32), ("share_mode", ctypes.c_int32), ("tend", ctypes.c_double),
+        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64), ("rejects", ctypes.c_int64), ("rk1", ctypes.c_int64), ("stages", ctypes.c_int64),
+        ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
+        ("reserved", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
+        ("p_ref", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Load libspb6g.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise RuntimeError(f"CUDA library missing: {LIB}; run `python -m diffusionimex_b200.build`")
+    lib = ctypes.CDLL(LIB)
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        "spb6g_default_config": (None, [P]),
+        "spb6g_create": (I, [P, P]),
+        "spb6g_destroy": (I, [P]),
+        "spb6g_upload_state": (I, [P, P, I]),
+        "spb6g_download_state": (I, [P, P, I]),
+        "spb6g_init_pressure": (I, [P]),
+        "spb6g_set_pressure": (I, [P, P, D]),
+        "spb6g_get_pressure": (I, [P, P, P]),
+        "spb6g_caldt": (I, [P, I, P]),
+        "spb6g_step": (I, [P]),
+        "spb6g_advance": (I, [P, I]),
+        "spb6g_stage_dump": (I, [P, D, P, P, P, P, P, P]),
+        "spb6g_get_stats": (I, [P, P]),
+        "spb6g_set_time": (I, [P, D, D, I]),
+        "spb6g_timing_enable": (I, [P, I]),
+        "spb6g_timing_get": (I, [P, P, P, I, P]),
+        "spb6g_timing_name": (ctypes.c_char_p, [I]),
+        "spb6g_status_string": (ctypes.c_char_p, [I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    _lib = lib
+    return lib
+
+
+def make_config(case: dict, device: int = 0) -> Config:
+    c = Config()
+    library().spb6g_default_config(ctypes.byref(c))
+    for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
+        setattr(c, k, int(case[k]))
+    for k in ("x0", "x1", "y0", "y1", "cfl", "cfl_ac", "dtfix", "newton_tol", "bicg_tol", "tend"):
+        setattr(c, k, float(case[k]))
+    for q in range(4):
+        c.bc[q] = int(case["bc"][q])
+        c.bcu[q] = float(case["bcu"][q])
+        c.bcp[q] = float(case["bcp"][q])
+    for k in range(2):
+        ph = case["phases"][k]
+        c.gamma[k], c.pinf[k], c.q[k], c.qp[k], c.cv[k], c.b[k] = ph["g"], ph["pinf"], ph["q"], ph["qp"], ph["cv"], ph["b"]
+    c.device = device
+    return c
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Solver:
+    """One grid on one GPU: state, pressure unknown, time and statistics."""
+
+    def __init__(self, case: dict, device: int = 0, init_pressure: bool = True):
+        self.lib = library()
+        self.case = case
+        self.nx, self.ny = int(case["nx"]), int(case["ny"])
+        self.cfg = make_config(case, device)
+        h = ctypes.c_void_p()
+        self._check(self.lib.spb6g_create(ctypes.byref(self.cfg), ctypes.byref(h)), "spb6g_create")
+        self.h = h
+        if "U" in case:
+            self.upload(case["U"])
+            if init_pressure:
+                self.init_pressure()
+
+    def _check(self, rc: int, where: str):
+        if rc != 0:
+            raise SolverError(rc, where)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spb6g_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state ------------------------------------------------------------------------------
+    def upload(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.ny, self.nx, NV)
+        self._check(self.lib.spb6g_upload_state(self.h, _ptr(U), 0), "spb6g_upload_state")
+
+    def state(self) -> np.ndarray:
+        U = np.empty((self.ny, self.nx, NV))
+        self._check(self.lib.spb6g_download_state(self.h, _ptr(U), 0), "spb6g_download_state")
+        return U
+
+    def init_pressure(self):
+        self._check(self.lib.spb6g_init_pressure(self.h), "spb6g_init_pressure")
+
+    def pressure(self):
+        P = np.empty((self.ny, self.nx))
+        pref = ctypes.c_double()
+        self._check(self.lib.spb6g_get_pressure(self.h, _ptr(P), ctypes.byref(pref)), "spb6g_get_pressure")
+        return P, pref.value
+
+    def set_pressure(self, P: np.ndarray, p_ref: float):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        self._check(self.lib.spb6g_set_pressure(self.h, _ptr(P), float(p_ref)), "spb6g_set_pressure")
+
+    # reference driver entry points --------------------------------------------------------
+    def caldt(self, acoustic: bool = False) -> float:
+        out = ctypes.c_double()
+        self._check(self.lib.spb6g_caldt(self.h, int(acoustic), ctypes.byref(out)), "caldt")
+        return out.value
+
+    def step(self):
+        self._check(self.lib.spb6g_step(self.h), "step")
+
+    def advance(self, nsteps: int = 0):
+        """nsteps > 0: that many steps (or until t_end); 0: run to t_end."""
+        self._check(self.lib.spb6g_advance(self.h, int(nsteps)), "advance")
+
+    def stage_dump(self, dt: float) -> dict:
+        nx, ny = self.nx, self.ny
+        out = dict(Xs=np.empty((ny, nx, NV)), a2s=np.empty((ny, nx)), ube_x=np.empty((ny, nx + 1)),
+                   ube_y=np.empty((ny + 1, nx)), phi_x=np.empty((ny, nx)), phi_y=np.empty((ny, nx)))
+        self._check(self.lib.spb6g_stage_dump(self.h, float(dt), *(_ptr(out[k]) for k in
+                                                                  ("Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y"))),
+                    "stage_dump")
+        return out
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.spb6g_get_stats(self.h, ctypes.byref(s)), "spb6g_get_stats")
+        return {k: getattr(s, k) for k, _ in Stats._fields_ if k != "reserved"}
+
+    def timing(self, enable: bool | None = None) -> dict:
+        if enable is not None:
+            self._check(self.lib.spb6g_timing_enable(self.h, int(enable)), "timing")
+            return {}
+        ms = (ctypes.c_double * 16)()
+        cnt = (ctypes.c_int64 * 16)()
+        ng = ctypes.c_int()
+        self._check(self.lib.spb6g_timing_get(self.h, ms, cnt, 16, ctypes.byref(ng)), "timing")
+        return {self.lib.spb6g_timing_name(g).decode(): (ms[g], cnt[g]) for g in range(ng.value)}

@@ -1,0 +1,133 @@
+/* spb6g.h -- C ABI of the B200 SPB 6+1-equation IMEX solver.
+ *
+ * The reference (src/SPB6_PC_IMEX_omp.cpp + src/spb6_physics_omp.h) has no
+ * library interface: its API is main()'s time loop over mutable globals and
+ * the stage functions TVDReconstruction / Update / PressureSubsystem / caldt /
+ * bound_cond_u.  This header is the boundary a host driver (the reference's
+ * main() loop, a cgo / ctypes / JNI binding, or this package's Python layer)
+ * links against instead.  Every entry point names the reference code it
+ * replaces.  Plain C types only; all functions return an spb6g_status; no
+ * exceptions cross the ABI.  One solver handle = one CUDA stream = one host
+ * thread at a time; the handle owns its device memory, the caller owns every
+ * host buffer.
+ *
+ * State layout on the host side: SPB6G_LAYOUT_AOS is the reference Grid's
+ * interior cells (Grid, :124-143, without the two ghost layers): index
+ * ((j * nx + i) * 8 + k); SPB6G_LAYOUT_SOA is k-major: (k * ny + j) * nx + i.
+ * Variables k follow the reference order alpha1, m1, m2, rho u, rho v, eps1,
+ * eps2, E (src/spb6_physics_omp.h:27-28).
+ */
+#ifndef SPB6G_H
+#define SPB6G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SPB6G_OK = 0,
+    SPB6G_INADMISSIBLE = 1,     /* Update / stage prep found rho <= 0 or sum alpha <= 0 (:272, :929) */
+    SPB6G_NEWTON_FAIL = 2,      /* Newton_Solver returned false (:799-904) */
+    SPB6G_LINEAR_FAIL = 3,      /* GMRES_Solver (BiCGStab) returned false (:752-794) */
+    SPB6G_STEP_FAILED = 4,      /* 30 halvings without success: the reference's "FAILED" exit (:1378) */
+    SPB6G_DT_UNDERFLOW = 5,     /* dt <= 1e-12 t_end (:1326) */
+    SPB6G_CUDA_ERROR = 6,
+    SPB6G_BAD_ARG = 7,
+    SPB6G_UNSUPPORTED = 8,
+    SPB6G_NO_DEVICE = 9
+} spb6g_status;
+
+enum { SPB6G_BC_TRANS = 0, SPB6G_BC_WALL = 1, SPB6G_BC_PERIODIC = 2, SPB6G_BC_PRES = 3 };
+enum { SPB6G_LAYOUT_AOS = 0, SPB6G_LAYOUT_SOA = 1 };
+
+/* Replaces main()'s globals and test_setup()'s TestSetup
+ * (src/SPB6_PC_IMEX_omp.cpp:55-95, src/spb6_physics_omp.h:954-961, :1014).
+ * Phases are stiffened gas / NASG: p = (gamma-1)(e - q)/(v - b) - gamma pinf. */
+typedef struct {
+    int32_t nx, ny;                 /* interior cells; ny = 1 is the 1D solver */
+    double x0, x1, y0, y1;          /* domain */
+    int32_t bc[4];                  /* left, right, bottom, top: SPB6G_BC_* (BCS, physics :964) */
+    double bcu[4];                  /* wall normal velocity (piston), BCU */
+    double bcp[4];                  /* outlet pressure, BCP */
+    double gamma[2], pinf[2], q[2], qp[2], cv[2], b[2]; /* PH[2], physics :55-56 */
+    int32_t rk;                     /* 1 backward Euler, 2 LSDIRK2(2,2,2), 3 SSP2(3,3,2) (RKs, :69) */
+    double cfl, cfl_ac;             /* material CFL, start-up acoustic CFL (:71-72) */
+    int32_t ramp;                   /* start-up ramp (RAMP, :75) */
+    double dtfix;                   /* > 0: fixed step (DTFIX, :77) */
+    int32_t rus_local;              /* RUS_LOCAL (:93); only 1 is implemented */
+    int32_t limiter;                /* LIMITER (physics :969) */
+    int32_t acdt;                   /* 1: acoustic CFL every step (caltimestep = Fullydt, :55) */
+    double newton_tol;              /* NewtonTol (:79) */
+    int32_t newton_iter;            /* NewtonIter (:82) */
+    double bicg_tol;                /* GMREStol (:84) */
+    int32_t bicg_iter;              /* GMRESiter (:85) */
+    int32_t share_mode;             /* SHARE_MODE (physics :436) */
+    double tend;                    /* time_stop */
+    int32_t device;                 /* CUDA device ordinal */
+    int32_t reserved[7];
+} spb6g_config;
+
+/* Run statistics: the counters of the reference's stats line (:98-99, :1425). */
+typedef struct {
+    int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it;
+    int64_t reserved;
+    double t, dt, maxres, p_ref;
+} spb6g_stats;
+
+typedef struct spb6g_solver spb6g_solver;
+
+/* Fills *cfg with the reference defaults (SPB6_PC_IMEX_omp.cpp:55-95, set_SG physics :1014). */
+void spb6g_default_config(spb6g_config* cfg);
+
+/* Allocates the device state of one grid (replaces main's Grid/Array allocations :1245-1248). */
+int spb6g_create(const spb6g_config* cfg, spb6g_solver** out);
+int spb6g_destroy(spb6g_solver* s);
+
+/* Initial / current conservative state of the interior cells (u_initialization :475-492). */
+int spb6g_upload_state(spb6g_solver* s, const double* U, int layout);
+int spb6g_download_state(spb6g_solver* s, double* U, int layout);
+
+/* P_REF = min pbar and P = pbar - P_REF, the plain Newton guess at t = 0 (:1307-1312). */
+int spb6g_init_pressure(spb6g_solver* s);
+/* The pressure unknown P - P_REF (PField, :172), nx*ny doubles. */
+int spb6g_set_pressure(spb6g_solver* s, const double* P, double p_ref);
+int spb6g_get_pressure(spb6g_solver* s, double* P, double* p_ref);
+
+/* caldt (:502-514): returns 1 / (a_x/dx + a_y/dy) (INFINITY if the rate is 0). */
+int spb6g_caldt(spb6g_solver* s, int acoustic, double* inv_rate);
+
+/* One iteration of main()'s time loop (:1316-1384): step size, ramp, stages,
+ * halving on failure, acceptance.  Statistics accumulate in the handle. */
+int spb6g_step(spb6g_solver* s);
+/* Steps until nsteps steps are taken (nsteps > 0) or t reaches t_end. */
+int spb6g_advance(spb6g_solver* s, int nsteps);
+
+/* Stage-level API, the reference's stage functions on the device state:
+ * stage 0 of the configured tableau with step dt -- TVDReconstruction + Update
+ * (:369, :264) followed by PressureSubsystem (:908) -- leaving the new state in
+ * the handle.  Optional outputs (NULL to skip) mirror the stage globals the
+ * reference passes between them: X* (AoS), alpha2*, ube_x ((nx+1)*ny),
+ * ube_y (nx*(ny+1)), phi_x, phi_y (nx*ny). */
+int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double* ube_x, double* ube_y,
+                     double* phi_x, double* phi_y);
+
+int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st);
+/* Simulation time t (settable, e.g. when restarting from a dump). */
+int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup);
+
+/* Per-kernel device time (ms, CUDA events on the solver's stream) accumulated
+ * since the last reset; names[] enumerates the timed kernel groups. */
+int spb6g_timing_enable(spb6g_solver* s, int on);
+int spb6g_timing_get(spb6g_solver* s, double* ms, int64_t* launches, int max_groups, int* n_groups);
+const char* spb6g_timing_name(int group);
+
+/* Human-readable status name. */
+const char* spb6g_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,109 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py
+
+Needs oracle/_ref/spb6_ref (built by `make -C oracle ref` from the reference
+sources) and the reference tree for the archived profiles.  Each fixture is
+the reference solver's output on one small seeded case; the GPU parity tests
+compare against these files (and against the C restatement) on machines
+where the reference tree does not exist.
+
+Fixtures:
+  ref_<name>.npz      U0 (initial state), U, P, p_ref and run counters of the
+                      compiled reference on the case built by CASES[name]
+  archived_case5_N100.npz, archived_case87_N200.npz
+                      columns x, p, u, rho, alpha2 of the reference's archived
+                      profiles data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat
+                      and data/Schropff2026_Riemann_problems/c87_200.dat
+                      (produced by the serial-root program src/SPB6_PC_IMEX.cpp)
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from diffusionimex_b200 import cases  # noqa: E402
+
+REF_TREE = "/root/reference"
+
+
+def _tube(n):
+    return cases.water_air_tube(n)
+
+
+def _bubble(n, seed=1, nbub=3):
+    c = cases.bubble_field(n, seed=seed, nbub=nbub)
+    return c
+
+
+def _lowmach(n):
+    return cases.lowmach_bubbles(n, seed=3, nbub=2, amp=15.0)
+
+
+def _shock(nx, ny):
+    return cases.shock_bubble(nx, ny)
+
+
+def _nasg(n):
+    b = cases.riemann_batch(count=8, seed=5, nmin=n, nmax=n)
+    return next(c for c in b if c["nasg"])
+
+
+# name -> (builder, mode, nsteps, overrides)
+CASES = {
+    "case87_N200_tend": (lambda: cases.reference_case(87, 200), "tend", 0, {}),
+    "case5_N100_tend": (lambda: cases.reference_case(5, 100), "tend", 0, {}),
+    "case83_N200_10steps": (lambda: cases.reference_case(83, 200), "steps", 10, {}),
+    "tube_N1000_1step": (lambda: _tube(1000), "steps", 1, {}),
+    "tube_N1000_tend": (lambda: _tube(1000), "tend", 0, {}),
+    "tube_N200_stage": (lambda: _tube(200), "stage", 0, {"dtfix": 2e-7}),
+    "bubble48_stage": (lambda: _bubble(48), "stage", 0, {"dtfix": 1e-5, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "bubble48_4steps": (lambda: _bubble(48), "steps", 4, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "lowmach32_3steps": (lambda: _lowmach(32), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "shock64x32_3steps": (lambda: _shock(64, 32), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "nasg256_20steps": (lambda: _nasg(256), "steps", 20, {}),
+}
+
+
+def build_case(name):
+    fn, mode, nsteps, over = CASES[name]
+    c = fn()
+    c.update(over)
+    return c, mode, nsteps
+
+
+def main():
+    import refio
+
+    if not refio.ref_available():
+        raise SystemExit("oracle/_ref/spb6_ref is missing: run `make -C oracle ref` first")
+    modes = {"tend": refio.MODE_TEND, "steps": refio.MODE_STEPS, "stage": refio.MODE_STAGE}
+    for name in CASES:
+        c, mode, nsteps = build_case(name)
+        r = refio.run_ref(c, mode=modes[mode], nsteps=nsteps)
+        meta = {k: r[k] for k in ("status", "steps", "rejects", "rk1", "stages", "newton_it", "floor_count", "t", "dt",
+                                  "maxres", "p_ref")}
+        extra = {}
+        if mode == "stage":
+            extra = {k: r[k] for k in ("Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y")}
+        np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), U0=c["U"], U=r["U"], P=r["P"],
+                            meta=json.dumps(meta), **extra)
+        print(name, meta)
+    for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
+                      ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):
+        d = np.loadtxt(os.path.join(REF_TREE, path))
+        np.savez_compressed(os.path.join(HERE, f"{tag}.npz"), x=d[:, 0], p=d[:, 2], u=d[:, 3], rho=d[:, 5],
+                            alpha2=d[:, 6], source=path)
+        print(tag, d.shape)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,68 @@
+"""CPU tests of the C ABI: the in-tree library loads without a GPU and exports
+every entry point include/spb6g.h declares; a handle cannot be created without
+a device, and bad arguments are rejected before any device call."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from diffusionimex_b200 import build, solver
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "spb6g.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(spb6g_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("spb6g_create", "spb6g_step", "spb6g_caldt", "spb6g_stage_dump", "spb6g_destroy"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    if build.needs_build():
+        build.build()
+    lib = ctypes.CDLL(build.LIB)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_config_and_status_strings():
+    lib = solver.library()
+    c = solver.Config()
+    lib.spb6g_default_config(ctypes.byref(c))
+    assert c.rk == 2 and c.cfl == 0.2 and c.newton_tol == 1e-13 and c.bicg_iter == 4000
+    assert lib.spb6g_status_string(0) == b"ok"
+    assert lib.spb6g_status_string(4).startswith(b"step failed")
+
+
+def test_bad_arguments_rejected_before_device_use():
+    lib = solver.library()
+    c = solver.Config()
+    lib.spb6g_default_config(ctypes.byref(c))
+    h = ctypes.c_void_p()
+    c.nx = 0
+    assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 7  # SPB6G_BAD_ARG
+    lib.spb6g_default_config(ctypes.byref(c))
+    c.bc[0] = 2  # periodic on one side only
+    assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 7
+    assert lib.spb6g_destroy(None) == 7
+
+
+def test_no_device_reported_on_cpu_host():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = solver.library()
+    c = solver.Config()
+    lib.spb6g_default_config(ctypes.byref(c))
+    h = ctypes.c_void_p()
+    assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 9  # SPB6G_NO_DEVICE
