@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark of the SPB6 IMEX stage loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workload (default): water at rest with 8 seeded air bubbles on a 1024 x 1024
+grid, FP64, transmissive, material CFL 0.5, Newton tol 1e-10, BiCGStab tol
+1e-12 -- the plain-method 2D configuration.  A "step" is one time step of the
+solver (explicit predictor + implicit pressure Newton with BiCGStab per stage,
+step-size control, acceptance).  The run takes W untimed steps from t = 0 and
+times the next K steps on the device (CUDA events on the solver's stream,
+max over ranks).  The working set (~1 GB) is far larger than L2.
+
+metric: cell-updates/s = interior cells x accepted steps / device time.
+
+Multi-GPU: the path is one grid per GPU (north_star is single-GPU), so N > 1
+runs N independent replicas ("scaling": "weak"); value is the total over ranks.
+
+--impl reference times the reference's own CPU solver (oracle/_ref, compiled from
+its sources) on the same workload on all host cores; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic FP64 bytes per interior cell (each distinct array element read or
+# written once) of the kernel groups the solver times; 2D values.
+ALG_BYTES = {
+    # recon: Qe 8 reads + 8 recon outputs; update: Qe 8 + Qs 8 + 8 recon + X* 8 + a2s + 2 face velocities
+    "explicit": (8 + 8) * 8 + (8 + 8 + 8 + 8 + 1 + 2) * 8,
+    "jacobian": (9 + 5 + 2 + 10 + 2 + 1 + 1 + 1 + 1 + 7) * 8,  # X*,a2s | Qe vol | phi | faces | v* | qph | kw | P | G | sc | A,A1,dinv
+    "residual": (9 + 5 + 2 + 10 + 2 + 2 + 1 + 1 + 1) * 8,       # ... + P, G, sc
+    "linear": 272,                                            # per BiCGStab iteration (4 passes), x iterations
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="bubbles1024")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_workload(name: str):
+    from diffusionimex_b200 import cases
+
+    if name == "bubbles1024":
+        c = cases.bubble_field(1024, seed=0, nbub=8)
+    elif name == "bubbles2048":
+        c = cases.bubble_field(2048, seed=0, nbub=8)
+    elif name == "bubbles256":
+        c = cases.bubble_field(256, seed=0, nbub=8)
+    elif name == "tube1000":
+        c = cases.water_air_tube(1000)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return c
+
+
+def workload_config(c: dict, name: str) -> dict:
+    return {"workload": c.get("workload", name), "nx": c["nx"], "ny": c["ny"], "fp": "fp64",
+            "newton_tol": c["newton_tol"], "bicg_tol": c["bicg_tol"], "cfl": c["cfl"], "seed": c.get("seed", 0),
+            "l2": "working set > L2 (no flush needed)"}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.lines = gpu, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_baseline(case: dict, steps: int = 2) -> dict:
+    """The reference CPU solver (oracle/_ref when present, else the C restatement) on the first
+    `steps` steps of the same workload, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+
+    cores = os.cpu_count() or 1
+    n = case["nx"] * case["ny"]
+    if refio.ref_available():
+        r = refio.run_ref(case, mode=refio.MODE_STEPS, nsteps=steps, threads=cores)
+        kind = "reference"
+    else:
+        r = refio.run_port(case, mode=refio.MODE_STEPS, nsteps=steps)
+        kind, cores = "port", 1
+    return {"value": n * r["timed_steps"] / r["wall_s"], "unit": "cell-updates/s", "cores": cores, "kind": kind,
+            "sample": f"first {r['timed_steps']} time steps from t=0 of the same workload "
+                      f"({r['newton_it']} Newton iterations), {r['wall_s']:.1f} s"}
+
+
+def dist_init(world: int, local_rank: int):
+    if world <= 1:
+        return None
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
+    return dist
+
+
+def run_reference(args, case, rank: int):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refio
+
+    cores = os.cpu_count() or 1
+    n = case["nx"] * case["ny"]
+    budget = 150.0
+    if refio.ref_available():
+        r = refio.run_ref(case, mode=refio.MODE_STEPS, nsteps=args.warmup + args.steps, threads=cores,
+                          warmup=args.warmup, budget_s=budget)
+        kind = "reference"
+    else:
+        r = refio.run_port(case, mode=refio.MODE_STEPS, nsteps=args.warmup + args.steps, warmup=args.warmup,
+                           budget_s=budget)
+        kind, cores = "port", 1
+    k = max(int(r["timed_steps"]), 1)
+    value = n * k / r["wall_s"]
+    sample = (f"steps {args.warmup + 1}..{args.warmup + k} from t=0 after {args.warmup} untimed steps"
+              + (" (stopped at the time budget)" if k < args.steps else ""))
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * r["wall_s"] / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(case, args.workload),
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "newton_it": r["newton_it"], "stages": r["stages"],
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
+    import numpy as np
+    import torch
+
+    from diffusionimex_b200 import Solver
+
+    n = case["nx"] * case["ny"]
+    s = Solver(case, device=local_rank)
+    s.advance(args.warmup)
+    st0 = s.stats()
+    l0 = s.kernel_launches()
+    s.timing(True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    s.region_begin()
+    s.advance(args.steps)
+    ms = s.region_end()
+    clocks = clk.stop()
+    torch.cuda.synchronize()
+    st1 = s.stats()
+    launches = s.kernel_launches() - l0
+    groups = s.timing()
+    s.timing(False)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        dist.barrier()
+    steps_done = st1["steps"] - st0["steps"]
+    value = n * steps_done * world / (ms_max / 1e3)
+
+    # end to end through the public API: the state goes host -> device before every step and
+    # comes back after it (pinned host buffer, SoA layout)
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(8 * n, dtype=torch.float64, pin_memory=True)
+        ptr = host.data_ptr()
+        s.download_soa(ptr)
+        ke = max(1, min(args.steps, 5))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s.region_begin()
+        for _ in range(ke):
+            s.upload_soa(ptr)
+            s.step()
+            s.download_soa(ptr)
+        ems = s.region_end()
+        if dist:
+            t = torch.tensor([ems], dtype=torch.float64, device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": n * ke * world / (ems / 1e3), "unit": "cell-updates/s", "h2d_bytes_per_step": 64 * n,
+               "d2h_bytes_per_step": 64 * n, "steps": ke}
+
+    # roofline of the dominant kernel group
+    peak, peak_kind = peaks()
+    newton_its = st1["newton_it"] - st0["newton_it"]
+    bicg_its = st1["bicg_it"] - st0["bicg_it"]
+    stages = st1["stages"] - st0["stages"]
+    dom = max((g for g in groups if g in ALG_BYTES), key=lambda g: groups[g][0])
+    gms, gcnt = groups[dom]
+    if dom == "linear":
+        units = bicg_its * n
+    else:
+        units = gcnt * n
+    achieved = ALG_BYTES[dom] * units / (gms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+            "alg_bytes_per_cell": ALG_BYTES[dom]}
+    total_ms = sum(v[0] for v in groups.values())
+    shares = {g: {"ms": round(v[0], 3), "launch_groups": int(v[1]), "share": round(v[0] / ms, 4)} for g, v in groups.items()}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps_done,
+            "warmup": args.warmup, "ms_per_step": ms_max / max(steps_done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(case, args.workload),
+            "bicg_iters_per_step": bicg_its / max(steps_done, 1),
+            "newton_iters_per_stage": newton_its / max(stages, 1),
+            "stages": stages, "rejects": st1["rejects"] - st0["rejects"],
+            "roofline": roof, "kernel_groups": shares, "timed_groups_ms": round(total_ms, 3),
+            "gpu_launches": launches, "clocks": clocks, "e2e": e2e,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(case)
+        print(json.dumps(line))
+    s.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    case = make_workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, case, rank)
+        return
+    dist = dist_init(world, local_rank)
+    try:
+        run_ours(args, case, rank, world, local_rank, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -58,6 +58,7 @@ struct Ctx {
     unsigned* counters;  // [16]
     NewtonScalars* ns;
     BicgScalars* bs_;
+    long long* nlaunch;  // host-side count of kernel launches (never dereferenced on the device)
 };
 
 SPB6G_DEV size_t fxi(const Geom& g, int i, int j) { return (size_t)(i + 1) + (size_t)j * (g.nx + 1); }

@@ -15,6 +15,9 @@ static int blocks_for(long n, int tpb = TPB) {
     if (b > 148L * 32) b = 148L * 32;
     return (int)b;
 }
+static inline void count(const Ctx& c, int k) {
+    if (c.nlaunch) *c.nlaunch += k;
+}
 int red_blocks(int n) {
     long b = ((long)n + RED_THREADS - 1) / RED_THREADS;
     if (b < 1) b = 1;
@@ -50,6 +53,7 @@ void launch_combine(const Ctx& c, cudaStream_t st, const double* const* U, const
     const double c0e = nH > 0 ? ae[0] * dt : 0, c1e = nH > 1 ? ae[1] * dt : 0;
     const double c0i = nH > 0 ? ai[0] * dt : 0, c1i = nH > 1 ? ai[1] * dt : 0;
     k_combine<<<blocks_for(c.n), TPB, 0, st>>>(c.n, u, Hs, nH, c0e, c1e, c0i, c1i, qe, qs);
+    count(c, 1);
 }
 
 // ============================================================ reconstruction (TVDReconstruction :369-471)
@@ -160,6 +164,7 @@ __global__ void k_recon(Ctx c) {
 void launch_recon(const Ctx& c, cudaStream_t st) {
     const long tot = (long)(c.g.nx + 2) * (c.g.ny > 1 ? c.g.ny + 2 : 1);
     k_recon<<<blocks_for(tot), TPB, 0, st>>>(c);
+    count(c, 1);
 }
 
 // Face state of cell (ci, cj) on its left (right = false) or right side in direction dir (:433-467).
@@ -244,7 +249,10 @@ __global__ void k_update(Ctx c) {
         c.a2s[x] = 1.0 - X[IA1];
     }
 }
-void launch_update(const Ctx& c, cudaStream_t st) { k_update<<<blocks_for(c.n), TPB, 0, st>>>(c); }
+void launch_update(const Ctx& c, cudaStream_t st) {
+    k_update<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    count(c, 1);
+}
 
 // ============================================================ stage data (PressureSubsystem prep :922-1039)
 SPB6G_DEV void xs_at(const Ctx& c, int i, int j, double* q) {
@@ -379,6 +387,7 @@ void launch_prep(const Ctx& c, cudaStream_t st) {
     k_prep_cell<<<blocks_for(c.n), TPB, 0, st>>>(c);
     k_prep_fx<<<blocks_for((long)(c.g.nx + 1) * c.g.ny), TPB, 0, st>>>(c);
     if (c.g.ny > 1) k_prep_fy<<<blocks_for((long)c.g.nx * (c.g.ny + 1)), TPB, 0, st>>>(c);
+    count(c, c.g.ny > 1 ? 3 : 2);
 }
 
 // ============================================================ shock budget (shock_budget physics :405-428)
@@ -447,6 +456,7 @@ __global__ void k_shock_strong(Ctx c) {
 void launch_shock(const Ctx& c, cudaStream_t st) {
     k_shock_weak<<<blocks_for(c.n), TPB, 0, st>>>(c);
     k_shock_strong<<<148 * 4, 32, 0, st>>>(c);
+    count(c, 2);
 }
 
 // ============================================================ implicit residual (:610-731)
@@ -629,6 +639,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_residual(Ctx c, int mode, doubl
 }
 void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
     k_residual<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, mode, lam);
+    count(c, 1);
 }
 
 // FD Jacobian rows (:837-853) with the BiCGStab set-up sums E = 1^T A 1, 1^T b, b^T b.
@@ -671,7 +682,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_jacobian(Ctx c) {
         c.ns->E = tot[0]; c.ns->sumb = tot[1]; c.ns->bb = tot[2];
     }
 }
-void launch_jacobian(const Ctx& c, cudaStream_t st) { k_jacobian<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c); }
+void launch_jacobian(const Ctx& c, cudaStream_t st) {
+    k_jacobian<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c);
+    count(c, 1);
+}
 
 // ============================================================ BiCGStab (GMRES_Solver :752-794)
 // Jacobi + Nicolaides preconditioner M^-1 r = D^-1 r + 1 (1^T r)/E.  The coarse
@@ -830,12 +844,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
 }
 void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit) {
     k_bicg_init<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, tol, maxit);
+    count(c, 1);
 }
 // `count` iterations.  p is double-buffered (pass 1 reads neighbours' old p
 // while writing the new one); `parity` selects the buffer holding the current p.
-void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity) {
+void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count_, int& parity) {
     const int nb = red_blocks(c.n);
-    for (int k = 0; k < count; k++) {
+    for (int k = 0; k < count_; k++) {
         double* p0 = parity ? c.tcp : c.bp;  // tcp is the Thomas scratch, free on the BiCGStab path
         double* p1 = parity ? c.bp : c.tcp;
         k_bicg_p<<<nb, RED_THREADS, 0, st>>>(c, p0, p1);
@@ -844,6 +859,7 @@ void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity) {
         k_bicg_x<<<nb, RED_THREADS, 0, st>>>(c, p1);
         parity ^= 1;
     }
+    count(c, 4 * count_);
 }
 
 // ============================================================ Thomas (1D non-periodic, :858-863)
@@ -874,7 +890,10 @@ __global__ void k_thomas(Ctx c) {
     c.dP[n - 1] = dp[n - 1];
     for (int r = n - 2; r >= 0; r--) c.dP[r] = dp[r] - cp[r] * c.dP[r + 1];
 }
-void launch_thomas(const Ctx& c, cudaStream_t st) { k_thomas<<<1, 32, 0, st>>>(c); }
+void launch_thomas(const Ctx& c, cudaStream_t st) {
+    k_thomas<<<1, 32, 0, st>>>(c);
+    count(c, 1);
+}
 
 // ============================================================ Newton step control (:870-879, :890-899)
 __global__ void __launch_bounds__(RED_THREADS) k_stepnorm(Ctx c) {
@@ -884,11 +903,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_stepnorm(Ctx c) {
     double tot[1];
     if (grid_fold<RedMax, 1>(m, c.partials, &c.counters[7], tot) && threadIdx.x == 0) c.ns->sn = tot[0];
 }
-void launch_stepnorm(const Ctx& c, cudaStream_t st) { k_stepnorm<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c); }
+void launch_stepnorm(const Ctx& c, cudaStream_t st) {
+    k_stepnorm<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c);
+    count(c, 1);
+}
 __global__ void k_apply_step(Ctx c) {
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) c.P[x] += c.dP[x];
 }
-void launch_apply_step(const Ctx& c, cudaStream_t st) { k_apply_step<<<blocks_for(c.n), TPB, 0, st>>>(c); }
+void launch_apply_step(const Ctx& c, cudaStream_t st) {
+    k_apply_step<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    count(c, 1);
+}
 __global__ void k_floor(Ctx c, double tol) {
     const Geom& g = c.g;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
@@ -901,7 +926,10 @@ __global__ void k_floor(Ctx c, double tol) {
         if (fabs(Gr) > tol * (fabs(c.p_ref + p.c) + c.kw[x] + 1.0) + sig) atomicOr(&c.ns->fail, 4);
     }
 }
-void launch_floor(const Ctx& c, cudaStream_t st, double tol) { k_floor<<<blocks_for(c.n), TPB, 0, st>>>(c, tol); }
+void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
+    k_floor<<<blocks_for(c.n), TPB, 0, st>>>(c, tol);
+    count(c, 1);
+}
 
 // ============================================================ final state (:1056-1073) and H_s (:1363-1371)
 __global__ void k_final(Ctx c) {
@@ -922,7 +950,10 @@ __global__ void k_final(Ctx c) {
         }
     }
 }
-void launch_final(const Ctx& c, cudaStream_t st) { k_final<<<blocks_for(c.n), TPB, 0, st>>>(c); }
+void launch_final(const Ctx& c, cudaStream_t st) {
+    k_final<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    count(c, 1);
+}
 
 // ============================================================ caldt (:502-514) and P_REF (:1309-1312)
 __global__ void __launch_bounds__(RED_THREADS) k_caldt(Ctx c, CState U, int acoustic) {
@@ -945,6 +976,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_caldt(Ctx c, CState U, int acou
 }
 void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic) {
     k_caldt<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U, acoustic);
+    count(c, 1);
 }
 __global__ void __launch_bounds__(RED_THREADS) k_pbar_min(Ctx c, CState U) {
     double m[1] = {INFINITY};
@@ -957,7 +989,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_pbar_min(Ctx c, CState U) {
     double tot[1];
     if (grid_fold<RedMin, 1>(m, c.partials, &c.counters[9], tot) && threadIdx.x == 0) c.ns->pmin = tot[0];
 }
-void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U) { k_pbar_min<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U); }
+void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U) {
+    k_pbar_min<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U);
+    count(c, 1);
+}
 __global__ void k_pbar_init(Ctx c, CState U, double p_ref, double* P) {
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         double q[NV];
@@ -968,6 +1003,7 @@ __global__ void k_pbar_init(Ctx c, CState U, double p_ref, double* P) {
 }
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P) {
     k_pbar_init<<<blocks_for(c.n), TPB, 0, st>>>(c, U, p_ref, P);
+    count(c, 1);
 }
 
 }  // namespace spb6g

@@ -47,13 +47,16 @@ struct spb6g_solver {
     bool startup = true;
     spb6g_stats stats{};
     int bicg_parity = 0;
-    // timing
+    // timing: events recorded around kernel groups, resolved at the next host sync
     bool timing = false;
-    cudaEvent_t ev[2 * TG_COUNT];
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending { int group; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    cudaEvent_t open_ev = nullptr;
     double tms[TG_COUNT] = {};
     int64_t tcnt[TG_COUNT] = {};
-    int open_group = -1;
-    int err = SPB6G_OK;
+    cudaEvent_t region[2] = {nullptr, nullptr};
+    long long nlaunch = 0;
 };
 
 namespace {
@@ -75,26 +78,48 @@ double* dalloc(spb6g_solver* s, size_t count) {
     return (double*)p;
 }
 
-void tbegin(spb6g_solver* s, int g) {
+cudaEvent_t pool_event(spb6g_solver* s) {
+    if (s->ev_pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        return e;
+    }
+    cudaEvent_t e = s->ev_pool.back();
+    s->ev_pool.pop_back();
+    return e;
+}
+void tbegin(spb6g_solver* s, int) {
     if (!s->timing) return;
-    cudaEventRecord(s->ev[2 * g], s->st);
-    s->open_group = g;
+    s->open_ev = pool_event(s);
+    if (s->open_ev) cudaEventRecord(s->open_ev, s->st);
 }
 void tend_(spb6g_solver* s, int g) {
-    if (!s->timing) return;
-    cudaEventRecord(s->ev[2 * g + 1], s->st);
-    cudaEventSynchronize(s->ev[2 * g + 1]);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, s->ev[2 * g], s->ev[2 * g + 1]);
-    s->tms[g] += ms;
-    s->tcnt[g] += 1;
-    s->open_group = -1;
+    if (!s->timing || !s->open_ev) return;
+    cudaEvent_t b = pool_event(s);
+    if (!b) return;
+    cudaEventRecord(b, s->st);
+    s->pending.push_back({g, s->open_ev, b});
+    s->open_ev = nullptr;
+}
+// Accumulates every completed group (called after a stream synchronisation).
+void resolve_timing(spb6g_solver* s) {
+    for (auto& p : s->pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            s->tms[p.group] += ms;
+            s->tcnt[p.group] += 1;
+        }
+        s->ev_pool.push_back(p.a);
+        s->ev_pool.push_back(p.b);
+    }
+    s->pending.clear();
 }
 
 int sync_read(spb6g_solver* s, bool bicg) {
     CK(cudaMemcpyAsync(&s->pin->ns, s->c.ns, sizeof(NewtonScalars), cudaMemcpyDeviceToHost, s->st));
     if (bicg) CK(cudaMemcpyAsync(&s->pin->bs, s->c.bs_, sizeof(BicgScalars), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
+    if (!s->pending.empty()) resolve_timing(s);
     return SPB6G_OK;
 }
 int reset_flags(spb6g_solver* s) {
@@ -323,7 +348,10 @@ int do_step(spb6g_solver* s) {
             ok = rc == SPB6G_OK;
         }
         if (ok) {
-            for (int k = 0; k < NV; k++) std::swap(s->U[k], s->Ust[k]);
+            for (int k = 0; k < NV; k++) {
+                std::swap(s->U[k], s->Ust[k]);
+                s->c.Ust.v[k] = s->Ust[k];
+            }
             s->Pmain = s->c.P;  // the converged stage pressure becomes P (main :1374)
             done = true;
         }
@@ -419,8 +447,9 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
     if (ok && cudaMallocHost((void**)&s->pin, sizeof(Pinned)) != cudaSuccess) ok = false;
     if (ok)
-        for (int e = 0; e < 2 * TG_COUNT; e++)
-            if (cudaEventCreate(&s->ev[e]) != cudaSuccess) ok = false;
+        for (int e = 0; e < 2; e++)
+            if (cudaEventCreate(&s->region[e]) != cudaSuccess) ok = false;
+    c.nlaunch = &s->nlaunch;
     c.p_ref = 0;
     if (!ok || cudaStreamSynchronize(s->st) != cudaSuccess) { spb6g_destroy(s); return SPB6G_CUDA_ERROR; }
     *out = s;
@@ -432,8 +461,10 @@ int spb6g_destroy(spb6g_solver* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     for (void* p : s->allocs) cudaFree(p);
     if (s->pin) cudaFreeHost(s->pin);
-    for (int e = 0; e < 2 * TG_COUNT; e++)
-        if (s->ev[e]) cudaEventDestroy(s->ev[e]);
+    resolve_timing(s);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (int e = 0; e < 2; e++)
+        if (s->region[e]) cudaEventDestroy(s->region[e]);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
     return SPB6G_OK;
@@ -599,12 +630,16 @@ int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup) {
 }
 int spb6g_timing_enable(spb6g_solver* s, int on) {
     if (!s) return SPB6G_BAD_ARG;
+    cudaStreamSynchronize(s->st);
+    resolve_timing(s);
     s->timing = on != 0;
     for (int g = 0; g < TG_COUNT; g++) { s->tms[g] = 0; s->tcnt[g] = 0; }
     return SPB6G_OK;
 }
 int spb6g_timing_get(spb6g_solver* s, double* ms, int64_t* launches, int max_groups, int* n_groups) {
     if (!s) return SPB6G_BAD_ARG;
+    cudaStreamSynchronize(s->st);
+    resolve_timing(s);
     for (int g = 0; g < TG_COUNT && g < max_groups; g++) {
         if (ms) ms[g] = s->tms[g];
         if (launches) launches[g] = s->tcnt[g];
@@ -612,6 +647,22 @@ int spb6g_timing_get(spb6g_solver* s, double* ms, int64_t* launches, int max_gro
     if (n_groups) *n_groups = TG_COUNT;
     return SPB6G_OK;
 }
+int spb6g_region_begin(spb6g_solver* s) {
+    if (!s) return SPB6G_BAD_ARG;
+    CK(cudaEventRecord(s->region[0], s->st));
+    return SPB6G_OK;
+}
+int spb6g_region_end(spb6g_solver* s, double* ms) {
+    if (!s || !ms) return SPB6G_BAD_ARG;
+    CK(cudaEventRecord(s->region[1], s->st));
+    CK(cudaEventSynchronize(s->region[1]));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, s->region[0], s->region[1]));
+    *ms = f;
+    return SPB6G_OK;
+}
+int64_t spb6g_kernel_launches(spb6g_solver* s) { return s ? (int64_t)s->nlaunch : -1; }
+
 const char* spb6g_timing_name(int group) { return (group >= 0 && group < TG_COUNT) ? kTimerNames[group] : "?"; }
 
 const char* spb6g_status_string(int status) {

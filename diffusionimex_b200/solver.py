@@ -90,6 +90,9 @@ def library() -> ctypes.CDLL:
         "spb6g_timing_get": (I, [P, P, P, I, P]),
         "spb6g_timing_name": (ctypes.c_char_p, [I]),
         "spb6g_status_string": (ctypes.c_char_p, [I]),
+        "spb6g_region_begin": (I, [P]),
+        "spb6g_region_end": (I, [P, P]),
+        "spb6g_kernel_launches": (ctypes.c_int64, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -206,6 +209,24 @@ class Solver:
         s = Stats()
         self._check(self.lib.spb6g_get_stats(self.h, ctypes.byref(s)), "spb6g_get_stats")
         return {k: getattr(s, k) for k, _ in Stats._fields_ if k != "reserved"}
+
+    def region_begin(self):
+        self._check(self.lib.spb6g_region_begin(self.h), "region_begin")
+
+    def region_end(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self.lib.spb6g_region_end(self.h, ctypes.byref(ms)), "region_end")
+        return ms.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.spb6g_kernel_launches(self.h))
+
+    def upload_soa(self, ptr: int):
+        """Upload from a host buffer (pointer) in k-major SoA layout (8 x ny x nx doubles)."""
+        self._check(self.lib.spb6g_upload_state(self.h, ctypes.c_void_p(ptr), 1), "spb6g_upload_state")
+
+    def download_soa(self, ptr: int):
+        self._check(self.lib.spb6g_download_state(self.h, ctypes.c_void_p(ptr), 1), "spb6g_download_state")
 
     def timing(self, enable: bool | None = None) -> dict:
         if enable is not None:

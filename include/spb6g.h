@@ -118,11 +118,18 @@ int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st);
 /* Simulation time t (settable, e.g. when restarting from a dump). */
 int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup);
 
-/* Per-kernel device time (ms, CUDA events on the solver's stream) accumulated
- * since the last reset; names[] enumerates the timed kernel groups. */
+/* Per-kernel-group device time (ms, CUDA events on the solver's stream)
+ * accumulated since timing was enabled; spb6g_timing_name(g) names group g. */
 int spb6g_timing_enable(spb6g_solver* s, int on);
 int spb6g_timing_get(spb6g_solver* s, double* ms, int64_t* launches, int max_groups, int* n_groups);
 const char* spb6g_timing_name(int group);
+
+/* Device time (ms) between region_begin and region_end, from CUDA events on the
+ * solver's stream: everything the handle enqueued in between, host waits included. */
+int spb6g_region_begin(spb6g_solver* s);
+int spb6g_region_end(spb6g_solver* s, double* ms);
+/* Number of kernels the handle has launched since creation. */
+int64_t spb6g_kernel_launches(spb6g_solver* s);
 
 /* Human-readable status name. */
 const char* spb6g_status_string(int status);

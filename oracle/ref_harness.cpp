@@ -295,18 +295,25 @@ int main(int argc, char** argv) {
     std::vector<double> extra;
     auto t0 = std::chrono::steady_clock::now();
     int rc = 0;
+    long timed_steps = 0;
     if (c.mode == SPB6_MODE_STAGE) {
         rc = stage_dump(H, c.dtfix, extra);
-    } else if (c.mode == SPB6_MODE_STEPS) {
-        for (int s = 0; s < c.nsteps && rc == 0 && t < time_stop * (1 - 1e-12); s++) rc = step(H);
     } else {
-        do { rc = step(H); } while (rc == 0 && t < time_stop * (1 - 1e-12));
+        const bool to_end = c.mode == SPB6_MODE_TEND;
+        for (int s = 0; (to_end || s < c.nsteps) && rc == 0 && t < time_stop * (1 - 1e-12); s++) {
+            if (s == c.warmup) t0 = std::chrono::steady_clock::now();
+            rc = step(H);
+            if (s >= c.warmup) timed_steps++;
+            if (c.budget_s > 0 && s >= c.warmup &&
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > c.budget_s) break;
+        }
     }
     r.wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    r.timed_steps = timed_steps;
     double M1[3]; totals(*H.u_con, M1);
     for (int q = 0; q < 3; q++) r.dM[q] = (M1[q] - M0[q]) / M0[q];
     r.status = rc; r.steps = st_steps; r.rejects = st_reject; r.rk1 = st_rk1; r.stages = st_stage;
-    r.newton_it = st_newton_it; r.floor_count = st_floor; r.closure_fails = st_cl_fail;
+    r.newton_it = st_newton_it; r.floor_count = st_floor;
     r.t = t; r.dt = dt; r.maxres = st_maxres; r.p_ref = P_REF;
     std::vector<double> U, P(H.P.P);
     for (int j = 0; j < c.ny; j++)

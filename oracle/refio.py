@@ -29,22 +29,25 @@ CASE_DT = np.dtype([
     ("x0", "<f8"), ("x1", "<f8"), ("y0", "<f8"), ("y1", "<f8"), ("bcu", "<f8", 4), ("bcp", "<f8", 4),
     ("g", "<f8", 2), ("pinf", "<f8", 2), ("q", "<f8", 2), ("qp", "<f8", 2), ("cv", "<f8", 2), ("b", "<f8", 2),
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
+    ("budget_s", "<f8"), ("warmup", "<i4"), ("pad2", "<i4"),
 ])
 RESULT_DT = np.dtype([
     ("magic", "<u4"), ("status", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
     ("steps", "<i8"), ("rejects", "<i8"), ("rk1", "<i8"), ("stages", "<i8"), ("newton_it", "<i8"),
-    ("floor_count", "<i8"), ("bicg_it", "<i8"), ("closure_fails", "<i8"),
+    ("floor_count", "<i8"), ("bicg_it", "<i8"), ("timed_steps", "<i8"),
     ("t", "<f8"), ("dt", "<f8"), ("maxres", "<f8"), ("p_ref", "<f8"), ("wall_s", "<f8"), ("dM", "<f8", 3),
 ])
 
 
-def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0) -> np.ndarray:
+def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, warmup: int = 0,
+                budget_s: float = 0.0) -> np.ndarray:
     r = np.zeros((), CASE_DT)
     r["magic"], r["version"] = MAGIC, 1
     for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
         r[k] = int(cfg[k])
     r["bc"] = cfg["bc"]
     r["mode"], r["nsteps"], r["threads"] = mode, nsteps, threads
+    r["warmup"], r["budget_s"] = warmup, budget_s
     for k in ("x0", "x1", "y0", "y1", "cfl", "cfl_ac", "dtfix", "newton_tol", "bicg_tol", "tend"):
         r[k] = float(cfg[k])
     r["bcu"], r["bcp"] = cfg["bcu"], cfg["bcp"]
@@ -75,13 +78,15 @@ def ref_available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def run_ref(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, timeout: float = 3600) -> dict:
-    """Run the reference solver (compiled from its sources) on cfg['U']."""
+def run_ref(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, timeout: float = 3600,
+            warmup: int = 0, budget_s: float = 0.0) -> dict:
+    """Run the reference solver (compiled from its sources) on cfg['U'].  With `warmup`, the first
+    steps are excluded from wall_s; with `budget_s`, stepping stops once the timed steps used it."""
     U = np.ascontiguousarray(cfg["U"], dtype="<f8")
     with tempfile.TemporaryDirectory() as d:
         ci, co = os.path.join(d, "case.bin"), os.path.join(d, "out.bin")
         with open(ci, "wb") as f:
-            f.write(case_record(cfg, mode, nsteps, threads).tobytes())
+            f.write(case_record(cfg, mode, nsteps, threads, warmup, budget_s).tobytes())
             f.write(U.tobytes())
         env = dict(os.environ)
         if threads:
@@ -116,10 +121,11 @@ def _port_lib():
     return _port
 
 
-def run_port(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 1) -> dict:
+def run_port(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 1, warmup: int = 0,
+             budget_s: float = 0.0) -> dict:
     """Run the C restatement on cfg['U'] (same record format as run_ref)."""
     lib = _port_lib()
-    rec = case_record(cfg, mode, nsteps, threads)
+    rec = case_record(cfg, mode, nsteps, threads, warmup, budget_s)
     U = np.ascontiguousarray(cfg["U"], dtype="<f8")
     nx, ny = cfg["nx"], cfg["ny"]
     n = nx * ny

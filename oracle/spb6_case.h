@@ -37,13 +37,16 @@ typedef struct {
     double bcu[4], bcp[4];
     double g[2], pinf[2], q[2], qp[2], cv[2], b[2];
     double cfl, cfl_ac, dtfix, newton_tol, bicg_tol, tend;
+    double budget_s;   /* > 0: stop stepping once the timed steps have used this much wall time */
+    int32_t warmup;    /* steps run before the timed region (wall_s counts the rest) */
+    int32_t pad2;
 } spb6_case;
 
 typedef struct {
     uint32_t magic;
     int32_t status; /* 0 ok, 1 bad input, 2 solver failure (as the reference's exit code 2) */
     int32_t nx, ny;
-    int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it, closure_fails;
+    int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it, timed_steps; /* steps inside the timed region (all steps when warmup = 0) */
     double t, dt, maxres, p_ref, wall_s;
     double dM[3];
 } spb6_result;

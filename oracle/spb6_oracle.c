@@ -1307,7 +1307,7 @@ int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap)
     memset(r, 0, sizeof *r);
     double* arr = (double*)(o + sizeof(spb6_result));
     size_t off = (size_t)n * 8 + n;
-    const double t0 = now_s();
+    double t0 = now_s();
     int rc = 0;
     if (c->mode == SPB6_MODE_STAGE) {
         double Ae[3][3], Ai[3][3];
@@ -1338,17 +1338,26 @@ int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap)
         ok = ok && pressure_subsystem(O.Pst, O.adt);
         if (ok) { memcpy(O.u, O.ust, ncell * NV * sizeof(double)); memcpy(O.P, O.Pst, (size_t)n * sizeof(double)); }
         rc = ok ? 0 : 2;
-    } else if (c->mode == SPB6_MODE_STEPS) {
-        for (int s = 0; s < c->nsteps && rc == 0 && O.t < O.tend * (1 - 1e-12); s++) rc = step();
     } else {
-        do { rc = step(); } while (rc == 0 && O.t < O.tend * (1 - 1e-12));
+        const int to_end = c->mode == SPB6_MODE_TEND;
+        double tw = t0;
+        long timed = 0;
+        for (int s = 0; (to_end || s < c->nsteps) && rc == 0 && O.t < O.tend * (1 - 1e-12); s++) {
+            if (s == c->warmup) tw = now_s();
+            rc = step();
+            if (s >= c->warmup) timed++;
+            if (c->budget_s > 0 && s >= c->warmup && now_s() - tw > c->budget_s) break;
+        }
+        r->timed_steps = timed;
+        (void)tw;
+        t0 = tw;
     }
     const double wall = now_s() - t0;
     double M1[3];
     totals(O.u, M1);
     r->magic = SPB6_CASE_MAGIC; r->status = rc; r->nx = nx; r->ny = ny;
     r->steps = O.st_steps; r->rejects = O.st_reject; r->rk1 = O.st_rk1; r->stages = O.st_stage; r->newton_it = O.st_newton_it;
-    r->floor_count = O.st_floor; r->bicg_it = O.st_bicg_it; r->closure_fails = 0;
+    r->floor_count = O.st_floor; r->bicg_it = O.st_bicg_it;
     r->t = O.t; r->dt = O.dt; r->maxres = O.st_maxres; r->p_ref = O.p_ref; r->wall_s = wall;
     for (int q = 0; q < 3; q++) r->dM[q] = (M1[q] - M0[q]) / M0[q];
     size_t w = 0;
