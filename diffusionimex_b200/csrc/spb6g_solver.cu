@@ -615,6 +615,30 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     s->Pmain = c.P;
     return SPB6G_OK;
 }
+int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double* qph) {
+    if (!s) return SPB6G_BAD_ARG;
+    const Ctx& c = s->c;
+    const size_t nfx = (size_t)(s->g.nx + 1) * s->g.ny, nfy = (size_t)s->g.nx * (s->g.ny + 1), n = s->n;
+    CK(cudaStreamSynchronize(s->st));
+    if (fx) {
+        const double* a[4] = {c.fx_ubs, c.fx_kp, c.fx_wl, c.fx_pv};
+        for (int k = 0; k < 4; k++) CK(cudaMemcpy(fx + k * nfx, a[k], nfx * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (fy) {
+        const double* a[4] = {c.fy_ubs, c.fy_kp, c.fy_wl, c.fy_pv};
+        for (int k = 0; k < 4; k++) {
+            if (s->g.ny > 1) CK(cudaMemcpy(fy + k * nfy, a[k], nfy * sizeof(double), cudaMemcpyDeviceToHost));
+            else memset(fy + k * nfy, 0, nfy * sizeof(double));
+        }
+    }
+    if (kw) CK(cudaMemcpy(kw, c.kw, n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (qph) {
+        CK(cudaMemcpy(qph, c.qph0, n * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(qph + n, c.qph1, n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return SPB6G_OK;
+}
+
 int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st) {
     if (!s || !st) return SPB6G_BAD_ARG;
     *st = s->stats;

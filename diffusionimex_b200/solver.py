@@ -93,6 +93,7 @@ def library() -> ctypes.CDLL:
         "spb6g_region_begin": (I, [P]),
         "spb6g_region_end": (I, [P, P]),
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
+        "spb6g_stage_data": (I, [P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -203,6 +204,19 @@ class Solver:
         self._check(self.lib.spb6g_stage_dump(self.h, float(dt), *(_ptr(out[k]) for k in
                                                                   ("Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y"))),
                     "stage_dump")
+        return out
+
+    def stage_data(self) -> dict:
+        """Face coefficients, residual scale and shock budget of the last stage."""
+        nx, ny, n = self.nx, self.ny, self.nx * self.ny
+        fx = np.empty((4, ny, nx + 1))
+        fy = np.empty((4, ny + 1, nx))
+        kw = np.empty((ny, nx))
+        qph = np.empty((2, ny, nx))
+        self._check(self.lib.spb6g_stage_data(self.h, _ptr(fx), _ptr(fy), _ptr(kw), _ptr(qph)), "stage_data")
+        out = {f"fx_{k}": fx[q] for q, k in enumerate(("ubs", "kp", "wl", "pv"))}
+        out.update({f"fy_{k}": fy[q] for q, k in enumerate(("ubs", "kp", "wl", "pv"))})
+        out.update(kw=kw, qph0=qph[0], qph1=qph[1])
         return out
 
     def stats(self) -> dict:

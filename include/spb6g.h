@@ -114,6 +114,11 @@ int spb6g_advance(spb6g_solver* s, int nsteps);
 int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double* ube_x, double* ube_y,
                      double* phi_x, double* phi_y);
 
+/* Stage data of the last stage (StageData, :591-608): x-face coefficients ubs, kp, wL, pv
+ * (4 blocks of (nx+1)*ny, faces i-1/2 .. nx-1/2), y-face coefficients (4 blocks of nx*(ny+1)),
+ * the residual scale K + P_E (nx*ny) and the shock budget Q_1, Q_2 (2 blocks of nx*ny). */
+int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double* qph);
+
 int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st);
 /* Simulation time t (settable, e.g. when restarting from a dump). */
 int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup);

@@ -71,6 +71,13 @@ def parse_result(buf: bytes, nx: int, ny: int, mode: int) -> dict:
         out["ube_y"] = arr[o:o + nx * (ny + 1)].reshape(ny + 1, nx).copy(); o += nx * (ny + 1)
         out["phi_x"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
         out["phi_y"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
+        if arr.size >= o + 4 * (nx + 1) * ny + 4 * nx * (ny + 1) + 3 * n:  # stage data (C restatement only)
+            for k in ("fx_ubs", "fx_kp", "fx_wl", "fx_pv"):
+                out[k] = arr[o:o + (nx + 1) * ny].reshape(ny, nx + 1).copy(); o += (nx + 1) * ny
+            for k in ("fy_ubs", "fy_kp", "fy_wl", "fy_pv"):
+                out[k] = arr[o:o + nx * (ny + 1)].reshape(ny + 1, nx).copy(); o += nx * (ny + 1)
+            for k in ("kw", "qph0", "qph1"):
+                out[k] = arr[o:o + n].reshape(ny, nx).copy(); o += n
     return out
 
 
@@ -129,7 +136,8 @@ def run_port(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 
     U = np.ascontiguousarray(cfg["U"], dtype="<f8")
     nx, ny = cfg["nx"], cfg["ny"]
     n = nx * ny
-    cap = RESULT_DT.itemsize + 8 * (n * 8 + n + n * 8 + n + (nx + 1) * ny + nx * (ny + 1) + 2 * n)
+    cap = RESULT_DT.itemsize + 8 * (n * 8 + n + n * 8 + n + (nx + 1) * ny + nx * (ny + 1) + 2 * n
+                                    + 4 * (nx + 1) * ny + 4 * nx * (ny + 1) + 3 * n)
     out = np.zeros(cap, np.uint8)
     size = lib.spb6_oracle_run(rec.ctypes.data, U.ctypes.data, out.ctypes.data, cap)
     if size <= 0:

@@ -57,6 +57,9 @@ typedef struct {
 } Orc;
 
 static Orc O; /* one case at a time */
+/* stage-mode capture of the stage data (faces, residual scale, shock budget) right after the prep */
+static double* g_prep_capture = NULL;
+static size_t g_prep_len = 0;
 
 static inline size_t cid(int i, int j) { return (size_t)i + (size_t)j * O.NXT; }
 static inline double* cell(double* g, int i, int j) { return g + NV * cid(i, j); }
@@ -1127,6 +1130,24 @@ static int pressure_subsystem(double* P, double tau) {
         const int i = q % nx + G, j = q / nx + G;
         shock_budget(O.ust, i, j, ny > 1, &O.qph[cid(i, j) * 2]);
     }
+    if (g_prep_capture) { /* x faces i-1/2..nx-1/2 of interior rows, y faces, Kw, Qph */
+        size_t w = 0;
+        double* fxs[4] = {O.ubsx, O.kpx, O.wlx, O.pvx};
+        double* fys[4] = {O.ubsy, O.kpy, O.wly, O.pvy};
+        for (int a = 0; a < 4; a++)
+            for (int j = 0; j < ny; j++)
+                for (int i = -1; i < nx; i++) g_prep_capture[w++] = fxs[a][cid(i + G, j + G)];
+        for (int a = 0; a < 4; a++)
+            for (int j = -1; j < ny; j++)
+                for (int i = 0; i < nx; i++) g_prep_capture[w++] = ny > 1 ? fys[a][cid(i + G, j + G)] : 0.0;
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) g_prep_capture[w++] = O.kw[cid(i + G, j + G)];
+        for (int k = 0; k < 2; k++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) g_prep_capture[w++] = O.qph[cid(i + G, j + G) * 2 + k];
+        g_prep_len = w;
+        g_prep_capture = NULL;
+    }
     double res;
     const int ok = newton(P, &res);
     if (ok) O.st_maxres = SMAX(O.st_maxres, res);
@@ -1258,7 +1279,9 @@ static void totals(const double* u, double M[3]) {
 int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap) {
     if (!c || c->magic != SPB6_CASE_MAGIC || c->version != SPB6_CASE_VERSION || c->nx < 1 || c->ny < 1) return -1;
     const int nx = c->nx, ny = c->ny, n = nx * ny;
-    const size_t need = sizeof(spb6_result) + sizeof(double) * ((size_t)n * 8 + n + (c->mode == SPB6_MODE_STAGE ? (size_t)n * 8 + n + (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1) + 2 * (size_t)n : 0));
+    const size_t nstage = (size_t)n * 8 + n + (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1) + 2 * (size_t)n +
+                          4 * (size_t)(nx + 1) * ny + 4 * (size_t)nx * (ny + 1) + 3 * (size_t)n;
+    const size_t need = sizeof(spb6_result) + sizeof(double) * ((size_t)n * 8 + n + (c->mode == SPB6_MODE_STAGE ? nstage : 0));
     if (cap < need) return -2;
     memset(&O, 0, sizeof O);
     O.nx = nx; O.ny = ny; O.NXT = nx + 2 * G; O.NYT = ny + 2 * G;
@@ -1335,7 +1358,11 @@ int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap)
             for (int i = 0; i < nx; i++) arr[off++] = O.phx[cid(i + G, j + G)];
         for (int j = 0; j < ny; j++)
             for (int i = 0; i < nx; i++) arr[off++] = O.phy[cid(i + G, j + G)];
+        g_prep_capture = arr + off;
+        g_prep_len = 0;
         ok = ok && pressure_subsystem(O.Pst, O.adt);
+        g_prep_capture = NULL;
+        off += g_prep_len;
         if (ok) { memcpy(O.u, O.ust, ncell * NV * sizeof(double)); memcpy(O.P, O.Pst, (size_t)n * sizeof(double)); }
         rc = ok ? 0 : 2;
     } else {

@@ -68,6 +68,8 @@ CASES = {
     "bubble48_stage": (lambda: _bubble(48), "stage", 0, {"dtfix": 1e-5, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "bubble48_4steps": (lambda: _bubble(48), "steps", 4, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "lowmach32_3steps": (lambda: _lowmach(32), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "lowmach32_stage": (lambda: _lowmach(32), "stage", 0, {"dtfix": 2e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "shock64x32_stage": (lambda: _shock(64, 32), "stage", 0, {"dtfix": 5e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "shock64x32_3steps": (lambda: _shock(64, 32), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "nasg256_20steps": (lambda: _nasg(256), "steps", 20, {}),
 }
