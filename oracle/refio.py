@@ -29,7 +29,7 @@ CASE_DT = np.dtype([
     ("x0", "<f8"), ("x1", "<f8"), ("y0", "<f8"), ("y1", "<f8"), ("bcu", "<f8", 4), ("bcp", "<f8", 4),
     ("g", "<f8", 2), ("pinf", "<f8", 2), ("q", "<f8", 2), ("qp", "<f8", 2), ("cv", "<f8", 2), ("b", "<f8", 2),
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
-    ("budget_s", "<f8"), ("warmup", "<i4"), ("pad2", "<i4"),
+    ("budget_s", "<f8"), ("warmup", "<i4"), ("inject_qph", "<i4"),
 ])
 RESULT_DT = np.dtype([
     ("magic", "<u4"), ("status", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
@@ -113,27 +113,35 @@ def run_ref_main(args: list[str], nx: int, ny: int = 1, timeout: float = 3600) -
             return parse_result(f.read(), nx, ny, MODE_STEPS)
 
 
-_port = None
+_port = {}
+VARIANTS = {None: "libspb6_oracle.so", "ulp": "libspb6_oracle_ulp.so", "fd": "libspb6_oracle_fd.so"}
 
 
-def _port_lib():
-    global _port
-    if _port is None:
-        if not os.path.exists(PORT_LIB):
+def _port_lib(variant=None):
+    if variant not in _port:
+        path = os.path.join(HERE, "_build", VARIANTS[variant])
+        if not os.path.exists(path):
             subprocess.run(["make", "-C", HERE, "oracle"], check=True, stdout=subprocess.DEVNULL)
-        lib = ctypes.CDLL(PORT_LIB)
+        lib = ctypes.CDLL(path)
         lib.spb6_oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         lib.spb6_oracle_run.restype = ctypes.c_int
-        _port = lib
-    return _port
+        _port[variant] = lib
+    return _port[variant]
 
 
 def run_port(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 1, warmup: int = 0,
-             budget_s: float = 0.0) -> dict:
-    """Run the C restatement on cfg['U'] (same record format as run_ref)."""
-    lib = _port_lib()
+             budget_s: float = 0.0, variant: str | None = None, qph: np.ndarray | None = None) -> dict:
+    """Run the C restatement on cfg['U'] (same record format as run_ref).
+
+    variant: None, "ulp" (shock-shooting exp/log/pow one ulp up) or "fd" (FD Jacobian step
+    1.01e-7) -- the round-off perturbations that define the reference's own noise level.
+    qph: stage mode only -- (2, ny, nx) shock budget Q_1, Q_2 used instead of the computed one."""
+    lib = _port_lib(variant)
     rec = case_record(cfg, mode, nsteps, threads, warmup, budget_s)
     U = np.ascontiguousarray(cfg["U"], dtype="<f8")
+    if qph is not None:
+        rec["inject_qph"] = 1
+        U = np.concatenate([U.ravel(), np.ascontiguousarray(qph, dtype="<f8").ravel()])
     nx, ny = cfg["nx"], cfg["ny"]
     n = nx * ny
     cap = RESULT_DT.itemsize + 8 * (n * 8 + n + n * 8 + n + (nx + 1) * ny + nx * (ny + 1) + 2 * n

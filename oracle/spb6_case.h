@@ -39,7 +39,7 @@ typedef struct {
     double cfl, cfl_ac, dtfix, newton_tol, bicg_tol, tend;
     double budget_s;   /* > 0: stop stepping once the timed steps have used this much wall time */
     int32_t warmup;    /* steps run before the timed region (wall_s counts the rest) */
-    int32_t pad2;
+    int32_t inject_qph; /* stage mode, C restatement only: U0 is followed by Q_1, Q_2 (2 x nx*ny) */
 } spb6_case;
 
 typedef struct {

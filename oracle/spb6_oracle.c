@@ -10,12 +10,34 @@
  * Used by tests/ (the CPU checker of the CUDA path), __graft_entry__.smoke()
  * and bench.py's CPU-baseline leg.  Entry point: spb6_oracle_run (spb6_oracle.h).
  */
+#define _POSIX_C_SOURCE 199309L
 #include "spb6_oracle.h"
 
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+
+/* Round-off perturbation variants (the reference's own acceptance criterion for a changed
+ * implementation, docs/code/openmp_optimisation.md:81-82, is "no larger than the code's own
+ * change under a round-off perturbation"):
+ *   SPB6_ORACLE_ULP   exp / log / pow of the shock-profile shooting return the next double up;
+ *   SPB6_ORACLE_FD    finite-difference Jacobian step 1.01e-7 instead of 1e-7 (the perturbation
+ *                     the reference's report uses). */
+#ifdef SPB6_ORACLE_ULP
+static double sh_exp(double x) { return nextafter(exp(x), INFINITY); }
+static double sh_log(double x) { return nextafter(log(x), INFINITY); }
+static double sh_pow(double x, double y) { return nextafter(pow(x, y), INFINITY); }
+#else
+#define sh_exp exp
+#define sh_log log
+#define sh_pow pow
+#endif
+#ifdef SPB6_ORACLE_FD
+#define FD_STEP 1.01e-7
+#else
+#define FD_STEP 1e-7
+#endif
 
 /* std::max / std::min semantics (the second argument wins only on a strict compare) */
 #define SMAX(a, b) ((a) < (b) ? (b) : (a))
@@ -60,6 +82,7 @@ static Orc O; /* one case at a time */
 /* stage-mode capture of the stage data (faces, residual scale, shock budget) right after the prep */
 static double* g_prep_capture = NULL;
 static size_t g_prep_len = 0;
+static const double* g_qph_inject = NULL; /* stage mode: Q_1, Q_2 (2 blocks of nx*ny) replacing the shock budget */
 
 static inline size_t cid(int i, int j) { return (size_t)i + (size_t)j * O.NXT; }
 static inline double* cell(double* g, int i, int j) { return g + NV * cid(i, j); }
@@ -311,19 +334,19 @@ static int prof_integrate(const ShockProf* S, double c, double* v1end, double* q
                 err = SMAX(err, fabs(h * (d5 - d4)) / sc[n]);
             }
         if (!ok || !(err <= 1e-8)) {
-            h *= ok ? SMAX(0.1, 0.9 * pow(1e-8 / err, 0.25)) : 0.25;
+            h *= ok ? SMAX(0.1, 0.9 * sh_pow(1e-8 / err, 0.25)) : 0.25;
             if (fabs(h) < 1e-14 * fabs(L)) return 0;
             continue;
         }
         for (int n = 0; n < 3; n++) y[n] = y5[n];
         if (last) { *v1end = y[1]; *qend = y[2]; return 1; }
         v += h;
-        h *= SMIN(5.0, 0.9 * pow(1e-8 / SMAX(err, 1e-30), 0.2));
+        h *= SMIN(5.0, 0.9 * sh_pow(1e-8 / SMAX(err, 1e-30), 0.2));
     }
     return 0;
 }
 static double shoot_F(const ShockProf* S, const double vH[2], const double vpre[2], double t, double* qq) {
-    const double c = 1.0 / (1.0 + exp(-t));
+    const double c = 1.0 / (1.0 + sh_exp(-t));
     double v1e;
     if (!prof_integrate(S, c, &v1e, qq)) return NAN;
     return (v1e - vH[0]) / vpre[0];
@@ -360,7 +383,7 @@ static int shock_share(const double Y[2], const double vpre[2], double p0, doubl
         double ww[2];
         for (int k = 0; k < 2; k++) ww[k] = Y[k] * vpre[k] * Gm[k] / (K[k] * K[k]);
         const double c0 = SMIN(1.0 - 1e-12, SMAX(1e-12, ww[0] / (ww[0] + ww[1])));
-        t0 = isfinite(c0) ? log(c0 / (1.0 - c0)) : 0.0;
+        t0 = isfinite(c0) ? sh_log(c0 / (1.0 - c0)) : 0.0;
     }
     double ta = SMAX(-40.0, t0 - 1.0), tb = SMIN(40.0, t0 + 1.0), qa = 0, qb = 0;
     double fa = shoot_F(&S, vH, vpre, ta, &qa), fb = shoot_F(&S, vH, vpre, tb, &qb);
@@ -393,7 +416,7 @@ static int shock_share(const double Y[2], const double vpre[2], double p0, doubl
             else { tb = t; fb = ft; if (side == 1) fa *= 0.5; side = 1; }
         }
     }
-    const double c = 1.0 / (1.0 + exp(-t));
+    const double c = 1.0 / (1.0 + sh_exp(-t));
     lam[0] = c; lam[1] = 1.0 - c;
     *q = qt;
     return *q > 0;
@@ -932,7 +955,7 @@ static int newton(double* P, double* resfinal) { /* Newton_Solver, :799-904 (jre
         }
         for (int r = 0; r < n; r++) {
             const int i = r % nx, j = r / nx;
-            const double h = 1e-7 * O.sc[r];
+            const double h = FD_STEP * O.sc[r];
             double g1;
             if (!residual_at(P, i, j, h, -1, 0, &g1, NULL)) return 0;
             int cnt = 0;
@@ -941,7 +964,7 @@ static int newton(double* P, double* resfinal) { /* Newton_Solver, :799-904 (jre
             for (int w = 0; w < 4; w++) {
                 if (ny == 1 && w >= 2) break;
                 const int c = M_P(i + G + dd[w][0], j + G + dd[w][1]);
-                const double hn = 1e-7 * O.sc[c];
+                const double hn = FD_STEP * O.sc[c];
                 double g2;
                 if (!residual_at(P, i, j, 0, w, hn, &g2, NULL)) return 0;
                 O.acol[5 * r + cnt] = c; O.aval[5 * r + cnt] = (g2 - O.Gv[r]) / hn; cnt++;
@@ -1128,7 +1151,11 @@ static int pressure_subsystem(double* P, double tau) {
             }
     for (int q = 0; q < nx * ny; q++) {
         const int i = q % nx + G, j = q / nx + G;
-        shock_budget(O.ust, i, j, ny > 1, &O.qph[cid(i, j) * 2]);
+        if (g_qph_inject) { /* stage data supplied by the caller (test hook) */
+            O.qph[cid(i, j) * 2] = g_qph_inject[q];
+            O.qph[cid(i, j) * 2 + 1] = g_qph_inject[nx * ny + q];
+        } else
+            shock_budget(O.ust, i, j, ny > 1, &O.qph[cid(i, j) * 2]);
     }
     if (g_prep_capture) { /* x faces i-1/2..nx-1/2 of interior rows, y faces, Kw, Qph */
         size_t w = 0;
@@ -1360,8 +1387,10 @@ int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap)
             for (int i = 0; i < nx; i++) arr[off++] = O.phy[cid(i + G, j + G)];
         g_prep_capture = arr + off;
         g_prep_len = 0;
+        g_qph_inject = c->inject_qph ? U0 + (size_t)n * NV : NULL;
         ok = ok && pressure_subsystem(O.Pst, O.adt);
         g_prep_capture = NULL;
+        g_qph_inject = NULL;
         off += g_prep_len;
         if (ok) { memcpy(O.u, O.ust, ncell * NV * sizeof(double)); memcpy(O.P, O.Pst, (size_t)n * sizeof(double)); }
         rc = ok ? 0 : 2;
