@@ -44,6 +44,10 @@ struct Ctx {
     double *ust, *vst, *kw, *qph0, *qph1;
     double *fx_ubs, *fx_kp, *fx_wl, *fx_pv;
     double *fy_ubs, *fy_kp, *fy_wl, *fy_pv;
+    // per face, fixed for the stage: donors m1, m2, eps1, eps2 of the reconstructed left / right
+    // face values (the reference's dxL/dxR, :936-944) and the tangential velocities of the two
+    // cells (vst / ust): planes 0-3 left donor, 4-7 right donor, 8 utL, 9 utR
+    double *fxd, *fyd;  // 10 planes of (nx+1)*ny / nx*(ny+1)
     int* strong_list;
     // Newton
     double *P, *Pn, *G, *Gn, *sc, *scn, *dP;
@@ -67,7 +71,7 @@ SPB6G_DEV size_t rxi(const Geom& g, int i, int j) { return (size_t)(i + 1) + (si
 SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(j + 1) * g.nx; }
 
 // ------------------------------------------------------------ launchers (spb6g_kernels.cu)
-int red_blocks(int n);
+int red_blocks(int n, int threads = RED_THREADS);
 void launch_combine(const Ctx& c, cudaStream_t st, const double* const* U, const double* Hs, int nH,
                     const double* ae, const double* ai, double dt, double* const* Qe, double* const* Qs);
 void launch_recon(const Ctx& c, cudaStream_t st);

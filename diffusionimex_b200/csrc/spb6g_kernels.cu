@@ -18,8 +18,8 @@ static int blocks_for(long n, int tpb = TPB) {
 static inline void count(const Ctx& c, int k) {
     if (c.nlaunch) *c.nlaunch += k;
 }
-int red_blocks(int n) {
-    long b = ((long)n + RED_THREADS - 1) / RED_THREADS;
+int red_blocks(int n, int threads) {
+    long b = ((long)n + threads - 1) / threads;
     if (b < 1) b = 1;
     if (b > 148L * 8) b = 148L * 8;
     return (int)b;
@@ -361,6 +361,22 @@ SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, dou
     kp += phi * psiP / (ZL + ZR);
     pv = phi * psiU * ZL * ZR / (ZL + ZR) * D;
 }
+SPB6G_DEV void donor(const Ctx& c, int ci, int cj, int dir, bool right, double* d);
+// Donors and tangential velocities of one face (fixed for the stage).
+SPB6G_DEV void face_fixed(const Ctx& c, int i, int j, int ydir, double* plane, size_t f, size_t stride) {
+    double dl[4], dr[4], u, v;
+    donor(c, i, j, ydir, true, dl);
+    donor(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), ydir, false, dr);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        plane[q * stride + f] = dl[q];
+        plane[(4 + q) * stride + f] = dr[q];
+    }
+    vel_at(c, i, j, u, v);
+    plane[8 * stride + f] = ydir ? u : v;
+    vel_at(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), u, v);
+    plane[9 * stride + f] = ydir ? u : v;
+}
 __global__ void k_prep_fx(Ctx c) {
     const Geom& g = c.g;
     const long tot = (long)(g.nx + 1) * g.ny;
@@ -370,6 +386,7 @@ __global__ void k_prep_fx(Ctx c) {
         set_face(c, i, j, 0, ubs, kp, wl, pv);
         const size_t f = fxi(g, i, j);
         c.fx_ubs[f] = ubs; c.fx_kp[f] = kp; c.fx_wl[f] = wl; c.fx_pv[f] = pv;
+        face_fixed(c, i, j, 0, c.fxd, f, (size_t)tot);
     }
 }
 __global__ void k_prep_fy(Ctx c) {
@@ -381,6 +398,7 @@ __global__ void k_prep_fy(Ctx c) {
         set_face(c, i, j, 1, ubs, kp, wl, pv);
         const size_t f = fyi(g, i, j);
         c.fy_ubs[f] = ubs; c.fy_kp[f] = kp; c.fy_wl[f] = wl; c.fy_pv[f] = pv;
+        face_fixed(c, i, j, 1, c.fyd, f, (size_t)tot);
     }
 }
 void launch_prep(const Ctx& c, cudaStream_t st) {
@@ -496,13 +514,17 @@ SPB6G_DEV void face_eval(const Ctx& c, int i, int j, int ydir, double PL, double
         wl = c.fy_wl[fi]; pv = c.fy_pv[fi]; ubs = c.fy_ubs[fi]; kp = c.fy_kp[fi]; ube = c.ube_y[fi];
     }
     f.pf = wl * PL + (1.0 - wl) * PR - pv;
-    donor(c, i, j, ydir, true, f.cL);
-    donor(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), ydir, false, f.cR);
-    double u, v;
-    vel_at(c, i, j, u, v);
-    f.utL = ydir ? u : v;
-    vel_at(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), u, v);
-    f.utR = ydir ? u : v;
+    {
+        const double* pl = ydir ? c.fyd : c.fxd;
+        const size_t st = ydir ? (size_t)g.nx * (g.ny + 1) : (size_t)(g.nx + 1) * g.ny;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            f.cL[q] = pl[q * st + fi];
+            f.cR[q] = pl[(4 + q) * st + fi];
+        }
+        f.utL = pl[8 * st + fi];
+        f.utR = pl[9 * st + fi];
+    }
     int w = -1;
     if (!ydir) { if (i == -1 && g.bcs[0] == BC_WALL) w = 0; else if (i == g.nx - 1 && g.bcs[1] == BC_WALL) w = 1; }
     else { if (j == -1 && g.bcs[2] == BC_WALL) w = 2; else if (j == g.ny - 1 && g.bcs[3] == BC_WALL) w = 3; }
@@ -532,39 +554,46 @@ struct CellRes {
     ClOut o;
     double mx, my, E;
 };
-// cell_residual (:666-704): G = pbar_closure(P) - P_REF - Pc.
+// cell_residual (:666-704): G = pbar_closure(P) - P_REF - Pc.  The faces are
+// evaluated in pairs (x: east/west, then y: north/south) so only two face records
+// are live; each conservative quantity still receives its x difference before its
+// y difference, exactly the reference's order.
 SPB6G_DEV bool cell_residual(const Ctx& c, int i, int j, double Pc, double PW, double PE, double PS, double PN, double& Gr,
                              CellRes* out) {
     const Geom& g = c.g;
     const size_t x = (size_t)i + (size_t)j * g.nx;
-    FaceV fe, fw, fn, fs;
-    face_eval(c, i, j, 0, Pc, PE, fe);
-    face_eval(c, i - 1, j, 0, PW, Pc, fw);
     const bool twoD = g.ny > 1;
+    double X[6] = {c.Xs.v[IA1][x], c.a2s[x], c.Xs.v[IM1][x], c.Xs.v[IM2][x], c.Xs.v[IE1][x], c.Xs.v[IE2][x]};
+    double s, mx, my, E;
+    {
+        FaceV fe, fw;
+        face_eval(c, i, j, 0, Pc, PE, fe);
+        face_eval(c, i - 1, j, 0, PW, Pc, fw);
+#pragma unroll
+        for (int k = 2; k < 6; k++) X[k] -= c.rx * (finc(fe, k - 2) - finc(fw, k - 2));
+        s = c.rx * (fe.uf - fw.uf);
+        const FFlux FEe = face_flux(fe, c.p_ref), FEw = face_flux(fw, c.p_ref);
+        mx = c.Xs.v[IMU][x] - c.rx * (fe.pf - fw.pf) - c.rx * (fe.uf * FEe.M - fw.uf * FEw.M);
+        my = c.Xs.v[IMV][x] - c.rx * (FEe.Mt - FEw.Mt);
+        E = c.Xs.v[IEN][x] - c.rx * (FEe.E - FEw.E);
+    }
     if (twoD) {
+        FaceV fn, fs;
         face_eval(c, i, j, 1, Pc, PN, fn);
         face_eval(c, i, j - 1, 1, PS, Pc, fs);
-    }
-    double X[6] = {c.Xs.v[IA1][x], c.a2s[x], c.Xs.v[IM1][x], c.Xs.v[IM2][x], c.Xs.v[IE1][x], c.Xs.v[IE2][x]};
 #pragma unroll
-    for (int k = 2; k < 6; k++) {
-        X[k] -= c.rx * (finc(fe, k - 2) - finc(fw, k - 2));
-        if (twoD) X[k] -= c.ry * (finc(fn, k - 2) - finc(fs, k - 2));
-    }
-    X[1] = 1.0 - X[0];
-    const double s = c.rx * (fe.uf - fw.uf) + (twoD ? c.ry * (fn.uf - fs.uf) : 0.0);
-    X[0] *= 1.0 - s;
-    X[1] *= 1.0 - s;
-    const FFlux FEe = face_flux(fe, c.p_ref), FEw = face_flux(fw, c.p_ref);
-    double mx = c.Xs.v[IMU][x] - c.rx * (fe.pf - fw.pf) - c.rx * (fe.uf * FEe.M - fw.uf * FEw.M);
-    double my = c.Xs.v[IMV][x] - c.rx * (FEe.Mt - FEw.Mt);
-    double E = c.Xs.v[IEN][x] - c.rx * (FEe.E - FEw.E);
-    if (twoD) {
+        for (int k = 2; k < 6; k++) X[k] -= c.ry * (finc(fn, k - 2) - finc(fs, k - 2));
+        s = s + c.ry * (fn.uf - fs.uf);
         const FFlux FEn = face_flux(fn, c.p_ref), FEs = face_flux(fs, c.p_ref);
         my -= c.ry * (fn.pf - fs.pf) + c.ry * (fn.uf * FEn.M - fs.uf * FEs.M);
         mx -= c.ry * (FEn.Mt - FEs.Mt);
         E -= c.ry * (FEn.E - FEs.E);
+    } else {
+        s = s + 0.0;
     }
+    X[1] = 1.0 - X[0];
+    X[0] *= 1.0 - s;
+    X[1] *= 1.0 - s;
     const double rho = X[2] + X[3];
     if (!(rho > 0)) return false;
     ClIn in;
@@ -617,7 +646,7 @@ SPB6G_DEV double row_scale(const Ctx& c, int i, int j, double Pc) {  // natural 
 }
 
 // evalAll + norm (:805-814), optionally at Pn = P + lam dP (line search :880-886).
-__global__ void __launch_bounds__(RED_THREADS) k_residual(Ctx c, int mode, double lam) {
+__global__ void __launch_bounds__(RED_THREADS, 2) k_residual(Ctx c, int mode, double lam) {
     const Geom& g = c.g;
     double m[1] = {0.0};
     const double* P = c.P;
@@ -643,7 +672,8 @@ void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
 }
 
 // FD Jacobian rows (:837-853) with the BiCGStab set-up sums E = 1^T A 1, 1^T b, b^T b.
-__global__ void __launch_bounds__(RED_THREADS) k_jacobian(Ctx c) {
+constexpr int JAC_THREADS = 128;
+__global__ void __launch_bounds__(JAC_THREADS, 3) k_jacobian(Ctx c) {
     const Geom& g = c.g;
     double acc[3] = {0.0, 0.0, 0.0};
     const bool twoD = g.ny > 1;
@@ -683,7 +713,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_jacobian(Ctx c) {
     }
 }
 void launch_jacobian(const Ctx& c, cudaStream_t st) {
-    k_jacobian<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c);
+    k_jacobian<<<red_blocks(c.n, JAC_THREADS), JAC_THREADS, 0, st>>>(c);
     count(c, 1);
 }
 

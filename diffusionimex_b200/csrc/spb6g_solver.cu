@@ -435,6 +435,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     const size_t nfx = (size_t)(nx + 1) * ny, nfy = (size_t)nx * (ny + 1);
     c.fx_ubs = A(nfx); c.fx_kp = A(nfx); c.fx_wl = A(nfx); c.fx_pv = A(nfx);
     c.fy_ubs = A(nfy); c.fy_kp = A(nfy); c.fy_wl = A(nfy); c.fy_pv = A(nfy);
+    c.fxd = A(10 * nfx); c.fyd = A(10 * nfy);
     c.strong_list = (int*)A(n / 2 + 1);
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
     c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
