@@ -442,7 +442,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.br = A(n); c.br0 = A(n); c.bp = A(n); c.bv = A(n); c.bq = A(n); c.bs = A(n); c.bu = A(n); c.bt = A(n);
     c.tcp = A(n); c.tdp = A(n);
     for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];
-    c.partials = A((size_t)red_blocks((int)n) * MAXQ);
+    c.partials = A((size_t)red_blocks((int)n, 32) * MAXQ);  // enough for any launch width >= 32
     c.counters = (unsigned*)A(16);
     c.ns = (NewtonScalars*)A(sizeof(NewtonScalars) / sizeof(double) + 1);
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
