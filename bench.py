@@ -39,8 +39,9 @@ FALLBACK_HBM_GBS = 6650.0
 # Algorithmic FP64 bytes per interior cell (each distinct array element read or
 # written once) of the kernel groups the solver times; 2D values.
 ALG_BYTES = {
-    # recon: Qe 8 reads + 8 recon outputs; update: Qe 8 + Qs 8 + 8 recon + X* 8 + a2s + 2 face velocities
-    "explicit": (8 + 8) * 8 + (8 + 8 + 8 + 8 + 1 + 2) * 8,
+    # fused explicit kernel: reads U^n (8; + 8 per earlier stage H, counted as the stage-1 case here),
+    # writes X* 8, alpha2* 1, face velocities 2, limiter factors 2, face donors 16
+    "explicit": (8 + 8 + 2 + 2 + 16 + 1 + 8) * 8 + 4 * 8,
     "jacobian": (9 + 5 + 2 + 10 + 2 + 1 + 1 + 1 + 1 + 7) * 8,  # X*,a2s | Qe vol | phi | faces | v* | qph | kw | P | G | sc | A,A1,dinv
     "residual": (9 + 5 + 2 + 10 + 2 + 2 + 1 + 1 + 1) * 8,       # ... + P, G, sc
     "linear": 272,                                            # per BiCGStab iteration (4 passes), x iterations

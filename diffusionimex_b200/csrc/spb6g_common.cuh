@@ -163,13 +163,14 @@ template <class R, int NQ>
 SPB6G_DEV bool grid_fold(double (&v)[NQ], double* partials, unsigned* counter, double (&tot)[NQ]) {
     __shared__ double sh[NQ * 32];
     __shared__ bool last;
+    const unsigned nblocks = gridDim.x * gridDim.y, bid = blockIdx.x + blockIdx.y * gridDim.x;
     block_fold<R, NQ>(v, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) partials[(size_t)blockIdx.x * NQ + q] = v[q];
+        for (int q = 0; q < NQ; q++) partials[(size_t)bid * NQ + q] = v[q];
         __threadfence();
         const unsigned t = atomicAdd(counter, 1u);
-        last = (t == gridDim.x - 1);
+        last = (t == nblocks - 1);
     }
     __syncthreads();
     if (!last) return false;
@@ -177,9 +178,9 @@ SPB6G_DEV bool grid_fold(double (&v)[NQ], double* partials, unsigned* counter, d
     double acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) acc[q] = R::id();
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) acc[q] = R::op(acc[q], ((volatile double*)partials)[(size_t)b * NQ + q]);
+        for (int q = 0; q < NQ; q++) acc[q] = R::op(acc[q], __ldcg(partials + (size_t)b * NQ + q));
     }
     block_fold<R, NQ>(acc, sh);
     if (threadIdx.x == 0) {

@@ -33,13 +33,17 @@ struct Ctx {
     Geom g;
     int n;
     double tau, rx, ry, p_ref, adt;
-    // explicit stage
-    CState Qe, Qs;
+    // explicit stage: Qe = Un + sum_r ce[r] H_r, Qs = Un + sum_r ci[r] H_r (main :1341-1351),
+    // formed on the fly from the step's initial state and the previous stages' H
+    CState Un;
+    const double* Hprev;  // 8*n per earlier stage
+    int nH;
+    double ce[2], ci[2];
     State Xs;
     double* a2s;
-    double *ube_x, *ube_y;                   // (nx+1)*ny, nx*(ny+1)
-    double *phiv_x, *phis_x, *slu_x, *slv_x;  // (nx+2)*ny
-    double *phiv_y, *phis_y, *slu_y, *slv_y;  // nx*(ny+2)
+    double *ube_x, *ube_y;  // (nx+1)*ny, nx*(ny+1)
+    double* phis_x;         // min(phi, velocity smoothness) of cells -1..nx, (nx+2)*ny
+    double* phis_y;         // nx*(ny+2)
     // stage data
     double *ust, *vst, *kw, *qph0, *qph1;
     double *fx_ubs, *fx_kp, *fx_wl, *fx_pv;
@@ -72,10 +76,8 @@ SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(
 
 // ------------------------------------------------------------ launchers (spb6g_kernels.cu)
 int red_blocks(int n, int threads = RED_THREADS);
-void launch_combine(const Ctx& c, cudaStream_t st, const double* const* U, const double* Hs, int nH,
-                    const double* ae, const double* ai, double dt, double* const* Qe, double* const* Qs);
-void launch_recon(const Ctx& c, cudaStream_t st);
-void launch_update(const Ctx& c, cudaStream_t st);
+// fused stage combination + reconstruction + Rusanov update + face donors (replaces combine/recon/update)
+void launch_flux(const Ctx& c, cudaStream_t st);
 void launch_prep(const Ctx& c, cudaStream_t st);
 void launch_shock(const Ctx& c, cudaStream_t st);
 // mode 0: evaluate at P (writes G, sc);  mode 1: at Pn = P + lam dP (writes Pn, Gn, scn)

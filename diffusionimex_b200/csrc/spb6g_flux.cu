@@ -1,0 +1,351 @@
+// Fused explicit stage kernel: stage combination, MUSCL reconstruction with the
+// shared minmod limiter, Rusanov fluxes at the material speed, the explicit
+// update X* = Qs - tau div F(Qe) with the path-conservative alpha term, and the
+// per-face donor states the implicit part needs.
+//
+// Reference: main's stage combination (src/SPB6_PC_IMEX_omp.cpp:1341-1351),
+// TVDReconstruction (:369-471), RusanovC_x/y (:237-259), Update (:264-346) and
+// the donor copy of PressureSubsystem (:936-944).  Arithmetic per cell and per
+// face is the reference's, in its order; each quantity is computed once per
+// tile from shared memory instead of once per use.
+//
+// One CTA owns a TX x TY tile of interior cells.  It stages Qe for the tile plus
+// a two-cell halo (cross-shaped) in shared memory -- ghost cells through the
+// boundary maps -- then computes per-cell scales, the reconstruction of every
+// cell one layer around the tile, every face flux of the tile once, and the
+// update of the tile's cells.
+#include "spb6g_ctx.cuh"
+
+namespace spb6g {
+
+namespace {
+
+template <int TX, int TY, bool TWO_D>
+struct FluxTile {
+    static constexpr int HY = TWO_D ? 2 : 0;
+    static constexpr int NLX = TX + 4, NLY = TY + 2 * HY;
+    static constexpr int NRX = TX + 2;                      // x-reconstructed cells -1..TX
+    static constexpr int NRY = TWO_D ? TY + 2 : 1;          // y-reconstructed cells -1..TY
+    static constexpr int NFX = TX + 1, NFY = TWO_D ? TY + 1 : 1;
+    static constexpr int Q_SZ = NV * NLX * NLY;
+    static constexpr int S_SZ = 2 * NLX * NLY;
+    static constexpr int RX_SZ = 3 * NRX * TY;              // phi (volume), slope u, slope v
+    static constexpr int RY_SZ = TWO_D ? 3 * TX * NRY : 0;
+    static constexpr int FX_SZ = 9 * NFX * TY;              // 8 fluxes + face velocity
+    static constexpr int FY_SZ = TWO_D ? 9 * TX * NFY : 0;
+    static constexpr int TOTAL = Q_SZ + S_SZ + RX_SZ + RY_SZ + FX_SZ + FY_SZ;
+    static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
+};
+
+// Qe of a (possibly ghost) cell: the stage combination at the mapped source, then the ghost transforms.
+SPB6G_DEV void load_qe(const Ctx& c, int i, int j, double* q) {
+    int sx, sy;
+    const int si = src_x(c.g, i, sx), sj = src_y(c.g, j, sy);
+    const size_t x = (size_t)si + (size_t)sj * c.g.nx;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double e = c.Un.v[k][x];
+        for (int r = 0; r < c.nH; r++) e = e + c.ce[r] * c.Hprev[((size_t)r * NV + k) * c.n + x];
+        q[k] = e;
+    }
+    if (sx >= 0) ghost_transform(c.phy, c.g, sx, q);
+    if (sy >= 0) ghost_transform(c.phy, c.g, sy, q);
+}
+
+SPB6G_DEV void scales_of(const Phys& P, const double* q, double& vsc, double& esc) {
+    Prim w;
+    const double rho = q[IM1] + q[IM2], mm = hypot(q[IMU], q[IMV]);
+    vsc = (rho > 0 ? mm / rho : 0.0) + (prim_of(P, q, w) ? w.cf : 0.0);
+    esc = fabs(q[IE1]) + fabs(q[IE2]) + (rho > 0 ? 0.5 * mm * mm / rho : 0.0);
+}
+
+// Shared limiter, face-admissibility cap and velocity slopes (TVDReconstruction :399-463).
+SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const double* Ub, double vsa, double vsc,
+                      double vsb, double esa, double esc, double esb, double& phi_out, double& phis_out, double& slu,
+                      double& slv) {
+    const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
+    double phi = 1.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int k = VOL[q];
+        const double xa = Ua[k], xc = Uc[k], xb = Ub[k];
+        double sc;
+        if (k == IA1) sc = 3.0;
+        else if (k == IM1 || k == IM2) sc = fabs(xa) + fabs(xc) + fabs(xb);
+        else sc = esa + esc + esb;
+        const double a = xc - xa, b = xb - xc, tiny = 1e-12 * sc + 1e-300;
+        if (!P.limiter) break;
+        if (fabs(a) <= tiny && fabs(b) <= tiny) continue;
+        if (a * b <= 0) { phi = 0.0; break; }
+        const double cc = 0.5 * (a + b), m = fabs(a) < fabs(b) ? a : b;
+        phi = SMIN(phi, m / cc);
+    }
+    if (P.limiter && phi > 0.0) {
+        const double* cs[3] = {Ua, Uc, Ub};
+#pragma unroll
+        for (int ph = 0; ph < 2; ph++) {
+            double L1[3], L2[3];
+#pragma unroll
+            for (int n = 0; n < 3; n++) {
+                const double a = ph == 0 ? cs[n][IA1] : 1.0 - cs[n][IA1], m = cs[n][ph == 0 ? IM1 : IM2],
+                             e = cs[n][ph == 0 ? IE1 : IE2];
+                L1[n] = a - m * P.ph[ph].b;
+                L2[n] = e - m * P.ph[ph].q - L1[n] * P.ph[ph].pi;
+            }
+            {
+                const double dL = fabs(L1[2] - L1[0]);
+                if (L1[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L1[1] / dL);
+            }
+            {
+                const double dL = fabs(L2[2] - L2[0]);
+                if (L2[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L2[1] / dL);
+            }
+        }
+    }
+    const double ra = Ua[IM1] + Ua[IM2], rc = Uc[IM1] + Uc[IM2], rb = Ub[IM1] + Ub[IM2];
+    const double tiny = 1e-12 * (vsa + vsc + vsb) + 1e-300;
+    double sm = 1.0, sl[2];
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+        const int k = d == 0 ? IMU : IMV;
+        const double va = Ua[k] / ra, vc = Uc[k] / rc, vb = Ub[k] / rb, a = vc - va, b = vb - vc;
+        double s = 0.0;
+        if (!P.limiter) s = 0.5 * (a + b);
+        else if (!(fabs(a) <= tiny && fabs(b) <= tiny)) {
+            if (a * b > 0) { s = fabs(a) < fabs(b) ? a : b; sm = SMIN(sm, s / (0.5 * (a + b))); }
+            else sm = 0.0;
+        }
+        sl[d] = s;
+    }
+    phi_out = phi;
+    phis_out = SMIN(phi, sm);
+    slu = sl[0];
+    slv = sl[1];
+}
+
+// Face value of a cell on its right (+) or left (-) side from the cell's stencil and its reconstruction.
+SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, double phi, double slu, double slv,
+                          bool right, double* w) {
+    const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int k = VOL[q];
+        const double sig = phi * 0.5 * (Ub[k] - Ua[k]);
+        w[k] = right ? Uc[k] + 0.5 * sig : Uc[k] - 0.5 * sig;
+    }
+    const double rc = Uc[IM1] + Uc[IM2];
+    const double vcu = Uc[IMU] / rc, vcv = Uc[IMV] / rc;
+    const double v0 = right ? vcu + 0.5 * slu : vcu - 0.5 * slu, v1 = right ? vcv + 0.5 * slv : vcv - 0.5 * slv;
+    const double r = w[IM1] + w[IM2];
+    w[IMU] = r * v0;
+    w[IMV] = r * v1;
+    w[IEN] = w[IE1] + w[IE2] + 0.5 * r * (v0 * v0 + v1 * v1);
+}
+
+SPB6G_DEV void rusanov_flux(const double* QL, const double* QR, int d, double* flux) {
+    const int km = d == 0 ? IMU : IMV;
+    const double vL = QL[km] / (QL[IM1] + QL[IM2]), vR = QR[km] / (QR[IM1] + QR[IM2]);
+    const double a = SMAX(fabs(QL[km] / (QL[IM1] + QL[IM2])), fabs(QR[km] / (QR[IM1] + QR[IM2])));
+#pragma unroll
+    for (int k = 0; k < NV; k++) flux[k] = 0.5 * (QL[k] * vL + QR[k] * vR) - 0.5 * a * (QR[k] - QL[k]);
+}
+
+template <int TX, int TY, bool TWO_D>
+__global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
+    using T = FluxTile<TX, TY, TWO_D>;
+    constexpr int HY = T::HY, NLX = T::NLX, NLY = T::NLY, NRX = T::NRX, NRY = T::NRY, NFX = T::NFX, NFY = T::NFY;
+    extern __shared__ double smem[];
+    double* Qs_ = smem;                      // [NV][NLY][NLX]
+    double* VS = Qs_ + T::Q_SZ;              // [NLY][NLX]
+    double* ES = VS + NLX * NLY;
+    double* RX = ES + NLX * NLY;             // [3][TY][NRX]
+    double* RY = RX + T::RX_SZ;              // [3][NRY][TX]
+    double* FX = RY + T::RY_SZ;              // [9][TY][NFX]
+    double* FY = FX + T::FX_SZ;              // [9][NFY][TX]
+    const Geom& g = c.g;
+    const int tid = threadIdx.x, nth = TX * TY;
+    const int i0 = blockIdx.x * TX, j0 = TWO_D ? blockIdx.y * TY : 0;
+    auto Q = [&](int k, int ly, int lx) -> double& { return Qs_[(k * NLY + ly) * NLX + lx]; };
+    auto in_cross = [&](int lx, int ly) {
+        if (!TWO_D) return true;
+        const bool cx = lx >= 2 && lx < TX + 2, cy = ly >= HY && ly < HY + TY;
+        return cx || cy;
+    };
+    auto exists = [&](int gi, int gj) {
+        return gi >= -2 && gi <= g.nx + 1 && (TWO_D ? (gj >= -2 && gj <= g.ny + 1) : true);
+    };
+
+    // 1. Qe of the tile and its halo; per-cell scales
+    for (int t = tid; t < NLX * NLY; t += nth) {
+        const int lx = t % NLX, ly = t / NLX;
+        const int gi = i0 - 2 + lx, gj = TWO_D ? j0 - HY + ly : 0;
+        if (!in_cross(lx, ly) || !exists(gi, gj)) continue;
+        double q[NV];
+        load_qe(c, gi, gj, q);
+#pragma unroll
+        for (int k = 0; k < NV; k++) Q(k, ly, lx) = q[k];
+        double vs, es;
+        scales_of(c.phy, q, vs, es);
+        VS[ly * NLX + lx] = vs;
+        ES[ly * NLX + lx] = es;
+    }
+    __syncthreads();
+
+    // 2. reconstruction of cells -1..TX (x) and -1..TY (y)
+    for (int t = tid; t < NRX * TY; t += nth) {
+        const int rx = t % NRX, ry = t / NRX;  // cell i0 - 1 + rx, row j0 + ry
+        const int gi = i0 - 1 + rx, gj = j0 + ry;
+        if (gi > g.nx || gj >= g.ny) continue;
+        const int lx = rx + 1, ly = ry + HY;
+        double Ua[NV], Uc[NV], Ub[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, lx - 1); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly, lx + 1); }
+        double phi, phis, slu, slv;
+        recon3(c.phy, Ua, Uc, Ub, VS[ly * NLX + lx - 1], VS[ly * NLX + lx], VS[ly * NLX + lx + 1], ES[ly * NLX + lx - 1],
+               ES[ly * NLX + lx], ES[ly * NLX + lx + 1], phi, phis, slu, slv);
+        RX[(0 * TY + ry) * NRX + rx] = phi;
+        RX[(1 * TY + ry) * NRX + rx] = slu;
+        RX[(2 * TY + ry) * NRX + rx] = slv;
+        const bool own = (gi >= i0 && gi < i0 + TX) || gi == -1 || gi == g.nx;
+        if (own) c.phis_x[rxi(g, gi, gj)] = phis;
+    }
+    if (TWO_D) {
+        for (int t = tid; t < TX * NRY; t += nth) {
+            const int rx = t % TX, ry = t / TX;  // cell i0 + rx, row j0 - 1 + ry
+            const int gi = i0 + rx, gj = j0 - 1 + ry;
+            if (gi >= g.nx || gj > g.ny) continue;
+            const int lx = rx + 2, ly = ry + 1;
+            double Ua[NV], Uc[NV], Ub[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly - 1, lx); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly + 1, lx); }
+            double phi, phis, slu, slv;
+            recon3(c.phy, Ua, Uc, Ub, VS[(ly - 1) * NLX + lx], VS[ly * NLX + lx], VS[(ly + 1) * NLX + lx],
+                   ES[(ly - 1) * NLX + lx], ES[ly * NLX + lx], ES[(ly + 1) * NLX + lx], phi, phis, slu, slv);
+            RY[(0 * NRY + ry) * TX + rx] = phi;
+            RY[(1 * NRY + ry) * TX + rx] = slu;
+            RY[(2 * NRY + ry) * TX + rx] = slv;
+            const bool own = (gj >= j0 && gj < j0 + TY) || gj == -1 || gj == g.ny;
+            if (own) c.phis_y[ryi(g, gi, gj)] = phis;
+        }
+    }
+    __syncthreads();
+
+    // 3. face fluxes, face velocities ube and donors, once per face
+    const size_t nfx = (size_t)(g.nx + 1) * g.ny, nfy = (size_t)g.nx * (g.ny + 1);
+    for (int t = tid; t < NFX * TY; t += nth) {
+        const int f = t % NFX, ry = t / NFX;  // face between cells i0 - 1 + f and i0 + f
+        const int gl = i0 - 1 + f, gj = j0 + ry;
+        if (gl > g.nx - 1 || gj >= g.ny) continue;
+        const int ly = ry + HY, la = f + 1;   // local column of the left cell
+        double Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
+        // right face value of the left cell
+#pragma unroll
+        for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, la - 1); Uc[k] = Q(k, ly, la); Ub[k] = Q(k, ly, la + 1); }
+        face_value(Ua, Uc, Ub, RX[(0 * TY + ry) * NRX + f], RX[(1 * TY + ry) * NRX + f], RX[(2 * TY + ry) * NRX + f],
+                   true, wR);
+        // left face value of the right cell
+#pragma unroll
+        for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, ly, la + 2); }
+        face_value(Ua, Uc, Ub, RX[(0 * TY + ry) * NRX + f + 1], RX[(1 * TY + ry) * NRX + f + 1],
+                   RX[(2 * TY + ry) * NRX + f + 1], false, wL);
+        rusanov_flux(wR, wL, 0, fl);
+        const double ube = 0.5 * (wR[IMU] / (wR[IM1] + wR[IM2]) + wL[IMU] / (wL[IM1] + wL[IM2]));
+#pragma unroll
+        for (int k = 0; k < NV; k++) FX[(k * TY + ry) * NFX + f] = fl[k];
+        FX[(8 * TY + ry) * NFX + f] = ube;
+        if (f >= 1 || i0 == 0) {  // faces i0 .. i0+TX-1 belong to this tile, face -1/2 to the first
+            const size_t fi = fxi(g, gl, gj);
+            c.ube_x[fi] = ube;
+            const int K[4] = {IM1, IM2, IE1, IE2};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                c.fxd[q * nfx + fi] = wR[K[q]];
+                c.fxd[(4 + q) * nfx + fi] = wL[K[q]];
+            }
+        }
+    }
+    if (TWO_D) {
+        for (int t = tid; t < TX * NFY; t += nth) {
+            const int rx = t % TX, f = t / TX;  // face between rows j0 - 1 + f and j0 + f
+            const int gi = i0 + rx, gl = j0 - 1 + f;
+            if (gi >= g.nx || gl > g.ny - 1) continue;
+            const int lx = rx + 2, la = f + 1;
+            double Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) { Ua[k] = Q(k, la - 1, lx); Uc[k] = Q(k, la, lx); Ub[k] = Q(k, la + 1, lx); }
+            face_value(Ua, Uc, Ub, RY[(0 * NRY + f) * TX + rx], RY[(1 * NRY + f) * TX + rx], RY[(2 * NRY + f) * TX + rx],
+                       true, wR);
+#pragma unroll
+            for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, la + 2, lx); }
+            face_value(Ua, Uc, Ub, RY[(0 * NRY + f + 1) * TX + rx], RY[(1 * NRY + f + 1) * TX + rx],
+                       RY[(2 * NRY + f + 1) * TX + rx], false, wL);
+            rusanov_flux(wR, wL, 1, fl);
+            const double ube = 0.5 * (wR[IMV] / (wR[IM1] + wR[IM2]) + wL[IMV] / (wL[IM1] + wL[IM2]));
+#pragma unroll
+            for (int k = 0; k < NV; k++) FY[(k * NFY + f) * TX + rx] = fl[k];
+            FY[(8 * NFY + f) * TX + rx] = ube;
+            if (f >= 1 || j0 == 0) {
+                const size_t fi = fyi(g, gi, gl);
+                c.ube_y[fi] = ube;
+                const int K[4] = {IM1, IM2, IE1, IE2};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    c.fyd[q * nfy + fi] = wR[K[q]];
+                    c.fyd[(4 + q) * nfy + fi] = wL[K[q]];
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // 4. explicit update of the tile's cells (Update :300-341)
+    for (int t = tid; t < TX * TY; t += nth) {
+        const int rx = t % TX, ry = t / TX;
+        const int gi = i0 + rx, gj = j0 + ry;
+        if (gi >= g.nx || gj >= g.ny) continue;
+        const size_t x = (size_t)gi + (size_t)gj * g.nx;
+        const int lx = rx + 2, ly = ry + HY;
+        if (!(Q(IM1, ly, lx) + Q(IM2, ly, lx) > 0)) atomicOr(&c.ns->err, 1);
+        double X[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = c.Un.v[k][x];
+            for (int r = 0; r < c.nH; r++) s = s + c.ci[r] * c.Hprev[((size_t)r * NV + k) * c.n + x];
+            X[k] = s - c.adt / g.dx * (FX[(k * TY + ry) * NFX + rx + 1] - FX[(k * TY + ry) * NFX + rx]);
+        }
+        const double qa1 = Q(IA1, ly, lx);
+        X[IA1] += c.adt / g.dx * qa1 * (FX[(8 * TY + ry) * NFX + rx + 1] - FX[(8 * TY + ry) * NFX + rx]);
+        if (TWO_D) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) X[k] -= c.adt / g.dy * (FY[(k * NFY + ry + 1) * TX + rx] - FY[(k * NFY + ry) * TX + rx]);
+            X[IA1] += c.adt / g.dy * qa1 * (FY[(8 * NFY + ry + 1) * TX + rx] - FY[(8 * NFY + ry) * TX + rx]);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) c.Xs.v[k][x] = X[k];
+        c.a2s[x] = 1.0 - X[IA1];
+    }
+}
+
+template <int TX, int TY, bool TWO_D>
+void launch_tile(const Ctx& c, cudaStream_t st) {
+    using T = FluxTile<TX, TY, TWO_D>;
+    static unsigned long long configured = 0;  // one bit per device: the attribute is per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(configured & (1ull << dev))) {
+        cudaFuncSetAttribute(k_flux<TX, TY, TWO_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
+        configured |= 1ull << dev;
+    }
+    const dim3 grid((unsigned)((c.g.nx + TX - 1) / TX), TWO_D ? (unsigned)((c.g.ny + TY - 1) / TY) : 1u);
+    k_flux<TX, TY, TWO_D><<<grid, TX * TY, T::BYTES, st>>>(c);
+}
+
+}  // namespace
+
+void launch_flux(const Ctx& c, cudaStream_t st) {
+    if (c.g.ny > 1) launch_tile<32, 8, true>(c, st);
+    else launch_tile<256, 1, false>(c, st);
+    if (c.nlaunch) *c.nlaunch += 1;
+}
+
+}  // namespace spb6g

@@ -25,235 +25,6 @@ int red_blocks(int n, int threads) {
     return (int)b;
 }
 
-// ============================================================ stage combination (main :1341-1351)
-__global__ void k_combine(int n, CState U, const double* __restrict__ Hs, int nH, double c0e, double c1e, double c0i,
-                          double c1i, State Qe, State Qs) {
-    const double ce[2] = {c0e, c1e}, ci[2] = {c0i, c1i};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-            double e = U.v[k][x], s = e;
-            for (int r = 0; r < nH; r++) {
-                const double h = Hs[((size_t)r * NV + k) * n + x];
-                e = e + ce[r] * h;
-                s = s + ci[r] * h;
-            }
-            Qe.v[k][x] = e;
-            Qs.v[k][x] = s;
-        }
-    }
-}
-
-void launch_combine(const Ctx& c, cudaStream_t st, const double* const* U, const double* Hs, int nH, const double* ae,
-                    const double* ai, double dt, double* const* Qe, double* const* Qs) {
-    CState u;
-    State qe, qs;
-    for (int k = 0; k < NV; k++) { u.v[k] = U[k]; qe.v[k] = Qe[k]; qs.v[k] = Qs[k]; }
-    // coefficients Ae[s][r] * dt and Ai[s][r] * dt, as the reference forms them (Ae * dt * H)
-    const double c0e = nH > 0 ? ae[0] * dt : 0, c1e = nH > 1 ? ae[1] * dt : 0;
-    const double c0i = nH > 0 ? ai[0] * dt : 0, c1i = nH > 1 ? ai[1] * dt : 0;
-    k_combine<<<blocks_for(c.n), TPB, 0, st>>>(c.n, u, Hs, nH, c0e, c1e, c0i, c1i, qe, qs);
-    count(c, 1);
-}
-
-// ============================================================ reconstruction (TVDReconstruction :369-471)
-SPB6G_DEV void cell_scales(const Phys& P, const double* q, double& vsc, double& esc) {
-    Prim w;
-    const double rho = q[IM1] + q[IM2], mm = hypot(q[IMU], q[IMV]);
-    vsc = (rho > 0 ? mm / rho : 0.0) + (prim_of(P, q, w) ? w.cf : 0.0);
-    esc = fabs(q[IE1]) + fabs(q[IE2]) + (rho > 0 ? 0.5 * mm * mm / rho : 0.0);
-}
-
-// Shared limiter phi of the volume-transported quantities with the face
-// admissibility cap (:399-432), and the velocity minmod slopes (:450-463).
-SPB6G_DEV void recon_dir(const Phys& P, const double* Ua, const double* Uc, const double* Ub, double vsa, double vsc,
-                         double vsb, double esa, double esc, double esb, double& phi_out, double& phis_out, double& slu,
-                         double& slv) {
-    const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
-    double phi = 1.0;
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-        const int k = VOL[q];
-        const double xa = Ua[k], xc = Uc[k], xb = Ub[k];
-        double sc;
-        if (k == IA1) sc = 3.0;
-        else if (k == IM1 || k == IM2) sc = fabs(xa) + fabs(xc) + fabs(xb);
-        else sc = esa + esc + esb;
-        const double a = xc - xa, b = xb - xc, tiny = 1e-12 * sc + 1e-300;
-        if (!P.limiter) break;
-        if (fabs(a) <= tiny && fabs(b) <= tiny) continue;
-        if (a * b <= 0) { phi = 0.0; break; }
-        const double c = 0.5 * (a + b), m = fabs(a) < fabs(b) ? a : b;
-        phi = SMIN(phi, m / c);
-    }
-    if (P.limiter && phi > 0.0) {
-        const double* cs[3] = {Ua, Uc, Ub};
-#pragma unroll
-        for (int ph = 0; ph < 2; ph++) {
-            double L1[3], L2[3];
-#pragma unroll
-            for (int n = 0; n < 3; n++) {
-                const double a = ph == 0 ? cs[n][IA1] : 1.0 - cs[n][IA1], m = cs[n][ph == 0 ? IM1 : IM2],
-                             e = cs[n][ph == 0 ? IE1 : IE2];
-                L1[n] = a - m * P.ph[ph].b;
-                L2[n] = e - m * P.ph[ph].q - L1[n] * P.ph[ph].pi;
-            }
-            {
-                const double dL = fabs(L1[2] - L1[0]);
-                if (L1[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L1[1] / dL);
-            }
-            {
-                const double dL = fabs(L2[2] - L2[0]);
-                if (L2[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L2[1] / dL);
-            }
-        }
-    }
-    const double ra = Ua[IM1] + Ua[IM2], rc = Uc[IM1] + Uc[IM2], rb = Ub[IM1] + Ub[IM2];
-    const double tiny = 1e-12 * (vsa + vsc + vsb) + 1e-300;
-    double sm = 1.0, sl[2];
-#pragma unroll
-    for (int d = 0; d < 2; d++) {
-        const int k = d == 0 ? IMU : IMV;
-        const double va = Ua[k] / ra, vc = Uc[k] / rc, vb = Ub[k] / rb, a = vc - va, b = vb - vc;
-        double s = 0.0;
-        if (!P.limiter) s = 0.5 * (a + b);
-        else if (!(fabs(a) <= tiny && fabs(b) <= tiny)) {
-            if (a * b > 0) { s = fabs(a) < fabs(b) ? a : b; sm = SMIN(sm, s / (0.5 * (a + b))); }
-            else sm = 0.0;
-        }
-        sl[d] = s;
-    }
-    phi_out = phi;
-    phis_out = SMIN(phi, sm);
-    slu = sl[0];
-    slv = sl[1];
-}
-
-// Cells i in [-1, nx], j in [-1, ny]: x-reconstruction on interior rows, y on interior columns.
-__global__ void k_recon(Ctx c) {
-    const Geom& g = c.g;
-    const int W = g.nx + 2, Hh = g.ny > 1 ? g.ny + 2 : 1;
-    const long tot = (long)W * Hh;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % W) - 1, j = g.ny > 1 ? (int)(t / W) - 1 : 0;
-        double qc[NV], qa[NV], qb[NV], vs_c, es_c, vs_a, es_a, vs_b, es_b;
-        load_state(c.phy, g, c.Qe, i, j, qc);
-        cell_scales(c.phy, qc, vs_c, es_c);
-        if (j >= 0 && j < g.ny) {
-            load_state(c.phy, g, c.Qe, i - 1, j, qa);
-            load_state(c.phy, g, c.Qe, i + 1, j, qb);
-            cell_scales(c.phy, qa, vs_a, es_a);
-            cell_scales(c.phy, qb, vs_b, es_b);
-            double phi, phis, slu, slv;
-            recon_dir(c.phy, qa, qc, qb, vs_a, vs_c, vs_b, es_a, es_c, es_b, phi, phis, slu, slv);
-            const size_t x = rxi(g, i, j);
-            c.phiv_x[x] = phi; c.phis_x[x] = phis; c.slu_x[x] = slu; c.slv_x[x] = slv;
-        }
-        if (g.ny > 1 && i >= 0 && i < g.nx) {
-            load_state(c.phy, g, c.Qe, i, j - 1, qa);
-            load_state(c.phy, g, c.Qe, i, j + 1, qb);
-            cell_scales(c.phy, qa, vs_a, es_a);
-            cell_scales(c.phy, qb, vs_b, es_b);
-            double phi, phis, slu, slv;
-            recon_dir(c.phy, qa, qc, qb, vs_a, vs_c, vs_b, es_a, es_c, es_b, phi, phis, slu, slv);
-            const size_t x = ryi(g, i, j);
-            c.phiv_y[x] = phi; c.phis_y[x] = phis; c.slu_y[x] = slu; c.slv_y[x] = slv;
-        }
-    }
-}
-void launch_recon(const Ctx& c, cudaStream_t st) {
-    const long tot = (long)(c.g.nx + 2) * (c.g.ny > 1 ? c.g.ny + 2 : 1);
-    k_recon<<<blocks_for(tot), TPB, 0, st>>>(c);
-    count(c, 1);
-}
-
-// Face state of cell (ci, cj) on its left (right = false) or right side in direction dir (:433-467).
-SPB6G_DEV void face_state(const Ctx& c, int ci, int cj, int dir, bool right, double* w) {
-    double qa[NV], qc[NV], qb[NV];
-    const int di = dir == 0, dj = dir == 1;
-    load_state(c.phy, c.g, c.Qe, ci - di, cj - dj, qa);
-    load_state(c.phy, c.g, c.Qe, ci, cj, qc);
-    load_state(c.phy, c.g, c.Qe, ci + di, cj + dj, qb);
-    double phi, slu, slv;
-    if (dir == 0) {
-        const size_t x = rxi(c.g, ci, cj);
-        phi = c.phiv_x[x]; slu = c.slu_x[x]; slv = c.slv_x[x];
-    } else {
-        const size_t x = ryi(c.g, ci, cj);
-        phi = c.phiv_y[x]; slu = c.slu_y[x]; slv = c.slv_y[x];
-    }
-    const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
-#pragma unroll
-    for (int q = 0; q < 5; q++) {
-        const int k = VOL[q];
-        const double sig = phi * 0.5 * (qb[k] - qa[k]);
-        w[k] = right ? qc[k] + 0.5 * sig : qc[k] - 0.5 * sig;
-    }
-    const double rc = qc[IM1] + qc[IM2];
-    const double vcu = qc[IMU] / rc, vcv = qc[IMV] / rc;
-    const double v0 = right ? vcu + 0.5 * slu : vcu - 0.5 * slu, v1 = right ? vcv + 0.5 * slv : vcv - 0.5 * slv;
-    const double r = w[IM1] + w[IM2];
-    w[IMU] = r * v0;
-    w[IMV] = r * v1;
-    w[IEN] = w[IE1] + w[IE2] + 0.5 * r * (v0 * v0 + v1 * v1);
-}
-// Rusanov flux at the material speed (RusanovC_x/y :237-259), local speed per face.
-SPB6G_DEV void rusanov(const double* QL, const double* QR, int d, double* flux) {
-    const int km = d == 0 ? IMU : IMV;
-    const double vL = QL[km] / (QL[IM1] + QL[IM2]), vR = QR[km] / (QR[IM1] + QR[IM2]);
-    const double a = SMAX(fabs(QL[km] / (QL[IM1] + QL[IM2])), fabs(QR[km] / (QR[IM1] + QR[IM2])));
-#pragma unroll
-    for (int k = 0; k < NV; k++) flux[k] = 0.5 * (QL[k] * vL + QR[k] * vR) - 0.5 * a * (QR[k] - QL[k]);
-}
-
-// Explicit update X* = Qs - tau div F(Qe) with the path-conservative alpha term (Update :264-346).
-__global__ void k_update(Ctx c) {
-    const Geom& g = c.g;
-    const int nx = g.nx, ny = g.ny;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % nx, j = x / nx;
-        const double rho = c.Qe.v[IM1][x] + c.Qe.v[IM2][x];
-        if (!(rho > 0)) atomicOr(&c.ns->err, 1);
-        double wRm[NV], wLc[NV], wRc[NV], wLp[NV], fp[NV], fm[NV], X[NV];
-        face_state(c, i - 1, j, 0, true, wRm);
-        face_state(c, i, j, 0, false, wLc);
-        face_state(c, i, j, 0, true, wRc);
-        face_state(c, i + 1, j, 0, false, wLp);
-        const double ubr = 0.5 * (wRc[IMU] / (wRc[IM1] + wRc[IM2]) + wLp[IMU] / (wLp[IM1] + wLp[IM2]));
-        const double ubl = 0.5 * (wRm[IMU] / (wRm[IM1] + wRm[IM2]) + wLc[IMU] / (wLc[IM1] + wLc[IM2]));
-        c.ube_x[fxi(g, i, j)] = ubr;
-        if (i == 0) c.ube_x[fxi(g, -1, j)] = ubl;
-        rusanov(wRc, wLp, 0, fp);
-        rusanov(wRm, wLc, 0, fm);
-        const double qe_a1 = c.Qe.v[IA1][x];
-#pragma unroll
-        for (int k = 0; k < NV; k++) X[k] = c.Qs.v[k][x] - c.adt / g.dx * (fp[k] - fm[k]);
-        X[IA1] += c.adt / g.dx * qe_a1 * (ubr - ubl);
-        if (ny > 1) {
-            face_state(c, i, j - 1, 1, true, wRm);
-            face_state(c, i, j, 1, false, wLc);
-            face_state(c, i, j, 1, true, wRc);
-            face_state(c, i, j + 1, 1, false, wLp);
-            const double vbr = 0.5 * (wRc[IMV] / (wRc[IM1] + wRc[IM2]) + wLp[IMV] / (wLp[IM1] + wLp[IM2]));
-            const double vbl = 0.5 * (wRm[IMV] / (wRm[IM1] + wRm[IM2]) + wLc[IMV] / (wLc[IM1] + wLc[IM2]));
-            c.ube_y[fyi(g, i, j)] = vbr;
-            if (j == 0) c.ube_y[fyi(g, i, -1)] = vbl;
-            rusanov(wRc, wLp, 1, fp);
-            rusanov(wRm, wLc, 1, fm);
-#pragma unroll
-            for (int k = 0; k < NV; k++) X[k] -= c.adt / g.dy * (fp[k] - fm[k]);
-            X[IA1] += c.adt / g.dy * qe_a1 * (vbr - vbl);
-        }
-#pragma unroll
-        for (int k = 0; k < NV; k++) c.Xs.v[k][x] = X[k];
-        c.a2s[x] = 1.0 - X[IA1];
-    }
-}
-void launch_update(const Ctx& c, cudaStream_t st) {
-    k_update<<<blocks_for(c.n), TPB, 0, st>>>(c);
-    count(c, 1);
-}
-
 // ============================================================ stage data (PressureSubsystem prep :922-1039)
 SPB6G_DEV void xs_at(const Ctx& c, int i, int j, double* q) {
     CState X;
@@ -361,17 +132,10 @@ SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, dou
     kp += phi * psiP / (ZL + ZR);
     pv = phi * psiU * ZL * ZR / (ZL + ZR) * D;
 }
-SPB6G_DEV void donor(const Ctx& c, int ci, int cj, int dir, bool right, double* d);
-// Donors and tangential velocities of one face (fixed for the stage).
+// Tangential velocities of the two cells of a face (fixed for the stage; the donors
+// of planes 0-7 are written by the explicit kernel).
 SPB6G_DEV void face_fixed(const Ctx& c, int i, int j, int ydir, double* plane, size_t f, size_t stride) {
-    double dl[4], dr[4], u, v;
-    donor(c, i, j, ydir, true, dl);
-    donor(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), ydir, false, dr);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        plane[q * stride + f] = dl[q];
-        plane[(4 + q) * stride + f] = dr[q];
-    }
+    double u, v;
     vel_at(c, i, j, u, v);
     plane[8 * stride + f] = ydir ? u : v;
     vel_at(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), u, v);
@@ -481,22 +245,6 @@ void launch_shock(const Ctx& c, cudaStream_t st) {
 struct FaceV {
     double uf, pf, wL, wR, utL, utR, cL[4], cR[4];  // donors: m1, m2, e1, e2
 };
-// Donor m1, m2, e1, e2 of the reconstructed face value of cell (ci, cj): right (+) or left (-) face.
-SPB6G_DEV void donor(const Ctx& c, int ci, int cj, int dir, bool right, double* d) {
-    double qa[NV], qc[NV], qb[NV];
-    const int di = dir == 0, dj = dir == 1;
-    load_state(c.phy, c.g, c.Qe, ci - di, cj - dj, qa);
-    load_state(c.phy, c.g, c.Qe, ci, cj, qc);
-    load_state(c.phy, c.g, c.Qe, ci + di, cj + dj, qb);
-    const double phi = dir == 0 ? c.phiv_x[rxi(c.g, ci, cj)] : c.phiv_y[ryi(c.g, ci, cj)];
-    const int K[4] = {IM1, IM2, IE1, IE2};
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int k = K[q];
-        const double sig = phi * 0.5 * (qb[k] - qa[k]);
-        d[q] = right ? qc[k] + 0.5 * sig : qc[k] - 0.5 * sig;
-    }
-}
 SPB6G_DEV void face_weights(FaceV& f, double ube) {
     f.wL = SMAX(f.uf, 0.0) - SMAX(ube, 0.0);
     f.wR = SMIN(f.uf, 0.0) - SMIN(ube, 0.0);
@@ -671,41 +419,53 @@ void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
     count(c, 1);
 }
 
-// FD Jacobian rows (:837-853) with the BiCGStab set-up sums E = 1^T A 1, 1^T b, b^T b.
-constexpr int JAC_THREADS = 128;
-__global__ void __launch_bounds__(JAC_THREADS, 3) k_jacobian(Ctx c) {
+// FD Jacobian (:837-853).  One thread per matrix entry: entry 0 perturbs the own
+// cell by h = 1e-7 s_r, entries 1-4 the W, E, S, N neighbour by 1e-7 s_col; each is
+// one residual evaluation, so the 5 closures of a row run in 5 independent threads.
+__global__ void __launch_bounds__(RED_THREADS, 2) k_jac_entries(Ctx c) {
     const Geom& g = c.g;
-    double acc[3] = {0.0, 0.0, 0.0};
     const bool twoD = g.ny > 1;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+    const long nw = twoD ? 5 : 3, tot = nw * c.n;
+    double* planes[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
+    const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+        const int w = (int)(t / c.n), x = (int)(t - (long)w * c.n);
         const int i = x % g.nx, j = x / g.nx;
         const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
         const double G0 = c.G[x];
-        bool ok = true;
-        double g1;
-        const double h = 1e-7 * c.sc[x];
-        ok = ok && residual_at(c, i, j, p, h, -1, 0, g1, nullptr);
-        const double aC = (g1 - G0) / h;
-        double av[4] = {0, 0, 0, 0};
-        const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
-        for (int w = 0; w < (twoD ? 4 : 2); w++) {
-            const int col = mp_index(g, i + nb[w][0], j + nb[w][1]);
+        double gv, a;
+        bool ok;
+        if (w == 0) {
+            const double h = 1e-7 * c.sc[x];
+            ok = residual_at(c, i, j, p, h, -1, 0, gv, nullptr);
+            a = (gv - G0) / h;
+        } else {
+            const int col = mp_index(g, i + nb[w - 1][0], j + nb[w - 1][1]);
             const double hn = 1e-7 * c.sc[col];
-            double g2;
-            ok = ok && residual_at(c, i, j, p, 0, w, hn, g2, nullptr);
-            av[w] = (g2 - G0) / hn;
+            ok = residual_at(c, i, j, p, 0, w - 1, hn, gv, nullptr);
+            a = (gv - G0) / hn;
         }
         if (!ok) atomicOr(&c.ns->fail, 2);
-        c.aC[x] = aC; c.aW[x] = av[0]; c.aE[x] = av[1]; c.aS[x] = av[2]; c.aN[x] = av[3];
+        planes[w][x] = a;
+    }
+}
+// Row sums A 1 (summed in the row's entry order, as block_sum's terms :763), Jacobi
+// inverse, and the set-up sums E = 1^T A 1, 1^T b, b^T b with b = -G.
+__global__ void __launch_bounds__(RED_THREADS) k_jac_finish(Ctx c) {
+    const bool twoD = c.g.ny > 1;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < c.n) {
+        const double aC = c.aC[x];
         double e = 0;
-        e += aC; e += av[0]; e += av[1];
-        if (twoD) { e += av[2]; e += av[3]; }
+        e += aC; e += c.aW[x]; e += c.aE[x];
+        if (twoD) { e += c.aS[x]; e += c.aN[x]; }
         c.A1[x] = e;
         c.dinv[x] = aC != 0 ? 1.0 / aC : 1.0;
-        const double b = -G0;
-        acc[0] += e;
-        acc[1] += b;
-        acc[2] += b * b;
+        const double b = -c.G[x];
+        acc[0] = e;
+        acc[1] = b;
+        acc[2] = b * b;
     }
     double tot[3];
     if (grid_fold<RedSum, 3>(acc, c.partials, &c.counters[1], tot) && threadIdx.x == 0) {
@@ -713,46 +473,64 @@ __global__ void __launch_bounds__(JAC_THREADS, 3) k_jacobian(Ctx c) {
     }
 }
 void launch_jacobian(const Ctx& c, cudaStream_t st) {
-    k_jacobian<<<red_blocks(c.n, JAC_THREADS), JAC_THREADS, 0, st>>>(c);
-    count(c, 1);
+    const long tot = (long)(c.g.ny > 1 ? 5 : 3) * c.n;
+    k_jac_entries<<<(int)((tot + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c);
+    k_jac_finish<<<(c.n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, st>>>(c);
+    count(c, 2);
 }
 
 // ============================================================ BiCGStab (GMRES_Solver :752-794)
 // Jacobi + Nicolaides preconditioner M^-1 r = D^-1 r + 1 (1^T r)/E.  The coarse
 // term is carried through the matrix as A M^-1 r = A (D^-1 r) + (1^T r / E) A 1,
 // so each iteration is four passes: p & q = A D^-1 p; v, s & u = A D^-1 s; t; x & r.
+// Every pass runs one row per thread on a (nx/256, ny) grid.
+struct Nbr {
+    int w, e, s, n;
+};
+SPB6G_DEV Nbr neighbours(const Geom& g, int i, int j, int x) {
+    Nbr r;
+    if (i > 0 && i < g.nx - 1) { r.w = x - 1; r.e = x + 1; }
+    else { r.w = mp_index(g, i - 1, j); r.e = mp_index(g, i + 1, j); }
+    if (j > 0 && j < g.ny - 1) { r.s = x - g.nx; r.n = x + g.nx; }
+    else { r.s = mp_index(g, i, j - 1); r.n = mp_index(g, i, j + 1); }
+    return r;
+}
+// Row of the SpMV in the reference's entry order: self, W, E, S, N (Pressure_Subsystem_AX :737-741).
 template <class F>
-SPB6G_DEV double spmv_row(const Ctx& c, int i, int j, int x, F val) {
-    const Geom& g = c.g;
+SPB6G_DEV double spmv_row(const Ctx& c, const Nbr& nb, int x, F val) {
     double s = 0;
     s += c.aC[x] * val(x);
-    s += c.aW[x] * val(mp_index(g, i - 1, j));
-    s += c.aE[x] * val(mp_index(g, i + 1, j));
-    if (g.ny > 1) {
-        s += c.aS[x] * val(mp_index(g, i, j - 1));
-        s += c.aN[x] * val(mp_index(g, i, j + 1));
+    s += c.aW[x] * val(nb.w);
+    s += c.aE[x] * val(nb.e);
+    if (c.g.ny > 1) {
+        s += c.aS[x] * val(nb.s);
+        s += c.aN[x] * val(nb.n);
     }
     return s;
 }
+#define ROW_INDEX                                                   \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y; \
+    const bool live = i < c.g.nx;                                   \
+    const int x = live ? i + j * c.g.nx : 0;
 
 __global__ void __launch_bounds__(RED_THREADS) k_bicg_init(Ctx c, double tol, int maxit) {
-    const Geom& g = c.g;
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
     const double cb = ns.sumb * Einv;
     double acc[2] = {0.0, 0.0};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % g.nx, j = x / g.nx;
+    ROW_INDEX
+    if (live) {
+        const Nbr nb = neighbours(c.g, i, j, x);
         auto xv = [&](int q) { return c.dinv[q] * (-c.G[q]) + cb; };
-        const double Ax = spmv_row(c, i, j, x, xv);
+        const double Ax = spmv_row(c, nb, x, xv);
         const double r = -c.G[x] - Ax;
         c.dP[x] = xv(x);
         c.br[x] = r;
         c.br0[x] = r;
         c.bp[x] = 0.0;
         c.bv[x] = 0.0;
-        acc[0] += r * r;
-        acc[1] += r * c.A1[x];
+        acc[0] = r * r;
+        acc[1] = r * c.A1[x];
     }
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[2], tot) && threadIdx.x == 0) {
@@ -767,25 +545,26 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_init(Ctx c, double tol, in
         b.tol = tol;
         b.maxit = maxit;
         b.iters = 0;
-        b.status = sqrt(b.rr) <= tol * b.bn ? BICG_CONV : (b.r0r == 0 ? BICG_FAIL : BICG_RUNNING);
+        // a failed Jacobian (closure failure) ends the solve before it starts
+        b.status = ns.fail ? BICG_FAIL : (sqrt(b.rr) <= tol * b.bn ? BICG_CONV : (b.r0r == 0 ? BICG_FAIL : BICG_RUNNING));
     }
 }
 // pass 1: p = r + beta (p - omega v); q = A D^-1 p; sums 1^T p, r0^T q
 __global__ void __launch_bounds__(RED_THREADS) k_bicg_p(Ctx c, const double* __restrict__ p_old, double* __restrict__ p_new) {
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
-    const Geom& g = c.g;
     const double beta = (b.r0r / b.rho) * (b.alpha / b.omega), om = b.omega;
     double acc[2] = {0.0, 0.0};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % g.nx, j = x / g.nx;
+    ROW_INDEX
+    if (live) {
+        const Nbr nb = neighbours(c.g, i, j, x);
         auto pn = [&](int q) { return c.br[q] + beta * (p_old[q] - om * c.bv[q]); };
         const double p = pn(x);
-        const double q = spmv_row(c, i, j, x, [&](int k) { return c.dinv[k] * pn(k); });
+        const double q = spmv_row(c, nb, x, [&](int k) { return c.dinv[k] * pn(k); });
         p_new[x] = p;
         c.bq[x] = q;
-        acc[0] += p;
-        acc[1] += c.br0[x] * q;
+        acc[0] = p;
+        acc[1] = c.br0[x] * q;
     }
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[3], tot) && threadIdx.x == 0) {
@@ -799,20 +578,20 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_p(Ctx c, const double* __r
 __global__ void __launch_bounds__(RED_THREADS) k_bicg_s(Ctx c) {
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
-    const Geom& g = c.g;
     const double al = b.alpha, cc = b.cc;
     double acc[2] = {0.0, 0.0};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % g.nx, j = x / g.nx;
+    ROW_INDEX
+    if (live) {
+        const Nbr nb = neighbours(c.g, i, j, x);
         auto sv = [&](int q) { return c.br[q] - al * (c.bq[q] + cc * c.A1[q]); };
         const double v = c.bq[x] + cc * c.A1[x];
         const double s = c.br[x] - al * v;
-        const double u = spmv_row(c, i, j, x, [&](int k) { return c.dinv[k] * sv(k); });
+        const double u = spmv_row(c, nb, x, [&](int k) { return c.dinv[k] * sv(k); });
         c.bv[x] = v;
         c.bs[x] = s;
         c.bu[x] = u;
-        acc[0] += s * s;
-        acc[1] += s;
+        acc[0] = s * s;
+        acc[1] = s;
     }
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[4], tot) && threadIdx.x == 0) {
@@ -827,11 +606,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_t(Ctx c) {
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
     double acc[2] = {0.0, 0.0};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+    ROW_INDEX
+    if (live) {
         const double t = c.bu[x] + b.cs * c.A1[x];
         c.bt[x] = t;
-        acc[0] += t * c.bs[x];
-        acc[1] += t * t;
+        acc[0] = t * c.bs[x];
+        acc[1] = t * t;
     }
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[5], tot) && threadIdx.x == 0) {
@@ -847,7 +627,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
     if (b.status != BICG_RUNNING && b.status != BICG_CONV_HALF) return;
     const bool half = b.status == BICG_CONV_HALF;
     double acc[2] = {0.0, 0.0};
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+    ROW_INDEX
+    if (live) {
         const double ph = c.dinv[x] * p[x] + b.cc;
         if (half) {
             c.dP[x] += b.alpha * ph;
@@ -856,8 +637,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
             c.dP[x] += b.alpha * ph + b.omega * sh;
             const double r = c.bs[x] - b.omega * c.bt[x];
             c.br[x] = r;
-            acc[0] += r * r;
-            acc[1] += c.br0[x] * r;
+            acc[0] = r * r;
+            acc[1] = c.br0[x] * r;
         }
     }
     double tot[2];
@@ -870,23 +651,25 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
         if (sqrt(B.rr) <= B.tol * B.bn) B.status = BICG_CONV;
         else if (B.iters >= B.maxit) B.status = sqrt(B.rr) <= 1e3 * B.tol * B.bn ? BICG_CONV : BICG_FAIL;
         else if (B.r0r == 0) B.status = BICG_FAIL;
+        else if (!isfinite(B.rr)) B.status = BICG_FAIL;  // NaN never converges; the reference loops to GMRESiter and fails
     }
 }
+static dim3 row_grid(const Ctx& c) { return dim3((unsigned)((c.g.nx + RED_THREADS - 1) / RED_THREADS), (unsigned)c.g.ny); }
 void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit) {
-    k_bicg_init<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, tol, maxit);
+    k_bicg_init<<<row_grid(c), RED_THREADS, 0, st>>>(c, tol, maxit);
     count(c, 1);
 }
 // `count` iterations.  p is double-buffered (pass 1 reads neighbours' old p
 // while writing the new one); `parity` selects the buffer holding the current p.
 void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count_, int& parity) {
-    const int nb = red_blocks(c.n);
+    const dim3 gr = row_grid(c);
     for (int k = 0; k < count_; k++) {
         double* p0 = parity ? c.tcp : c.bp;  // tcp is the Thomas scratch, free on the BiCGStab path
         double* p1 = parity ? c.bp : c.tcp;
-        k_bicg_p<<<nb, RED_THREADS, 0, st>>>(c, p0, p1);
-        k_bicg_s<<<nb, RED_THREADS, 0, st>>>(c);
-        k_bicg_t<<<nb, RED_THREADS, 0, st>>>(c);
-        k_bicg_x<<<nb, RED_THREADS, 0, st>>>(c, p1);
+        k_bicg_p<<<gr, RED_THREADS, 0, st>>>(c, p0, p1);
+        k_bicg_s<<<gr, RED_THREADS, 0, st>>>(c);
+        k_bicg_t<<<gr, RED_THREADS, 0, st>>>(c);
+        k_bicg_x<<<gr, RED_THREADS, 0, st>>>(c, p1);
         parity ^= 1;
     }
     count(c, 4 * count_);
@@ -975,8 +758,10 @@ __global__ void k_final(Ctx c) {
         U[IE1] = o.o.e[0]; U[IE2] = o.o.e[1]; U[IEN] = o.E;
 #pragma unroll
         for (int k = 0; k < NV; k++) {
+            double qs = c.Un.v[k][x];  // Qs of this stage, formed as the explicit kernel forms it
+            for (int r = 0; r < c.nH; r++) qs = qs + c.ci[r] * c.Hprev[((size_t)r * NV + k) * c.n + x];
             c.Ust.v[k][x] = U[k];
-            c.H[(size_t)k * c.n + x] = (U[k] - c.Qs.v[k][x]) / c.adt;
+            c.H[(size_t)k * c.n + x] = (U[k] - qs) / c.adt;
         }
     }
 }

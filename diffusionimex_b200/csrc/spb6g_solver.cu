@@ -36,7 +36,7 @@ struct spb6g_solver {
     cudaStream_t st = nullptr;
     std::vector<void*> allocs;
     // state
-    double *U[NV], *Ust[NV], *Qe[NV], *Qs[NV], *Xs[NV];
+    double *U[NV], *Ust[NV], *Xs[NV];
     double* Hs = nullptr;  // 3 stages x 8 x n
     double* Pbuf[3] = {nullptr, nullptr, nullptr};
     double* Pmain = nullptr;  // accepted pressure unknown; the other two buffers hold the Newton iterate and trial
@@ -273,12 +273,12 @@ int newton(spb6g_solver* s, double& resfinal) {
 int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double dt) {
     Ctx& c = s->c;
     tbegin(s, TG_EXPLICIT);
-    if (rks == 0) {
-        for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->U[k]; c.Qs.v[k] = s->U[k]; }
-    } else {
-        const double ae[2] = {Ae[rks][0], Ae[rks][1]}, ai[2] = {Ai[rks][0], Ai[rks][1]};
-        launch_combine(c, s->st, s->U, s->Hs, rks, ae, ai, dt, s->Qe, s->Qs);
-        for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->Qe[k]; c.Qs.v[k] = s->Qs[k]; }
+    for (int k = 0; k < NV; k++) c.Un.v[k] = s->U[k];
+    c.Hprev = s->Hs;
+    c.nH = rks;
+    for (int r = 0; r < 2; r++) {  // Ae[s][r] * dt and Ai[s][r] * dt, as main forms them (:1346-1347)
+        c.ce[r] = r < rks ? Ae[rks][r] * dt : 0.0;
+        c.ci[r] = r < rks ? Ai[rks][r] * dt : 0.0;
     }
     c.adt = Ai[rks][rks] * dt;
     c.tau = c.adt;
@@ -286,8 +286,7 @@ int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double
     c.ry = c.tau / s->g.dy;
     c.H = s->Hs + (size_t)rks * NV * s->n;
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
-    launch_recon(c, s->st);
-    launch_update(c, s->st);
+    launch_flux(c, s->st);
     tend_(s, TG_EXPLICIT);
     tbegin(s, TG_PREP);
     launch_prep(c, s->st);
@@ -415,7 +414,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { delete s; return SPB6G_CUDA_ERROR; }
     bool ok = true;
     auto A = [&](size_t cnt) { double* p = dalloc(s, cnt); if (!p) ok = false; return p; };
-    for (int k = 0; k < NV; k++) { s->U[k] = A(n); s->Ust[k] = A(n); s->Qe[k] = A(n); s->Qs[k] = A(n); s->Xs[k] = A(n); }
+    for (int k = 0; k < NV; k++) { s->U[k] = A(n); s->Ust[k] = A(n); s->Xs[k] = A(n); }
     s->Hs = A(3 * NV * n);
     for (int b = 0; b < 3; b++) s->Pbuf[b] = A(n);
     s->Pmain = s->Pbuf[0];
@@ -429,8 +428,8 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.a2s = A(n);
     c.ube_x = A((size_t)(nx + 1) * ny); c.ube_y = A((size_t)nx * (ny + 1));
     const size_t nrx = (size_t)(nx + 2) * ny, nry = (size_t)nx * (ny + 2);
-    c.phiv_x = A(nrx); c.phis_x = A(nrx); c.slu_x = A(nrx); c.slv_x = A(nrx);
-    c.phiv_y = A(nry); c.phis_y = A(nry); c.slu_y = A(nry); c.slv_y = A(nry);
+    c.phis_x = A(nrx);
+    c.phis_y = A(nry);
     c.ust = A(n); c.vst = A(n); c.kw = A(n); c.qph0 = A(n); c.qph1 = A(n);
     const size_t nfx = (size_t)(nx + 1) * ny, nfy = (size_t)nx * (ny + 1);
     c.fx_ubs = A(nfx); c.fx_kp = A(nfx); c.fx_wl = A(nfx); c.fx_pv = A(nfx);
@@ -442,7 +441,8 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.br = A(n); c.br0 = A(n); c.bp = A(n); c.bv = A(n); c.bq = A(n); c.bs = A(n); c.bu = A(n); c.bt = A(n);
     c.tcp = A(n); c.tdp = A(n);
     for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];
-    c.partials = A((size_t)red_blocks((int)n, 32) * MAXQ);  // enough for any launch width >= 32
+    // one partial record per block of the widest reduction launch (one row of 256 per block, or one 256-thread block per 256 cells)
+    c.partials = A(((size_t)n / 32 + (size_t)ny * 2 + 4096) * MAXQ);
     c.counters = (unsigned*)A(16);
     c.ns = (NewtonScalars*)A(sizeof(NewtonScalars) / sizeof(double) + 1);
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
@@ -575,12 +575,14 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
     // explicit predictor, then the outputs, then the implicit part
     Ctx& c = s->c;
-    for (int k = 0; k < NV; k++) { c.Qe.v[k] = s->U[k]; c.Qs.v[k] = s->U[k]; }
+    for (int k = 0; k < NV; k++) c.Un.v[k] = s->U[k];
+    c.Hprev = s->Hs;
+    c.nH = 0;
+    c.ce[0] = c.ce[1] = c.ci[0] = c.ci[1] = 0.0;
     c.adt = Ai[0][0] * dt; c.tau = c.adt; c.rx = c.tau / s->g.dx; c.ry = c.tau / s->g.dy;
     c.H = s->Hs;
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
-    launch_recon(c, s->st);
-    launch_update(c, s->st);
+    launch_flux(c, s->st);
     CK(cudaStreamSynchronize(s->st));
     if (Xs) {
         if (copy_state(s, s->Xs, Xs, nullptr, SPB6G_LAYOUT_AOS)) return SPB6G_CUDA_ERROR;
