@@ -65,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp,
-           "-lcudart"]
+           "-lcudadevrt", "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -85,6 +85,8 @@ void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam);
 void launch_jacobian(const Ctx& c, cudaStream_t st);
 void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit);
 void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity);
+int build_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t* exec);
+void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int expected_iters);
 void launch_thomas(const Ctx& c, cudaStream_t st);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);

@@ -508,18 +508,24 @@ SPB6G_DEV double spmv_row(const Ctx& c, const Nbr& nb, int x, F val) {
     }
     return s;
 }
-#define ROW_INDEX                                                   \
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y; \
-    const bool live = i < c.g.nx;                                   \
-    const int x = live ? i + j * c.g.nx : 0;
+// Each block covers 256 columns of ROWS_PER_BLOCK rows; a thread folds its rows
+// in row order, so every sum below is deterministic for a given grid.
+constexpr int ROWS_PER_BLOCK = 4;
+#define ROW_LOOP_BEGIN                                                           \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;                         \
+    if (i < c.g.nx)                                                              \
+        for (int jj = 0; jj < ROWS_PER_BLOCK; jj++) {                            \
+            const int j = blockIdx.y * ROWS_PER_BLOCK + jj;                      \
+            if (j >= c.g.ny) break;                                              \
+            const int x = i + j * c.g.nx;
+#define ROW_LOOP_END }
 
 __global__ void __launch_bounds__(RED_THREADS) k_bicg_init(Ctx c, double tol, int maxit) {
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
     const double cb = ns.sumb * Einv;
     double acc[2] = {0.0, 0.0};
-    ROW_INDEX
-    if (live) {
+    ROW_LOOP_BEGIN
         const Nbr nb = neighbours(c.g, i, j, x);
         auto xv = [&](int q) { return c.dinv[q] * (-c.G[q]) + cb; };
         const double Ax = spmv_row(c, nb, x, xv);
@@ -529,9 +535,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_init(Ctx c, double tol, in
         c.br0[x] = r;
         c.bp[x] = 0.0;
         c.bv[x] = 0.0;
-        acc[0] = r * r;
-        acc[1] = r * c.A1[x];
-    }
+        acc[0] += r * r;
+        acc[1] += r * c.A1[x];
+    ROW_LOOP_END
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[2], tot) && threadIdx.x == 0) {
         BicgScalars& b = *c.bs_;
@@ -554,18 +560,20 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_p(Ctx c, const double* __r
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
     const double beta = (b.r0r / b.rho) * (b.alpha / b.omega), om = b.omega;
+    const double* __restrict__ br = c.br;
+    const double* __restrict__ bv = c.bv;
+    const double* __restrict__ dinv = c.dinv;
     double acc[2] = {0.0, 0.0};
-    ROW_INDEX
-    if (live) {
+    ROW_LOOP_BEGIN
         const Nbr nb = neighbours(c.g, i, j, x);
-        auto pn = [&](int q) { return c.br[q] + beta * (p_old[q] - om * c.bv[q]); };
+        auto pn = [&](int q) { return br[q] + beta * (p_old[q] - om * bv[q]); };
         const double p = pn(x);
-        const double q = spmv_row(c, nb, x, [&](int k) { return c.dinv[k] * pn(k); });
+        const double q = spmv_row(c, nb, x, [&](int k) { return dinv[k] * pn(k); });
         p_new[x] = p;
         c.bq[x] = q;
-        acc[0] = p;
-        acc[1] = c.br0[x] * q;
-    }
+        acc[0] += p;
+        acc[1] += c.br0[x] * q;
+    ROW_LOOP_END
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[3], tot) && threadIdx.x == 0) {
         BicgScalars& B = *c.bs_;
@@ -579,20 +587,23 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_s(Ctx c) {
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
     const double al = b.alpha, cc = b.cc;
+    const double* __restrict__ br = c.br;
+    const double* __restrict__ bq = c.bq;
+    const double* __restrict__ A1 = c.A1;
+    const double* __restrict__ dinv = c.dinv;
     double acc[2] = {0.0, 0.0};
-    ROW_INDEX
-    if (live) {
+    ROW_LOOP_BEGIN
         const Nbr nb = neighbours(c.g, i, j, x);
-        auto sv = [&](int q) { return c.br[q] - al * (c.bq[q] + cc * c.A1[q]); };
-        const double v = c.bq[x] + cc * c.A1[x];
-        const double s = c.br[x] - al * v;
-        const double u = spmv_row(c, nb, x, [&](int k) { return c.dinv[k] * sv(k); });
+        auto sv = [&](int q) { return br[q] - al * (bq[q] + cc * A1[q]); };
+        const double v = bq[x] + cc * A1[x];
+        const double s = br[x] - al * v;
+        const double u = spmv_row(c, nb, x, [&](int k) { return dinv[k] * sv(k); });
         c.bv[x] = v;
         c.bs[x] = s;
         c.bu[x] = u;
-        acc[0] = s * s;
-        acc[1] = s;
-    }
+        acc[0] += s * s;
+        acc[1] += s;
+    ROW_LOOP_END
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[4], tot) && threadIdx.x == 0) {
         BicgScalars& B = *c.bs_;
@@ -606,13 +617,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_t(Ctx c) {
     const BicgScalars b = *c.bs_;
     if (b.status != BICG_RUNNING) return;
     double acc[2] = {0.0, 0.0};
-    ROW_INDEX
-    if (live) {
+    ROW_LOOP_BEGIN
         const double t = c.bu[x] + b.cs * c.A1[x];
         c.bt[x] = t;
-        acc[0] = t * c.bs[x];
-        acc[1] = t * t;
-    }
+        acc[0] += t * c.bs[x];
+        acc[1] += t * t;
+    ROW_LOOP_END
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[5], tot) && threadIdx.x == 0) {
         BicgScalars& B = *c.bs_;
@@ -627,8 +637,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
     if (b.status != BICG_RUNNING && b.status != BICG_CONV_HALF) return;
     const bool half = b.status == BICG_CONV_HALF;
     double acc[2] = {0.0, 0.0};
-    ROW_INDEX
-    if (live) {
+    ROW_LOOP_BEGIN
         const double ph = c.dinv[x] * p[x] + b.cc;
         if (half) {
             c.dP[x] += b.alpha * ph;
@@ -637,10 +646,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
             c.dP[x] += b.alpha * ph + b.omega * sh;
             const double r = c.bs[x] - b.omega * c.bt[x];
             c.br[x] = r;
-            acc[0] = r * r;
-            acc[1] = c.br0[x] * r;
+            acc[0] += r * r;
+            acc[1] += c.br0[x] * r;
         }
-    }
+    ROW_LOOP_END
     double tot[2];
     if (grid_fold<RedSum, 2>(acc, c.partials, &c.counters[6], tot) && threadIdx.x == 0) {
         BicgScalars& B = *c.bs_;
@@ -654,10 +663,22 @@ __global__ void __launch_bounds__(RED_THREADS) k_bicg_x(Ctx c, const double* __r
         else if (!isfinite(B.rr)) B.status = BICG_FAIL;  // NaN never converges; the reference loops to GMRESiter and fails
     }
 }
-static dim3 row_grid(const Ctx& c) { return dim3((unsigned)((c.g.nx + RED_THREADS - 1) / RED_THREADS), (unsigned)c.g.ny); }
+// Loop condition of the device-side iteration: continue while the solve is running.
+__global__ void k_bicg_cond(const BicgScalars* b, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, b->status == BICG_RUNNING ? 1u : 0u);
+}
+static dim3 row_grid(const Ctx& c) {
+    return dim3((unsigned)((c.g.nx + RED_THREADS - 1) / RED_THREADS), (unsigned)((c.g.ny + ROWS_PER_BLOCK - 1) / ROWS_PER_BLOCK));
+}
 void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit) {
     k_bicg_init<<<row_grid(c), RED_THREADS, 0, st>>>(c, tol, maxit);
     count(c, 1);
+}
+static void enqueue_iteration(const Ctx& c, cudaStream_t st, const dim3& gr, double* p_old, double* p_new) {
+    k_bicg_p<<<gr, RED_THREADS, 0, st>>>(c, p_old, p_new);
+    k_bicg_s<<<gr, RED_THREADS, 0, st>>>(c);
+    k_bicg_t<<<gr, RED_THREADS, 0, st>>>(c);
+    k_bicg_x<<<gr, RED_THREADS, 0, st>>>(c, p_new);
 }
 // `count` iterations.  p is double-buffered (pass 1 reads neighbours' old p
 // while writing the new one); `parity` selects the buffer holding the current p.
@@ -666,13 +687,43 @@ void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count_, int& parity) {
     for (int k = 0; k < count_; k++) {
         double* p0 = parity ? c.tcp : c.bp;  // tcp is the Thomas scratch, free on the BiCGStab path
         double* p1 = parity ? c.bp : c.tcp;
-        k_bicg_p<<<gr, RED_THREADS, 0, st>>>(c, p0, p1);
-        k_bicg_s<<<gr, RED_THREADS, 0, st>>>(c);
-        k_bicg_t<<<gr, RED_THREADS, 0, st>>>(c);
-        k_bicg_x<<<gr, RED_THREADS, 0, st>>>(c, p1);
+        enqueue_iteration(c, st, gr, p0, p1);
         parity ^= 1;
     }
     count(c, 4 * count_);
+}
+// The whole BiCGStab loop as one graph launch: a while-node whose body is two
+// iterations (the p buffers alternate) and the condition kernel.  The loop ends
+// on the device when the status leaves RUNNING (converged, failed, or GMRESiter
+// reached); no host round trip per iteration.  Kernel arguments are the solver's
+// fixed buffers, so the graph is built once per solver.
+int build_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t* exec) {
+    cudaGraph_t graph = nullptr;
+    if (cudaGraphCreate(&graph, 0) != cudaSuccess) return -1;
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) return -2;
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = h;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, graph, nullptr, 0, &params) != cudaSuccess) return -3;
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -4;
+    const dim3 gr = row_grid(c);
+    enqueue_iteration(c, st, gr, c.bp, c.tcp);
+    enqueue_iteration(c, st, gr, c.tcp, c.bp);
+    k_bicg_cond<<<1, 1, 0, st>>>(c.bs_, h);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(st, &captured) != cudaSuccess) return -5;
+    if (cudaGraphInstantiate(exec, graph, 0) != cudaSuccess) return -6;
+    cudaGraphDestroy(graph);
+    return 0;
+}
+void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int expected_iters) {
+    cudaGraphLaunch(exec, st);
+    count(c, 4 * (expected_iters + (expected_iters & 1)) + (expected_iters + 2) / 2);
 }
 
 // ============================================================ Thomas (1D non-periodic, :858-863)

@@ -57,6 +57,8 @@ struct spb6g_solver {
     int64_t tcnt[TG_COUNT] = {};
     cudaEvent_t region[2] = {nullptr, nullptr};
     long long nlaunch = 0;
+    cudaGraphExec_t bicg_exec = nullptr;  // device-side BiCGStab loop (built once per solver)
+    int last_bicg_iters = 8;
 };
 
 namespace {
@@ -205,13 +207,19 @@ int newton(spb6g_solver* s, double& resfinal) {
             if (s->pin->ns.fail) { tend_(s, TG_LINEAR); return SPB6G_NEWTON_FAIL; }
             launch_bicg_init(c, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter);
             s->bicg_parity = 0;
-            int chunk = 4;
-            for (;;) {
-                launch_bicg_iters(c, s->st, chunk, s->bicg_parity);
+            if (s->bicg_exec) {
+                launch_bicg_graph(c, s->st, s->bicg_exec, s->last_bicg_iters);
                 if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
-                if (s->pin->bs.status != BICG_RUNNING) break;
-                if (chunk < 32) chunk *= 2;
+            } else {  // host-polled chunks (used when the graph could not be built)
+                int chunk = 4;
+                for (;;) {
+                    launch_bicg_iters(c, s->st, chunk, s->bicg_parity);
+                    if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
+                    if (s->pin->bs.status != BICG_RUNNING) break;
+                    if (chunk < 32) chunk *= 2;
+                }
             }
+            s->last_bicg_iters = s->pin->bs.iters;
             s->stats.bicg_it += s->pin->bs.iters;
             if (s->pin->bs.status == BICG_FAIL) { tend_(s, TG_LINEAR); return SPB6G_LINEAR_FAIL; }
         }
@@ -453,6 +461,12 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.nlaunch = &s->nlaunch;
     c.p_ref = 0;
     if (!ok || cudaStreamSynchronize(s->st) != cudaSuccess) { spb6g_destroy(s); return SPB6G_CUDA_ERROR; }
+    if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC)) {  // BiCGStab path: capture its device-side loop
+        if (build_bicg_graph(c, s->st, &s->bicg_exec) != 0) {
+            s->bicg_exec = nullptr;
+            cudaGetLastError();
+        }
+    }
     *out = s;
     return SPB6G_OK;
 }
@@ -460,6 +474,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
 int spb6g_destroy(spb6g_solver* s) {
     if (!s) return SPB6G_BAD_ARG;
     if (s->st) cudaStreamSynchronize(s->st);
+    if (s->bicg_exec) cudaGraphExecDestroy(s->bicg_exec);
     for (void* p : s->allocs) cudaFree(p);
     if (s->pin) cudaFreeHost(s->pin);
     resolve_timing(s);
