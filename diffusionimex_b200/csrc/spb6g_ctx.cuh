@@ -45,7 +45,8 @@ struct Ctx {
     double* phis_x;         // min(phi, velocity smoothness) of cells -1..nx, (nx+2)*ny
     double* phis_y;         // nx*(ny+2)
     // stage data
-    double *ust, *vst, *kw, *qph0, *qph1;
+    double *kw, *qph0, *qph1;
+    double *pad_rho, *pad_u, *pad_v, *pad_cz;  // per-cell prep data on the padded grid (nx+4)*(ny+4)
     double *fx_ubs, *fx_kp, *fx_wl, *fx_pv;
     double *fy_ubs, *fy_kp, *fy_wl, *fy_pv;
     // per face, fixed for the stage: donors m1, m2, eps1, eps2 of the reconstructed left / right

@@ -28,7 +28,7 @@ struct FluxTile {
     static constexpr int NRY = TWO_D ? TY + 2 : 1;          // y-reconstructed cells -1..TY
     static constexpr int NFX = TX + 1, NFY = TWO_D ? TY + 1 : 1;
     static constexpr int Q_SZ = NV * NLX * NLY;
-    static constexpr int S_SZ = 2 * NLX * NLY;
+    static constexpr int S_SZ = 4 * NLX * NLY;              // vsc, esc, u, v per staged cell
     static constexpr int RX_SZ = 3 * NRX * TY;              // phi (volume), slope u, slope v
     static constexpr int RY_SZ = TWO_D ? 3 * TX * NRY : 0;
     static constexpr int FX_SZ = 9 * NFX * TY;              // 8 fluxes + face velocity
@@ -52,17 +52,29 @@ SPB6G_DEV void load_qe(const Ctx& c, int i, int j, double* q) {
     if (sy >= 0) ghost_transform(c.phy, c.g, sy, q);
 }
 
+// Frozen sound speed of prim_of (physics :893-902) without the velocity and mixture pressure,
+// which the scales do not use; false where prim_of is false.
+SPB6G_DEV bool frozen_cf(const Phys& P, const double* Q, double& cf) {
+    const double a1 = Q[IA1], a2 = 1 - a1, m1 = Q[IM1], m2 = Q[IM2];
+    if (!(a1 > 0 && a2 > 0 && m1 > 0 && m2 > 0)) return false;
+    const double rho = m1 + m2, r1 = m1 / a1, r2 = m2 / a2;
+    const double p1 = p_ame(P, 0, a1, m1, Q[IE1]), p2 = p_ame(P, 1, a2, m2, Q[IE2]);
+    if (!(p_admissible(P, 0, p1) && p_admissible(P, 1, p2))) return false;
+    cf = sqrt((m1 * c2_rp(P, 0, r1, p1) + m2 * c2_rp(P, 1, r2, p2)) / rho);
+    return true;
+}
+// Round-off scales of TVDReconstruction (:379-385): |u| + c_f and sum |eps| + kinetic energy.
 SPB6G_DEV void scales_of(const Phys& P, const double* q, double& vsc, double& esc) {
-    Prim w;
+    double cf;
     const double rho = q[IM1] + q[IM2], mm = hypot(q[IMU], q[IMV]);
-    vsc = (rho > 0 ? mm / rho : 0.0) + (prim_of(P, q, w) ? w.cf : 0.0);
+    vsc = (rho > 0 ? mm / rho : 0.0) + (frozen_cf(P, q, cf) ? cf : 0.0);
     esc = fabs(q[IE1]) + fabs(q[IE2]) + (rho > 0 ? 0.5 * mm * mm / rho : 0.0);
 }
 
 // Shared limiter, face-admissibility cap and velocity slopes (TVDReconstruction :399-463).
 SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const double* Ub, double vsa, double vsc,
-                      double vsb, double esa, double esc, double esb, double& phi_out, double& phis_out, double& slu,
-                      double& slv) {
+                      double vsb, double esa, double esc, double esb, const double* va_, const double* vc_,
+                      const double* vb_, double& phi_out, double& phis_out, double& slu, double& slv) {
     const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
     double phi = 1.0;
 #pragma unroll
@@ -102,13 +114,12 @@ SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const d
             }
         }
     }
-    const double ra = Ua[IM1] + Ua[IM2], rc = Uc[IM1] + Uc[IM2], rb = Ub[IM1] + Ub[IM2];
+    // va_, vc_, vb_: the cells' velocities (u, v) = (rho u, rho v) / (m1 + m2), computed once per cell
     const double tiny = 1e-12 * (vsa + vsc + vsb) + 1e-300;
     double sm = 1.0, sl[2];
 #pragma unroll
     for (int d = 0; d < 2; d++) {
-        const int k = d == 0 ? IMU : IMV;
-        const double va = Ua[k] / ra, vc = Uc[k] / rc, vb = Ub[k] / rb, a = vc - va, b = vb - vc;
+        const double va = va_[d], vc = vc_[d], vb = vb_[d], a = vc - va, b = vb - vc;
         double s = 0.0;
         if (!P.limiter) s = 0.5 * (a + b);
         else if (!(fabs(a) <= tiny && fabs(b) <= tiny)) {
@@ -124,8 +135,8 @@ SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const d
 }
 
 // Face value of a cell on its right (+) or left (-) side from the cell's stencil and its reconstruction.
-SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, double phi, double slu, double slv,
-                          bool right, double* w) {
+SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, double vcu, double vcv, double phi,
+                          double slu, double slv, bool right, double* w) {
     const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
 #pragma unroll
     for (int q = 0; q < 5; q++) {
@@ -133,8 +144,6 @@ SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, 
         const double sig = phi * 0.5 * (Ub[k] - Ua[k]);
         w[k] = right ? Uc[k] + 0.5 * sig : Uc[k] - 0.5 * sig;
     }
-    const double rc = Uc[IM1] + Uc[IM2];
-    const double vcu = Uc[IMU] / rc, vcv = Uc[IMV] / rc;
     const double v0 = right ? vcu + 0.5 * slu : vcu - 0.5 * slu, v1 = right ? vcv + 0.5 * slv : vcv - 0.5 * slv;
     const double r = w[IM1] + w[IM2];
     w[IMU] = r * v0;
@@ -142,10 +151,13 @@ SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, 
     w[IEN] = w[IE1] + w[IE2] + 0.5 * r * (v0 * v0 + v1 * v1);
 }
 
-SPB6G_DEV void rusanov_flux(const double* QL, const double* QR, int d, double* flux) {
+// Rusanov flux (RusanovC_x/y :237-259); returns the normal face-state velocities, which are
+// also the terms of the face velocity ube (Update :283-294).
+SPB6G_DEV void rusanov_flux(const double* QL, const double* QR, int d, double* flux, double& vL, double& vR) {
     const int km = d == 0 ? IMU : IMV;
-    const double vL = QL[km] / (QL[IM1] + QL[IM2]), vR = QR[km] / (QR[IM1] + QR[IM2]);
-    const double a = SMAX(fabs(QL[km] / (QL[IM1] + QL[IM2])), fabs(QR[km] / (QR[IM1] + QR[IM2])));
+    vL = QL[km] / (QL[IM1] + QL[IM2]);
+    vR = QR[km] / (QR[IM1] + QR[IM2]);
+    const double a = SMAX(fabs(vL), fabs(vR));
 #pragma unroll
     for (int k = 0; k < NV; k++) flux[k] = 0.5 * (QL[k] * vL + QR[k] * vR) - 0.5 * a * (QR[k] - QL[k]);
 }
@@ -158,7 +170,9 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     double* Qs_ = smem;                      // [NV][NLY][NLX]
     double* VS = Qs_ + T::Q_SZ;              // [NLY][NLX]
     double* ES = VS + NLX * NLY;
-    double* RX = ES + NLX * NLY;             // [3][TY][NRX]
+    double* VU = ES + NLX * NLY;             // cell velocity u
+    double* VV = VU + NLX * NLY;             // cell velocity v
+    double* RX = VV + NLX * NLY;             // [3][TY][NRX]
     double* RY = RX + T::RX_SZ;              // [3][NRY][TX]
     double* FX = RY + T::RY_SZ;              // [9][TY][NFX]
     double* FY = FX + T::FX_SZ;              // [9][NFY][TX]
@@ -188,7 +202,11 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         scales_of(c.phy, q, vs, es);
         VS[ly * NLX + lx] = vs;
         ES[ly * NLX + lx] = es;
+        const double rho = q[IM1] + q[IM2];
+        VU[ly * NLX + lx] = q[IMU] / rho;
+        VV[ly * NLX + lx] = q[IMV] / rho;
     }
+    auto vel = [&](int ly, int lx, double* v) { v[0] = VU[ly * NLX + lx]; v[1] = VV[ly * NLX + lx]; };
     __syncthreads();
 
     // 2. reconstruction of cells -1..TX (x) and -1..TY (y)
@@ -200,9 +218,10 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         double Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
         for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, lx - 1); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly, lx + 1); }
-        double phi, phis, slu, slv;
+        double phi, phis, slu, slv, va[2], vc[2], vb[2];
+        vel(ly, lx - 1, va); vel(ly, lx, vc); vel(ly, lx + 1, vb);
         recon3(c.phy, Ua, Uc, Ub, VS[ly * NLX + lx - 1], VS[ly * NLX + lx], VS[ly * NLX + lx + 1], ES[ly * NLX + lx - 1],
-               ES[ly * NLX + lx], ES[ly * NLX + lx + 1], phi, phis, slu, slv);
+               ES[ly * NLX + lx], ES[ly * NLX + lx + 1], va, vc, vb, phi, phis, slu, slv);
         RX[(0 * TY + ry) * NRX + rx] = phi;
         RX[(1 * TY + ry) * NRX + rx] = slu;
         RX[(2 * TY + ry) * NRX + rx] = slv;
@@ -218,9 +237,10 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
             double Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly - 1, lx); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly + 1, lx); }
-            double phi, phis, slu, slv;
+            double phi, phis, slu, slv, va[2], vc[2], vb[2];
+            vel(ly - 1, lx, va); vel(ly, lx, vc); vel(ly + 1, lx, vb);
             recon3(c.phy, Ua, Uc, Ub, VS[(ly - 1) * NLX + lx], VS[ly * NLX + lx], VS[(ly + 1) * NLX + lx],
-                   ES[(ly - 1) * NLX + lx], ES[ly * NLX + lx], ES[(ly + 1) * NLX + lx], phi, phis, slu, slv);
+                   ES[(ly - 1) * NLX + lx], ES[ly * NLX + lx], ES[(ly + 1) * NLX + lx], va, vc, vb, phi, phis, slu, slv);
             RY[(0 * NRY + ry) * TX + rx] = phi;
             RY[(1 * NRY + ry) * TX + rx] = slu;
             RY[(2 * NRY + ry) * TX + rx] = slv;
@@ -241,15 +261,16 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         // right face value of the left cell
 #pragma unroll
         for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, la - 1); Uc[k] = Q(k, ly, la); Ub[k] = Q(k, ly, la + 1); }
-        face_value(Ua, Uc, Ub, RX[(0 * TY + ry) * NRX + f], RX[(1 * TY + ry) * NRX + f], RX[(2 * TY + ry) * NRX + f],
-                   true, wR);
+        face_value(Ua, Uc, Ub, VU[ly * NLX + la], VV[ly * NLX + la], RX[(0 * TY + ry) * NRX + f],
+                   RX[(1 * TY + ry) * NRX + f], RX[(2 * TY + ry) * NRX + f], true, wR);
         // left face value of the right cell
 #pragma unroll
         for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, ly, la + 2); }
-        face_value(Ua, Uc, Ub, RX[(0 * TY + ry) * NRX + f + 1], RX[(1 * TY + ry) * NRX + f + 1],
-                   RX[(2 * TY + ry) * NRX + f + 1], false, wL);
-        rusanov_flux(wR, wL, 0, fl);
-        const double ube = 0.5 * (wR[IMU] / (wR[IM1] + wR[IM2]) + wL[IMU] / (wL[IM1] + wL[IM2]));
+        face_value(Ua, Uc, Ub, VU[ly * NLX + la + 1], VV[ly * NLX + la + 1], RX[(0 * TY + ry) * NRX + f + 1],
+                   RX[(1 * TY + ry) * NRX + f + 1], RX[(2 * TY + ry) * NRX + f + 1], false, wL);
+        double uL, uR;
+        rusanov_flux(wR, wL, 0, fl, uL, uR);
+        const double ube = 0.5 * (uL + uR);
 #pragma unroll
         for (int k = 0; k < NV; k++) FX[(k * TY + ry) * NFX + f] = fl[k];
         FX[(8 * TY + ry) * NFX + f] = ube;
@@ -273,14 +294,15 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
             double Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) { Ua[k] = Q(k, la - 1, lx); Uc[k] = Q(k, la, lx); Ub[k] = Q(k, la + 1, lx); }
-            face_value(Ua, Uc, Ub, RY[(0 * NRY + f) * TX + rx], RY[(1 * NRY + f) * TX + rx], RY[(2 * NRY + f) * TX + rx],
-                       true, wR);
+            face_value(Ua, Uc, Ub, VU[la * NLX + lx], VV[la * NLX + lx], RY[(0 * NRY + f) * TX + rx],
+                       RY[(1 * NRY + f) * TX + rx], RY[(2 * NRY + f) * TX + rx], true, wR);
 #pragma unroll
             for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, la + 2, lx); }
-            face_value(Ua, Uc, Ub, RY[(0 * NRY + f + 1) * TX + rx], RY[(1 * NRY + f + 1) * TX + rx],
-                       RY[(2 * NRY + f + 1) * TX + rx], false, wL);
-            rusanov_flux(wR, wL, 1, fl);
-            const double ube = 0.5 * (wR[IMV] / (wR[IM1] + wR[IM2]) + wL[IMV] / (wL[IM1] + wL[IM2]));
+            face_value(Ua, Uc, Ub, VU[(la + 1) * NLX + lx], VV[(la + 1) * NLX + lx], RY[(0 * NRY + f + 1) * TX + rx],
+                       RY[(1 * NRY + f + 1) * TX + rx], RY[(2 * NRY + f + 1) * TX + rx], false, wL);
+            double vL, vR;
+            rusanov_flux(wR, wL, 1, fl, vL, vR);
+            const double ube = 0.5 * (vL + vR);
 #pragma unroll
             for (int k = 0; k < NV; k++) FY[(k * NFY + f) * TX + rx] = fl[k];
             FY[(8 * NFY + f) * TX + rx] = ube;
@@ -299,6 +321,7 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     __syncthreads();
 
     // 4. explicit update of the tile's cells (Update :300-341)
+    const double rx_ = c.adt / g.dx, ry_ = c.adt / g.dy;  // adt / dx, formed as the reference forms it per use
     for (int t = tid; t < TX * TY; t += nth) {
         const int rx = t % TX, ry = t / TX;
         const int gi = i0 + rx, gj = j0 + ry;
@@ -311,14 +334,14 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         for (int k = 0; k < NV; k++) {
             double s = c.Un.v[k][x];
             for (int r = 0; r < c.nH; r++) s = s + c.ci[r] * c.Hprev[((size_t)r * NV + k) * c.n + x];
-            X[k] = s - c.adt / g.dx * (FX[(k * TY + ry) * NFX + rx + 1] - FX[(k * TY + ry) * NFX + rx]);
+            X[k] = s - rx_ * (FX[(k * TY + ry) * NFX + rx + 1] - FX[(k * TY + ry) * NFX + rx]);
         }
         const double qa1 = Q(IA1, ly, lx);
-        X[IA1] += c.adt / g.dx * qa1 * (FX[(8 * TY + ry) * NFX + rx + 1] - FX[(8 * TY + ry) * NFX + rx]);
+        X[IA1] += rx_ * qa1 * (FX[(8 * TY + ry) * NFX + rx + 1] - FX[(8 * TY + ry) * NFX + rx]);
         if (TWO_D) {
 #pragma unroll
-            for (int k = 0; k < NV; k++) X[k] -= c.adt / g.dy * (FY[(k * NFY + ry + 1) * TX + rx] - FY[(k * NFY + ry) * TX + rx]);
-            X[IA1] += c.adt / g.dy * qa1 * (FY[(8 * NFY + ry + 1) * TX + rx] - FY[(8 * NFY + ry) * TX + rx]);
+            for (int k = 0; k < NV; k++) X[k] -= ry_ * (FY[(k * NFY + ry + 1) * TX + rx] - FY[(k * NFY + ry) * TX + rx]);
+            X[IA1] += ry_ * qa1 * (FY[(8 * NFY + ry + 1) * TX + rx] - FY[(8 * NFY + ry) * TX + rx]);
         }
 #pragma unroll
         for (int k = 0; k < NV; k++) c.Xs.v[k][x] = X[k];

@@ -57,16 +57,30 @@ SPB6G_DEV void vel_at(const Ctx& c, int i, int j, double& u, double& v) {
 }
 SPB6G_DEV double pold_at(const Ctx& c, int i, int j) { return c.P[mp_index(c.g, i, j)]; }
 
+// Per-cell quantities of the stage prep on the padded grid (cells -2..nx+1 x
+// -2..ny+1, ghosts through the boundary maps): rho*, u* = rho u*/rho*, v*, and
+// the frozen sound speed c_f (cfz :948-955); interior cells also get the
+// residual scale K + P_E (:960-971) and the admissibility check (:928-929).
+SPB6G_DEV int pad_index(const Geom& g, int i, int j) { return (i + 2) + (g.ny > 1 ? (j + 2) * (g.nx + 4) : 0); }  // 1D: one row
 __global__ void k_prep_cell(Ctx c) {
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+    const Geom& g = c.g;
+    const int W = g.nx + 4, Hh = g.ny > 1 ? g.ny + 4 : 1;
+    const long tot = (long)W * Hh;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % W) - 2, j = g.ny > 1 ? (int)(t / W) - 2 : 0;
         double X[NV];
-#pragma unroll
-        for (int k = 0; k < NV; k++) X[k] = c.Xs.v[k][x];
-        const double a1 = X[IA1], a2 = c.a2s[x], m1 = X[IM1], m2 = X[IM2], sa = a1 + a2, rho = m1 + m2;
+        xs_at(c, i, j, X);
+        const double a2 = load_arr(g, c.a2s, i, j);
+        const double rho = X[IM1] + X[IM2];
+        const int p = pad_index(g, i, j);
+        c.pad_rho[p] = rho;
+        c.pad_u[p] = X[IMU] / rho;
+        c.pad_v[p] = X[IMV] / rho;
+        c.pad_cz[p] = cfz(c.phy, X, a2);
+        if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) continue;
+        const size_t x = (size_t)i + (size_t)j * g.nx;
+        const double a1 = X[IA1], m1 = X[IM1], m2 = X[IM2], sa = a1 + a2;
         if (!(sa > 0 && rho > 0)) atomicOr(&c.ns->err, 2);
-        c.ust[x] = X[IMU] / rho;
-        c.vst[x] = X[IMV] / rho;
-        // residual scale K + P_E (:960-971)
         double K = SMAX(c.phy.ph[0].pi, c.phy.ph[1].pi), PE = 0.0;
         if (a1 > 0 && a2 > 0 && m1 > 0 && m2 > 0) {
             const double p1 = p_ame(c.phy, 0, a1, m1, X[IE1]), p2 = p_ame(c.phy, 1, a2, m2, X[IE2]);
@@ -79,21 +93,26 @@ __global__ void k_prep_cell(Ctx c) {
     }
 }
 
-// Face coefficients of the implicit face velocity / pressure (set_face :1001-1023, dil_jump :989-1000).
-SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, double& kp, double& wl, double& pv) {
+// Face coefficients of the implicit face velocity / pressure (set_face :1001-1023, dil_jump :989-1000)
+// and the tangential velocities of the face's two cells.
+SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, double& kp, double& wl, double& pv,
+                        double& utL, double& utR) {
     const Geom& g = c.g;
     const int iR = iL + (ydir ? 0 : 1), jR = jL + (ydir ? 1 : 0);
     const double hh = ydir ? g.dy : g.dx;
-    double XL[NV], XR[NV];
-    xs_at(c, iL, jL, XL);
-    xs_at(c, iR, jR, XR);
-    const double rL = XL[IM1] + XL[IM2], rR = XR[IM1] + XR[IM2];
-    const double uL = (ydir ? XL[IMV] : XL[IMU]) / rL, uR = (ydir ? XR[IMV] : XR[IMU]) / rR;
+    const int pL = pad_index(g, iL, jL), pR = pad_index(g, iR, jR);
+    const double* U = c.pad_u;
+    const double* V = c.pad_v;
+    const double* N = ydir ? V : U;  // normal velocity
+    const double rL = c.pad_rho[pL], rR = c.pad_rho[pR];
+    const double uL = N[pL], uR = N[pR];
+    utL = ydir ? U[pL] : V[pL];
+    utR = ydir ? U[pR] : V[pR];
     ubs = 0.5 * (uL + uR);
     kp = c.tau / hh / (0.5 * (rL + rR));
     wl = rR / (rL + rR);
     pv = 0.0;
-    const double cL = cfz(c.phy, XL, load_arr(g, c.a2s, iL, jL)), cR = cfz(c.phy, XR, load_arr(g, c.a2s, iR, jR));
+    const double cL = c.pad_cz[pL], cR = c.pad_cz[pR];
     if (!(isfinite(cL) && isfinite(cR))) return;
     const double phi = SMAX(0.0, 1.0 - c.tau * SMIN(cL, cR) / hh);
     if (phi == 0.0) return;
@@ -102,55 +121,37 @@ SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, dou
     const double phis = ydir ? SMIN(c.phis_y[ryi(g, iL, jL)], c.phis_y[ryi(g, iR, jR)])
                              : SMIN(c.phis_x[rxi(g, iL, jL)], c.phis_x[rxi(g, iR, jR)]);
     const double psiP = 1.0 - (1.0 - psi_face(c.phy.limiter, pold_at(c, im, jm), pold_at(c, iL, jL), pold_at(c, iR, jR), pold_at(c, ip, jp))) * phis;
-    double um, vm, up, vp;
-    vel_at(c, im, jm, um, vm);
-    vel_at(c, ip, jp, up, vp);
-    const double psiU = psi_face(c.phy.limiter, ydir ? vm : um, uL, uR, ydir ? vp : up);
-    // dil_jump
+    const double psiU = psi_face(c.phy.limiter, N[pad_index(g, im, jm)], uL, uR, N[pad_index(g, ip, jp)]);
     double D;
     if (!ydir) {
         const double d = uR - uL;
         if (g.ny == 1) D = d;
         else {
-            double u0p, v0p, u1p, v1p, u0m, v0m, u1m, v1m;
-            vel_at(c, iL, jL + 1, u0p, v0p);
-            vel_at(c, iL + 1, jL + 1, u1p, v1p);
-            vel_at(c, iL, jL - 1, u0m, v0m);
-            vel_at(c, iL + 1, jL - 1, u1m, v1m);
-            D = 0.25 * (2.0 * d + ((u1p - u0p) + (u1m - u0m))) + 0.25 * (g.dx / g.dy) * ((v0p - v0m) + (v1p - v1m));
+            const int p0p = pad_index(g, iL, jL + 1), p1p = pad_index(g, iL + 1, jL + 1);
+            const int p0m = pad_index(g, iL, jL - 1), p1m = pad_index(g, iL + 1, jL - 1);
+            D = 0.25 * (2.0 * d + ((U[p1p] - U[p0p]) + (U[p1m] - U[p0m]))) + 0.25 * (g.dx / g.dy) * ((V[p0p] - V[p0m]) + (V[p1p] - V[p1m]));
         }
     } else {
-        const double d = uR - uL;  // v(i, j+1) - v(i, j)
-        double up1, vp1, up0, vp0, um1, vm1, um0, vm0;
-        vel_at(c, iL + 1, jL + 1, up1, vp1);
-        vel_at(c, iL + 1, jL, up0, vp0);
-        vel_at(c, iL - 1, jL + 1, um1, vm1);
-        vel_at(c, iL - 1, jL, um0, vm0);
-        D = 0.25 * (2.0 * d + ((vp1 - vp0) + (vm1 - vm0))) + 0.25 * (g.dy / g.dx) * ((up0 - um0) + (up1 - um1));
+        const double d = uR - uL;
+        const int pp1 = pad_index(g, iL + 1, jL + 1), pp0 = pad_index(g, iL + 1, jL);
+        const int pm1 = pad_index(g, iL - 1, jL + 1), pm0 = pad_index(g, iL - 1, jL);
+        D = 0.25 * (2.0 * d + ((V[pp1] - V[pp0]) + (V[pm1] - V[pm0]))) + 0.25 * (g.dy / g.dx) * ((U[pp0] - U[pm0]) + (U[pp1] - U[pm1]));
     }
     const double ZL = rL * cL, ZR = rR * cR;
     kp += phi * psiP / (ZL + ZR);
     pv = phi * psiU * ZL * ZR / (ZL + ZR) * D;
-}
-// Tangential velocities of the two cells of a face (fixed for the stage; the donors
-// of planes 0-7 are written by the explicit kernel).
-SPB6G_DEV void face_fixed(const Ctx& c, int i, int j, int ydir, double* plane, size_t f, size_t stride) {
-    double u, v;
-    vel_at(c, i, j, u, v);
-    plane[8 * stride + f] = ydir ? u : v;
-    vel_at(c, i + (ydir ? 0 : 1), j + (ydir ? 1 : 0), u, v);
-    plane[9 * stride + f] = ydir ? u : v;
 }
 __global__ void k_prep_fx(Ctx c) {
     const Geom& g = c.g;
     const long tot = (long)(g.nx + 1) * g.ny;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
         const int i = (int)(t % (g.nx + 1)) - 1, j = (int)(t / (g.nx + 1));
-        double ubs, kp, wl, pv;
-        set_face(c, i, j, 0, ubs, kp, wl, pv);
+        double ubs, kp, wl, pv, utL, utR;
+        set_face(c, i, j, 0, ubs, kp, wl, pv, utL, utR);
         const size_t f = fxi(g, i, j);
         c.fx_ubs[f] = ubs; c.fx_kp[f] = kp; c.fx_wl[f] = wl; c.fx_pv[f] = pv;
-        face_fixed(c, i, j, 0, c.fxd, f, (size_t)tot);
+        c.fxd[8 * (size_t)tot + f] = utL;
+        c.fxd[9 * (size_t)tot + f] = utR;
     }
 }
 __global__ void k_prep_fy(Ctx c) {
@@ -158,15 +159,17 @@ __global__ void k_prep_fy(Ctx c) {
     const long tot = (long)g.nx * (g.ny + 1);
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
         const int i = (int)(t % g.nx), j = (int)(t / g.nx) - 1;
-        double ubs, kp, wl, pv;
-        set_face(c, i, j, 1, ubs, kp, wl, pv);
+        double ubs, kp, wl, pv, utL, utR;
+        set_face(c, i, j, 1, ubs, kp, wl, pv, utL, utR);
         const size_t f = fyi(g, i, j);
         c.fy_ubs[f] = ubs; c.fy_kp[f] = kp; c.fy_wl[f] = wl; c.fy_pv[f] = pv;
-        face_fixed(c, i, j, 1, c.fyd, f, (size_t)tot);
+        c.fyd[8 * (size_t)tot + f] = utL;
+        c.fyd[9 * (size_t)tot + f] = utR;
     }
 }
 void launch_prep(const Ctx& c, cudaStream_t st) {
-    k_prep_cell<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    const long pad = (long)(c.g.nx + 4) * (c.g.ny > 1 ? c.g.ny + 4 : 1);
+    k_prep_cell<<<blocks_for(pad), TPB, 0, st>>>(c);
     k_prep_fx<<<blocks_for((long)(c.g.nx + 1) * c.g.ny), TPB, 0, st>>>(c);
     if (c.g.ny > 1) k_prep_fy<<<blocks_for((long)c.g.nx * (c.g.ny + 1)), TPB, 0, st>>>(c);
     count(c, c.g.ny > 1 ? 3 : 2);
@@ -429,7 +432,8 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_jac_entries(Ctx c) {
     double* planes[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
     const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
-        const int w = (int)(t / c.n), x = (int)(t - (long)w * c.n);
+        // the entries of one row sit in adjacent threads, so the row's stage data is fetched once
+        const int x = (int)(t / nw), w = (int)(t - (long)x * nw);
         const int i = x % g.nx, j = x / g.nx;
         const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
         const double G0 = c.G[x];

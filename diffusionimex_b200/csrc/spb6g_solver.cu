@@ -438,7 +438,11 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     const size_t nrx = (size_t)(nx + 2) * ny, nry = (size_t)nx * (ny + 2);
     c.phis_x = A(nrx);
     c.phis_y = A(nry);
-    c.ust = A(n); c.vst = A(n); c.kw = A(n); c.qph0 = A(n); c.qph1 = A(n);
+    c.kw = A(n); c.qph0 = A(n); c.qph1 = A(n);
+    {
+        const size_t npad = (size_t)(nx + 4) * (ny > 1 ? ny + 4 : 1);
+        c.pad_rho = A(npad); c.pad_u = A(npad); c.pad_v = A(npad); c.pad_cz = A(npad);
+    }
     const size_t nfx = (size_t)(nx + 1) * ny, nfy = (size_t)nx * (ny + 1);
     c.fx_ubs = A(nfx); c.fx_kp = A(nfx); c.fx_wl = A(nfx); c.fx_pv = A(nfx);
     c.fy_ubs = A(nfy); c.fy_kp = A(nfy); c.fy_wl = A(nfy); c.fy_pv = A(nfy);
