@@ -428,30 +428,32 @@ void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
 __global__ void __launch_bounds__(RED_THREADS, 2) k_jac_entries(Ctx c) {
     const Geom& g = c.g;
     const bool twoD = g.ny > 1;
-    const long nw = twoD ? 5 : 3, tot = nw * c.n;
+    const int nw = twoD ? 5 : 3;
     double* planes[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
     const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
-        // the entries of one row sit in adjacent threads, so the row's stage data is fetched once
-        const int x = (int)(t / nw), w = (int)(t - (long)x * nw);
-        const int i = x % g.nx, j = x / g.nx;
-        const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
-        const double G0 = c.G[x];
-        double gv, a;
-        bool ok;
-        if (w == 0) {
-            const double h = 1e-7 * c.sc[x];
-            ok = residual_at(c, i, j, p, h, -1, 0, gv, nullptr);
-            a = (gv - G0) / h;
-        } else {
-            const int col = mp_index(g, i + nb[w - 1][0], j + nb[w - 1][1]);
-            const double hn = 1e-7 * c.sc[col];
-            ok = residual_at(c, i, j, p, 0, w - 1, hn, gv, nullptr);
-            a = (gv - G0) / hn;
-        }
-        if (!ok) atomicOr(&c.ns->fail, 2);
-        planes[w][x] = a;
+    // blocks nw*r .. nw*r + nw-1 evaluate the nw entries of the same 256 rows: they run side by
+    // side, so the rows' stage data comes from DRAM once and from L2 for the other entries,
+    // while every warp follows one entry's code path
+    const int w = blockIdx.x % nw, rb = blockIdx.x / nw;
+    const int x = rb * blockDim.x + threadIdx.x;
+    if (x >= c.n) return;
+    const int i = x % g.nx, j = x / g.nx;
+    const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
+    const double G0 = c.G[x];
+    double gv, a;
+    bool ok;
+    if (w == 0) {
+        const double h = 1e-7 * c.sc[x];
+        ok = residual_at(c, i, j, p, h, -1, 0, gv, nullptr);
+        a = (gv - G0) / h;
+    } else {
+        const int col = mp_index(g, i + nb[w - 1][0], j + nb[w - 1][1]);
+        const double hn = 1e-7 * c.sc[col];
+        ok = residual_at(c, i, j, p, 0, w - 1, hn, gv, nullptr);
+        a = (gv - G0) / hn;
     }
+    if (!ok) atomicOr(&c.ns->fail, 2);
+    planes[w][x] = a;
 }
 // Row sums A 1 (summed in the row's entry order, as block_sum's terms :763), Jacobi
 // inverse, and the set-up sums E = 1^T A 1, 1^T b, b^T b with b = -G.
@@ -477,8 +479,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_jac_finish(Ctx c) {
     }
 }
 void launch_jacobian(const Ctx& c, cudaStream_t st) {
-    const long tot = (long)(c.g.ny > 1 ? 5 : 3) * c.n;
-    k_jac_entries<<<(int)((tot + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c);
+    const int nw = c.g.ny > 1 ? 5 : 3;
+    k_jac_entries<<<nw * ((c.n + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c);
     k_jac_finish<<<(c.n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, st>>>(c);
     count(c, 2);
 }

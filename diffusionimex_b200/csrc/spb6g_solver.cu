@@ -58,6 +58,8 @@ struct spb6g_solver {
     cudaEvent_t region[2] = {nullptr, nullptr};
     long long nlaunch = 0;
     cudaGraphExec_t bicg_exec = nullptr;  // device-side BiCGStab loop (built once per solver)
+    cudaStream_t st2 = nullptr;           // side stream: shock budget, overlapped with the stage prep
+    cudaEvent_t ev_flux = nullptr, ev_shock = nullptr;
     int last_bicg_iters = 8;
 };
 
@@ -90,18 +92,33 @@ cudaEvent_t pool_event(spb6g_solver* s) {
     s->ev_pool.pop_back();
     return e;
 }
-void tbegin(spb6g_solver* s, int) {
+void tbegin(spb6g_solver* s, int, cudaStream_t st = nullptr) {
     if (!s->timing) return;
     s->open_ev = pool_event(s);
-    if (s->open_ev) cudaEventRecord(s->open_ev, s->st);
+    if (s->open_ev) cudaEventRecord(s->open_ev, st ? st : s->st);
 }
-void tend_(spb6g_solver* s, int g) {
+void tend_(spb6g_solver* s, int g, cudaStream_t st = nullptr) {
     if (!s->timing || !s->open_ev) return;
     cudaEvent_t b = pool_event(s);
     if (!b) return;
-    cudaEventRecord(b, s->st);
+    cudaEventRecord(b, st ? st : s->st);
     s->pending.push_back({g, s->open_ev, b});
     s->open_ev = nullptr;
+}
+// Stage prep on the main stream while the shock budget (whose strong-shock cells each
+// integrate a shock profile serially) runs on the side stream; joined before Newton.
+void prep_and_shock(spb6g_solver* s) {
+    Ctx& c = s->c;
+    cudaEventRecord(s->ev_flux, s->st);
+    cudaStreamWaitEvent(s->st2, s->ev_flux, 0);
+    tbegin(s, TG_SHOCK, s->st2);
+    launch_shock(c, s->st2);
+    tend_(s, TG_SHOCK, s->st2);
+    cudaEventRecord(s->ev_shock, s->st2);
+    tbegin(s, TG_PREP);
+    launch_prep(c, s->st);
+    tend_(s, TG_PREP);
+    cudaStreamWaitEvent(s->st, s->ev_shock, 0);
 }
 // Accumulates every completed group (called after a stream synchronisation).
 void resolve_timing(spb6g_solver* s) {
@@ -296,12 +313,7 @@ int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
     launch_flux(c, s->st);
     tend_(s, TG_EXPLICIT);
-    tbegin(s, TG_PREP);
-    launch_prep(c, s->st);
-    tend_(s, TG_PREP);
-    tbegin(s, TG_SHOCK);
-    launch_shock(c, s->st);
-    tend_(s, TG_SHOCK);
+    prep_and_shock(s);
     double res = 0;
     const int rc = newton(s, res);
     if (rc != SPB6G_OK) return rc;
@@ -419,7 +431,13 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     const int nx = cfg->nx, ny = cfg->ny;
     const size_t n = (size_t)nx * ny;
     s->n = (int)n;
-    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { delete s; return SPB6G_CUDA_ERROR; }
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_flux, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_shock, cudaEventDisableTiming) != cudaSuccess) {
+        spb6g_destroy(s);
+        return SPB6G_CUDA_ERROR;
+    }
     bool ok = true;
     auto A = [&](size_t cnt) { double* p = dalloc(s, cnt); if (!p) ok = false; return p; };
     for (int k = 0; k < NV; k++) { s->U[k] = A(n); s->Ust[k] = A(n); s->Xs[k] = A(n); }
@@ -485,6 +503,9 @@ int spb6g_destroy(spb6g_solver* s) {
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (int e = 0; e < 2; e++)
         if (s->region[e]) cudaEventDestroy(s->region[e]);
+    if (s->st2) { cudaStreamSynchronize(s->st2); cudaStreamDestroy(s->st2); }
+    if (s->ev_flux) cudaEventDestroy(s->ev_flux);
+    if (s->ev_shock) cudaEventDestroy(s->ev_shock);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
     return SPB6G_OK;
@@ -622,8 +643,7 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
                 if (phi_y) phi_y[(size_t)j * nx + i] = ny > 1 ? ty[(size_t)i + (size_t)(j + 1) * nx] : 0.0;
             }
     }
-    launch_prep(c, s->st);
-    launch_shock(c, s->st);
+    prep_and_shock(s);
     double res;
     int rc = newton(s, res);
     if (rc != SPB6G_OK) return rc;
