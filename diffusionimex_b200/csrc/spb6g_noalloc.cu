@@ -1,0 +1,124 @@
+// Allocation-free time-step rate (caldt) on caller-owned device buffers.
+//
+// Some callers cannot let a library call cudaMalloc: a host framework that owns
+// every device byte through its own arena or pool, a time-critical loop that
+// cannot afford the device-wide synchronisation cudaMalloc / cudaFree may cause,
+// or a long-running service whose device footprint must not grow after start-up.  For them this entry point takes
+// the state as device pointers the caller already owns and keeps its only
+// scratch -- one partial (max |u| + c, max |v| + c) per block, a block counter
+// and the two results -- in file-scope __device__ arrays that every GPU loading
+// the library holds until the process exits.
+//
+// Limits and rules:
+//   * at most SPB6G_NOALLOC_MAX_CELLS interior cells (one cell per thread,
+//     one partial per 256-thread block); larger grids are rejected with
+//     SPB6G_TOO_LARGE before any device work;
+//   * the first call on a device looks up the device addresses of the scratch
+//     arrays (cudaGetSymbolAddress, with that device current) -- make that
+//     first call before any stream capture;
+//   * every call shares the scratch: the block counter is cleared at the start
+//     of each call, and two calls whose work overlaps on the GPU (different
+//     streams, or host threads, at the same time) race on it.
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/spb6g.h"
+#include "spb6g_common.cuh"
+
+using namespace spb6g;
+
+namespace {
+
+constexpr int NOALLOC_THREADS = 256;
+constexpr int NOALLOC_MAX_BLOCKS = SPB6G_NOALLOC_MAX_CELLS / NOALLOC_THREADS;
+
+static __device__ __align__(256) double g_na_partials[NOALLOC_MAX_BLOCKS * 2];
+static __device__ __align__(256) unsigned g_na_counter[64];
+static __device__ __align__(256) double g_na_result[2];
+
+// Device addresses of the scratch arrays for each device, looked up on first use.
+struct NoallocSymbols {
+    bool ready = false;
+    double* partials = nullptr;
+    unsigned* counter = nullptr;
+    double* result = nullptr;
+};
+NoallocSymbols g_syms[64];
+std::mutex g_syms_mutex;
+
+// One cell per thread: the maxima of caldt (:502-514) over admissible cells.
+__global__ void __launch_bounds__(NOALLOC_THREADS) k_caldt_noalloc(Phys P, int n, CState U, int acoustic,
+                                                                   double* partials, unsigned* counter, double* result) {
+    double m[2] = {0.0, 0.0};
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < n) {
+        double q[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) q[k] = U.v[k][x];
+        Prim w;
+        if (prim_of(P, q, w)) {
+            const double cs = acoustic ? w.cf : 0.0;
+            m[0] = SMAX(0.0, fabs(w.u) + cs);
+            m[1] = SMAX(0.0, fabs(w.v) + cs);
+        }
+    }
+    double tot[2];
+    if (grid_fold<RedMax, 2>(m, partials, counter, tot) && threadIdx.x == 0) {
+        result[0] = tot[0];
+        result[1] = tot[1];
+    }
+}
+
+}  // namespace
+
+extern "C" int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
+                                   double* inv_rate) {
+    if (!cfg || !U_dev || !inv_rate || cfg->nx < 1 || cfg->ny < 1) return SPB6G_BAD_ARG;
+    for (int k = 0; k < NV; k++)
+        if (!U_dev[k]) return SPB6G_BAD_ARG;
+    const long long n = (long long)cfg->nx * cfg->ny;
+    if (n > SPB6G_NOALLOC_MAX_CELLS) {
+        fprintf(stderr, "spb6g_caldt_noalloc: %lld cells exceed the fixed scratch of %d cells\n", n,
+                (int)SPB6G_NOALLOC_MAX_CELLS);
+        return SPB6G_TOO_LARGE;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SPB6G_NO_DEVICE;
+    {
+        std::lock_guard<std::mutex> lock(g_syms_mutex);
+        NoallocSymbols& sy = g_syms[dev];
+        if (!sy.ready) {
+            if (cudaGetSymbolAddress((void**)&sy.partials, g_na_partials) != cudaSuccess ||
+                cudaGetSymbolAddress((void**)&sy.counter, g_na_counter) != cudaSuccess ||
+                cudaGetSymbolAddress((void**)&sy.result, g_na_result) != cudaSuccess) {
+                cudaGetLastError();
+                return SPB6G_CUDA_ERROR;
+            }
+            sy.ready = true;
+        }
+    }
+    const NoallocSymbols& sy = g_syms[dev];
+    cudaStream_t st = (cudaStream_t)stream;
+    Phys P{};
+    for (int k = 0; k < 2; k++) {
+        P.ph[k].g = cfg->gamma[k]; P.ph[k].pi = cfg->pinf[k]; P.ph[k].q = cfg->q[k];
+        P.ph[k].qp = cfg->qp[k]; P.ph[k].cv = cfg->cv[k]; P.ph[k].b = cfg->b[k];
+    }
+    P.share_mode = cfg->share_mode;
+    P.limiter = cfg->limiter;
+    P.rus_local = cfg->rus_local;
+    CState U;
+    for (int k = 0; k < NV; k++) U.v[k] = U_dev[k];
+    double host[2];
+    const int blocks = (int)((n + NOALLOC_THREADS - 1) / NOALLOC_THREADS);
+    if (cudaMemsetAsync(sy.counter, 0, sizeof(unsigned), st) != cudaSuccess) return SPB6G_CUDA_ERROR;
+    k_caldt_noalloc<<<blocks, NOALLOC_THREADS, 0, st>>>(P, (int)n, U, acoustic ? 1 : 0, sy.partials, sy.counter, sy.result);
+    if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
+    if (cudaMemcpyAsync(host, sy.result, sizeof host, cudaMemcpyDeviceToHost, st) != cudaSuccess) return SPB6G_CUDA_ERROR;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SPB6G_CUDA_ERROR;
+    const double dx = (cfg->x1 - cfg->x0) / cfg->nx, dy = (cfg->y1 - cfg->y0) / cfg->ny;
+    const double rate = host[0] / dx + (cfg->ny > 1 ? host[1] / dy : 0.0);
+    *inv_rate = rate > 0 ? 1.0 / rate : INFINITY;
+    return SPB6G_OK;
+}

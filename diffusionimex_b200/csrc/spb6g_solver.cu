@@ -743,6 +743,7 @@ const char* spb6g_status_string(int status) {
         case SPB6G_BAD_ARG: return "bad argument";
         case SPB6G_UNSUPPORTED: return "unsupported configuration";
         case SPB6G_NO_DEVICE: return "no CUDA device";
+        case SPB6G_TOO_LARGE: return "grid larger than the allocation-free entry point's fixed scratch";
     }
     return "unknown";
 }

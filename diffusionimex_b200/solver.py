@@ -26,6 +26,7 @@ NV = 8
 STATUS = {
     0: "ok", 1: "inadmissible state", 2: "Newton failed", 3: "BiCGStab failed", 4: "step failed after 30 halvings",
     5: "time step underflow", 6: "CUDA error", 7: "bad argument", 8: "unsupported configuration", 9: "no CUDA device",
+    10: "grid larger than the allocation-free entry point's fixed scratch",
 }
 
 
@@ -94,6 +95,7 @@ def library() -> ctypes.CDLL:
         "spb6g_region_end": (I, [P, P]),
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
+        "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -37,7 +37,8 @@ typedef enum {
     SPB6G_CUDA_ERROR = 6,
     SPB6G_BAD_ARG = 7,
     SPB6G_UNSUPPORTED = 8,
-    SPB6G_NO_DEVICE = 9
+    SPB6G_NO_DEVICE = 9,
+    SPB6G_TOO_LARGE = 10        /* grid larger than spb6g_caldt_noalloc's fixed scratch */
 } spb6g_status;
 
 enum { SPB6G_BC_TRANS = 0, SPB6G_BC_WALL = 1, SPB6G_BC_PERIODIC = 2, SPB6G_BC_PRES = 3 };
@@ -135,6 +136,25 @@ int spb6g_region_begin(spb6g_solver* s);
 int spb6g_region_end(spb6g_solver* s, double* ms);
 /* Number of kernels the handle has launched since creation. */
 int64_t spb6g_kernel_launches(spb6g_solver* s);
+
+/* Allocation-free time-step rate.  No counterpart in the reference: it is for
+ * callers that cannot let a library call cudaMalloc -- a host framework that
+ * owns all device memory through its own arena or pool, a time-critical loop
+ * that cannot afford the device-wide synchronisation cudaMalloc / cudaFree may
+ * cause, or a service whose device footprint must not grow after start-up.  Computes what spb6g_caldt computes, 1 / (a_x/dx + a_y/dy),
+ * for a state the caller already holds on the device: U_dev is a host array of
+ * 8 device pointers, one per conservative variable, each nx*ny interior cells
+ * (SoA, cell (i, j) at i + j*nx); cfg supplies the grid and phases.  The only
+ * scratch is a file-scope device array sized for SPB6G_NOALLOC_MAX_CELLS cells,
+ * held by every GPU that loads the library until the process exits; larger
+ * grids return SPB6G_TOO_LARGE.  The first call on a device looks up the
+ * scratch's device address, so make it before any stream capture.  All calls
+ * share the scratch (its counter is cleared at the start of each call): calls
+ * whose GPU work overlaps race.  stream: a cudaStream_t, or NULL for the
+ * default stream; the call returns after the result has reached *inv_rate. */
+#define SPB6G_NOALLOC_MAX_CELLS (4 * 1024 * 1024)
+int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
+                        double* inv_rate);
 
 /* Human-readable status name. */
 const char* spb6g_status_string(int status);
