@@ -13,7 +13,14 @@ struct BicgScalars {
     double tol;
     int maxit, iters, status, pad;
 };
-enum { BICG_RUNNING = 0, BICG_CONV = 1, BICG_FAIL = 2, BICG_CONV_HALF = 3 };
+enum { BICG_RUNNING = 0, BICG_CONV = 1, BICG_FAIL = 2, BICG_CONV_HALF = 3, BICG_TIMEOUT = 4 };
+
+// State of the software grid barrier of the persistent BiCGStab kernel.
+struct GridBarrier {
+    unsigned count, gen;
+    int err, pad;
+};
+constexpr int PB_THREADS = 512;  // threads (and rows per chunk) of a persistent BiCGStab block
 
 // Reduction results read back by the host after a Newton decision point.
 struct NewtonScalars {
@@ -67,6 +74,8 @@ struct Ctx {
     unsigned* counters;  // [16]
     NewtonScalars* ns;
     BicgScalars* bs_;
+    GridBarrier* gbar;  // persistent BiCGStab: barrier state (zero at start)
+    double* gpart;      // persistent BiCGStab: 5 slots x G blocks x 2 partial sums
     long long* nlaunch;  // host-side count of kernel launches (never dereferenced on the device)
 };
 
@@ -88,6 +97,9 @@ void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit);
 void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity);
 int build_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t* exec);
 void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int expected_iters);
+// persistent form: number of co-resident blocks (0 when cooperative launch is unavailable) and the launch
+int bicg_solve_blocks(int device, int n);
+int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int G);
 void launch_thomas(const Ctx& c, cudaStream_t st);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);

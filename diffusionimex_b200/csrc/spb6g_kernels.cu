@@ -732,6 +732,434 @@ void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int 
     count(c, 4 * (expected_iters + (expected_iters & 1)) + (expected_iters + 2) / 2);
 }
 
+// ============================================================ BiCGStab, persistent form
+// The whole solve (set-up and every iteration of GMRES_Solver :752-794) in one
+// cooperative launch: every block stays resident, owns the row chunks
+// blockIdx.x, blockIdx.x + G, ... (PB_THREADS rows each) for the whole solve, and
+// the four passes of an iteration are separated by a software grid barrier.
+// Each barrier carries one reduction: blocks publish their partial sums, and
+// after the barrier every block folds all G partials in block order, so every
+// block holds bit-identical scalars without a further round trip.  The
+// arithmetic per row is the one of the four-pass kernels above.
+constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 21;  // polls of >= 0.3 us each: gives up after about a second
+
+SPB6G_DEV unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+SPB6G_DEV int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+// Sense-counting grid barrier.  Thread 0 of each block arrives with a release
+// add on the counter; the last arrival resets the counter and bumps the
+// generation; the others poll the generation with acquire loads.  The wait is
+// bounded: past BARRIER_SPIN_LIMIT polls (or once another block has given up)
+// the block records the failure and the barrier returns false in every thread.
+SPB6G_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned gen = ld_acquire_gpu(&gb->gen);
+        unsigned old;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&gb->count) : "memory");
+        if (old == nblocks - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&gb->count) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->gen) : "memory");
+        } else {
+            unsigned it = 0;
+            while (ld_acquire_gpu(&gb->gen) == gen) {
+                if (++it > BARRIER_SPIN_LIMIT || ld_relaxed_gpu(&gb->err)) {
+                    atomicExch(&gb->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Publishes this block's two partial sums, waits for every block, and folds
+// all G records in block order; `tot` is the same in every thread of every block.
+SPB6G_DEV bool sync_fold(double (&acc)[2], double* slot, unsigned G, GridBarrier* gb, double (&tot)[2]) {
+    __shared__ double sh[2 * 32];
+    __shared__ double bc[2];
+    block_fold<RedSum, 2>(acc, sh);
+    if (threadIdx.x == 0) {
+        slot[2 * blockIdx.x] = acc[0];
+        slot[2 * blockIdx.x + 1] = acc[1];
+    }
+    if (!grid_barrier(gb, G)) return false;
+    double f[2] = {0.0, 0.0};
+    for (unsigned b = threadIdx.x; b < G; b += blockDim.x) {
+        f[0] += __ldcg(slot + 2 * b);
+        f[1] += __ldcg(slot + 2 * b + 1);
+    }
+    block_fold<RedSum, 2>(f, sh);
+    if (threadIdx.x == 0) { bc[0] = f[0]; bc[1] = f[1]; }
+    __syncthreads();
+    tot[0] = bc[0];
+    tot[1] = bc[1];
+    return true;
+}
+
+// Work unit of the persistent passes: a strip of 32 columns x J rows owned by one
+// warp for the whole solve.  Lane l holds column i0 + l and walks the rows
+// upward; west / east neighbours come from the row's values in shared memory,
+// south / north ones from the rows below and above, which the walk loads anyway.
+// Rows arrive through a PS_D-deep cp.async pipeline (loads for row t + PS_D - 1
+// are in flight while row t is used), so each warp keeps several rows of every
+// operand in flight instead of one.
+constexpr int PB_WARPS = PB_THREADS / 32;
+constexpr int PS_D = 4;                           // rows in flight per warp
+constexpr int PS_HV = 4;                          // operands needed at the neighbours (34 columns)
+constexpr int PS_RV = 6;                          // operands needed at the row itself (32 columns)
+constexpr int PS_STAGE = PS_HV * 34 + PS_RV * 32;  // doubles per row stage
+constexpr int PS_WARP = PS_D * PS_STAGE + 3 * 34;  // + three rows of scaled stencil values
+constexpr size_t PB_SMEM = (size_t)PB_WARPS * PS_WARP * sizeof(double);
+
+struct Strip {
+    int i0, j0, J;
+};
+struct StripGrid {
+    int ncols, J, nstrips;
+};
+SPB6G_DEV StripGrid strip_grid(const Geom& g, int warps) {
+    StripGrid s;
+    s.ncols = (g.nx + 31) / 32;
+    const long cells = (long)g.ny * s.ncols;
+    s.J = (int)((cells + warps - 1) / warps);
+    if (s.J < 1) s.J = 1;
+    s.nstrips = s.ncols * ((g.ny + s.J - 1) / s.J);
+    return s;
+}
+SPB6G_DEV Strip strip_at(const Geom& g, const StripGrid& sg, int s) {
+    Strip st;
+    st.i0 = (s % sg.ncols) * 32;
+    st.j0 = (s / sg.ncols) * sg.J;
+    st.J = min(sg.J, g.ny - st.j0);
+    return st;
+}
+// Column / row of the pressure-unknown map M_P (mp_index is separable); columns
+// beyond the east neighbour of the last cell are never used and read column 0.
+SPB6G_DEV int map_col(const Geom& g, int i) {
+    if (i < -1 || i > g.nx) return 0;
+    const bool xp = g.bcs[0] == BC_PERIODIC;
+    if (i < 0) return xp ? g.nx + i : 0;
+    if (i > g.nx - 1) return xp ? i - g.nx : g.nx - 1;
+    return i;
+}
+SPB6G_DEV int map_row(const Geom& g, int j) {
+    const bool yp = g.bcs[2] == BC_PERIODIC && g.ny > 1;
+    if (j < 0) return yp ? g.ny + j : 0;
+    if (j > g.ny - 1) return yp ? j - g.ny : g.ny - 1;
+    return j;
+}
+SPB6G_DEV void cp_async8(double* s, const double* gp) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)), "l"(gp) : "memory");
+}
+SPB6G_DEV void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+SPB6G_DEV void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Five-point pass over one strip.  hv: the PS_HV operands of the scaled stencil
+// value ph(k) (rows j0-1 .. j0+J, columns i0-1 .. i0+32, boundary-mapped);
+// rv: NRV operands read at the row itself.  phf(stage, col) gives ph from a row
+// stage; out(stage, col, phS, phW, phC, phE, phN, x) consumes a row.
+template <int NRV, class PH, class OUT>
+SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const double* const (&hv)[PS_HV],
+                             const double* const (&rv)[NRV], PH phf, OUT out) {
+    const int lane = threadIdx.x & 31;
+    const int nload = st.J + 2;
+    double* stages = ws;
+    double* phr = ws + PS_D * PS_STAGE;
+    const int ic_own = map_col(g, st.i0 + lane);
+    const int ic_halo = lane == 0 ? map_col(g, st.i0 - 1) : map_col(g, st.i0 + 32);
+    const bool own = st.i0 + lane < g.nx;
+    auto issue = [&](int t) {
+        if (t < nload) {
+            double* sp = stages + (t % PS_D) * PS_STAGE;
+            const size_t rb = (size_t)map_row(g, st.j0 - 1 + t) * g.nx;
+#pragma unroll
+            for (int v = 0; v < PS_HV; v++) cp_async8(sp + v * 34 + lane + 1, hv[v] + rb + ic_own);
+            if (lane < 2) {
+#pragma unroll
+                for (int v = 0; v < PS_HV; v++) cp_async8(sp + v * 34 + (lane ? 33 : 0), hv[v] + rb + ic_halo);
+            }
+            if (own && t >= 1 && t <= st.J) {
+#pragma unroll
+                for (int v = 0; v < NRV; v++) cp_async8(sp + PS_HV * 34 + v * 32 + lane, rv[v] + rb + ic_own);
+            }
+        }
+        cp_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < PS_D - 1; t++) issue(t);
+    for (int t = 0; t < nload; t++) {
+        cp_wait<PS_D - 2>();
+        __syncwarp();
+        const double* sp = stages + (t % PS_D) * PS_STAGE;
+        double* pr = phr + (t % 3) * 34;
+        pr[lane + 1] = phf(sp, lane + 1);
+        if (lane < 2) pr[lane ? 33 : 0] = phf(sp, lane ? 33 : 0);
+        __syncwarp();
+        if (t >= 2 && own) {
+            const double* so = stages + ((t - 1) % PS_D) * PS_STAGE;
+            const double* pS = phr + ((t - 2) % 3) * 34;
+            const double* pC = phr + ((t - 1) % 3) * 34;
+            out(so, lane + 1, pS[lane + 1], pC[lane], pC[lane + 1], pC[lane + 2], pr[lane + 1],
+                (st.j0 + t - 2) * g.nx + st.i0 + lane);
+        }
+        __syncwarp();
+        issue(t + PS_D - 1);
+    }
+    cp_wait<0>();
+    __syncwarp();
+}
+// Row-local pass over one strip: NRV operands of each own cell through the same pipeline.
+template <int NRV, class OUT>
+SPB6G_DEV void row_strip(const Geom& g, const Strip& st, double* ws, const double* const (&rv)[NRV], OUT out) {
+    const int lane = threadIdx.x & 31;
+    const bool own = st.i0 + lane < g.nx;
+    auto issue = [&](int t) {
+        if (t < st.J && own) {
+            double* sp = ws + (t % PS_D) * PS_STAGE;
+            const size_t x = (size_t)(st.j0 + t) * g.nx + st.i0 + lane;
+#pragma unroll
+            for (int v = 0; v < NRV; v++) cp_async8(sp + v * 32 + lane, rv[v] + x);
+        }
+        cp_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < PS_D - 1; t++) issue(t);
+    for (int t = 0; t < st.J; t++) {
+        cp_wait<PS_D - 2>();
+        __syncwarp();
+        if (own) out(ws + (t % PS_D) * PS_STAGE, lane, (st.j0 + t) * g.nx + st.i0 + lane);
+        __syncwarp();
+        issue(t + PS_D - 1);
+    }
+    cp_wait<0>();
+    __syncwarp();
+}
+
+#define PB_STRIPS_BEGIN                                                         \
+    for (int s_ = wid; s_ < sg.nstrips; s_ += nwarps) {                         \
+        const Strip st = strip_at(c.g, sg, s_);
+#define PB_STRIPS_END }
+
+__global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol, int maxit) {
+    extern __shared__ double pb_smem[];
+    const int n = c.n, nx = c.g.nx;
+    const unsigned G = gridDim.x;
+    const int nwarps = G * PB_WARPS, wid = blockIdx.x * PB_WARPS + (threadIdx.x >> 5);
+    double* ws = pb_smem + (threadIdx.x >> 5) * PS_WARP;
+    const StripGrid sg = strip_grid(c.g, nwarps);
+    const bool two_d = c.g.ny > 1;
+    GridBarrier* gb = c.gbar;
+    double* slots = c.gpart;  // 5 slots of G records of 2
+    const double* __restrict__ dinv = c.dinv;
+    const double* __restrict__ A1 = c.A1;
+    double* __restrict__ br = c.br;
+    double* __restrict__ bv = c.bv;
+    double* __restrict__ bq = c.bq;
+    double* __restrict__ bs = c.bs;
+    double* __restrict__ bu = c.bu;
+    double* __restrict__ bt = c.bt;
+    double* __restrict__ dP = c.dP;
+
+    const NewtonScalars ns = *c.ns;
+    const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
+    const double cb = ns.sumb * Einv;
+    double acc[2], tot[2];
+    // set-up: x = M^-1 b, r = r0 = b - A x, p = v = 0 (plain row loop, once per solve)
+    acc[0] = acc[1] = 0.0;
+    for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
+        const int j = x / nx, i = x - j * nx;
+        const Nbr nb = neighbours(c.g, i, j, x);
+        auto xv = [&](int q) { return dinv[q] * (-c.G[q]) + cb; };
+        const double Ax = spmv_row(c, nb, x, xv);
+        const double r = -c.G[x] - Ax;
+        dP[x] = xv(x);
+        br[x] = r;
+        c.br0[x] = r;
+        c.bp[x] = 0.0;
+        bv[x] = 0.0;
+        acc[0] += r * r;
+        acc[1] += r * A1[x];
+    }
+    if (!sync_fold(acc, slots, G, gb, tot)) goto timeout;
+    {
+        double rho = 1.0, alpha = 1.0, omega = 1.0, cc = 0.0, cs = 0.0, ss = 0.0, ts = 0.0, tt = 0.0;
+        const double bn = sqrt(ns.bb) + 1e-300;
+        double rr = tot[0], r0r = tot[0];
+        const double r0A1 = tot[1];
+        int status = ns.fail ? BICG_FAIL : (sqrt(rr) <= tol * bn ? BICG_CONV : (r0r == 0 ? BICG_FAIL : BICG_RUNNING));
+        int iters = 0, parity = 0;
+        while (status == BICG_RUNNING) {
+            const double* p_old = parity ? c.tcp : c.bp;
+            double* p_new = parity ? c.bp : c.tcp;
+            // pass 1: p = r + beta (p - omega v); q = A D^-1 p; sums 1^T p, r0^T q
+            {
+                const double beta = (r0r / rho) * (alpha / omega), om = omega;
+                const double* const hv[PS_HV] = {br, p_old, bv, dinv};
+                const double* const rv[6] = {c.aC, c.aW, c.aE, c.aS, c.aN, c.br0};
+                auto pn = [&](const double* sp, int k) { return sp[k] + beta * (sp[34 + k] - om * sp[68 + k]); };
+                auto phf = [&](const double* sp, int k) { return sp[102 + k] * pn(sp, k); };
+                acc[0] = acc[1] = 0.0;
+                PB_STRIPS_BEGIN
+                    stencil_strip<6>(c.g, st, ws, hv, rv, phf,
+                        [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
+                            const double* a = so + PS_HV * 34 + (k - 1);
+                            const double p = pn(so, k);
+                            double q = 0;
+                            q += a[0] * phC;
+                            q += a[32] * phW;
+                            q += a[64] * phE;
+                            if (two_d) {
+                                q += a[96] * phS;
+                                q += a[128] * phN;
+                            }
+                            p_new[x] = p;
+                            bq[x] = q;
+                            acc[0] += p;
+                            acc[1] += a[160] * q;
+                        });
+                PB_STRIPS_END
+            }
+            if (!sync_fold(acc, slots + 2 * G, G, gb, tot)) goto timeout;
+            rho = r0r;
+            cc = tot[0] * Einv;
+            alpha = rho / (tot[1] + cc * r0A1);
+            // pass 2: v = q + cc A1; s = r - alpha v; u = A D^-1 s; sums s^T s, 1^T s
+            {
+                const double al = alpha, ccv = cc;
+                const double* const hv[PS_HV] = {br, bq, A1, dinv};
+                const double* const rv[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
+                auto sv = [&](const double* sp, int k) { return sp[k] - al * (sp[34 + k] + ccv * sp[68 + k]); };
+                auto phf = [&](const double* sp, int k) { return sp[102 + k] * sv(sp, k); };
+                acc[0] = acc[1] = 0.0;
+                PB_STRIPS_BEGIN
+                    stencil_strip<5>(c.g, st, ws, hv, rv, phf,
+                        [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
+                            const double* a = so + PS_HV * 34 + (k - 1);
+                            const double v = so[34 + k] + ccv * so[68 + k];
+                            const double s = so[k] - al * v;
+                            double u = 0;
+                            u += a[0] * phC;
+                            u += a[32] * phW;
+                            u += a[64] * phE;
+                            if (two_d) {
+                                u += a[96] * phS;
+                                u += a[128] * phN;
+                            }
+                            bv[x] = v;
+                            bs[x] = s;
+                            bu[x] = u;
+                            acc[0] += s * s;
+                            acc[1] += s;
+                        });
+                PB_STRIPS_END
+            }
+            if (!sync_fold(acc, slots + 4 * G, G, gb, tot)) goto timeout;
+            ss = tot[0];
+            cs = tot[1] * Einv;
+            const bool half = sqrt(ss) <= tol * bn;
+            if (!half) {
+                // pass 3: t = u + cs A1; sums t^T s, t^T t
+                const double csv = cs;
+                const double* const rv[3] = {bu, A1, bs};
+                acc[0] = acc[1] = 0.0;
+                PB_STRIPS_BEGIN
+                    row_strip<3>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
+                        const double t = sp[k] + csv * sp[32 + k];
+                        bt[x] = t;
+                        acc[0] += t * sp[64 + k];
+                        acc[1] += t * t;
+                    });
+                PB_STRIPS_END
+                if (!sync_fold(acc, slots + 6 * G, G, gb, tot)) goto timeout;
+                ts = tot[0];
+                tt = tot[1];
+                omega = ts / tt;
+            }
+            // pass 4: x += alpha ph + omega sh; r = s - omega t; sums r^T r, r0^T r
+            acc[0] = acc[1] = 0.0;
+            if (half) {
+                const double al = alpha, ccv = cc;
+                const double* const rv[3] = {dinv, p_new, dP};
+                PB_STRIPS_BEGIN
+                    row_strip<3>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
+                        const double ph = sp[k] * sp[32 + k] + ccv;
+                        dP[x] = sp[64 + k] + al * ph;
+                    });
+                PB_STRIPS_END
+            } else {
+                const double al = alpha, om = omega, ccv = cc, csv = cs;
+                const double* const rv[6] = {dinv, p_new, bs, bt, dP, c.br0};
+                PB_STRIPS_BEGIN
+                    row_strip<6>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
+                        const double ph = sp[k] * sp[32 + k] + ccv;
+                        const double sh = sp[k] * sp[64 + k] + csv;
+                        dP[x] = sp[128 + k] + (al * ph + om * sh);
+                        const double r = sp[64 + k] - om * sp[96 + k];
+                        br[x] = r;
+                        acc[0] += r * r;
+                        acc[1] += sp[160 + k] * r;
+                    });
+                PB_STRIPS_END
+            }
+            iters += 1;
+            if (half) { status = BICG_CONV; break; }
+            if (!sync_fold(acc, slots + 8 * G, G, gb, tot)) goto timeout;
+            rr = tot[0];
+            r0r = tot[1];
+            if (sqrt(rr) <= tol * bn) status = BICG_CONV;
+            else if (iters >= maxit) status = sqrt(rr) <= 1e3 * tol * bn ? BICG_CONV : BICG_FAIL;
+            else if (r0r == 0) status = BICG_FAIL;
+            else if (!isfinite(rr)) status = BICG_FAIL;  // NaN never converges; the reference loops to GMRESiter and fails
+            parity ^= 1;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            BicgScalars& B = *c.bs_;
+            B.rho = rho; B.alpha = alpha; B.omega = omega; B.bn = bn; B.Einv = Einv; B.cb = cb;
+            B.r0A1 = r0A1; B.cc = cc; B.cs = cs; B.rr = rr; B.r0r = r0r; B.ts = ts; B.tt = tt; B.ss = ss;
+            B.tol = tol; B.maxit = maxit; B.iters = iters; B.status = status;
+        }
+        return;
+    }
+timeout:
+    if (threadIdx.x == 0) c.bs_->status = BICG_TIMEOUT;
+}
+#undef PB_STRIPS_BEGIN
+#undef PB_STRIPS_END
+
+int bicg_solve_blocks(int device, int n) {
+    int per_sm = 0, sms = 0, coop = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_bicg_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicg_solve, PB_THREADS, PB_SMEM) != cudaSuccess) return 0;
+    // about four rows per thread at least: small grids use fewer blocks (cheaper barriers)
+    const long want = ((long)n + 4L * PB_THREADS - 1) / (4L * PB_THREADS);
+    long G = (long)per_sm * sms;
+    if (G > want) G = want;
+    return G > 0 ? (int)G : 0;
+}
+int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int G) {
+    void* args[] = {(void*)&c, (void*)&tol, (void*)&maxit};
+    count(c, 1);
+    return cudaLaunchCooperativeKernel((const void*)k_bicg_solve, dim3(G), dim3(PB_THREADS), args, PB_SMEM, st) == cudaSuccess ? 0 : -1;
+}
+
 // ============================================================ Thomas (1D non-periodic, :858-863)
 __global__ void k_thomas(Ctx c) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;

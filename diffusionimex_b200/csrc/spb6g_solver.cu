@@ -57,6 +57,7 @@ struct spb6g_solver {
     int64_t tcnt[TG_COUNT] = {};
     cudaEvent_t region[2] = {nullptr, nullptr};
     long long nlaunch = 0;
+    int bicg_G = 0;                       // blocks of the persistent BiCGStab launch (0: not available)
     cudaGraphExec_t bicg_exec = nullptr;  // device-side BiCGStab loop (built once per solver)
     cudaStream_t st2 = nullptr;           // side stream: shock budget, overlapped with the stage prep
     cudaEvent_t ev_flux = nullptr, ev_shock = nullptr;
@@ -222,6 +223,16 @@ int newton(spb6g_solver* s, double& resfinal) {
         } else {
             if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
             if (s->pin->ns.fail) { tend_(s, TG_LINEAR); return SPB6G_NEWTON_FAIL; }
+            if (s->bicg_G > 0) {  // the whole solve in one persistent launch
+                CK(cudaMemsetAsync(c.gbar, 0, sizeof(GridBarrier), s->st));
+                if (launch_bicg_solve(c, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter, s->bicg_G) != 0) return SPB6G_CUDA_ERROR;
+                if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
+                if (s->pin->bs.status == BICG_TIMEOUT) {  // a grid barrier gave up (blocks not co-resident)
+                    fprintf(stderr, "spb6g: BiCGStab grid barrier timed out\n");
+                    tend_(s, TG_LINEAR);
+                    return SPB6G_CUDA_ERROR;
+                }
+            } else {
             launch_bicg_init(c, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter);
             s->bicg_parity = 0;
             if (s->bicg_exec) {
@@ -235,6 +246,7 @@ int newton(spb6g_solver* s, double& resfinal) {
                     if (s->pin->bs.status != BICG_RUNNING) break;
                     if (chunk < 32) chunk *= 2;
                 }
+            }
             }
             s->last_bicg_iters = s->pin->bs.iters;
             s->stats.bicg_it += s->pin->bs.iters;
@@ -476,6 +488,9 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.counters = (unsigned*)A(16);
     c.ns = (NewtonScalars*)A(sizeof(NewtonScalars) / sizeof(double) + 1);
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
+    c.gbar = (GridBarrier*)A(sizeof(GridBarrier) / sizeof(double) + 1);
+    if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC)) s->bicg_G = bicg_solve_blocks(cfg->device, (int)n);
+    c.gpart = A(10 * (size_t)(s->bicg_G > 0 ? s->bicg_G : 1));
     if (ok && cudaMallocHost((void**)&s->pin, sizeof(Pinned)) != cudaSuccess) ok = false;
     if (ok)
         for (int e = 0; e < 2; e++)
@@ -483,7 +498,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.nlaunch = &s->nlaunch;
     c.p_ref = 0;
     if (!ok || cudaStreamSynchronize(s->st) != cudaSuccess) { spb6g_destroy(s); return SPB6G_CUDA_ERROR; }
-    if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC)) {  // BiCGStab path: capture its device-side loop
+    if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC) && s->bicg_G == 0) {  // no cooperative launch: capture the loop as a graph
         if (build_bicg_graph(c, s->st, &s->bicg_exec) != 0) {
             s->bicg_exec = nullptr;
             cudaGetLastError();
