@@ -44,7 +44,9 @@ ALG_BYTES = {
     "explicit": (8 + 8 + 2 + 2 + 16 + 1 + 8) * 8 + 4 * 8,
     "jacobian": (9 + 5 + 2 + 10 + 2 + 1 + 1 + 1 + 1 + 7) * 8,  # X*,a2s | Qe vol | phi | faces | v* | qph | kw | P | G | sc | A,A1,dinv
     "residual": (9 + 5 + 2 + 10 + 2 + 2 + 1 + 1 + 1) * 8,       # ... + P, G, sc
-    "linear": 272,                                            # per BiCGStab iteration (4 passes), x iterations
+    # per BiCGStab iteration: pass 1 reads r, p, v, D^-1, 5 diagonals, r0 and writes p, q; pass 2 reads
+    # r, q, A1, D^-1, 5 diagonals and writes v, s, t; pass 3 reads D^-1, p, s, t, x, r0 and writes x, r
+    "linear": (12 + 12 + 8) * 8,
 }
 
 

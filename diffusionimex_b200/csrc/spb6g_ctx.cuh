@@ -75,7 +75,7 @@ struct Ctx {
     NewtonScalars* ns;
     BicgScalars* bs_;
     GridBarrier* gbar;  // persistent BiCGStab: barrier state (zero at start)
-    double* gpart;      // persistent BiCGStab: 5 slots x G blocks x 2 partial sums
+    double* gpart;      // persistent BiCGStab: 2 slots x G blocks x 4 partial sums
     long long* nlaunch;  // host-side count of kernel launches (never dereferenced on the device)
 };
 

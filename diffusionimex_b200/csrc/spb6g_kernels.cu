@@ -753,62 +753,63 @@ SPB6G_DEV int ld_relaxed_gpu(const int* p) {
     asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-// Sense-counting grid barrier.  Thread 0 of each block arrives with a release
-// add on the counter; the last arrival resets the counter and bumps the
-// generation; the others poll the generation with acquire loads.  The wait is
-// bounded: past BARRIER_SPIN_LIMIT polls (or once another block has given up)
-// the block records the failure and the barrier returns false in every thread.
-SPB6G_DEV bool grid_barrier(GridBarrier* gb, unsigned nblocks) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned gen = ld_acquire_gpu(&gb->gen);
-        unsigned old;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(&gb->count) : "memory");
-        if (old == nblocks - 1) {
-            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(&gb->count) : "memory");
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->gen) : "memory");
-        } else {
-            unsigned it = 0;
-            while (ld_acquire_gpu(&gb->gen) == gen) {
-                if (++it > BARRIER_SPIN_LIMIT || ld_relaxed_gpu(&gb->err)) {
-                    atomicExch(&gb->err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
+// Grid barrier on a monotone arrival counter: thread 0 of every block adds 1
+// with release semantics, and barrier number e of a launch is complete once the
+// counter reaches e * G (acquire polls).  The counter is cleared before every
+// launch.  The wait is bounded: past BARRIER_SPIN_LIMIT polls, or once another
+// block has given up, the block records the failure and returns false.
+SPB6G_DEV bool barrier_arrive_wait(GridBarrier* gb, unsigned target) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->count) : "memory");
+    unsigned it = 0;
+    while (ld_acquire_gpu(&gb->count) < target) {
+        if (++it > BARRIER_SPIN_LIMIT || ld_relaxed_gpu(&gb->err)) {
+            atomicExch(&gb->err, 1);
+            return false;
         }
-        __threadfence();
-        s_ok = ok;
     }
-    __syncthreads();
-    return s_ok != 0;
+    return true;
 }
 
-// Publishes this block's two partial sums, waits for every block, and folds
-// all G records in block order; `tot` is the same in every thread of every block.
-SPB6G_DEV bool sync_fold(double (&acc)[2], double* slot, unsigned G, GridBarrier* gb, double (&tot)[2]) {
-    __shared__ double sh[2 * 32];
-    __shared__ double bc[2];
-    block_fold<RedSum, 2>(acc, sh);
-    if (threadIdx.x == 0) {
-        slot[2 * blockIdx.x] = acc[0];
-        slot[2 * blockIdx.x + 1] = acc[1];
+// Publishes this block's NQ partial sums (records of 4), waits for every block,
+// and folds all G records in block order in warp 0; `tot` is then the same in
+// every thread of every block.  `epoch` counts the barriers of the launch.
+template <int NQ>
+SPB6G_DEV bool sync_fold(double (&acc)[NQ], double* slot, unsigned G, GridBarrier* gb, unsigned& epoch, double (&tot)[NQ]) {
+    __shared__ double sh[4 * 32];
+    __shared__ double bc[4];
+    __shared__ int s_ok;
+    block_fold<RedSum, NQ>(acc, sh);
+    epoch += 1;
+    if (threadIdx.x < 32) {
+        int ok = 1;
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++) slot[4 * blockIdx.x + q] = acc[q];
+            ok = barrier_arrive_wait(gb, epoch * G) ? 1 : 0;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (ok) {
+            double f[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; q++) f[q] = 0.0;
+            for (unsigned b = threadIdx.x; b < G; b += 32) {
+#pragma unroll
+                for (int q = 0; q < NQ; q++) f[q] += __ldcg(slot + 4 * b + q);
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; q++) f[q] = warp_fold<RedSum>(f[q]);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; q++) bc[q] = f[q];
+            }
+        }
+        if (threadIdx.x == 0) s_ok = ok;
     }
-    if (!grid_barrier(gb, G)) return false;
-    double f[2] = {0.0, 0.0};
-    for (unsigned b = threadIdx.x; b < G; b += blockDim.x) {
-        f[0] += __ldcg(slot + 2 * b);
-        f[1] += __ldcg(slot + 2 * b + 1);
-    }
-    block_fold<RedSum, 2>(f, sh);
-    if (threadIdx.x == 0) { bc[0] = f[0]; bc[1] = f[1]; }
     __syncthreads();
-    tot[0] = bc[0];
-    tot[1] = bc[1];
-    return true;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) tot[q] = bc[q];
+    return s_ok != 0;
 }
 
 // Work unit of the persistent passes: a strip of 32 columns x J rows owned by one
@@ -956,6 +957,12 @@ SPB6G_DEV void row_strip(const Geom& g, const Strip& st, double* ws, const doubl
         const Strip st = strip_at(c.g, sg, s_);
 #define PB_STRIPS_END }
 
+// Three passes per iteration.  Besides the A 1 trick of the four-pass kernels
+// (A M^-1 r = A (D^-1 r) + (1^T r / E) A 1), the coarse coefficient of s is
+// formed from sums the first barrier already carries: 1^T s = 1^T r - alpha 1^T v
+// with 1^T v = 1^T q + cc 1^T A1, so t = A M^-1 s and its two inner products are
+// finished in the same pass as s (the reference sums s itself; the identity is
+// exact, the rounding of this one scalar differs).
 __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol, int maxit) {
     extern __shared__ double pb_smem[];
     const int n = c.n, nx = c.g.nx;
@@ -965,23 +972,23 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     const StripGrid sg = strip_grid(c.g, nwarps);
     const bool two_d = c.g.ny > 1;
     GridBarrier* gb = c.gbar;
-    double* slots = c.gpart;  // 5 slots of G records of 2
+    unsigned epoch = 0;
+    double* slots = c.gpart;  // G records of 4 per barrier, two barriers apart
     const double* __restrict__ dinv = c.dinv;
     const double* __restrict__ A1 = c.A1;
     double* __restrict__ br = c.br;
     double* __restrict__ bv = c.bv;
     double* __restrict__ bq = c.bq;
     double* __restrict__ bs = c.bs;
-    double* __restrict__ bu = c.bu;
     double* __restrict__ bt = c.bt;
     double* __restrict__ dP = c.dP;
+    auto slot = [&](int k) { return slots + (size_t)(k & 1) * 4 * G; };
 
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
     const double cb = ns.sumb * Einv;
-    double acc[2], tot[2];
     // set-up: x = M^-1 b, r = r0 = b - A x, p = v = 0 (plain row loop, once per solve)
-    acc[0] = acc[1] = 0.0;
+    double a4[4] = {0.0, 0.0, 0.0, 0.0}, t4[4];
     for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
         const int j = x / nx, i = x - j * nx;
         const Nbr nb = neighbours(c.g, i, j, x);
@@ -993,28 +1000,31 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
         c.br0[x] = r;
         c.bp[x] = 0.0;
         bv[x] = 0.0;
-        acc[0] += r * r;
-        acc[1] += r * A1[x];
+        a4[0] += r * r;
+        a4[1] += r * A1[x];
+        a4[2] += r;
+        a4[3] += A1[x];
     }
-    if (!sync_fold(acc, slots, G, gb, tot)) goto timeout;
+    if (!sync_fold<4>(a4, slot(0), G, gb, epoch, t4)) goto timeout;
     {
         double rho = 1.0, alpha = 1.0, omega = 1.0, cc = 0.0, cs = 0.0, ss = 0.0, ts = 0.0, tt = 0.0;
         const double bn = sqrt(ns.bb) + 1e-300;
-        double rr = tot[0], r0r = tot[0];
-        const double r0A1 = tot[1];
+        double rr = t4[0], r0r = t4[0], sr = t4[2];
+        const double r0A1 = t4[1], sA1 = t4[3];
         int status = ns.fail ? BICG_FAIL : (sqrt(rr) <= tol * bn ? BICG_CONV : (r0r == 0 ? BICG_FAIL : BICG_RUNNING));
-        int iters = 0, parity = 0;
+        int iters = 0, parity = 0, bar = 1;
+        double a3[3], t3[3];
         while (status == BICG_RUNNING) {
             const double* p_old = parity ? c.tcp : c.bp;
             double* p_new = parity ? c.bp : c.tcp;
-            // pass 1: p = r + beta (p - omega v); q = A D^-1 p; sums 1^T p, r0^T q
+            // pass 1: p = r + beta (p - omega v); q = A D^-1 p; sums 1^T p, r0^T q, 1^T q
             {
                 const double beta = (r0r / rho) * (alpha / omega), om = omega;
                 const double* const hv[PS_HV] = {br, p_old, bv, dinv};
                 const double* const rv[6] = {c.aC, c.aW, c.aE, c.aS, c.aN, c.br0};
                 auto pn = [&](const double* sp, int k) { return sp[k] + beta * (sp[34 + k] - om * sp[68 + k]); };
                 auto phf = [&](const double* sp, int k) { return sp[102 + k] * pn(sp, k); };
-                acc[0] = acc[1] = 0.0;
+                a3[0] = a3[1] = a3[2] = 0.0;
                 PB_STRIPS_BEGIN
                     stencil_strip<6>(c.g, st, ws, hv, rv, phf,
                         [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
@@ -1030,23 +1040,25 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
                             }
                             p_new[x] = p;
                             bq[x] = q;
-                            acc[0] += p;
-                            acc[1] += a[160] * q;
+                            a3[0] += p;
+                            a3[1] += a[160] * q;
+                            a3[2] += q;
                         });
                 PB_STRIPS_END
             }
-            if (!sync_fold(acc, slots + 2 * G, G, gb, tot)) goto timeout;
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
             rho = r0r;
-            cc = tot[0] * Einv;
-            alpha = rho / (tot[1] + cc * r0A1);
-            // pass 2: v = q + cc A1; s = r - alpha v; u = A D^-1 s; sums s^T s, 1^T s
+            cc = t3[0] * Einv;
+            alpha = rho / (t3[1] + cc * r0A1);
+            cs = (sr - alpha * (t3[2] + cc * sA1)) * Einv;
+            // pass 2: v = q + cc A1; s = r - alpha v; t = A D^-1 s + cs A1; sums s^T s, t^T s, t^T t
             {
-                const double al = alpha, ccv = cc;
+                const double al = alpha, ccv = cc, csv = cs;
                 const double* const hv[PS_HV] = {br, bq, A1, dinv};
                 const double* const rv[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
                 auto sv = [&](const double* sp, int k) { return sp[k] - al * (sp[34 + k] + ccv * sp[68 + k]); };
                 auto phf = [&](const double* sp, int k) { return sp[102 + k] * sv(sp, k); };
-                acc[0] = acc[1] = 0.0;
+                a3[0] = a3[1] = a3[2] = 0.0;
                 PB_STRIPS_BEGIN
                     stencil_strip<5>(c.g, st, ws, hv, rv, phf,
                         [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
@@ -1061,38 +1073,26 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
                                 u += a[96] * phS;
                                 u += a[128] * phN;
                             }
+                            const double tv = u + csv * so[68 + k];
                             bv[x] = v;
                             bs[x] = s;
-                            bu[x] = u;
-                            acc[0] += s * s;
-                            acc[1] += s;
+                            bt[x] = tv;
+                            a3[0] += s * s;
+                            a3[1] += tv * s;
+                            a3[2] += tv * tv;
                         });
                 PB_STRIPS_END
             }
-            if (!sync_fold(acc, slots + 4 * G, G, gb, tot)) goto timeout;
-            ss = tot[0];
-            cs = tot[1] * Einv;
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
+            ss = t3[0];
             const bool half = sqrt(ss) <= tol * bn;
             if (!half) {
-                // pass 3: t = u + cs A1; sums t^T s, t^T t
-                const double csv = cs;
-                const double* const rv[3] = {bu, A1, bs};
-                acc[0] = acc[1] = 0.0;
-                PB_STRIPS_BEGIN
-                    row_strip<3>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
-                        const double t = sp[k] + csv * sp[32 + k];
-                        bt[x] = t;
-                        acc[0] += t * sp[64 + k];
-                        acc[1] += t * t;
-                    });
-                PB_STRIPS_END
-                if (!sync_fold(acc, slots + 6 * G, G, gb, tot)) goto timeout;
-                ts = tot[0];
-                tt = tot[1];
+                ts = t3[1];
+                tt = t3[2];
                 omega = ts / tt;
             }
-            // pass 4: x += alpha ph + omega sh; r = s - omega t; sums r^T r, r0^T r
-            acc[0] = acc[1] = 0.0;
+            // pass 3: x += alpha ph + omega sh; r = s - omega t; sums r^T r, r0^T r, 1^T r
+            a3[0] = a3[1] = a3[2] = 0.0;
             if (half) {
                 const double al = alpha, ccv = cc;
                 const double* const rv[3] = {dinv, p_new, dP};
@@ -1112,16 +1112,18 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
                         dP[x] = sp[128 + k] + (al * ph + om * sh);
                         const double r = sp[64 + k] - om * sp[96 + k];
                         br[x] = r;
-                        acc[0] += r * r;
-                        acc[1] += sp[160 + k] * r;
+                        a3[0] += r * r;
+                        a3[1] += sp[160 + k] * r;
+                        a3[2] += r;
                     });
                 PB_STRIPS_END
             }
             iters += 1;
             if (half) { status = BICG_CONV; break; }
-            if (!sync_fold(acc, slots + 8 * G, G, gb, tot)) goto timeout;
-            rr = tot[0];
-            r0r = tot[1];
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
+            rr = t3[0];
+            r0r = t3[1];
+            sr = t3[2];
             if (sqrt(rr) <= tol * bn) status = BICG_CONV;
             else if (iters >= maxit) status = sqrt(rr) <= 1e3 * tol * bn ? BICG_CONV : BICG_FAIL;
             else if (r0r == 0) status = BICG_FAIL;

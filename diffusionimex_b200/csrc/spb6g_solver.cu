@@ -490,7 +490,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
     c.gbar = (GridBarrier*)A(sizeof(GridBarrier) / sizeof(double) + 1);
     if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC)) s->bicg_G = bicg_solve_blocks(cfg->device, (int)n);
-    c.gpart = A(10 * (size_t)(s->bicg_G > 0 ? s->bicg_G : 1));
+    c.gpart = A(8 * (size_t)(s->bicg_G > 0 ? s->bicg_G : 1));
     if (ok && cudaMallocHost((void**)&s->pin, sizeof(Pinned)) != cudaSuccess) ok = false;
     if (ok)
         for (int e = 0; e < 2; e++)
