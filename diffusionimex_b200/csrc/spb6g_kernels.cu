@@ -397,7 +397,7 @@ SPB6G_DEV double row_scale(const Ctx& c, int i, int j, double Pc) {  // natural 
 }
 
 // evalAll + norm (:805-814), optionally at Pn = P + lam dP (line search :880-886).
-__global__ void __launch_bounds__(RED_THREADS, 2) k_residual(Ctx c, int mode, double lam) {
+__global__ void __launch_bounds__(RED_THREADS, 3) k_residual(Ctx c, int mode, double lam) {
     const Geom& g = c.g;
     double m[1] = {0.0};
     const double* P = c.P;
@@ -425,12 +425,10 @@ void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
 // FD Jacobian (:837-853).  One thread per matrix entry: entry 0 perturbs the own
 // cell by h = 1e-7 s_r, entries 1-4 the W, E, S, N neighbour by 1e-7 s_col; each is
 // one residual evaluation, so the 5 closures of a row run in 5 independent threads.
-__global__ void __launch_bounds__(RED_THREADS, 2) k_jac_entries(Ctx c) {
+__global__ void __launch_bounds__(RED_THREADS, 3) k_jac_entries(Ctx c) {
     const Geom& g = c.g;
     const bool twoD = g.ny > 1;
     const int nw = twoD ? 5 : 3;
-    double* planes[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
-    const int nb[4][2] = {{-1, 0}, {1, 0}, {0, -1}, {0, 1}};
     // blocks nw*r .. nw*r + nw-1 evaluate the nw entries of the same 256 rows: they run side by
     // side, so the rows' stage data comes from DRAM once and from L2 for the other entries,
     // while every warp follows one entry's code path
@@ -447,13 +445,15 @@ __global__ void __launch_bounds__(RED_THREADS, 2) k_jac_entries(Ctx c) {
         ok = residual_at(c, i, j, p, h, -1, 0, gv, nullptr);
         a = (gv - G0) / h;
     } else {
-        const int col = mp_index(g, i + nb[w - 1][0], j + nb[w - 1][1]);
+        const int di = w == 1 ? -1 : (w == 2 ? 1 : 0), dj = w == 3 ? -1 : (w == 4 ? 1 : 0);
+        const int col = mp_index(g, i + di, j + dj);
         const double hn = 1e-7 * c.sc[col];
         ok = residual_at(c, i, j, p, 0, w - 1, hn, gv, nullptr);
         a = (gv - G0) / hn;
     }
     if (!ok) atomicOr(&c.ns->fail, 2);
-    planes[w][x] = a;
+    double* plane = w == 0 ? c.aC : w == 1 ? c.aW : w == 2 ? c.aE : w == 3 ? c.aS : c.aN;
+    plane[x] = a;
 }
 // Row sums A 1 (summed in the row's entry order, as block_sum's terms :763), Jacobi
 // inverse, and the set-up sums E = 1^T A 1, 1^T b, b^T b with b = -G.
