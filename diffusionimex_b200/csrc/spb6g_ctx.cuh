@@ -61,6 +61,7 @@ struct Ctx {
     // cells (vst / ust): planes 0-3 left donor, 4-7 right donor, 8 utL, 9 utR
     double *fxd, *fyd;  // 10 planes of (nx+1)*ny / nx*(ny+1)
     int* strong_list;
+    unsigned char* smask;  // 1 for cells on the strong-shock worklist of the stage
     // Newton
     double *P, *Pn, *G, *Gn, *sc, *scn, *dP;
     double *aC, *aW, *aE, *aS, *aN, *A1, *dinv;
@@ -89,10 +90,17 @@ int red_blocks(int n, int threads = RED_THREADS);
 // fused stage combination + reconstruction + Rusanov update + face donors (replaces combine/recon/update)
 void launch_flux(const Ctx& c, cudaStream_t st);
 void launch_prep(const Ctx& c, cudaStream_t st);
-void launch_shock(const Ctx& c, cudaStream_t st);
+// weak-shock budget + strong-shock worklist (and smask); strong-shock budget of the worklist
+void launch_shock_weak(const Ctx& c, cudaStream_t st);
+void launch_shock_strong(const Ctx& c, cudaStream_t st);
 // mode 0: evaluate at P (writes G, sc);  mode 1: at Pn = P + lam dP (writes Pn, Gn, scn)
-void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam);
+// skip_strong = 1 (mode 0): rows on the strong-shock worklist get only their scale s_q
+void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam, int skip_strong = 0);
+void launch_residual_strong(const Ctx& c, cudaStream_t st);
 void launch_jacobian(const Ctx& c, cudaStream_t st);
+void launch_jac_entries(const Ctx& c, cudaStream_t st, int skip_strong);
+void launch_jac_strong(const Ctx& c, cudaStream_t st);
+void launch_jac_finish(const Ctx& c, cudaStream_t st);
 void launch_bicg_init(const Ctx& c, cudaStream_t st, double tol, int maxit);
 void launch_bicg_iters(const Ctx& c, cudaStream_t st, int count, int& parity);
 int build_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t* exec);

@@ -220,6 +220,7 @@ __global__ void k_shock_weak(Ctx c) {
         const int r = shock_cell(c, x % c.g.nx, x / c.g.nx, Q, false);
         c.qph0[x] = Q[0];
         c.qph1[x] = Q[1];
+        c.smask[x] = r == 2 ? 1 : 0;
         if (r == 2) {
             const int slot = atomicAdd(&c.ns->nstrong, 1);
             c.strong_list[slot] = x;
@@ -238,10 +239,13 @@ __global__ void k_shock_strong(Ctx c) {
 }
 // Weak-shock cells are finished in place; strong-shock cells (Kapila profile
 // shooting, 6-9 RK45 integrations each) go through a compacted worklist.
-void launch_shock(const Ctx& c, cudaStream_t st) {
+void launch_shock_weak(const Ctx& c, cudaStream_t st) {
     k_shock_weak<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    count(c, 1);
+}
+void launch_shock_strong(const Ctx& c, cudaStream_t st) {
     k_shock_strong<<<148 * 4, 32, 0, st>>>(c);
-    count(c, 2);
+    count(c, 1);
 }
 
 // ============================================================ implicit residual (:610-731)
@@ -397,13 +401,19 @@ SPB6G_DEV double row_scale(const Ctx& c, int i, int j, double Pc) {  // natural 
 }
 
 // evalAll + norm (:805-814), optionally at Pn = P + lam dP (line search :880-886).
-__global__ void __launch_bounds__(RED_THREADS, 3) k_residual(Ctx c, int mode, double lam) {
+// skip_strong (mode 0 only): cells whose strong-shock budget is still being computed on
+// the side stream get their row scale only; k_residual_strong finishes them.
+__global__ void __launch_bounds__(RED_THREADS, 3) k_residual(Ctx c, int mode, double lam, int skip_strong) {
     const Geom& g = c.g;
     double m[1] = {0.0};
     const double* P = c.P;
     const double* dP = c.dP;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const int i = x % g.nx, j = x / g.nx;
+        if (skip_strong && c.smask[x]) {
+            c.sc[x] = row_scale(c, i, j, P[x]);
+            continue;
+        }
         Nb5 p = mode == 0 ? gather_p(g, i, j, [&](int q) { return P[q]; })
                           : gather_p(g, i, j, [&](int q) { return P[q] + lam * dP[q]; });
         double Gr;
@@ -417,24 +427,40 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_residual(Ctx c, int mode, do
     double tot[1];
     if (grid_fold<RedMax, 1>(m, c.partials, &c.counters[0], tot) && threadIdx.x == 0) c.ns->res = tot[0];
 }
-void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam) {
-    k_residual<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, mode, lam);
+void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam, int skip_strong) {
+    k_residual<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, mode, lam, skip_strong);
+    count(c, 1);
+}
+// Mode-0 residual of the strong-shock cells (the worklist), folded into the
+// max-norm that k_residual(skip_strong) left in ns->res.
+__global__ void __launch_bounds__(RED_THREADS, 3) k_residual_strong(Ctx c) {
+    const Geom& g = c.g;
+    double m[1] = {0.0};
+    const double* P = c.P;
+    const int cnt = c.ns->nstrong;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const int x = c.strong_list[t];
+        const int i = x % g.nx, j = x / g.nx;
+        const Nb5 p = gather_p(g, i, j, [&](int q) { return P[q]; });
+        double Gr;
+        const bool ok = residual_at(c, i, j, p, 0, -1, 0, Gr, nullptr);
+        c.G[x] = Gr;
+        if (!ok) atomicOr(&c.ns->fail, 1);
+        else m[0] = SMAX(m[0], SMAX(0.0, fabs(Gr) / (fabs(c.p_ref + p.c) + c.kw[x] + 1.0)));
+    }
+    double tot[1];
+    if (grid_fold<RedMax, 1>(m, c.partials, &c.counters[10], tot) && threadIdx.x == 0) c.ns->res = SMAX(c.ns->res, tot[0]);
+}
+void launch_residual_strong(const Ctx& c, cudaStream_t st) {
+    k_residual_strong<<<148 * 2, RED_THREADS, 0, st>>>(c);
     count(c, 1);
 }
 
 // FD Jacobian (:837-853).  One thread per matrix entry: entry 0 perturbs the own
 // cell by h = 1e-7 s_r, entries 1-4 the W, E, S, N neighbour by 1e-7 s_col; each is
 // one residual evaluation, so the 5 closures of a row run in 5 independent threads.
-__global__ void __launch_bounds__(RED_THREADS, 3) k_jac_entries(Ctx c) {
+SPB6G_DEV void jac_entry(const Ctx& c, int x, int w) {
     const Geom& g = c.g;
-    const bool twoD = g.ny > 1;
-    const int nw = twoD ? 5 : 3;
-    // blocks nw*r .. nw*r + nw-1 evaluate the nw entries of the same 256 rows: they run side by
-    // side, so the rows' stage data comes from DRAM once and from L2 for the other entries,
-    // while every warp follows one entry's code path
-    const int w = blockIdx.x % nw, rb = blockIdx.x / nw;
-    const int x = rb * blockDim.x + threadIdx.x;
-    if (x >= c.n) return;
     const int i = x % g.nx, j = x / g.nx;
     const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
     const double G0 = c.G[x];
@@ -454,6 +480,24 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_jac_entries(Ctx c) {
     if (!ok) atomicOr(&c.ns->fail, 2);
     double* plane = w == 0 ? c.aC : w == 1 ? c.aW : w == 2 ? c.aE : w == 3 ? c.aS : c.aN;
     plane[x] = a;
+}
+// skip_strong: rows of strong-shock cells are left to k_jac_strong.
+__global__ void __launch_bounds__(RED_THREADS, 3) k_jac_entries(Ctx c, int skip_strong) {
+    const int nw = c.g.ny > 1 ? 5 : 3;
+    // blocks nw*r .. nw*r + nw-1 evaluate the nw entries of the same 256 rows: they run side by
+    // side, so the rows' stage data comes from DRAM once and from L2 for the other entries,
+    // while every warp follows one entry's code path
+    const int w = blockIdx.x % nw, rb = blockIdx.x / nw;
+    const int x = rb * blockDim.x + threadIdx.x;
+    if (x >= c.n || (skip_strong && c.smask[x])) return;
+    jac_entry(c, x, w);
+}
+// The nw entries of every strong-shock row (the worklist).
+__global__ void __launch_bounds__(RED_THREADS, 3) k_jac_strong(Ctx c) {
+    const int nw = c.g.ny > 1 ? 5 : 3;
+    const long cnt = (long)c.ns->nstrong * nw;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < cnt; t += (long)gridDim.x * blockDim.x)
+        jac_entry(c, c.strong_list[t / nw], (int)(t % nw));
 }
 // Row sums A 1 (summed in the row's entry order, as block_sum's terms :763), Jacobi
 // inverse, and the set-up sums E = 1^T A 1, 1^T b, b^T b with b = -G.
@@ -478,11 +522,22 @@ __global__ void __launch_bounds__(RED_THREADS) k_jac_finish(Ctx c) {
         c.ns->E = tot[0]; c.ns->sumb = tot[1]; c.ns->bb = tot[2];
     }
 }
-void launch_jacobian(const Ctx& c, cudaStream_t st) {
+void launch_jac_entries(const Ctx& c, cudaStream_t st, int skip_strong) {
     const int nw = c.g.ny > 1 ? 5 : 3;
-    k_jac_entries<<<nw * ((c.n + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c);
+    k_jac_entries<<<nw * ((c.n + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c, skip_strong);
+    count(c, 1);
+}
+void launch_jac_strong(const Ctx& c, cudaStream_t st) {
+    k_jac_strong<<<148 * 4, RED_THREADS, 0, st>>>(c);
+    count(c, 1);
+}
+void launch_jac_finish(const Ctx& c, cudaStream_t st) {
     k_jac_finish<<<(c.n + RED_THREADS - 1) / RED_THREADS, RED_THREADS, 0, st>>>(c);
-    count(c, 2);
+    count(c, 1);
+}
+void launch_jacobian(const Ctx& c, cudaStream_t st) {
+    launch_jac_entries(c, st, 0);
+    launch_jac_finish(c, st);
 }
 
 // ============================================================ BiCGStab (GMRES_Solver :752-794)

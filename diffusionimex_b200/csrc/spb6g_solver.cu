@@ -60,7 +60,7 @@ struct spb6g_solver {
     int bicg_G = 0;                       // blocks of the persistent BiCGStab launch (0: not available)
     cudaGraphExec_t bicg_exec = nullptr;  // device-side BiCGStab loop (built once per solver)
     cudaStream_t st2 = nullptr;           // side stream: shock budget, overlapped with the stage prep
-    cudaEvent_t ev_flux = nullptr, ev_shock = nullptr;
+    cudaEvent_t ev_flux = nullptr, ev_weak = nullptr, ev_shock = nullptr;
     int last_bicg_iters = 8;
 };
 
@@ -108,18 +108,23 @@ void tend_(spb6g_solver* s, int g, cudaStream_t st = nullptr) {
 }
 // Stage prep on the main stream while the shock budget (whose strong-shock cells each
 // integrate a shock profile serially) runs on the side stream; joined before Newton.
+// Stage data on the main stream, shock budget on the side stream.  The main
+// stream joins the side stream inside newton(): its first residual and the
+// Jacobian rows of cells without a strong-shock budget run while the
+// strong-shock worklist is still being integrated.
 void prep_and_shock(spb6g_solver* s) {
     Ctx& c = s->c;
     cudaEventRecord(s->ev_flux, s->st);
     cudaStreamWaitEvent(s->st2, s->ev_flux, 0);
     tbegin(s, TG_SHOCK, s->st2);
-    launch_shock(c, s->st2);
+    launch_shock_weak(c, s->st2);
+    cudaEventRecord(s->ev_weak, s->st2);
+    launch_shock_strong(c, s->st2);
     tend_(s, TG_SHOCK, s->st2);
     cudaEventRecord(s->ev_shock, s->st2);
     tbegin(s, TG_PREP);
     launch_prep(c, s->st);
     tend_(s, TG_PREP);
-    cudaStreamWaitEvent(s->st, s->ev_shock, 0);
 }
 // Accumulates every completed group (called after a stream synchronisation).
 void resolve_timing(spb6g_solver* s) {
@@ -201,19 +206,37 @@ int newton(spb6g_solver* s, double& resfinal) {
     const bool tri = s->g.ny == 1 && s->g.bcs[0] != BC_PERIODIC;
     const double tol = s->cfg.newton_tol;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+    // First evaluation (evalAll + norm).  Rows whose strong-shock budget is still
+    // being integrated on the side stream are skipped, and the Jacobian rows of all
+    // other cells are formed ahead (used only if the first norm is above tolerance);
+    // after the join the worklist rows follow.  Residual failures set bit 1 of
+    // ns.fail, Jacobian failures bit 2.
+    CK(cudaStreamWaitEvent(s->st, s->ev_weak, 0));
     tbegin(s, TG_RESIDUAL);
-    launch_residual(c, s->st, 0, 0.0);
+    launch_residual(c, s->st, 0, 0.0, 1);
+    tend_(s, TG_RESIDUAL);
+    tbegin(s, TG_JACOBIAN);
+    launch_jac_entries(c, s->st, 1);
+    tend_(s, TG_JACOBIAN);
+    CK(cudaStreamWaitEvent(s->st, s->ev_shock, 0));
+    tbegin(s, TG_RESIDUAL);
+    launch_residual_strong(c, s->st);
     tend_(s, TG_RESIDUAL);
     if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
     if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
-    if (s->pin->ns.fail) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
+    if (s->pin->ns.fail & 1) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
     double res = s->pin->ns.res;
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
         if (res < tol) return SPB6G_OK;
-        if (reset_fail(s)) return SPB6G_CUDA_ERROR;
         tbegin(s, TG_JACOBIAN);
-        launch_jacobian(c, s->st);
+        if (it == 0) {  // the rows formed ahead stand; add the worklist rows
+            launch_jac_strong(c, s->st);
+            launch_jac_finish(c, s->st);
+        } else {
+            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+            launch_jacobian(c, s->st);
+        }
         tend_(s, TG_JACOBIAN);
         tbegin(s, TG_LINEAR);
         if (tri) {
@@ -446,6 +469,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_flux, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_weak, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_shock, cudaEventDisableTiming) != cudaSuccess) {
         spb6g_destroy(s);
         return SPB6G_CUDA_ERROR;
@@ -478,6 +502,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.fy_ubs = A(nfy); c.fy_kp = A(nfy); c.fy_wl = A(nfy); c.fy_pv = A(nfy);
     c.fxd = A(10 * nfx); c.fyd = A(10 * nfy);
     c.strong_list = (int*)A(n / 2 + 1);
+    c.smask = (unsigned char*)A(n / 8 + 1);
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
     c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
     c.br = A(n); c.br0 = A(n); c.bp = A(n); c.bv = A(n); c.bq = A(n); c.bs = A(n); c.bu = A(n); c.bt = A(n);
@@ -520,6 +545,7 @@ int spb6g_destroy(spb6g_solver* s) {
         if (s->region[e]) cudaEventDestroy(s->region[e]);
     if (s->st2) { cudaStreamSynchronize(s->st2); cudaStreamDestroy(s->st2); }
     if (s->ev_flux) cudaEventDestroy(s->ev_flux);
+    if (s->ev_weak) cudaEventDestroy(s->ev_weak);
     if (s->ev_shock) cudaEventDestroy(s->ev_shock);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
