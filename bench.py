@@ -50,10 +50,18 @@ ALG_BYTES = {
 }
 
 
+# DRAM read + write per unit from ncu (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+# on this workload: k_bicg_solve moved 1.93 GB for 11 iterations of 1,048,576 rows
+# (profiles/k_bicg_solve_bubbles1024.md).
+DRAM_BYTES = {"linear": 1.934e9 / (11 * 1048576)}
+KERNEL_OF = {"linear": "k_bicg_solve (BiCGStab solve, one launch per Newton iteration)",
+             "jacobian": "k_jac_entries", "residual": "k_residual", "explicit": "k_flux"}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="bubbles1024")
@@ -279,9 +287,12 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
     else:
         units = gcnt * n
     achieved = ALG_BYTES[dom] * units / (gms / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-            "alg_bytes_per_cell": ALG_BYTES[dom]}
+    # DRAM bytes per launch: the ncu-measured bytes per unit, scaled to this run's average launch
+    traffic = DRAM_BYTES[dom] * units / max(gcnt, 1) if dom in DRAM_BYTES and args.workload == "bubbles1024" else None
+    roof = {"bound": "hbm", "kernel": KERNEL_OF[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+            "alg_bytes_per_cell": ALG_BYTES[dom],
+            "alg_bytes_per_launch": ALG_BYTES[dom] * units / max(gcnt, 1)}
     total_ms = sum(v[0] for v in groups.values())
     shares = {g: {"ms": round(v[0], 3), "launch_groups": int(v[1]), "share": round(v[0] / ms, 4)} for g, v in groups.items()}
 
