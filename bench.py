@@ -170,6 +170,23 @@ def cpu_baseline(case: dict, steps: int = 2) -> dict:
                       f"({r['newton_it']} Newton iterations), {r['wall_s']:.1f} s"}
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """Slowest rank's time: every rank contributes its own device-timed milliseconds (one
+    all-reduce, the same collective on every rank)."""
+    if not dist:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(cells: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job cell-updates/s of N independent replicas timed by the slowest rank."""
+    return cells * steps * world / (ms_max / 1e3)
+
+
 def dist_init(world: int, local_rank: int):
     if world <= 1:
         return None
@@ -242,14 +259,11 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
     launches = s.kernel_launches() - l0
     groups = s.timing()
     s.timing(False)
-    ms_max = ms
+    ms_max = max_over_ranks(ms, dist, f"cuda:{local_rank}")
     if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
         dist.barrier()
     steps_done = st1["steps"] - st0["steps"]
-    value = n * steps_done * world / (ms_max / 1e3)
+    value = job_value(n, steps_done, world, ms_max)
 
     # end to end through the public API: the state goes host -> device before every step and
     # comes back after it (pinned host buffer, SoA layout)
@@ -267,12 +281,8 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
             s.upload_soa(ptr)
             s.step()
             s.download_soa(ptr)
-        ems = s.region_end()
-        if dist:
-            t = torch.tensor([ems], dtype=torch.float64, device=f"cuda:{local_rank}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": n * ke * world / (ems / 1e3), "unit": "cell-updates/s", "h2d_bytes_per_step": 64 * n,
+        ems = max_over_ranks(s.region_end(), dist, f"cuda:{local_rank}")
+        e2e = {"value": job_value(n, ke, world, ems), "unit": "cell-updates/s", "h2d_bytes_per_step": 64 * n,
                "d2h_bytes_per_step": 64 * n, "steps": ke}
 
     # roofline of the dominant kernel group
