@@ -96,6 +96,13 @@ def library() -> ctypes.CDLL:
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
         "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
+        "spb6g_mlp_create": (I, [I, P]),
+        "spb6g_mlp_destroy": (None, [P]),
+        "spb6g_mlp_param_count": (I, []),
+        "spb6g_mlp_set_params": (I, [P, P]),
+        "spb6g_mlp_get_params": (I, [P, P]),
+        "spb6g_mlp_forward": (I, [P, P, I, P, P]),
+        "spb6g_mlp_train_step": (I, [P, P, P, I, ctypes.c_float, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

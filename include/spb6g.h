@@ -156,6 +156,27 @@ int64_t spb6g_kernel_launches(spb6g_solver* s);
 int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
                         double* inv_rate);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference: the reference always
+ * starts a stage's Newton from the previous stage's pressure).  A small MLP,
+ * 64 inputs (54 used) -> 64 -> 64 -> 64 -> 1 with SiLU, BF16 weights on the
+ * tensor cores and FP32 accumulation, FP32 master weights trained with Adam.
+ * Inputs are row-major BF16 feature rows of 64 values on the device; outputs
+ * and targets FP32 on the device.  One handle per device and host thread. */
+typedef struct spb6g_mlp spb6g_mlp;
+int spb6g_mlp_create(int device, spb6g_mlp** out);
+void spb6g_mlp_destroy(spb6g_mlp* m);
+/* Number of FP32 parameters: W1[64][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4. */
+int spb6g_mlp_param_count(void);
+int spb6g_mlp_set_params(spb6g_mlp* m, const float* params_host);  /* also resets the Adam state */
+int spb6g_mlp_get_params(spb6g_mlp* m, float* params_host);
+/* y[i] = MLP(X[i]) for n rows; stream NULL: the handle's stream, synchronised. */
+int spb6g_mlp_forward(spb6g_mlp* m, const void* X_dev, int n, float* y_dev, void* stream);
+/* One pass over the n rows: gradient of mean((y - target)^2) (copied to grad_host if not NULL),
+ * loss to *loss_out; with lr > 0 also one Adam step (beta 0.9 / 0.999, eps 1e-8). */
+int spb6g_mlp_train_step(spb6g_mlp* m, const void* X_dev, const float* target_dev, int n, float lr, float* loss_out,
+                         float* grad_host);
+
 /* Human-readable status name. */
 const char* spb6g_status_string(int status);
 
