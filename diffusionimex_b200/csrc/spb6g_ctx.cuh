@@ -85,6 +85,13 @@ SPB6G_DEV size_t fyi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(
 SPB6G_DEV size_t rxi(const Geom& g, int i, int j) { return (size_t)(i + 1) + (size_t)j * (g.nx + 2); }
 SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(j + 1) * g.nx; }
 
+// Normalisation of the warm-start features (mean / 1/std of the centre values,
+// 1/std of the neighbour differences, per field) and the target scale.
+struct FeatureNorm {
+    double mean[6], istd[6], idstd[6];
+    double tscale;
+};
+
 // ------------------------------------------------------------ launchers (spb6g_kernels.cu)
 int red_blocks(int n, int threads = RED_THREADS);
 // fused stage combination + reconstruction + Rusanov update + face donors (replaces combine/recon/update)
@@ -109,6 +116,10 @@ void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int 
 int bicg_solve_blocks(int device, int n);
 int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int G);
 void launch_thomas(const Ctx& c, cudaStream_t st);
+// learned warm start: BF16 feature rows (n x 64), dP = y * tscale, training targets
+void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale);
+void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);
 void launch_floor(const Ctx& c, cudaStream_t st, double tol);

@@ -3,6 +3,8 @@
 // cited per kernel; arithmetic follows them in operation order.
 #include <cstdio>
 
+#include <cuda_bf16.h>
+
 #include "spb6g_ctx.cuh"
 
 namespace spb6g {
@@ -1215,6 +1217,69 @@ int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int 
     void* args[] = {(void*)&c, (void*)&tol, (void*)&maxit};
     count(c, 1);
     return cudaLaunchCooperativeKernel((const void*)k_bicg_solve, dim3(G), dim3(PB_THREADS), args, PB_SMEM, st) == cudaSuccess ? 0 : -1;
+}
+
+// ============================================================ learned warm start (no counterpart in the reference)
+// Feature row of cell (i, j): for each field f of (rho, rho u, rho v, alpha1, E*, P)
+// taken from the explicit predictor X* (boundary-mapped like every stencil read)
+// and the stage's starting pressure (through M_P): the centre value normalised as
+// (v - mean_f) / std_f, then the 8 neighbours (rows below, same row, above; west
+// to east) as differences to the centre over dstd_f.  54 values, padded to 64, BF16.
+__global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X) {
+    const Geom& g = c.g;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+        const int i = x % g.nx, j = x / g.nx;
+        double v[9][6];
+        int k = 0;
+        for (int dj = -1; dj <= 1; dj++)
+            for (int di = -1; di <= 1; di++) {
+                double q[NV];
+                xs_at(c, i + di, j + dj, q);
+                double* f = v[(dj == 0 && di == 0) ? 0 : ++k];
+                f[0] = q[IM1] + q[IM2];
+                f[1] = q[IMU];
+                f[2] = q[IMV];
+                f[3] = q[IA1];
+                f[4] = q[IEN];
+                f[5] = c.P[mp_index(g, i + di, j + dj)];
+            }
+        __align__(16) __nv_bfloat16 row[64];
+#pragma unroll
+        for (int f = 0; f < 6; f++) {
+            row[f * 9] = __float2bfloat16_rn((float)((v[0][f] - nm.mean[f]) * nm.istd[f]));
+#pragma unroll
+            for (int m = 1; m < 9; m++) row[f * 9 + m] = __float2bfloat16_rn((float)((v[m][f] - v[0][f]) * nm.idstd[f]));
+        }
+#pragma unroll
+        for (int m = 54; m < 64; m++) row[m] = __float2bfloat16_rn(0.0f);
+        uint4* dst = (uint4*)(X + (size_t)x * 64);
+#pragma unroll
+        for (int q = 0; q < 8; q++) dst[q] = ((const uint4*)row)[q];
+    }
+}
+void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X) {
+    k_features<<<blocks_for(c.n), TPB, 0, st>>>(c, nm, (__nv_bfloat16*)X);
+    count(c, 1);
+}
+// Step towards the learned guess: the network predicts the stage's pressure rate
+// (P_converged - P_start) / tau in units of tscale, so dP = y * tscale * tau.
+__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale) {
+    const double f = tscale * c.adt;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) c.dP[x] = (double)y[x] * f;
+}
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale) {
+    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale);
+    count(c, 1);
+}
+// Training target of the stage: (P_converged - P_start) / (tau * tscale).
+__global__ void k_target(Ctx c, const double* __restrict__ P0, double itscale, float* __restrict__ t) {
+    const double f = itscale / c.adt;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x)
+        t[x] = (float)((c.P[x] - P0[x]) * f);
+}
+void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t) {
+    k_target<<<blocks_for(c.n), TPB, 0, st>>>(c, P0, itscale, t);
+    count(c, 1);
 }
 
 // ============================================================ Thomas (1D non-periodic, :858-863)

@@ -18,8 +18,8 @@ using namespace spb6g;
 
 namespace {
 
-enum TimerGroup { TG_EXPLICIT = 0, TG_PREP, TG_SHOCK, TG_RESIDUAL, TG_JACOBIAN, TG_LINEAR, TG_FINAL, TG_CALDT, TG_COUNT };
-const char* kTimerNames[TG_COUNT] = {"explicit", "prep", "shock", "residual", "jacobian", "linear", "final", "caldt"};
+enum TimerGroup { TG_EXPLICIT = 0, TG_PREP, TG_SHOCK, TG_RESIDUAL, TG_JACOBIAN, TG_LINEAR, TG_FINAL, TG_CALDT, TG_WARM, TG_COUNT };
+const char* kTimerNames[TG_COUNT] = {"explicit", "prep", "shock", "residual", "jacobian", "linear", "final", "caldt", "warmstart"};
 
 struct Pinned {
     NewtonScalars ns;
@@ -62,6 +62,17 @@ struct spb6g_solver {
     cudaStream_t st2 = nullptr;           // side stream: shock budget, overlapped with the stage prep
     cudaEvent_t ev_flux = nullptr, ev_weak = nullptr, ev_shock = nullptr;
     int last_bicg_iters = 8;
+    // learned warm start (no counterpart in the reference)
+    spb6g_mlp* warm = nullptr;          // network giving the first Newton guess (NULL: plain guess only)
+    FeatureNorm norm{};                 // feature normalisation and target scale
+    void* featbuf = nullptr;            // n x 64 BF16 feature rows of the current stage
+    float* ybuf = nullptr;              // network output per cell
+    double* Pstart = nullptr;           // stage's starting pressure (training targets)
+    void* rows_cur = nullptr;           // where this stage's feature rows were written
+    void* dumpX = nullptr;              // caller's buffers for (feature row, target) pairs
+    float* dumpT = nullptr;
+    int64_t dump_cap = 0, dump_count = 0;
+    bool dump_stage = false;
 };
 
 namespace {
@@ -211,13 +222,17 @@ int newton(spb6g_solver* s, double& resfinal) {
     // other cells are formed ahead (used only if the first norm is above tolerance);
     // after the join the worklist rows follow.  Residual failures set bit 1 of
     // ns.fail, Jacobian failures bit 2.
+    // (With a warm start the first iterate may change, so no rows are formed ahead.)
+    const bool ahead = s->warm == nullptr;
     CK(cudaStreamWaitEvent(s->st, s->ev_weak, 0));
     tbegin(s, TG_RESIDUAL);
     launch_residual(c, s->st, 0, 0.0, 1);
     tend_(s, TG_RESIDUAL);
-    tbegin(s, TG_JACOBIAN);
-    launch_jac_entries(c, s->st, 1);
-    tend_(s, TG_JACOBIAN);
+    if (ahead) {
+        tbegin(s, TG_JACOBIAN);
+        launch_jac_entries(c, s->st, 1);
+        tend_(s, TG_JACOBIAN);
+    }
     CK(cudaStreamWaitEvent(s->st, s->ev_shock, 0));
     tbegin(s, TG_RESIDUAL);
     launch_residual_strong(c, s->st);
@@ -226,11 +241,29 @@ int newton(spb6g_solver* s, double& resfinal) {
     if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
     if (s->pin->ns.fail & 1) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
     double res = s->pin->ns.res;
+    if (s->warm) {
+        // learned guess P + dP, dP = MLP(features) * tscale; it replaces the plain guess only
+        // when its residual norm is smaller (and every closure of it succeeded)
+        tbegin(s, TG_WARM);
+        if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
+        launch_guess(c, s->st, s->ybuf, s->norm.tscale);
+        launch_residual(c, s->st, 1, 1.0);
+        tend_(s, TG_WARM);
+        if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+        if (!s->pin->ns.fail && s->pin->ns.res < res) {
+            std::swap(c.P, c.Pn);
+            std::swap(c.G, c.Gn);
+            std::swap(c.sc, c.scn);
+            res = s->pin->ns.res;
+            s->stats.learned++;
+        }
+        if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+    }
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
         if (res < tol) return SPB6G_OK;
         tbegin(s, TG_JACOBIAN);
-        if (it == 0) {  // the rows formed ahead stand; add the worklist rows
+        if (it == 0 && ahead) {  // the rows formed ahead stand; add the worklist rows
             launch_jac_strong(c, s->st);
             launch_jac_finish(c, s->st);
         } else {
@@ -348,10 +381,24 @@ int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
     launch_flux(c, s->st);
     tend_(s, TG_EXPLICIT);
+    // warm-start features of the stage (X* and the starting pressure), into the caller's
+    // dump buffer when one has room, else into the solver's own rows
+    s->dump_stage = s->dumpX && s->dump_count + s->n <= s->dump_cap;
+    if (s->warm || s->dump_stage) {
+        tbegin(s, TG_WARM);
+        s->rows_cur = s->dump_stage ? (void*)((char*)s->dumpX + (size_t)s->dump_count * 128) : s->featbuf;
+        launch_features(c, s->st, s->norm, s->rows_cur);
+        if (s->dump_stage) CK(cudaMemcpyAsync(s->Pstart, c.P, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        tend_(s, TG_WARM);
+    }
     prep_and_shock(s);
     double res = 0;
     const int rc = newton(s, res);
     if (rc != SPB6G_OK) return rc;
+    if (s->dump_stage) {  // training pair: (features, (P_converged - P_start) / tscale)
+        launch_target(c, s->st, s->Pstart, 1.0 / s->norm.tscale, s->dumpT + s->dump_count);
+        s->dump_count += s->n;
+    }
     if (res > s->stats.maxres) s->stats.maxres = res;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
     tbegin(s, TG_FINAL);
@@ -719,6 +766,64 @@ int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double
         CK(cudaMemcpy(qph, c.qph0, n * sizeof(double), cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(qph + n, c.qph1, n * sizeof(double), cudaMemcpyDeviceToHost));
     }
+    return SPB6G_OK;
+}
+
+int spb6g_set_feature_norm(spb6g_solver* s, const double* norm) {
+    if (!s || !norm) return SPB6G_BAD_ARG;
+    for (int f = 0; f < 6; f++) {
+        if (!(norm[6 + f] > 0) || !(norm[12 + f] > 0)) return SPB6G_BAD_ARG;
+        s->norm.mean[f] = norm[f];
+        s->norm.istd[f] = 1.0 / norm[6 + f];
+        s->norm.idstd[f] = 1.0 / norm[12 + f];
+    }
+    if (!(norm[18] > 0)) return SPB6G_BAD_ARG;
+    s->norm.tscale = norm[18];
+    return SPB6G_OK;
+}
+static int ensure_warm_buffers(spb6g_solver* s) {
+    if (!s->featbuf) {
+        if (cudaMalloc(&s->featbuf, (size_t)s->n * 128) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(s->featbuf);
+    }
+    if (!s->ybuf) {
+        if (cudaMalloc((void**)&s->ybuf, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(s->ybuf);
+    }
+    if (!s->Pstart) {
+        if (cudaMalloc((void**)&s->Pstart, (size_t)s->n * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(s->Pstart);
+    }
+    return SPB6G_OK;
+}
+int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
+    if (!s) return SPB6G_BAD_ARG;
+    if (m && !(s->norm.tscale > 0)) return SPB6G_BAD_ARG;
+    if (m) {
+        cudaSetDevice(s->cfg.device);
+        const int rc = ensure_warm_buffers(s);
+        if (rc) return rc;
+    }
+    s->warm = m;
+    return SPB6G_OK;
+}
+int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity) {
+    if (!s || capacity < 0 || (capacity > 0 && (!X_dev || !target_dev))) return SPB6G_BAD_ARG;
+    if (capacity > 0 && !(s->norm.tscale > 0)) return SPB6G_BAD_ARG;
+    if (capacity > 0) {
+        cudaSetDevice(s->cfg.device);
+        const int rc = ensure_warm_buffers(s);
+        if (rc) return rc;
+    }
+    s->dumpX = capacity > 0 ? X_dev : nullptr;
+    s->dumpT = capacity > 0 ? target_dev : nullptr;
+    s->dump_cap = capacity;
+    s->dump_count = 0;
+    return SPB6G_OK;
+}
+int spb6g_dump_count(spb6g_solver* s, int64_t* count) {
+    if (!s || !count) return SPB6G_BAD_ARG;
+    *count = s->dump_count;
     return SPB6G_OK;
 }
 

@@ -55,7 +55,7 @@ class Stats(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_int64), ("rejects", ctypes.c_int64), ("rk1", ctypes.c_int64), ("stages", ctypes.c_int64),
         ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
-        ("reserved", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
+        ("learned", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
         ("p_ref", ctypes.c_double),
     ]
 
@@ -96,6 +96,10 @@ def library() -> ctypes.CDLL:
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
         "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
+        "spb6g_set_feature_norm": (I, [P, P]),
+        "spb6g_set_warmstart": (I, [P, P]),
+        "spb6g_set_dump": (I, [P, P, P, ctypes.c_int64]),
+        "spb6g_dump_count": (I, [P, P]),
         "spb6g_mlp_create": (I, [I, P]),
         "spb6g_mlp_destroy": (None, [P]),
         "spb6g_mlp_param_count": (I, []),
@@ -240,6 +244,31 @@ class Solver:
         ms = ctypes.c_double()
         self._check(self.lib.spb6g_region_end(self.h, ctypes.byref(ms)), "region_end")
         return ms.value
+
+    # ---- learned warm start (no counterpart in the reference)
+    def set_feature_norm(self, norm):
+        """19 values: mean[6], std[6] of the centre values, std[6] of the neighbour differences of
+        (rho, rho u, rho v, alpha1, E*, P - P_REF), then the target scale."""
+        a = (ctypes.c_double * 19)(*[float(v) for v in norm])
+        self._check(self.lib.spb6g_set_feature_norm(self.h, a), "spb6g_set_feature_norm")
+
+    def set_warmstart(self, mlp):
+        self._warm = mlp
+        self._check(self.lib.spb6g_set_warmstart(self.h, mlp.handle if mlp is not None else None), "spb6g_set_warmstart")
+
+    def set_dump(self, X=None, t=None):
+        """X: (cap, 64) torch.bfloat16, t: (cap,) torch.float32 on the device, or None to stop."""
+        self._dump = (X, t)
+        if X is None:
+            self._check(self.lib.spb6g_set_dump(self.h, None, None, 0), "spb6g_set_dump")
+            return
+        assert X.shape[0] == t.shape[0] and X.shape[1] == 64
+        self._check(self.lib.spb6g_set_dump(self.h, X.data_ptr(), t.data_ptr(), X.shape[0]), "spb6g_set_dump")
+
+    def dump_count(self) -> int:
+        v = ctypes.c_int64()
+        self._check(self.lib.spb6g_dump_count(self.h, ctypes.byref(v)), "spb6g_dump_count")
+        return v.value
 
     def kernel_launches(self) -> int:
         return int(self.lib.spb6g_kernel_launches(self.h))

@@ -74,11 +74,12 @@ typedef struct {
 /* Run statistics: the counters of the reference's stats line (:98-99, :1425). */
 typedef struct {
     int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it;
-    int64_t reserved;
+    int64_t learned;                /* stages whose Newton started from the learned guess */
     double t, dt, maxres, p_ref;
 } spb6g_stats;
 
 typedef struct spb6g_solver spb6g_solver;
+typedef struct spb6g_mlp spb6g_mlp;
 
 /* Fills *cfg with the reference defaults (SPB6_PC_IMEX_omp.cpp:55-95, set_SG physics :1014). */
 void spb6g_default_config(spb6g_config* cfg);
@@ -163,7 +164,6 @@ int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int
  * tensor cores and FP32 accumulation, FP32 master weights trained with Adam.
  * Inputs are row-major BF16 feature rows of 64 values on the device; outputs
  * and targets FP32 on the device.  One handle per device and host thread. */
-typedef struct spb6g_mlp spb6g_mlp;
 int spb6g_mlp_create(int device, spb6g_mlp** out);
 void spb6g_mlp_destroy(spb6g_mlp* m);
 /* Number of FP32 parameters: W1[64][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4. */
@@ -176,6 +176,19 @@ int spb6g_mlp_forward(spb6g_mlp* m, const void* X_dev, int n, float* y_dev, void
  * loss to *loss_out; with lr > 0 also one Adam step (beta 0.9 / 0.999, eps 1e-8). */
 int spb6g_mlp_train_step(spb6g_mlp* m, const void* X_dev, const float* target_dev, int n, float lr, float* loss_out,
                          float* grad_host);
+
+/* Warm start on the solver (no counterpart in the reference).  norm: 19 doubles:
+ * mean[6], std[6] of the centre values and std[6] of the neighbour differences of
+ * the fields (rho, rho u, rho v, alpha1, E*, P - P_REF), then the target scale. */
+int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
+/* m != NULL: every stage also evaluates the residual at P + tau * MLP(features) * scale
+ * (tau = the stage's implicit step) and starts Newton from it when its residual norm is
+ * below the plain guess's; NULL: off. */
+int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
+/* Training data: each stage appends n feature rows (64 BF16 each) to X_dev and n
+ * targets (P_converged - P_start) / (tau * scale) to target_dev while capacity allows. */
+int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity);
+int spb6g_dump_count(spb6g_solver* s, int64_t* count);
 
 /* Human-readable status name. */
 const char* spb6g_status_string(int status);
