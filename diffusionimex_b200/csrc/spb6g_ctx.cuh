@@ -39,6 +39,7 @@ struct Ctx {
     Phys phy;
     Geom g;
     int n;
+    int prec;  // 1: precision form (FP32 reconstruction, fluxes and SpMV), 0: FP64
     double tau, rx, ry, p_ref, adt;
     // explicit stage: Qe = Un + sum_r ce[r] H_r, Qs = Un + sum_r ci[r] H_r (main :1341-1351),
     // formed on the fly from the step's initial state and the previous stages' H
@@ -65,6 +66,7 @@ struct Ctx {
     // Newton
     double *P, *Pn, *G, *Gn, *sc, *scn, *dP;
     double *aC, *aW, *aE, *aS, *aN, *A1, *dinv;
+    float *fC, *fW, *fE, *fS, *fN;  // precision form: FP32 diagonals for the SpMV
     double *br, *br0, *bp, *bv, *bq, *bs, *bu, *bt;
     double *tcp, *tdp;
     // final state

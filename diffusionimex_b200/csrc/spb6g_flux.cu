@@ -20,7 +20,7 @@ namespace spb6g {
 
 namespace {
 
-template <int TX, int TY, bool TWO_D>
+template <class R, int TX, int TY, bool TWO_D>
 struct FluxTile {
     static constexpr int HY = TWO_D ? 2 : 0;
     static constexpr int NLX = TX + 4, NLY = TY + 2 * HY;
@@ -33,8 +33,11 @@ struct FluxTile {
     static constexpr int RY_SZ = TWO_D ? 3 * TX * NRY : 0;
     static constexpr int FX_SZ = 9 * NFX * TY;              // 8 fluxes + face velocity
     static constexpr int FY_SZ = TWO_D ? 9 * TX * NFY : 0;
-    static constexpr int TOTAL = Q_SZ + S_SZ + RX_SZ + RY_SZ + FX_SZ + FY_SZ;
-    static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
+    // precision form only: the admissibility terms L1, L2 of both phases per staged cell,
+    // formed in FP64 from the FP64 state (they subtract p_inf-sized values)
+    static constexpr int L_SZ = sizeof(R) == sizeof(double) ? 0 : 4 * NLX * NLY;
+    static constexpr int TOTAL = Q_SZ + S_SZ + RX_SZ + RY_SZ + FX_SZ + FY_SZ + L_SZ;
+    static constexpr size_t BYTES = (size_t)TOTAL * sizeof(R);
 };
 
 // Qe of a (possibly ghost) cell: the stage combination at the mapped source, then the ghost transforms.
@@ -72,58 +75,74 @@ SPB6G_DEV void scales_of(const Phys& P, const double* q, double& vsc, double& es
 }
 
 // Shared limiter, face-admissibility cap and velocity slopes (TVDReconstruction :399-463).
-SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const double* Ub, double vsa, double vsc,
-                      double vsb, double esa, double esc, double esb, const double* va_, const double* vc_,
-                      const double* vb_, double& phi_out, double& phis_out, double& slu, double& slv) {
+// Precision form (R = float): the same arithmetic in FP32, except the admissibility
+// terms L1, L2, which arrive precomputed in FP64 (Lx[4] = L1, L2 of phase 1, then phase 2)
+// because they subtract p_inf-sized energies; round-off thresholds scale with FP32's epsilon.
+template <class R>
+SPB6G_DEV R tiny_rel() { return sizeof(R) == sizeof(double) ? R(1e-12) : R(1e-5); }
+template <class R>
+SPB6G_DEV R tiny_abs() { return sizeof(R) == sizeof(double) ? R(1e-300) : R(1e-30); }
+
+template <class R>
+SPB6G_DEV void recon3(const Phys& P, const R* Ua, const R* Uc, const R* Ub, R vsa, R vsc,
+                      R vsb, R esa, R esc, R esb, const R* va_, const R* vc_,
+                      const R* vb_, R& phi_out, R& phis_out, R& slu, R& slv,
+                      const R* La = nullptr, const R* Lc = nullptr, const R* Lb = nullptr) {
     const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
-    double phi = 1.0;
+    R phi = 1.0;
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int k = VOL[q];
-        const double xa = Ua[k], xc = Uc[k], xb = Ub[k];
-        double sc;
+        const R xa = Ua[k], xc = Uc[k], xb = Ub[k];
+        R sc;
         if (k == IA1) sc = 3.0;
         else if (k == IM1 || k == IM2) sc = fabs(xa) + fabs(xc) + fabs(xb);
         else sc = esa + esc + esb;
-        const double a = xc - xa, b = xb - xc, tiny = 1e-12 * sc + 1e-300;
+        const R a = xc - xa, b = xb - xc, tiny = tiny_rel<R>() * sc + tiny_abs<R>();
         if (!P.limiter) break;
         if (fabs(a) <= tiny && fabs(b) <= tiny) continue;
         if (a * b <= 0) { phi = 0.0; break; }
-        const double cc = 0.5 * (a + b), m = fabs(a) < fabs(b) ? a : b;
+        const R cc = R(0.5) * (a + b), m = fabs(a) < fabs(b) ? a : b;
         phi = SMIN(phi, m / cc);
     }
-    if (P.limiter && phi > 0.0) {
-        const double* cs[3] = {Ua, Uc, Ub};
+    if (P.limiter && phi > R(0.0)) {
 #pragma unroll
         for (int ph = 0; ph < 2; ph++) {
-            double L1[3], L2[3];
+            R L1[3], L2[3];
+            if constexpr (sizeof(R) == sizeof(double)) {
+                const R* cs[3] = {Ua, Uc, Ub};
 #pragma unroll
-            for (int n = 0; n < 3; n++) {
-                const double a = ph == 0 ? cs[n][IA1] : 1.0 - cs[n][IA1], m = cs[n][ph == 0 ? IM1 : IM2],
-                             e = cs[n][ph == 0 ? IE1 : IE2];
-                L1[n] = a - m * P.ph[ph].b;
-                L2[n] = e - m * P.ph[ph].q - L1[n] * P.ph[ph].pi;
+                for (int n = 0; n < 3; n++) {
+                    const R a = ph == 0 ? cs[n][IA1] : 1.0 - cs[n][IA1], m = cs[n][ph == 0 ? IM1 : IM2],
+                            e = cs[n][ph == 0 ? IE1 : IE2];
+                    L1[n] = a - m * P.ph[ph].b;
+                    L2[n] = e - m * P.ph[ph].q - L1[n] * P.ph[ph].pi;
+                }
+            } else {
+                const R* ls[3] = {La, Lc, Lb};
+#pragma unroll
+                for (int n = 0; n < 3; n++) { L1[n] = ls[n][2 * ph]; L2[n] = ls[n][2 * ph + 1]; }
             }
             {
-                const double dL = fabs(L1[2] - L1[0]);
-                if (L1[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L1[1] / dL);
+                const R dL = fabs(L1[2] - L1[0]);
+                if (L1[1] > R(0.0) && dL > R(0.0)) phi = SMIN(phi, R(2.0) * L1[1] / dL);
             }
             {
-                const double dL = fabs(L2[2] - L2[0]);
-                if (L2[1] > 0.0 && dL > 0.0) phi = SMIN(phi, 2.0 * L2[1] / dL);
+                const R dL = fabs(L2[2] - L2[0]);
+                if (L2[1] > R(0.0) && dL > R(0.0)) phi = SMIN(phi, R(2.0) * L2[1] / dL);
             }
         }
     }
     // va_, vc_, vb_: the cells' velocities (u, v) = (rho u, rho v) / (m1 + m2), computed once per cell
-    const double tiny = 1e-12 * (vsa + vsc + vsb) + 1e-300;
-    double sm = 1.0, sl[2];
+    const R tiny = tiny_rel<R>() * (vsa + vsc + vsb) + tiny_abs<R>();
+    R sm = 1.0, sl[2];
 #pragma unroll
     for (int d = 0; d < 2; d++) {
-        const double va = va_[d], vc = vc_[d], vb = vb_[d], a = vc - va, b = vb - vc;
-        double s = 0.0;
-        if (!P.limiter) s = 0.5 * (a + b);
+        const R va = va_[d], vc = vc_[d], vb = vb_[d], a = vc - va, b = vb - vc;
+        R s = 0.0;
+        if (!P.limiter) s = R(0.5) * (a + b);
         else if (!(fabs(a) <= tiny && fabs(b) <= tiny)) {
-            if (a * b > 0) { s = fabs(a) < fabs(b) ? a : b; sm = SMIN(sm, s / (0.5 * (a + b))); }
+            if (a * b > 0) { s = fabs(a) < fabs(b) ? a : b; sm = SMIN(sm, s / (R(0.5) * (a + b))); }
             else sm = 0.0;
         }
         sl[d] = s;
@@ -135,51 +154,55 @@ SPB6G_DEV void recon3(const Phys& P, const double* Ua, const double* Uc, const d
 }
 
 // Face value of a cell on its right (+) or left (-) side from the cell's stencil and its reconstruction.
-SPB6G_DEV void face_value(const double* Ua, const double* Uc, const double* Ub, double vcu, double vcv, double phi,
-                          double slu, double slv, bool right, double* w) {
+template <class R>
+SPB6G_DEV void face_value(const R* Ua, const R* Uc, const R* Ub, R vcu, R vcv, R phi,
+                          R slu, R slv, bool right, R* w) {
     const int VOL[5] = {IA1, IM1, IM2, IE1, IE2};
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int k = VOL[q];
-        const double sig = phi * 0.5 * (Ub[k] - Ua[k]);
-        w[k] = right ? Uc[k] + 0.5 * sig : Uc[k] - 0.5 * sig;
+        const R sig = phi * R(0.5) * (Ub[k] - Ua[k]);
+        w[k] = right ? Uc[k] + R(0.5) * sig : Uc[k] - R(0.5) * sig;
     }
-    const double v0 = right ? vcu + 0.5 * slu : vcu - 0.5 * slu, v1 = right ? vcv + 0.5 * slv : vcv - 0.5 * slv;
-    const double r = w[IM1] + w[IM2];
+    const R v0 = right ? vcu + R(0.5) * slu : vcu - R(0.5) * slu, v1 = right ? vcv + R(0.5) * slv : vcv - R(0.5) * slv;
+    const R r = w[IM1] + w[IM2];
     w[IMU] = r * v0;
     w[IMV] = r * v1;
-    w[IEN] = w[IE1] + w[IE2] + 0.5 * r * (v0 * v0 + v1 * v1);
+    w[IEN] = w[IE1] + w[IE2] + R(0.5) * r * (v0 * v0 + v1 * v1);
 }
 
 // Rusanov flux (RusanovC_x/y :237-259); returns the normal face-state velocities, which are
 // also the terms of the face velocity ube (Update :283-294).
-SPB6G_DEV void rusanov_flux(const double* QL, const double* QR, int d, double* flux, double& vL, double& vR) {
+template <class R>
+SPB6G_DEV void rusanov_flux(const R* QL, const R* QR, int d, R* flux, R& vL, R& vR) {
     const int km = d == 0 ? IMU : IMV;
     vL = QL[km] / (QL[IM1] + QL[IM2]);
     vR = QR[km] / (QR[IM1] + QR[IM2]);
-    const double a = SMAX(fabs(vL), fabs(vR));
+    const R a = SMAX(fabs(vL), fabs(vR));
 #pragma unroll
-    for (int k = 0; k < NV; k++) flux[k] = 0.5 * (QL[k] * vL + QR[k] * vR) - 0.5 * a * (QR[k] - QL[k]);
+    for (int k = 0; k < NV; k++) flux[k] = R(0.5) * (QL[k] * vL + QR[k] * vR) - R(0.5) * a * (QR[k] - QL[k]);
 }
 
-template <int TX, int TY, bool TWO_D>
+template <class R, int TX, int TY, bool TWO_D>
 __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
-    using T = FluxTile<TX, TY, TWO_D>;
+    using T = FluxTile<R, TX, TY, TWO_D>;
+    constexpr bool MIXED = sizeof(R) != sizeof(double);
     constexpr int HY = T::HY, NLX = T::NLX, NLY = T::NLY, NRX = T::NRX, NRY = T::NRY, NFX = T::NFX, NFY = T::NFY;
-    extern __shared__ double smem[];
-    double* Qs_ = smem;                      // [NV][NLY][NLX]
-    double* VS = Qs_ + T::Q_SZ;              // [NLY][NLX]
-    double* ES = VS + NLX * NLY;
-    double* VU = ES + NLX * NLY;             // cell velocity u
-    double* VV = VU + NLX * NLY;             // cell velocity v
-    double* RX = VV + NLX * NLY;             // [3][TY][NRX]
-    double* RY = RX + T::RX_SZ;              // [3][NRY][TX]
-    double* FX = RY + T::RY_SZ;              // [9][TY][NFX]
-    double* FY = FX + T::FX_SZ;              // [9][NFY][TX]
+    extern __shared__ __align__(16) unsigned char flux_smem[];
+    R* Qs_ = (R*)flux_smem;                  // [NV][NLY][NLX]
+    R* VS = Qs_ + T::Q_SZ;                   // [NLY][NLX]
+    R* ES = VS + NLX * NLY;
+    R* VU = ES + NLX * NLY;                  // cell velocity u
+    R* VV = VU + NLX * NLY;                  // cell velocity v
+    R* RX = VV + NLX * NLY;                  // [3][TY][NRX]
+    R* RY = RX + T::RX_SZ;                   // [3][NRY][TX]
+    R* FX = RY + T::RY_SZ;                   // [9][TY][NFX]
+    R* FY = FX + T::FX_SZ;                   // [9][NFY][TX]
+    R* LS = FY + T::FY_SZ;                   // precision form: [NLY][NLX][4] admissibility terms
     const Geom& g = c.g;
     const int tid = threadIdx.x, nth = TX * TY;
     const int i0 = blockIdx.x * TX, j0 = TWO_D ? blockIdx.y * TY : 0;
-    auto Q = [&](int k, int ly, int lx) -> double& { return Qs_[(k * NLY + ly) * NLX + lx]; };
+    auto Q = [&](int k, int ly, int lx) -> R& { return Qs_[(k * NLY + ly) * NLX + lx]; };
     auto in_cross = [&](int lx, int ly) {
         if (!TWO_D) return true;
         const bool cx = lx >= 2 && lx < TX + 2, cy = ly >= HY && ly < HY + TY;
@@ -197,16 +220,26 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         double q[NV];
         load_qe(c, gi, gj, q);
 #pragma unroll
-        for (int k = 0; k < NV; k++) Q(k, ly, lx) = q[k];
+        for (int k = 0; k < NV; k++) Q(k, ly, lx) = (R)q[k];
         double vs, es;
         scales_of(c.phy, q, vs, es);
-        VS[ly * NLX + lx] = vs;
-        ES[ly * NLX + lx] = es;
+        VS[ly * NLX + lx] = (R)vs;
+        ES[ly * NLX + lx] = (R)es;
         const double rho = q[IM1] + q[IM2];
-        VU[ly * NLX + lx] = q[IMU] / rho;
-        VV[ly * NLX + lx] = q[IMV] / rho;
+        VU[ly * NLX + lx] = (R)(q[IMU] / rho);
+        VV[ly * NLX + lx] = (R)(q[IMV] / rho);
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int ph = 0; ph < 2; ph++) {
+                const double a = ph == 0 ? q[IA1] : 1.0 - q[IA1], m = q[ph == 0 ? IM1 : IM2], e = q[ph == 0 ? IE1 : IE2];
+                const double L1 = a - m * c.phy.ph[ph].b, L2 = e - m * c.phy.ph[ph].q - L1 * c.phy.ph[ph].pi;
+                LS[(ly * NLX + lx) * 4 + 2 * ph] = (R)L1;
+                LS[(ly * NLX + lx) * 4 + 2 * ph + 1] = (R)L2;
+            }
+        }
     }
-    auto vel = [&](int ly, int lx, double* v) { v[0] = VU[ly * NLX + lx]; v[1] = VV[ly * NLX + lx]; };
+    auto vel = [&](int ly, int lx, R* v) { v[0] = VU[ly * NLX + lx]; v[1] = VV[ly * NLX + lx]; };
+    auto lterms = [&](int ly, int lx) -> const R* { return MIXED ? LS + (ly * NLX + lx) * 4 : nullptr; };
     __syncthreads();
 
     // 2. reconstruction of cells -1..TX (x) and -1..TY (y)
@@ -215,18 +248,19 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         const int gi = i0 - 1 + rx, gj = j0 + ry;
         if (gi > g.nx || gj >= g.ny) continue;
         const int lx = rx + 1, ly = ry + HY;
-        double Ua[NV], Uc[NV], Ub[NV];
+        R Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
         for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, lx - 1); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly, lx + 1); }
-        double phi, phis, slu, slv, va[2], vc[2], vb[2];
+        R phi, phis, slu, slv, va[2], vc[2], vb[2];
         vel(ly, lx - 1, va); vel(ly, lx, vc); vel(ly, lx + 1, vb);
-        recon3(c.phy, Ua, Uc, Ub, VS[ly * NLX + lx - 1], VS[ly * NLX + lx], VS[ly * NLX + lx + 1], ES[ly * NLX + lx - 1],
-               ES[ly * NLX + lx], ES[ly * NLX + lx + 1], va, vc, vb, phi, phis, slu, slv);
+        recon3<R>(c.phy, Ua, Uc, Ub, VS[ly * NLX + lx - 1], VS[ly * NLX + lx], VS[ly * NLX + lx + 1], ES[ly * NLX + lx - 1],
+                  ES[ly * NLX + lx], ES[ly * NLX + lx + 1], va, vc, vb, phi, phis, slu, slv, lterms(ly, lx - 1),
+                  lterms(ly, lx), lterms(ly, lx + 1));
         RX[(0 * TY + ry) * NRX + rx] = phi;
         RX[(1 * TY + ry) * NRX + rx] = slu;
         RX[(2 * TY + ry) * NRX + rx] = slv;
         const bool own = (gi >= i0 && gi < i0 + TX) || gi == -1 || gi == g.nx;
-        if (own) c.phis_x[rxi(g, gi, gj)] = phis;
+        if (own) c.phis_x[rxi(g, gi, gj)] = (double)phis;
     }
     if (TWO_D) {
         for (int t = tid; t < TX * NRY; t += nth) {
@@ -234,18 +268,19 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
             const int gi = i0 + rx, gj = j0 - 1 + ry;
             if (gi >= g.nx || gj > g.ny) continue;
             const int lx = rx + 2, ly = ry + 1;
-            double Ua[NV], Uc[NV], Ub[NV];
+            R Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly - 1, lx); Uc[k] = Q(k, ly, lx); Ub[k] = Q(k, ly + 1, lx); }
-            double phi, phis, slu, slv, va[2], vc[2], vb[2];
+            R phi, phis, slu, slv, va[2], vc[2], vb[2];
             vel(ly - 1, lx, va); vel(ly, lx, vc); vel(ly + 1, lx, vb);
-            recon3(c.phy, Ua, Uc, Ub, VS[(ly - 1) * NLX + lx], VS[ly * NLX + lx], VS[(ly + 1) * NLX + lx],
-                   ES[(ly - 1) * NLX + lx], ES[ly * NLX + lx], ES[(ly + 1) * NLX + lx], va, vc, vb, phi, phis, slu, slv);
+            recon3<R>(c.phy, Ua, Uc, Ub, VS[(ly - 1) * NLX + lx], VS[ly * NLX + lx], VS[(ly + 1) * NLX + lx],
+                      ES[(ly - 1) * NLX + lx], ES[ly * NLX + lx], ES[(ly + 1) * NLX + lx], va, vc, vb, phi, phis, slu, slv,
+                      lterms(ly - 1, lx), lterms(ly, lx), lterms(ly + 1, lx));
             RY[(0 * NRY + ry) * TX + rx] = phi;
             RY[(1 * NRY + ry) * TX + rx] = slu;
             RY[(2 * NRY + ry) * TX + rx] = slv;
             const bool own = (gj >= j0 && gj < j0 + TY) || gj == -1 || gj == g.ny;
-            if (own) c.phis_y[ryi(g, gi, gj)] = phis;
+            if (own) c.phis_y[ryi(g, gi, gj)] = (double)phis;
         }
     }
     __syncthreads();
@@ -257,7 +292,7 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         const int gl = i0 - 1 + f, gj = j0 + ry;
         if (gl > g.nx - 1 || gj >= g.ny) continue;
         const int ly = ry + HY, la = f + 1;   // local column of the left cell
-        double Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
+        R Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
         // right face value of the left cell
 #pragma unroll
         for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, la - 1); Uc[k] = Q(k, ly, la); Ub[k] = Q(k, ly, la + 1); }
@@ -268,20 +303,20 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, ly, la + 2); }
         face_value(Ua, Uc, Ub, VU[ly * NLX + la + 1], VV[ly * NLX + la + 1], RX[(0 * TY + ry) * NRX + f + 1],
                    RX[(1 * TY + ry) * NRX + f + 1], RX[(2 * TY + ry) * NRX + f + 1], false, wL);
-        double uL, uR;
-        rusanov_flux(wR, wL, 0, fl, uL, uR);
-        const double ube = 0.5 * (uL + uR);
+        R uL, uR;
+        rusanov_flux<R>(wR, wL, 0, fl, uL, uR);
+        const R ube = R(0.5) * (uL + uR);
 #pragma unroll
         for (int k = 0; k < NV; k++) FX[(k * TY + ry) * NFX + f] = fl[k];
         FX[(8 * TY + ry) * NFX + f] = ube;
         if (f >= 1 || i0 == 0) {  // faces i0 .. i0+TX-1 belong to this tile, face -1/2 to the first
             const size_t fi = fxi(g, gl, gj);
-            c.ube_x[fi] = ube;
+            c.ube_x[fi] = (double)ube;
             const int K[4] = {IM1, IM2, IE1, IE2};
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                c.fxd[q * nfx + fi] = wR[K[q]];
-                c.fxd[(4 + q) * nfx + fi] = wL[K[q]];
+                c.fxd[q * nfx + fi] = (double)wR[K[q]];
+                c.fxd[(4 + q) * nfx + fi] = (double)wL[K[q]];
             }
         }
     }
@@ -291,7 +326,7 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
             const int gi = i0 + rx, gl = j0 - 1 + f;
             if (gi >= g.nx || gl > g.ny - 1) continue;
             const int lx = rx + 2, la = f + 1;
-            double Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
+            R Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) { Ua[k] = Q(k, la - 1, lx); Uc[k] = Q(k, la, lx); Ub[k] = Q(k, la + 1, lx); }
             face_value(Ua, Uc, Ub, VU[la * NLX + lx], VV[la * NLX + lx], RY[(0 * NRY + f) * TX + rx],
@@ -300,20 +335,20 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
             for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, la + 2, lx); }
             face_value(Ua, Uc, Ub, VU[(la + 1) * NLX + lx], VV[(la + 1) * NLX + lx], RY[(0 * NRY + f + 1) * TX + rx],
                        RY[(1 * NRY + f + 1) * TX + rx], RY[(2 * NRY + f + 1) * TX + rx], false, wL);
-            double vL, vR;
-            rusanov_flux(wR, wL, 1, fl, vL, vR);
-            const double ube = 0.5 * (vL + vR);
+            R vL, vR;
+            rusanov_flux<R>(wR, wL, 1, fl, vL, vR);
+            const R ube = R(0.5) * (vL + vR);
 #pragma unroll
             for (int k = 0; k < NV; k++) FY[(k * NFY + f) * TX + rx] = fl[k];
             FY[(8 * NFY + f) * TX + rx] = ube;
             if (f >= 1 || j0 == 0) {
                 const size_t fi = fyi(g, gi, gl);
-                c.ube_y[fi] = ube;
+                c.ube_y[fi] = (double)ube;
                 const int K[4] = {IM1, IM2, IE1, IE2};
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    c.fyd[q * nfy + fi] = wR[K[q]];
-                    c.fyd[(4 + q) * nfy + fi] = wL[K[q]];
+                    c.fyd[q * nfy + fi] = (double)wR[K[q]];
+                    c.fyd[(4 + q) * nfy + fi] = (double)wL[K[q]];
                 }
             }
         }
@@ -334,14 +369,15 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
         for (int k = 0; k < NV; k++) {
             double s = c.Un.v[k][x];
             for (int r = 0; r < c.nH; r++) s = s + c.ci[r] * c.Hprev[((size_t)r * NV + k) * c.n + x];
-            X[k] = s - rx_ * (FX[(k * TY + ry) * NFX + rx + 1] - FX[(k * TY + ry) * NFX + rx]);
+            X[k] = s - rx_ * (double)(FX[(k * TY + ry) * NFX + rx + 1] - FX[(k * TY + ry) * NFX + rx]);
         }
-        const double qa1 = Q(IA1, ly, lx);
-        X[IA1] += rx_ * qa1 * (FX[(8 * TY + ry) * NFX + rx + 1] - FX[(8 * TY + ry) * NFX + rx]);
+        const double qa1 = (double)Q(IA1, ly, lx);
+        X[IA1] += rx_ * qa1 * (double)(FX[(8 * TY + ry) * NFX + rx + 1] - FX[(8 * TY + ry) * NFX + rx]);
         if (TWO_D) {
 #pragma unroll
-            for (int k = 0; k < NV; k++) X[k] -= ry_ * (FY[(k * NFY + ry + 1) * TX + rx] - FY[(k * NFY + ry) * TX + rx]);
-            X[IA1] += ry_ * qa1 * (FY[(8 * NFY + ry + 1) * TX + rx] - FY[(8 * NFY + ry) * TX + rx]);
+            for (int k = 0; k < NV; k++)
+                X[k] -= ry_ * (double)(FY[(k * NFY + ry + 1) * TX + rx] - FY[(k * NFY + ry) * TX + rx]);
+            X[IA1] += ry_ * qa1 * (double)(FY[(8 * NFY + ry + 1) * TX + rx] - FY[(8 * NFY + ry) * TX + rx]);
         }
 #pragma unroll
         for (int k = 0; k < NV; k++) c.Xs.v[k][x] = X[k];
@@ -349,25 +385,30 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     }
 }
 
-template <int TX, int TY, bool TWO_D>
+template <class R, int TX, int TY, bool TWO_D>
 void launch_tile(const Ctx& c, cudaStream_t st) {
-    using T = FluxTile<TX, TY, TWO_D>;
+    using T = FluxTile<R, TX, TY, TWO_D>;
     static unsigned long long configured = 0;  // one bit per device: the attribute is per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(configured & (1ull << dev))) {
-        cudaFuncSetAttribute(k_flux<TX, TY, TWO_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
+        cudaFuncSetAttribute(k_flux<R, TX, TY, TWO_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
         configured |= 1ull << dev;
     }
     const dim3 grid((unsigned)((c.g.nx + TX - 1) / TX), TWO_D ? (unsigned)((c.g.ny + TY - 1) / TY) : 1u);
-    k_flux<TX, TY, TWO_D><<<grid, TX * TY, T::BYTES, st>>>(c);
+    k_flux<R, TX, TY, TWO_D><<<grid, TX * TY, T::BYTES, st>>>(c);
 }
 
 }  // namespace
 
 void launch_flux(const Ctx& c, cudaStream_t st) {
-    if (c.g.ny > 1) launch_tile<32, 8, true>(c, st);
-    else launch_tile<256, 1, false>(c, st);
+    if (c.prec) {  // precision form: reconstruction and fluxes in FP32
+        if (c.g.ny > 1) launch_tile<float, 32, 8, true>(c, st);
+        else launch_tile<float, 256, 1, false>(c, st);
+    } else {
+        if (c.g.ny > 1) launch_tile<double, 32, 8, true>(c, st);
+        else launch_tile<double, 256, 1, false>(c, st);
+    }
     if (c.nlaunch) *c.nlaunch += 1;
 }
 

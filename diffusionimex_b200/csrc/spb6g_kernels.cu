@@ -514,6 +514,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_jac_finish(Ctx c) {
         if (twoD) { e += c.aS[x]; e += c.aN[x]; }
         c.A1[x] = e;
         c.dinv[x] = aC != 0 ? 1.0 / aC : 1.0;
+        if (c.prec) {  // precision form: the SpMV's FP32 copy of the diagonals
+            c.fC[x] = (float)aC; c.fW[x] = (float)c.aW[x]; c.fE[x] = (float)c.aE[x];
+            if (twoD) { c.fS[x] = (float)c.aS[x]; c.fN[x] = (float)c.aN[x]; }
+        }
         const double b = -c.G[x];
         acc[0] = e;
         acc[1] = b;
@@ -930,11 +934,19 @@ SPB6G_DEV void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "
 
 // Five-point pass over one strip.  hv: the PS_HV operands of the scaled stencil
 // value ph(k) (rows j0-1 .. j0+J, columns i0-1 .. i0+32, boundary-mapped);
-// rv: NRV operands read at the row itself.  phf(stage, col) gives ph from a row
-// stage; out(stage, col, phS, phW, phC, phE, phN, x) consumes a row.
-template <int NRV, class PH, class OUT>
+// mat: the five matrix diagonals (self, W, E, S, N) at the row itself, of type MT
+// (FP64, or FP32 in the precision form); ex: NEX FP64 operands at the row itself.
+// phf(stage, col) gives ph from a row stage; out(a, e, stage, col, phS, phW, phC,
+// phE, phN, x) consumes a row, a[m * 32] being diagonal m and e[v * 32] operand v.
+constexpr int PS_HV_BYTES = PS_HV * 34 * 8;
+template <class MT>
+SPB6G_DEV void cp_async_el(MT* s, const MT* gp) {
+    if constexpr (sizeof(MT) == 8) cp_async8((double*)s, (const double*)gp);
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)), "l"(gp) : "memory");
+}
+template <class MT, int NEX, class PH, class OUT>
 SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const double* const (&hv)[PS_HV],
-                             const double* const (&rv)[NRV], PH phf, OUT out) {
+                             const MT* const (&mat)[5], const double* const* ex, PH phf, OUT out) {
     const int lane = threadIdx.x & 31;
     const int nload = st.J + 2;
     double* stages = ws;
@@ -942,6 +954,8 @@ SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const d
     const int ic_own = map_col(g, st.i0 + lane);
     const int ic_halo = lane == 0 ? map_col(g, st.i0 - 1) : map_col(g, st.i0 + 32);
     const bool own = st.i0 + lane < g.nx;
+    auto matp = [&](double* sp) { return (MT*)((char*)sp + PS_HV_BYTES); };
+    auto exp_ = [&](double* sp) { return (double*)((char*)sp + PS_HV_BYTES + 5 * 32 * sizeof(MT)); };
     auto issue = [&](int t) {
         if (t < nload) {
             double* sp = stages + (t % PS_D) * PS_STAGE;
@@ -953,8 +967,12 @@ SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const d
                 for (int v = 0; v < PS_HV; v++) cp_async8(sp + v * 34 + (lane ? 33 : 0), hv[v] + rb + ic_halo);
             }
             if (own && t >= 1 && t <= st.J) {
+                MT* mp = matp(sp);
 #pragma unroll
-                for (int v = 0; v < NRV; v++) cp_async8(sp + PS_HV * 34 + v * 32 + lane, rv[v] + rb + ic_own);
+                for (int m = 0; m < 5; m++) cp_async_el<MT>(mp + m * 32 + lane, mat[m] + rb + ic_own);
+                double* ep = exp_(sp);
+#pragma unroll
+                for (int v = 0; v < NEX; v++) cp_async8(ep + v * 32 + lane, ex[v] + rb + ic_own);
             }
         }
         cp_commit();
@@ -970,11 +988,11 @@ SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const d
         if (lane < 2) pr[lane ? 33 : 0] = phf(sp, lane ? 33 : 0);
         __syncwarp();
         if (t >= 2 && own) {
-            const double* so = stages + ((t - 1) % PS_D) * PS_STAGE;
+            double* so = stages + ((t - 1) % PS_D) * PS_STAGE;
             const double* pS = phr + ((t - 2) % 3) * 34;
             const double* pC = phr + ((t - 1) % 3) * 34;
-            out(so, lane + 1, pS[lane + 1], pC[lane], pC[lane + 1], pC[lane + 2], pr[lane + 1],
-                (st.j0 + t - 2) * g.nx + st.i0 + lane);
+            out((const MT*)matp(so) + lane, (const double*)exp_(so) + lane, (const double*)so, lane + 1, pS[lane + 1],
+                pC[lane], pC[lane + 1], pC[lane + 2], pr[lane + 1], (st.j0 + t - 2) * g.nx + st.i0 + lane);
         }
         __syncwarp();
         issue(t + PS_D - 1);
@@ -1009,6 +1027,18 @@ SPB6G_DEV void row_strip(const Geom& g, const Strip& st, double* ws, const doubl
     __syncwarp();
 }
 
+// The five diagonals in the SpMV's precision.
+template <class MT>
+SPB6G_DEV const MT* diag(const Ctx& c, int m);
+template <>
+SPB6G_DEV const double* diag<double>(const Ctx& c, int m) {
+    return m == 0 ? c.aC : m == 1 ? c.aW : m == 2 ? c.aE : m == 3 ? c.aS : c.aN;
+}
+template <>
+SPB6G_DEV const float* diag<float>(const Ctx& c, int m) {
+    return m == 0 ? c.fC : m == 1 ? c.fW : m == 2 ? c.fE : m == 3 ? c.fS : c.fN;
+}
+
 #define PB_STRIPS_BEGIN                                                         \
     for (int s_ = wid; s_ < sg.nstrips; s_ += nwarps) {                         \
         const Strip st = strip_at(c.g, sg, s_);
@@ -1020,6 +1050,7 @@ SPB6G_DEV void row_strip(const Geom& g, const Strip& st, double* ws, const doubl
 // with 1^T v = 1^T q + cc 1^T A1, so t = A M^-1 s and its two inner products are
 // finished in the same pass as s (the reference sums s itself; the identity is
 // exact, the rounding of this one scalar differs).
+template <class MT>
 __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol, int maxit) {
     extern __shared__ double pb_smem[];
     const int n = c.n, nx = c.g.nx;
@@ -1040,6 +1071,7 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     double* __restrict__ bt = c.bt;
     double* __restrict__ dP = c.dP;
     auto slot = [&](int k) { return slots + (size_t)(k & 1) * 4 * G; };
+    const MT* const mat[5] = {diag<MT>(c, 0), diag<MT>(c, 1), diag<MT>(c, 2), diag<MT>(c, 3), diag<MT>(c, 4)};
 
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
@@ -1078,27 +1110,28 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
             {
                 const double beta = (r0r / rho) * (alpha / omega), om = omega;
                 const double* const hv[PS_HV] = {br, p_old, bv, dinv};
-                const double* const rv[6] = {c.aC, c.aW, c.aE, c.aS, c.aN, c.br0};
+                const double* const ex[1] = {c.br0};
                 auto pn = [&](const double* sp, int k) { return sp[k] + beta * (sp[34 + k] - om * sp[68 + k]); };
                 auto phf = [&](const double* sp, int k) { return sp[102 + k] * pn(sp, k); };
                 a3[0] = a3[1] = a3[2] = 0.0;
                 PB_STRIPS_BEGIN
-                    stencil_strip<6>(c.g, st, ws, hv, rv, phf,
-                        [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
-                            const double* a = so + PS_HV * 34 + (k - 1);
+                    stencil_strip<MT, 1>(c.g, st, ws, hv, mat, ex, phf,
+                        [&](const MT* a, const double* e, const double* so, int k, double phS, double phW, double phC,
+                            double phE, double phN, int x) {
                             const double p = pn(so, k);
-                            double q = 0;
-                            q += a[0] * phC;
-                            q += a[32] * phW;
-                            q += a[64] * phE;
+                            MT qm = 0;  // the SpMV row in the matrix precision
+                            qm += a[0] * (MT)phC;
+                            qm += a[32] * (MT)phW;
+                            qm += a[64] * (MT)phE;
                             if (two_d) {
-                                q += a[96] * phS;
-                                q += a[128] * phN;
+                                qm += a[96] * (MT)phS;
+                                qm += a[128] * (MT)phN;
                             }
+                            const double q = (double)qm;
                             p_new[x] = p;
                             bq[x] = q;
                             a3[0] += p;
-                            a3[1] += a[160] * q;
+                            a3[1] += e[0] * q;
                             a3[2] += q;
                         });
                 PB_STRIPS_END
@@ -1112,24 +1145,24 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
             {
                 const double al = alpha, ccv = cc, csv = cs;
                 const double* const hv[PS_HV] = {br, bq, A1, dinv};
-                const double* const rv[5] = {c.aC, c.aW, c.aE, c.aS, c.aN};
                 auto sv = [&](const double* sp, int k) { return sp[k] - al * (sp[34 + k] + ccv * sp[68 + k]); };
                 auto phf = [&](const double* sp, int k) { return sp[102 + k] * sv(sp, k); };
                 a3[0] = a3[1] = a3[2] = 0.0;
                 PB_STRIPS_BEGIN
-                    stencil_strip<5>(c.g, st, ws, hv, rv, phf,
-                        [&](const double* so, int k, double phS, double phW, double phC, double phE, double phN, int x) {
-                            const double* a = so + PS_HV * 34 + (k - 1);
+                    stencil_strip<MT, 0>(c.g, st, ws, hv, mat, nullptr, phf,
+                        [&](const MT* a, const double*, const double* so, int k, double phS, double phW, double phC,
+                            double phE, double phN, int x) {
                             const double v = so[34 + k] + ccv * so[68 + k];
                             const double s = so[k] - al * v;
-                            double u = 0;
-                            u += a[0] * phC;
-                            u += a[32] * phW;
-                            u += a[64] * phE;
+                            MT um = 0;
+                            um += a[0] * (MT)phC;
+                            um += a[32] * (MT)phW;
+                            um += a[64] * (MT)phE;
                             if (two_d) {
-                                u += a[96] * phS;
-                                u += a[128] * phN;
+                                um += a[96] * (MT)phS;
+                                um += a[128] * (MT)phN;
                             }
+                            const double u = (double)um;
                             const double tv = u + csv * so[68 + k];
                             bv[x] = v;
                             bs[x] = s;
@@ -1205,8 +1238,14 @@ int bicg_solve_blocks(int device, int n) {
     int per_sm = 0, sms = 0, coop = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(k_bicg_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicg_solve, PB_THREADS, PB_SMEM) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_bicg_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(k_bicg_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess)
+        return 0;
+    int per_sm_f = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicg_solve<double>, PB_THREADS, PB_SMEM) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_bicg_solve<float>, PB_THREADS, PB_SMEM) != cudaSuccess)
+        return 0;
+    if (per_sm_f < per_sm) per_sm = per_sm_f;
     // about four rows per thread at least: small grids use fewer blocks (cheaper barriers)
     const long want = ((long)n + 4L * PB_THREADS - 1) / (4L * PB_THREADS);
     long G = (long)per_sm * sms;
@@ -1216,7 +1255,8 @@ int bicg_solve_blocks(int device, int n) {
 int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int G) {
     void* args[] = {(void*)&c, (void*)&tol, (void*)&maxit};
     count(c, 1);
-    return cudaLaunchCooperativeKernel((const void*)k_bicg_solve, dim3(G), dim3(PB_THREADS), args, PB_SMEM, st) == cudaSuccess ? 0 : -1;
+    const void* fn = c.prec ? (const void*)k_bicg_solve<float> : (const void*)k_bicg_solve<double>;
+    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(PB_THREADS), args, PB_SMEM, st) == cudaSuccess ? 0 : -1;
 }
 
 // ============================================================ learned warm start (no counterpart in the reference)

@@ -552,6 +552,11 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.smask = (unsigned char*)A(n / 8 + 1);
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
     c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
+    c.prec = cfg->precision ? 1 : 0;
+    if (c.prec) {
+        auto Af = [&](size_t cnt) { return (float*)A(cnt / 2 + 1); };
+        c.fC = Af(n); c.fW = Af(n); c.fE = Af(n); c.fS = Af(n); c.fN = Af(n);
+    }
     c.br = A(n); c.br0 = A(n); c.bp = A(n); c.bv = A(n); c.bq = A(n); c.bs = A(n); c.bu = A(n); c.bt = A(n);
     c.tcp = A(n); c.tdp = A(n);
     for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];

@@ -47,7 +47,7 @@ class Config(ctypes.Structure):
         ("dtfix", ctypes.c_double), ("rus_local", ctypes.c_int32), ("limiter", ctypes.c_int32), ("acdt", ctypes.c_int32),
         ("newton_tol", ctypes.c_double), ("newton_iter", ctypes.c_int32), ("bicg_tol", ctypes.c_double),
         ("bicg_iter", ctypes.c_int32), ("share_mode", ctypes.c_int32), ("tend", ctypes.c_double),
-        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -130,6 +130,7 @@ def make_config(case: dict, device: int = 0) -> Config:
         ph = case["phases"][k]
         c.gamma[k], c.pinf[k], c.q[k], c.qp[k], c.cv[k], c.b[k] = ph["g"], ph["pinf"], ph["q"], ph["qp"], ph["cv"], ph["b"]
     c.device = device
+    c.precision = int(case.get("precision", 0))
     return c
 
 

@@ -68,7 +68,10 @@ typedef struct {
     int32_t share_mode;             /* SHARE_MODE (physics :436) */
     double tend;                    /* time_stop */
     int32_t device;                 /* CUDA device ordinal */
-    int32_t reserved[7];
+    int32_t precision;              /* 0: FP64 throughout; 1: precision form -- FP32 reconstruction,
+                                       Rusanov fluxes and SpMV, FP64 EOS inversion, relaxation Newton,
+                                       BiCGStab reductions and residuals (no counterpart in the reference) */
+    int32_t reserved[6];
 } spb6g_config;
 
 /* Run statistics: the counters of the reference's stats line (:98-99, :1425). */
