@@ -94,10 +94,35 @@ struct FeatureNorm {
     double tscale;
 };
 
+// One instance of the batched form (1D, non-periodic: the Thomas path): its stage
+// context and the time-loop state that the host driver keeps for a single grid.
+struct BatchInst {
+    Ctx c;
+    double* U[NV];
+    double* Ust[NV];
+    double* Hs;
+    double* Pbuf[3];
+    int pmain;  // index of the accepted pressure in Pbuf
+    int status;
+    double t, dt, dtprev;
+    int startup;
+    // configuration
+    double cfl, cfl_ac, dtfix, tend, newton_tol;
+    int ramp, acdt, rk, newton_iter;
+    // statistics
+    long long steps, rejects, rk1, stages, newton_it, floor_count;
+    double maxres;
+};
+
 // ------------------------------------------------------------ launchers (spb6g_kernels.cu)
 int red_blocks(int n, int threads = RED_THREADS);
 // fused stage combination + reconstruction + Rusanov update + face donors (replaces combine/recon/update)
 void launch_flux(const Ctx& c, cudaStream_t st);
+// the fused explicit kernel's tile as a block-level device function (spb6g_flux.cu), and the
+// shared-memory bytes of a 1D tile of width tx (128 or 256)
+template <class R, int TX, int TY, bool TWO_D>
+__device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_bytes, int tid, int nth);
+size_t flux_tile_bytes_1d(int tx);
 void launch_prep(const Ctx& c, cudaStream_t st);
 // weak-shock budget + strong-shock worklist (and smask); strong-shock budget of the worklist
 void launch_shock_weak(const Ctx& c, cudaStream_t st);
@@ -118,6 +143,10 @@ void launch_bicg_graph(const Ctx& c, cudaStream_t st, cudaGraphExec_t exec, int 
 int bicg_solve_blocks(int device, int n);
 int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int G);
 void launch_thomas(const Ctx& c, cudaStream_t st);
+// batched form: `count` instances, `nsteps` time steps each, one block of `threads` per instance,
+// flux tiles of width tw (128 or 256); one persistent launch
+int launch_batch(BatchInst* insts, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st);
+int batch_max_blocks(int threads, int tw, int device);
 // learned warm start: BF16 feature rows (n x 64), dP = y * tscale, training targets
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
 void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale);

@@ -183,13 +183,17 @@ SPB6G_DEV void rusanov_flux(const R* QL, const R* QR, int d, R* flux, R& vL, R& 
     for (int k = 0; k < NV; k++) flux[k] = R(0.5) * (QL[k] * vL + QR[k] * vR) - R(0.5) * a * (QR[k] - QL[k]);
 }
 
+}  // namespace
+
+// One TX x TY tile (tile coordinates bx, by) computed by `nth` threads of a block
+// (thread index tid); `smem_bytes` holds FluxTile<...>::BYTES.  Used by k_flux
+// (one tile per block) and by the batched driver (a block walks its instance's tiles).
 template <class R, int TX, int TY, bool TWO_D>
-__global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
+__device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_bytes, int tid, int nth) {
     using T = FluxTile<R, TX, TY, TWO_D>;
     constexpr bool MIXED = sizeof(R) != sizeof(double);
     constexpr int HY = T::HY, NLX = T::NLX, NLY = T::NLY, NRX = T::NRX, NRY = T::NRY, NFX = T::NFX, NFY = T::NFY;
-    extern __shared__ __align__(16) unsigned char flux_smem[];
-    R* Qs_ = (R*)flux_smem;                  // [NV][NLY][NLX]
+    R* Qs_ = (R*)smem_bytes;                 // [NV][NLY][NLX]
     R* VS = Qs_ + T::Q_SZ;                   // [NLY][NLX]
     R* ES = VS + NLX * NLY;
     R* VU = ES + NLX * NLY;                  // cell velocity u
@@ -200,8 +204,7 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     R* FY = FX + T::FX_SZ;                   // [9][NFY][TX]
     R* LS = FY + T::FY_SZ;                   // precision form: [NLY][NLX][4] admissibility terms
     const Geom& g = c.g;
-    const int tid = threadIdx.x, nth = TX * TY;
-    const int i0 = blockIdx.x * TX, j0 = TWO_D ? blockIdx.y * TY : 0;
+    const int i0 = bx * TX, j0 = TWO_D ? by * TY : 0;
     auto Q = [&](int k, int ly, int lx) -> R& { return Qs_[(k * NLY + ly) * NLX + lx]; };
     auto in_cross = [&](int lx, int ly) {
         if (!TWO_D) return true;
@@ -385,6 +388,17 @@ __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     }
 }
 
+template __device__ void flux_tile<double, 128, 1, false>(const Ctx&, int, int, unsigned char*, int, int);
+template __device__ void flux_tile<double, 256, 1, false>(const Ctx&, int, int, unsigned char*, int, int);
+
+namespace {
+
+template <class R, int TX, int TY, bool TWO_D>
+__global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
+    extern __shared__ __align__(16) unsigned char flux_smem[];
+    flux_tile<R, TX, TY, TWO_D>(c, blockIdx.x, blockIdx.y, flux_smem, threadIdx.x, TX * TY);
+}
+
 template <class R, int TX, int TY, bool TWO_D>
 void launch_tile(const Ctx& c, cudaStream_t st) {
     using T = FluxTile<R, TX, TY, TWO_D>;
@@ -400,6 +414,10 @@ void launch_tile(const Ctx& c, cudaStream_t st) {
 }
 
 }  // namespace
+
+size_t flux_tile_bytes_1d(int tx) {
+    return tx == 128 ? FluxTile<double, 128, 1, false>::BYTES : FluxTile<double, 256, 1, false>::BYTES;
+}
 
 void launch_flux(const Ctx& c, cudaStream_t st) {
     if (c.prec) {  // precision form: reconstruction and fluxes in FP32

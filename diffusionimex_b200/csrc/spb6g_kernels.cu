@@ -5,6 +5,7 @@
 
 #include <cuda_bf16.h>
 
+#include "../../include/spb6g.h"
 #include "spb6g_ctx.cuh"
 
 namespace spb6g {
@@ -64,11 +65,11 @@ SPB6G_DEV double pold_at(const Ctx& c, int i, int j) { return c.P[mp_index(c.g, 
 // the frozen sound speed c_f (cfz :948-955); interior cells also get the
 // residual scale K + P_E (:960-971) and the admissibility check (:928-929).
 SPB6G_DEV int pad_index(const Geom& g, int i, int j) { return (i + 2) + (g.ny > 1 ? (j + 2) * (g.nx + 4) : 0); }  // 1D: one row
-__global__ void k_prep_cell(Ctx c) {
+SPB6G_DEV long prep_cells(const Geom& g) { return (long)(g.nx + 4) * (g.ny > 1 ? g.ny + 4 : 1); }
+SPB6G_DEV void prep_cell_at(const Ctx& c, long t) {
     const Geom& g = c.g;
-    const int W = g.nx + 4, Hh = g.ny > 1 ? g.ny + 4 : 1;
-    const long tot = (long)W * Hh;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+    const int W = g.nx + 4;
+    {
         const int i = (int)(t % W) - 2, j = g.ny > 1 ? (int)(t / W) - 2 : 0;
         double X[NV];
         xs_at(c, i, j, X);
@@ -79,7 +80,7 @@ __global__ void k_prep_cell(Ctx c) {
         c.pad_u[p] = X[IMU] / rho;
         c.pad_v[p] = X[IMV] / rho;
         c.pad_cz[p] = cfz(c.phy, X, a2);
-        if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) continue;
+        if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return;
         const size_t x = (size_t)i + (size_t)j * g.nx;
         const double a1 = X[IA1], m1 = X[IM1], m2 = X[IM2], sa = a1 + a2;
         if (!(sa > 0 && rho > 0)) atomicOr(&c.ns->err, 2);
@@ -93,6 +94,10 @@ __global__ void k_prep_cell(Ctx c) {
         }
         c.kw[x] = K + PE;
     }
+}
+__global__ void k_prep_cell(Ctx c) {
+    const long tot = prep_cells(c.g);
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) prep_cell_at(c, t);
 }
 
 // Face coefficients of the implicit face velocity / pressure (set_face :1001-1023, dil_jump :989-1000)
@@ -143,10 +148,10 @@ SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, dou
     kp += phi * psiP / (ZL + ZR);
     pv = phi * psiU * ZL * ZR / (ZL + ZR) * D;
 }
-__global__ void k_prep_fx(Ctx c) {
+SPB6G_DEV void prep_fx_at(const Ctx& c, long t) {
     const Geom& g = c.g;
     const long tot = (long)(g.nx + 1) * g.ny;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+    {
         const int i = (int)(t % (g.nx + 1)) - 1, j = (int)(t / (g.nx + 1));
         double ubs, kp, wl, pv, utL, utR;
         set_face(c, i, j, 0, ubs, kp, wl, pv, utL, utR);
@@ -155,6 +160,10 @@ __global__ void k_prep_fx(Ctx c) {
         c.fxd[8 * (size_t)tot + f] = utL;
         c.fxd[9 * (size_t)tot + f] = utR;
     }
+}
+__global__ void k_prep_fx(Ctx c) {
+    const long tot = (long)(c.g.nx + 1) * c.g.ny;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) prep_fx_at(c, t);
 }
 __global__ void k_prep_fy(Ctx c) {
     const Geom& g = c.g;
@@ -1323,8 +1332,7 @@ void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itsca
 }
 
 // ============================================================ Thomas (1D non-periodic, :858-863)
-__global__ void k_thomas(Ctx c) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+SPB6G_DEV void thomas_solve(const Ctx& c) {
     const Geom& g = c.g;
     const int n = g.nx;
     double* cp = c.tcp;
@@ -1350,6 +1358,10 @@ __global__ void k_thomas(Ctx c) {
     c.dP[n - 1] = dp[n - 1];
     for (int r = n - 2; r >= 0; r--) c.dP[r] = dp[r] - cp[r] * c.dP[r + 1];
 }
+__global__ void k_thomas(Ctx c) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    thomas_solve(c);
+}
 void launch_thomas(const Ctx& c, cudaStream_t st) {
     k_thomas<<<1, 32, 0, st>>>(c);
     count(c, 1);
@@ -1374,17 +1386,18 @@ void launch_apply_step(const Ctx& c, cudaStream_t st) {
     k_apply_step<<<blocks_for(c.n), TPB, 0, st>>>(c);
     count(c, 1);
 }
-__global__ void k_floor(Ctx c, double tol) {
+SPB6G_DEV void floor_at(const Ctx& c, int x, double tol) {
     const Geom& g = c.g;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % g.nx, j = x / g.nx;
-        const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
-        double Gr;
-        CellRes o;
-        if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 4); continue; }
-        const double sig = closure_roundoff(c.phy, o.in, o.o.pbar);
-        if (fabs(Gr) > tol * (fabs(c.p_ref + p.c) + c.kw[x] + 1.0) + sig) atomicOr(&c.ns->fail, 4);
-    }
+    const int i = x % g.nx, j = x / g.nx;
+    const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
+    double Gr;
+    CellRes o;
+    if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 4); return; }
+    const double sig = closure_roundoff(c.phy, o.in, o.o.pbar);
+    if (fabs(Gr) > tol * (fabs(c.p_ref + p.c) + c.kw[x] + 1.0) + sig) atomicOr(&c.ns->fail, 4);
+}
+__global__ void k_floor(Ctx c, double tol) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) floor_at(c, x, tol);
 }
 void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
     k_floor<<<blocks_for(c.n), TPB, 0, st>>>(c, tol);
@@ -1392,14 +1405,14 @@ void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
 }
 
 // ============================================================ final state (:1056-1073) and H_s (:1363-1371)
-__global__ void k_final(Ctx c) {
+SPB6G_DEV void final_at(const Ctx& c, int x) {
     const Geom& g = c.g;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+    {
         const int i = x % g.nx, j = x / g.nx;
         const Nb5 p = gather_p(g, i, j, [&](int q) { return c.P[q]; });
         double Gr;
         CellRes o;
-        if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 8); continue; }
+        if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 8); return; }
         double U[NV];
         U[IA1] = o.o.a[0]; U[IM1] = o.in.mtr[0]; U[IM2] = o.in.mtr[1]; U[IMU] = o.mx; U[IMV] = o.my;
         U[IE1] = o.o.e[0]; U[IE2] = o.o.e[1]; U[IEN] = o.E;
@@ -1411,6 +1424,9 @@ __global__ void k_final(Ctx c) {
             c.H[(size_t)k * c.n + x] = (U[k] - qs) / c.adt;
         }
     }
+}
+__global__ void k_final(Ctx c) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) final_at(c, x);
 }
 void launch_final(const Ctx& c, cudaStream_t st) {
     k_final<<<blocks_for(c.n), TPB, 0, st>>>(c);
@@ -1466,6 +1482,311 @@ __global__ void k_pbar_init(Ctx c, CState U, double p_ref, double* P) {
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P) {
     k_pbar_init<<<blocks_for(c.n), TPB, 0, st>>>(c, U, p_ref, P);
     count(c, 1);
+}
+
+
+// ============================================================ batched form (no counterpart in the reference)
+// Hundreds of independent 1D instances in one persistent launch: block b runs
+// instance b's time loop -- the host driver's do_step / run_stage / Newton_Solver
+// decision for decision -- with every grid pass done by the block's threads
+// through the same per-cell functions as the single-grid kernels, so each
+// instance computes exactly what a single-grid solver on it computes.
+struct BatchShared {
+    Ctx c;
+    double red[32];
+    double bc;
+};
+SPB6G_DEV double b_max(double v, BatchShared& s) {
+    double a[1] = {v};
+    block_fold<RedMax, 1>(a, s.red);
+    if (threadIdx.x == 0) s.bc = a[0];
+    __syncthreads();
+    const double r = s.bc;
+    __syncthreads();
+    return r;
+}
+SPB6G_DEV int b_flag(const int* p) {
+    __syncthreads();
+    const int v = *(volatile const int*)p;
+    __syncthreads();
+    return v;
+}
+SPB6G_DEV void b_clear(int* p, int nwords) {
+    __syncthreads();
+    if ((int)threadIdx.x < nwords) atomicExch(p + threadIdx.x, 0);
+    __syncthreads();
+}
+// evalAll + norm (mode 0: at P into G, sc; mode 1: at Pn = P + lam dP into Gn, scn, Pn)
+SPB6G_DEV double b_residual(BatchShared& s, int mode, double lam) {
+    const Ctx& c = s.c;
+    const Geom& g = c.g;
+    double m = 0.0;
+    for (int x = threadIdx.x; x < c.n; x += blockDim.x) {
+        const int i = x % g.nx, j = x / g.nx;
+        Nb5 p = mode == 0 ? gather_p(g, i, j, [&](int q) { return c.P[q]; })
+                          : gather_p(g, i, j, [&](int q) { return c.P[q] + lam * c.dP[q]; });
+        double Gr;
+        const bool ok = residual_at(c, i, j, p, 0, -1, 0, Gr, nullptr);
+        const double sc = row_scale(c, i, j, p.c);
+        if (mode == 0) { c.G[x] = Gr; c.sc[x] = sc; }
+        else { c.Gn[x] = Gr; c.scn[x] = sc; c.Pn[x] = p.c; }
+        if (!ok) atomicOr(&c.ns->fail, 1);
+        else m = SMAX(m, SMAX(0.0, fabs(Gr) / (fabs(c.p_ref + p.c) + c.kw[x] + 1.0)));
+    }
+    return b_max(m, s);
+}
+SPB6G_DEV double b_inv_rate(BatchShared& s, const BatchInst& B, int acoustic) {  // caldt (:502-514)
+    const Ctx& c = s.c;
+    double m = 0.0;
+    for (int x = threadIdx.x; x < c.n; x += blockDim.x) {
+        double q[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) q[k] = B.U[k][x];
+        Prim w;
+        if (!prim_of(c.phy, q, w)) continue;
+        m = SMAX(m, SMAX(0.0, fabs(w.u) + (acoustic ? w.cf : 0.0)));
+    }
+    const double rate = b_max(m, s) / c.g.dx;
+    return rate > 0 ? 1.0 / rate : INFINITY;
+}
+SPB6G_DEV int b_newton(BatchShared& s, BatchInst& B, double& resfinal) {  // Newton_Solver (:799-904), Thomas path
+    Ctx& c = s.c;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const double tol = B.newton_tol;
+    b_clear(&c.ns->fail, 1);
+    double res = b_residual(s, 0, 0.0);
+    if (b_flag(&c.ns->err)) return SPB6G_INADMISSIBLE;
+    if (b_flag(&c.ns->fail)) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
+    for (int it = 0; it < B.newton_iter; it++) {
+        resfinal = res;
+        if (res < tol) return SPB6G_OK;
+        b_clear(&c.ns->fail, 1);
+        for (int t = tid; t < 3 * c.n; t += nth) jac_entry(c, t / 3, t % 3);
+        __syncthreads();
+        if (tid == 0) thomas_solve(c);
+        __syncthreads();
+        if (b_flag(&c.ns->fail)) return SPB6G_NEWTON_FAIL;
+        b_clear(&c.ns->fail, 1);
+        double m = 0.0;  // step criterion (:870-879)
+        for (int x = tid; x < c.n; x += nth) m = SMAX(m, SMAX(0.0, fabs(c.dP[x]) / (fabs(c.P[x]) + c.sc[x])));
+        const double sn = b_max(m, s);
+        double rn = b_residual(s, 1, 1.0);
+        if (sn < tol) {
+            for (int x = tid; x < c.n; x += nth) c.P[x] += c.dP[x];
+            if (tid == 0) B.newton_it++;
+            b_clear(&c.ns->fail, 1);
+            res = b_residual(s, 0, 0.0);
+            if (b_flag(&c.ns->fail)) return SPB6G_NEWTON_FAIL;
+            resfinal = res;
+            return SPB6G_OK;
+        }
+        double lam = 1.0;
+        bool acc = false;
+        for (int ls = 0; ls < 40; ls++) {  // line search (:880-888)
+            if (ls > 0) {
+                b_clear(&c.ns->fail, 1);
+                rn = b_residual(s, 1, lam);
+            }
+            if (!b_flag(&c.ns->fail)) {
+                if (rn < res * (1.0 - 1e-4 * lam) || rn < tol) { acc = true; res = rn; break; }
+            }
+            lam *= 0.5;
+        }
+        if (!acc) {  // round-off floor acceptance (:890-899)
+            resfinal = res;
+            b_clear(&c.ns->fail, 1);
+            for (int x = tid; x < c.n; x += nth) floor_at(c, x, tol);
+            if (b_flag(&c.ns->fail)) return SPB6G_NEWTON_FAIL;
+            if (tid == 0) B.floor_count++;
+            return SPB6G_OK;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double* q;
+            q = c.P; c.P = c.Pn; c.Pn = q;
+            q = c.G; c.G = c.Gn; c.Gn = q;
+            q = c.sc; c.sc = c.scn; c.scn = q;
+            B.newton_it++;
+        }
+        __syncthreads();
+    }
+    resfinal = res;
+    return res < tol ? SPB6G_OK : SPB6G_NEWTON_FAIL;
+}
+SPB6G_DEV void b_set_tab(int rk, double Ae[3][3], double Ai[3][3]) {  // main's set_tab, :1281-1303
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) Ae[a][b] = Ai[a][b] = 0;
+    if (rk == 1) {
+        Ai[0][0] = 1.0;
+    } else if (rk == 2) {
+        const double bb = 1.0 - 1.0 / sqrt(2.0), cc = 1.0 / (2.0 * bb);
+        Ae[1][0] = cc;
+        Ai[0][0] = bb;
+        Ai[1][0] = 1 - bb;
+        Ai[1][1] = bb;
+    } else if (rk == 3) {
+        const double r12 = 0.5, r13 = 1.0 / 3.0, r14 = 1.0 / 4.0;
+        Ae[1][0] = r12; Ae[2][0] = r12; Ae[2][1] = r12;
+        Ai[0][0] = r14; Ai[1][1] = r14; Ai[2][0] = r13; Ai[2][1] = r13; Ai[2][2] = r13;
+    }
+}
+template <int TW>
+SPB6G_DEV int b_stage(BatchShared& s, BatchInst& B, int rks, double Ae[3][3], double Ai[3][3], double dt, unsigned char* fsm) {
+    Ctx& c = s.c;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    __syncthreads();
+    if (tid == 0) {
+        for (int k = 0; k < NV; k++) c.Un.v[k] = B.U[k];
+        c.Hprev = B.Hs;
+        c.nH = rks;
+        for (int r = 0; r < 2; r++) {
+            c.ce[r] = r < rks ? Ae[rks][r] * dt : 0.0;
+            c.ci[r] = r < rks ? Ai[rks][r] * dt : 0.0;
+        }
+        c.adt = Ai[rks][rks] * dt;
+        c.tau = c.adt;
+        c.rx = c.tau / c.g.dx;
+        c.ry = c.tau / c.g.dy;
+        c.H = B.Hs + (size_t)rks * NV * c.n;
+    }
+    b_clear(&c.ns->fail, 3);  // fail, err, nstrong
+    const int ntiles = (c.g.nx + TW - 1) / TW;
+    for (int tl = 0; tl < ntiles; tl++) {
+        flux_tile<double, TW, 1, false>(c, tl, 0, fsm, tid, nth);
+        __syncthreads();
+    }
+    const long npad = prep_cells(c.g);
+    for (long q = tid; q < npad; q += nth) prep_cell_at(c, q);
+    __syncthreads();
+    for (long q = tid; q < c.g.nx + 1; q += nth) prep_fx_at(c, q);
+    __syncthreads();
+    for (int x = tid; x < c.n; x += nth) {
+        double Q[2];
+        shock_cell(c, x % c.g.nx, x / c.g.nx, Q, true);
+        c.qph0[x] = Q[0];
+        c.qph1[x] = Q[1];
+    }
+    __syncthreads();
+    double res = 0;
+    const int rc = b_newton(s, B, res);
+    if (rc != SPB6G_OK) return rc;
+    if (tid == 0 && res > B.maxres) B.maxres = res;
+    b_clear(&c.ns->fail, 1);
+    for (int x = tid; x < c.n; x += nth) final_at(c, x);
+    if (b_flag(&c.ns->fail)) return SPB6G_NEWTON_FAIL;
+    if (tid == 0) B.stages++;
+    return SPB6G_OK;
+}
+template <int TW>
+SPB6G_DEV int b_step(BatchShared& s, BatchInst& B, unsigned char* fsm) {  // main's loop body (:1316-1384)
+    Ctx& c = s.c;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    bool ramping = false;
+    double dt = B.dt, dtprev = B.dtprev;
+    if (B.dtfix > 0) dt = B.dtfix;
+    else {
+        dt = B.cfl * b_inv_rate(s, B, B.acdt);
+        if (B.ramp) {
+            if (dtprev < 0) dtprev = B.cfl_ac * b_inv_rate(s, B, 1) / 1.2;
+            if (dt > 1.2 * dtprev) { dt = 1.2 * dtprev; ramping = true; }
+        }
+        if (!isfinite(dt)) dt = B.cfl_ac * b_inv_rate(s, B, 1);
+    }
+    dt = SMIN(dt, B.tend - B.t);
+    if (!(dt > 1e-12 * B.tend)) return SPB6G_DT_UNDERFLOW;
+    bool done = false;
+    double Ae[3][3], Ai[3][3];
+    for (int attempt = 0; attempt < 30 && !done; attempt++) {
+        const bool first_order = B.ramp && ramping && B.startup;
+        const int rk = first_order ? 1 : B.rk;
+        __syncthreads();
+        if (tid == 0 && rk == 1) B.rk1++;
+        b_set_tab(rk, Ae, Ai);
+        // begin_attempt_pressure: the Newton iterate starts as a copy of the accepted pressure
+        int other[2], k = 0;
+        for (int b = 0; b < 3; b++)
+            if (b != B.pmain) other[k++] = b;
+        for (int x = tid; x < c.n; x += nth) B.Pbuf[other[0]][x] = B.Pbuf[B.pmain][x];
+        __syncthreads();
+        if (tid == 0) { c.P = B.Pbuf[other[0]]; c.Pn = B.Pbuf[other[1]]; }
+        __syncthreads();
+        bool ok = true;
+        for (int rks = 0; rks < rk && ok; rks++) ok = b_stage<TW>(s, B, rks, Ae, Ai, dt, fsm) == SPB6G_OK;
+        __syncthreads();
+        if (ok) {
+            int pm = 0;
+            for (int b = 0; b < 3; b++)
+                if (B.Pbuf[b] == c.P) pm = b;
+            __syncthreads();
+            if (tid == 0) {
+                for (int q = 0; q < NV; q++) {
+                    double* u = B.U[q];
+                    B.U[q] = B.Ust[q];
+                    B.Ust[q] = u;
+                    c.Ust.v[q] = B.Ust[q];
+                }
+                B.pmain = pm;
+            }
+            done = true;
+        }
+        __syncthreads();
+        if (!done) {
+            if (tid == 0) B.rejects++;
+            dt *= 0.5;
+        }
+    }
+    if (!done) return SPB6G_STEP_FAILED;
+    __syncthreads();
+    if (tid == 0) {
+        B.t = B.t + dt;
+        B.dt = dt;
+        B.dtprev = dt;
+        B.steps++;
+        if (!ramping) B.startup = 0;
+    }
+    __syncthreads();
+    return SPB6G_OK;
+}
+template <int TW>
+__global__ void __launch_bounds__(256) k_batch(BatchInst* insts, int count, int nsteps) {
+    extern __shared__ __align__(16) unsigned char batch_smem[];
+    __shared__ BatchShared s;
+    for (int b = blockIdx.x; b < count; b += gridDim.x) {
+        BatchInst& B = insts[b];
+        __syncthreads();
+        if (threadIdx.x == 0) s.c = B.c;
+        __syncthreads();
+        for (int k = 0; k < nsteps; k++) {
+            const bool stop = B.status != SPB6G_OK || !(B.t < B.tend);
+            __syncthreads();
+            if (stop) break;
+            const int rc = b_step<TW>(s, B, batch_smem);
+            __syncthreads();
+            if (rc != SPB6G_OK) {
+                if (threadIdx.x == 0) B.status = rc;
+                __syncthreads();
+                break;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) B.c = s.c;
+        __syncthreads();
+    }
+}
+int batch_max_blocks(int threads, int tw, int device) {
+    int per_sm = 0, sms = 0;
+    const size_t smem = flux_tile_bytes_1d(tw);
+    const void* fn = tw == 128 ? (const void*)k_batch<128> : (const void*)k_batch<256>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    return per_sm * sms;
+}
+int launch_batch(BatchInst* insts, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st) {
+    const size_t smem = flux_tile_bytes_1d(tw);
+    if (tw == 128) k_batch<128><<<grid, threads, smem, st>>>(insts, count, nsteps);
+    else k_batch<256><<<grid, threads, smem, st>>>(insts, count, nsteps);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace spb6g

@@ -832,6 +832,200 @@ int spb6g_dump_count(spb6g_solver* s, int64_t* count) {
     return SPB6G_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------- batched form
+struct spb6g_batch {
+    int device = 0;
+    std::vector<spb6g_solver*> inst;
+    std::vector<BatchInst> host;
+    std::vector<int> status;
+    BatchInst* dev = nullptr;
+    cudaStream_t st = nullptr;
+    int threads = 128, tw = 256;
+    cudaGraphExec_t graph = nullptr;  // the persistent launch for (graph_steps, graph_threads, graph_tw)
+    int graph_steps = -1, graph_threads = 0, graph_tw = 0;
+};
+
+namespace {
+void batch_pack(spb6g_batch* b) {
+    for (size_t i = 0; i < b->inst.size(); i++) {
+        spb6g_solver* s = b->inst[i];
+        BatchInst& B = b->host[i];
+        memset(&B, 0, sizeof B);
+        B.c = s->c;
+        for (int k = 0; k < NV; k++) { B.U[k] = s->U[k]; B.Ust[k] = s->Ust[k]; B.c.Ust.v[k] = s->Ust[k]; }
+        B.Hs = s->Hs;
+        for (int q = 0; q < 3; q++) {
+            B.Pbuf[q] = s->Pbuf[q];
+            if (s->Pbuf[q] == s->Pmain) B.pmain = q;
+        }
+        B.status = SPB6G_OK;
+        B.t = s->t; B.dt = s->dt; B.dtprev = s->dtprev; B.startup = s->startup ? 1 : 0;
+        const spb6g_config& cf = s->cfg;
+        B.cfl = cf.cfl; B.cfl_ac = cf.cfl_ac; B.dtfix = cf.dtfix; B.tend = cf.tend; B.newton_tol = cf.newton_tol;
+        B.ramp = cf.ramp; B.acdt = cf.acdt; B.rk = cf.rk; B.newton_iter = cf.newton_iter;
+        B.steps = s->stats.steps; B.rejects = s->stats.rejects; B.rk1 = s->stats.rk1; B.stages = s->stats.stages;
+        B.newton_it = s->stats.newton_it; B.floor_count = s->stats.floor_count; B.maxres = s->stats.maxres;
+    }
+}
+void batch_unpack(spb6g_batch* b) {
+    for (size_t i = 0; i < b->inst.size(); i++) {
+        spb6g_solver* s = b->inst[i];
+        const BatchInst& B = b->host[i];
+        s->c = B.c;
+        for (int k = 0; k < NV; k++) { s->U[k] = B.U[k]; s->Ust[k] = B.Ust[k]; }
+        s->Pmain = B.Pbuf[B.pmain];
+        s->t = B.t; s->dt = B.dt; s->dtprev = B.dtprev; s->startup = B.startup != 0;
+        s->stats.steps = B.steps; s->stats.rejects = B.rejects; s->stats.rk1 = B.rk1; s->stats.stages = B.stages;
+        s->stats.newton_it = B.newton_it; s->stats.floor_count = B.floor_count; s->stats.maxres = B.maxres;
+        b->status[i] = B.status;
+    }
+}
+int batch_grid(spb6g_batch* b, int threads, int tw) {
+    int g = batch_max_blocks(threads, tw, b->device);
+    if (g <= 0) return 0;
+    return g < (int)b->inst.size() ? g : (int)b->inst.size();
+}
+// One persistent launch of nsteps steps per instance (a captured CUDA graph, rebuilt when the
+// step count or the launch shape changes), device time in *ms if not NULL.
+int batch_run(spb6g_batch* b, int nsteps, int threads, int tw, float* ms) {
+    const int grid = batch_grid(b, threads, tw);
+    if (grid <= 0) return SPB6G_UNSUPPORTED;
+    batch_pack(b);
+    CK(cudaMemcpyAsync(b->dev, b->host.data(), b->host.size() * sizeof(BatchInst), cudaMemcpyHostToDevice, b->st));
+    if (!b->graph || b->graph_steps != nsteps || b->graph_threads != threads || b->graph_tw != tw) {
+        if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        const int lrc = launch_batch(b->dev, (int)b->inst.size(), nsteps, threads, tw, grid, b->st);
+        CK(cudaStreamEndCapture(b->st, &g));
+        if (lrc) { cudaGraphDestroy(g); return SPB6G_CUDA_ERROR; }
+        CK(cudaGraphInstantiate(&b->graph, g, 0));
+        cudaGraphDestroy(g);
+        b->graph_steps = nsteps; b->graph_threads = threads; b->graph_tw = tw;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, b->st); }
+    CK(cudaGraphLaunch(b->graph, b->st));
+    if (ms) cudaEventRecord(e1, b->st);
+    CK(cudaMemcpyAsync(b->host.data(), b->dev, b->host.size() * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    if (ms) { cudaEventElapsedTime(ms, e0, e1); cudaEventDestroy(e0); cudaEventDestroy(e1); }
+    batch_unpack(b);
+    for (spb6g_solver* s : b->inst) s->nlaunch += 0;
+    for (size_t i = 0; i < b->status.size(); i++)
+        if (b->status[i] != SPB6G_OK) return b->status[i];
+    return SPB6G_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
+    if (!cfgs || !out || count < 1) return SPB6G_BAD_ARG;
+    *out = nullptr;
+    for (int i = 0; i < count; i++)
+        if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device) return SPB6G_UNSUPPORTED;
+    spb6g_batch* b = new spb6g_batch();
+    b->device = cfgs[0].device;
+    for (int i = 0; i < count; i++) {
+        spb6g_solver* s = nullptr;
+        const int rc = spb6g_create(&cfgs[i], &s);
+        if (rc != SPB6G_OK) { spb6g_batch_destroy(b); return rc; }
+        b->inst.push_back(s);
+    }
+    cudaSetDevice(b->device);
+    b->host.resize(count);
+    b->status.assign(count, SPB6G_OK);
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void**)&b->dev, (size_t)count * sizeof(BatchInst)) != cudaSuccess) {
+        spb6g_batch_destroy(b);
+        return SPB6G_CUDA_ERROR;
+    }
+    *out = b;
+    return SPB6G_OK;
+}
+void spb6g_batch_destroy(spb6g_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->dev) cudaFree(b->dev);
+    if (b->st) cudaStreamDestroy(b->st);
+    for (spb6g_solver* s : b->inst) spb6g_destroy(s);
+    delete b;
+}
+spb6g_solver* spb6g_batch_instance(spb6g_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->inst.size()) return nullptr;
+    return b->inst[i];
+}
+int spb6g_batch_status(spb6g_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->inst.size()) return SPB6G_BAD_ARG;
+    return b->status[i];
+}
+int spb6g_batch_set_shape(spb6g_batch* b, int threads, int tile) {
+    if (!b || (threads != 64 && threads != 128 && threads != 256) || (tile != 128 && tile != 256)) return SPB6G_BAD_ARG;
+    b->threads = threads;
+    b->tw = tile;
+    return SPB6G_OK;
+}
+int spb6g_batch_advance(spb6g_batch* b, int nsteps, float* ms) {
+    if (!b || nsteps < 1) return SPB6G_BAD_ARG;
+    cudaSetDevice(b->device);
+    for (spb6g_solver* s : b->inst) CK(cudaStreamSynchronize(s->st));  // uploads and set-up on the instances' streams
+    return batch_run(b, nsteps, b->threads, b->tw, ms);
+}
+// Times `nsteps` steps of every launch shape (threads per instance x flux tile width) from the
+// current state, restores the state after each trial, and keeps the fastest shape.
+int spb6g_batch_autotune(spb6g_batch* b, int nsteps, int* threads_out, int* tile_out, float* best_ms) {
+    if (!b || nsteps < 1) return SPB6G_BAD_ARG;
+    cudaSetDevice(b->device);
+    for (spb6g_solver* s : b->inst) CK(cudaStreamSynchronize(s->st));
+    const size_t n0 = b->inst.size();
+    // snapshot: the state arrays, the accepted pressure and the host-side time state
+    std::vector<std::vector<double*>> snap(n0);
+    std::vector<spb6g_solver> keep;
+    keep.reserve(n0);
+    for (size_t i = 0; i < n0; i++) {
+        spb6g_solver* s = b->inst[i];
+        keep.push_back(*s);
+        for (int k = 0; k < NV + 1; k++) {
+            double* d = nullptr;
+            if (cudaMalloc(&d, (size_t)s->n * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+            CK(cudaMemcpy(d, k < NV ? s->U[k] : s->Pmain, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice));
+            snap[i].push_back(d);
+        }
+    }
+    int bt = b->threads, bw = b->tw;
+    float bms = INFINITY;
+    for (int threads : {64, 128, 256})
+        for (int tw : {128, 256}) {
+            float ms = 0;
+            const int rc = batch_run(b, nsteps, threads, tw, &ms);
+            // restore
+            for (size_t i = 0; i < n0; i++) {
+                spb6g_solver* s = b->inst[i];
+                const spb6g_solver& k0 = keep[i];
+                s->c = k0.c;
+                for (int k = 0; k < NV; k++) { s->U[k] = k0.U[k]; s->Ust[k] = k0.Ust[k]; }
+                s->Pmain = k0.Pmain;
+                s->t = k0.t; s->dt = k0.dt; s->dtprev = k0.dtprev; s->startup = k0.startup; s->stats = k0.stats;
+                for (int k = 0; k < NV + 1; k++)
+                    CK(cudaMemcpy(k < NV ? s->U[k] : s->Pmain, snap[i][k], (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice));
+                b->status[i] = SPB6G_OK;
+            }
+            if (rc == SPB6G_OK && ms < bms) { bms = ms; bt = threads; bw = tw; }
+        }
+    for (auto& v : snap)
+        for (double* d : v) cudaFree(d);
+    b->threads = bt;
+    b->tw = bw;
+    if (threads_out) *threads_out = bt;
+    if (tile_out) *tile_out = bw;
+    if (best_ms) *best_ms = bms;
+    return isfinite(bms) ? SPB6G_OK : SPB6G_STEP_FAILED;
+}
+
 int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st) {
     if (!s || !st) return SPB6G_BAD_ARG;
     *st = s->stats;

@@ -96,6 +96,13 @@ def library() -> ctypes.CDLL:
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
         "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
+        "spb6g_batch_create": (I, [P, I, P]),
+        "spb6g_batch_destroy": (None, [P]),
+        "spb6g_batch_instance": (P, [P, I]),
+        "spb6g_batch_status": (I, [P, I]),
+        "spb6g_batch_set_shape": (I, [P, I, I]),
+        "spb6g_batch_advance": (I, [P, I, P]),
+        "spb6g_batch_autotune": (I, [P, I, P, P, P]),
         "spb6g_set_feature_norm": (I, [P, P]),
         "spb6g_set_warmstart": (I, [P, P]),
         "spb6g_set_dump": (I, [P, P, P, ctypes.c_int64]),
@@ -159,9 +166,9 @@ class Solver:
             raise SolverError(rc, where)
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and not getattr(self, "_borrowed", False):
             self.lib.spb6g_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -290,3 +297,71 @@ class Solver:
         ng = ctypes.c_int()
         self._check(self.lib.spb6g_timing_get(self.h, ms, cnt, 16, ctypes.byref(ng)), "timing")
         return {self.lib.spb6g_timing_name(g).decode(): (ms[g], cnt[g]) for g in range(ng.value)}
+
+
+class BatchSolver:
+    """Independent 1D grids advanced together: one persistent launch (a captured CUDA graph),
+    one thread block per grid.  `instance(i)` is an ordinary Solver view of grid i."""
+
+    def __init__(self, case_list, device: int = 0, init_pressure: bool = True):
+        self.lib = library()
+        self.cases = list(case_list)
+        cfgs = (Config * len(self.cases))(*[make_config(c, device) for c in self.cases])
+        h = ctypes.c_void_p()
+        rc = self.lib.spb6g_batch_create(cfgs, len(self.cases), ctypes.byref(h))
+        if rc != 0:
+            raise SolverError(rc, "spb6g_batch_create")
+        self.h = h
+        self._inst = []
+        for i, c in enumerate(self.cases):
+            v = Solver.__new__(Solver)
+            v.lib, v.case, v.nx, v.ny = self.lib, c, int(c["nx"]), int(c["ny"])
+            v.cfg, v._borrowed = cfgs[i], True
+            v.h = ctypes.c_void_p(self.lib.spb6g_batch_instance(h, i))
+            if "U" in c:
+                v.upload(c["U"])
+                if init_pressure:
+                    v.init_pressure()
+            self._inst.append(v)
+
+    def __len__(self):
+        return len(self._inst)
+
+    def instance(self, i: int) -> Solver:
+        return self._inst[i]
+
+    def set_shape(self, threads: int, tile: int):
+        self._check(self.lib.spb6g_batch_set_shape(self.h, threads, tile), "spb6g_batch_set_shape")
+
+    def advance(self, nsteps: int) -> float:
+        """nsteps steps of every grid; returns the launch's device time in ms."""
+        ms = ctypes.c_float()
+        self._check(self.lib.spb6g_batch_advance(self.h, int(nsteps), ctypes.byref(ms)), "spb6g_batch_advance")
+        return ms.value
+
+    def autotune(self, nsteps: int = 2):
+        t, w, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.lib.spb6g_batch_autotune(self.h, int(nsteps), ctypes.byref(t), ctypes.byref(w), ctypes.byref(ms)),
+                    "spb6g_batch_autotune")
+        return t.value, w.value, ms.value
+
+    def status(self, i: int) -> int:
+        return self.lib.spb6g_batch_status(self.h, i)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for v in self._inst:
+                v.h = None
+            self.lib.spb6g_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _check(rc, where):
+        if rc != 0:
+            raise SolverError(rc, where)
