@@ -64,7 +64,9 @@ def parse():
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="bubbles1024")
+    p.add_argument("--workload", default="bubbles1024",
+                   help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
+                        "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -81,9 +83,108 @@ def make_workload(name: str):
         c = cases.bubble_field(256, seed=0, nbub=8)
     elif name == "tube1000":
         c = cases.water_air_tube(1000)
+    elif name == "lowmach2048":
+        c = cases.lowmach_bubbles(2048, seed=0)
+    elif name == "shock2048x1024":
+        c = cases.shock_bubble(2048, 1024)
+    elif name in ("bubbles2048-mixed", "shock2048x1024-mixed"):
+        c = make_workload(name[:-len("-mixed")])
+        c["precision"] = 1
+        c["workload"] = c.get("workload", name) + " (precision form)"
+    elif name == "riemann512":
+        return {"batch": cases.riemann_batch(count=512, seed=0), "workload": "512 1D Riemann problems, 256-4096 cells"}
     else:
         raise SystemExit(f"unknown workload {name}")
     return c
+
+
+def run_reference_batch(args, case, rank: int):
+    """The reference solver on a sample of the batch: one grid per host core, single-threaded,
+    all at once; value = sum of cells x timed steps / the slowest grid's timed wall time."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from concurrent.futures import ThreadPoolExecutor
+
+    import refio
+
+    cores = os.cpu_count() or 1
+    sample = case["batch"][:cores]
+    run = (lambda c: refio.run_ref(c, mode=refio.MODE_STEPS, nsteps=args.warmup + args.steps, threads=1,
+                                   warmup=args.warmup, budget_s=150.0)) if refio.ref_available() else \
+          (lambda c: refio.run_port(c, mode=refio.MODE_STEPS, nsteps=args.warmup + args.steps, warmup=args.warmup,
+                                    budget_s=150.0))
+    with ThreadPoolExecutor(cores) as ex:
+        rs = list(ex.map(run, sample))
+    wall = max(r["wall_s"] for r in rs)
+    upd = sum(int(r["timed_steps"]) * c["nx"] for r, c in zip(rs, sample))
+    value = upd / wall
+    kind = "reference" if refio.ref_available() else "port"
+    line = {"impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": case["workload"], "instances": len(sample), "seed": 0},
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+                             "sample": f"first {len(sample)} grids of the batch, one per core, steps "
+                                       f"{args.warmup + 1}..{args.warmup + args.steps}"},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_batch(args, case, rank: int, world: int, local_rank: int, dist):
+    """Batched form: every grid advances `steps` steps in one persistent launch (after `warmup`
+    untimed steps in another); value = sum of cells x accepted steps / device time."""
+    import torch
+
+    from diffusionimex_b200 import BatchSolver
+
+    cs = case["batch"]
+    b = BatchSolver(cs, device=local_rank)
+    threads, tile, _ = b.autotune(2)
+    if args.warmup:
+        b.advance(args.warmup)
+    s0 = [b.instance(i).stats() for i in range(len(cs))]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    ms = b.advance(args.steps)
+    clocks = clk.stop()
+    s1 = [b.instance(i).stats() for i in range(len(cs))]
+    upd = sum((q["steps"] - p["steps"]) * c["nx"] for p, q, c in zip(s0, s1, cs))
+    ms_max = max_over_ranks(ms, dist, f"cuda:{local_rank}")
+    value = upd * world / (ms_max / 1e3)
+    # end to end: the states go host -> device before the launch and come back after it
+    e2e = None
+    if not args.no_e2e:
+        host = [b.instance(i).state() for i in range(len(cs))]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        import time as _t
+        w0 = _t.perf_counter()
+        for i in range(len(cs)):
+            b.instance(i).upload(host[i])
+        ms2 = b.advance(1)
+        for i in range(len(cs)):
+            host[i] = b.instance(i).state()
+        wall = max_over_ranks((_t.perf_counter() - w0) * 1e3, dist, f"cuda:{local_rank}")
+        cells = sum(c["nx"] for c in cs)
+        e2e = {"value": cells * world / (wall / 1e3), "unit": "cell-updates/s", "h2d_bytes_per_step": 64 * cells,
+               "d2h_bytes_per_step": 64 * cells, "steps": 1, "device_ms": ms2}
+    if rank == 0:
+        cells = sum(c["nx"] for c in cs)
+        line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / max(args.steps, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case["workload"], "instances": len(cs), "cells": cells, "seed": 0,
+                           "launch": {"threads_per_grid": threads, "flux_tile": tile}},
+                "rejects": sum(q["rejects"] - p["rejects"] for p, q in zip(s0, s1)),
+                "newton_iters": sum(q["newton_it"] - p["newton_it"] for p, q in zip(s0, s1)),
+                "gpu_launches": 1, "clocks": clocks, "e2e": e2e}
+        print(json.dumps(line))
+    b.close()
 
 
 def workload_config(c: dict, name: str) -> dict:
@@ -331,11 +432,17 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     case = make_workload(args.workload)
     if args.impl == "reference":
+        if "batch" in case:
+            run_reference_batch(args, case, rank)
+            return
         run_reference(args, case, rank)
         return
     dist = dist_init(world, local_rank)
     try:
-        run_ours(args, case, rank, world, local_rank, dist)
+        if "batch" in case:
+            run_batch(args, case, rank, world, local_rank, dist)
+        else:
+            run_ours(args, case, rank, world, local_rank, dist)
     finally:
         if dist:
             dist.destroy_process_group()

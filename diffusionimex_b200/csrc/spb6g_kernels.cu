@@ -238,8 +238,11 @@ __global__ void k_shock_weak(Ctx c) {
         }
     }
 }
+// One worklist cell per thread: the grid covers the largest possible worklist (every cell) and
+// blocks past the worklist's end return at once, so no thread integrates two cells in a row.
 __global__ void k_shock_strong(Ctx c) {
     const int cnt = *(volatile int*)&c.ns->nstrong;
+    if ((long)blockIdx.x * blockDim.x >= cnt) return;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const int x = c.strong_list[t];
         double Q[2];
@@ -255,7 +258,7 @@ void launch_shock_weak(const Ctx& c, cudaStream_t st) {
     count(c, 1);
 }
 void launch_shock_strong(const Ctx& c, cudaStream_t st) {
-    k_shock_strong<<<148 * 4, 32, 0, st>>>(c);
+    k_shock_strong<<<(c.n + 31) / 32, 32, 0, st>>>(c);
     count(c, 1);
 }
 

@@ -111,11 +111,19 @@ def test_1d_tube_one_step_bitwise():
 @pytest.mark.parametrize("name", ["case87_N200_tend", "case5_N100_tend", "tube_N1000_tend", "nasg256_20steps",
                                   "case83_N200_10steps"])
 def test_runs_match_reference_in_l1(name):
+    """Whole runs in L1: within 1e-6 of the field maximum, or within 10x the reference's own L1
+    change under round-off perturbations (one-ulp libm, FD step 1.01e-7) where that is larger --
+    case 87 to t_end moves by 1e-6 in rho u under either perturbation."""
     g = load_golden(name)
     c, mode, nsteps = golden_case(name)
     r = run_gpu(c, mode, nsteps)
     assert r["stats"]["steps"] == g["meta"]["steps"]
-    assert fieldwise_l1(r["U"], g["U"]).max() <= 1e-6, report(r["U"], g["U"])
+    d = fieldwise_l1(r["U"], g["U"])
+    if d.max() > 1e-6:
+        m = {"steps": refio.MODE_STEPS, "tend": refio.MODE_TEND}[mode]
+        noise = np.maximum(*[fieldwise_l1(refio.run_port(c, mode=m, nsteps=nsteps, variant=v)["U"], g["U"])
+                             for v in ("ulp", "fd")])
+        assert np.all(d <= np.maximum(10 * noise, 1e-6)), {"gpu": report(r["U"], g["U"]), "noise": noise.tolist()}
 
 
 def test_deterministic_repeat():
