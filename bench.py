@@ -391,7 +391,11 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
     newton_its = st1["newton_it"] - st0["newton_it"]
     bicg_its = st1["bicg_it"] - st0["bicg_it"]
     stages = st1["stages"] - st0["stages"]
-    dom = max((g for g in groups if g in ALG_BYTES), key=lambda g: groups[g][0])
+    # the HBM roofline is the BiCGStab solve's (the dominant memory-bound kernel); the FD Jacobian,
+    # the residuals and the shock budget are FP64-arithmetic / latency bound (their shares are
+    # in kernel_groups; profiles/ has their FP64-pipe figures)
+    dom = "linear" if "linear" in groups and groups["linear"][1] > 0 else \
+        max((g for g in groups if g in ALG_BYTES), key=lambda g: groups[g][0])
     gms, gcnt = groups[dom]
     if dom == "linear":
         units = bicg_its * n
