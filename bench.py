@@ -66,7 +66,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="bubbles1024",
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
-                        "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form)")
+                        "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
+                        "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -93,6 +94,10 @@ def make_workload(name: str):
         c["workload"] = c.get("workload", name) + " (precision form)"
     elif name == "riemann512":
         return {"batch": cases.riemann_batch(count=512, seed=0), "workload": "512 1D Riemann problems, 256-4096 cells"}
+    elif name == "mlp":
+        return {"mlp": True, "rows": 1 << 21,
+                "workload": "learned warm-start network: training passes (forward, backward, Adam) over 2,097,152 "
+                            "feature rows of 64 BF16 (54 used), 54-64-64-64-1 SiLU"}
     else:
         raise SystemExit(f"unknown workload {name}")
     return c
@@ -185,6 +190,142 @@ def run_batch(args, case, rank: int, world: int, local_rank: int, dist):
                 "gpu_launches": 1, "clocks": clocks, "e2e": e2e}
         print(json.dumps(line))
     b.close()
+
+
+# Learned warm-start network, per feature row of one training pass: tensor-core FLOPs (forward
+# 3 x 2*64*64, input gradients 2 x 2*64*64, weight and bias gradients 3 x 2*65*64), special-function
+# operations (exp2 and reciprocal of the logistic function, 64 per layer and three layers; the
+# backward pass reuses the derivatives the forward epilogues keep) and HBM bytes (the BF16 row
+# and the FP32 target).
+MLP_FLOP_PER_ROW = 3 * 2 * 64 * 64 + 2 * 2 * 64 * 64 + 3 * 2 * 65 * 64
+MLP_SFU_PER_ROW = 3 * 64 * 2
+MLP_BYTES_PER_ROW = 64 * 2 + 4
+SFU_PER_CLOCK_PER_SM = 16  # nominal special-function results per clock per SM
+
+
+def mlp_cpu_baseline(rows: int = 1 << 16) -> dict:
+    """The float64 numpy checker's training pass (oracle/mlp_ref.py) on a sample of rows."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import mlp_ref
+
+    rng = np.random.default_rng(0)
+    X = np.zeros((rows, 64), np.float32)
+    X[:, :54] = rng.standard_normal((rows, 54))
+    p = mlp_ref.init_params(rng)
+    t = np.zeros(rows, np.float32)
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        mlp_ref.loss_grad(p, X, t)
+    wall = time.perf_counter() - t0
+    return {"value": rows * reps / wall, "unit": "rows/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{reps} training passes of the float64 numpy checker over {rows} rows ({wall:.1f} s; "
+                      "numpy may use every host core)"}
+
+
+def run_mlp(args, case, rank: int, world: int, local_rank: int, dist):
+    """Training passes of the warm-start network over a fixed synthetic batch: value = rows x
+    passes / device time (CUDA events on the launching stream, max over ranks)."""
+    import torch
+
+    from diffusionimex_b200 import learned
+    from diffusionimex_b200.warmstart import MLP
+
+    n = case["rows"]
+    dev = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    X = torch.zeros((n, 64), dtype=torch.bfloat16, device=dev)
+    X[:, :54] = torch.randn((n, 54), generator=g, device=dev).to(torch.bfloat16)
+    T = torch.tanh(X[:, :54].float() @ torch.randn(54, generator=g, device=dev) / 8).contiguous()
+    m = MLP(local_rank)
+    m.set_params(learned._init_params(0))
+    st = torch.cuda.current_stream()
+    lr = 1e-3
+    for _ in range(args.warmup):
+        m.train_async(X, T, lr, st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    e0.record(st)
+    for _ in range(args.steps):
+        m.train_async(X, T, lr, st)
+    e1.record(st)
+    e1.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    loss = m.last_loss(st) / n
+    ms_max = max_over_ranks(ms, dist, dev)
+    value = n * args.steps * world / (ms_max / 1e3)
+    # inference passes over the same rows
+    y = torch.empty(n, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        m.forward(X, y, stream=st)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    f0.record(st)
+    for _ in range(args.steps):
+        m.forward(X, y, stream=st)
+    f1.record(st)
+    f1.synchronize()
+    fms = f0.elapsed_time(f1) / args.steps
+    # end to end: the batch goes host -> device every pass, the loss comes back
+    e2e = None
+    if not args.no_e2e:
+        Xh = X.cpu().pin_memory()
+        Th = T.cpu().pin_memory()
+        ke = max(1, min(args.steps, 5))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0.record(st)
+        for _ in range(ke):
+            X.copy_(Xh, non_blocking=True)
+            T.copy_(Th, non_blocking=True)
+            m.train_async(X, T, lr, st)
+            m.last_loss(st)
+        e1.record(st)
+        e1.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        e2e = {"value": n * ke * world / (ems / 1e3), "unit": "rows/s", "h2d_bytes_per_step": n * MLP_BYTES_PER_ROW,
+               "d2h_bytes_per_step": 4, "steps": ke}
+    peak = None
+    try:
+        with open(MEASURED_PEAKS) as f:
+            pk = json.load(f)
+        peak, peak_kind = float(pk["bf16_tflops"]), "measured (burst)"
+    except (OSError, KeyError, ValueError):
+        peak, peak_kind = 1590.0, "fallback"
+    per_pass_s = ms / args.steps / 1e3
+    tflops = MLP_FLOP_PER_ROW * n / per_pass_s / 1e12
+    smhz = clocks.get("sm_mhz") or 1965.0
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sfu_peak = SFU_PER_CLOCK_PER_SM * sms * smhz * 1e6
+    sfu = MLP_SFU_PER_ROW * n / per_pass_s
+    roof = {"bound": "tensor", "kernel": "k_mlp_grad (+ k_mlp_adam, timed together)", "achieved": tflops, "peak": peak,
+            "unit": "TFLOP/s", "frac": tflops / peak, "traffic": None, "peak_source": peak_kind,
+            "flop_per_row": MLP_FLOP_PER_ROW,
+            "special_function": {"ops_per_row": MLP_SFU_PER_ROW, "achieved_per_s": sfu, "nominal_peak_per_s": sfu_peak,
+                                 "frac": sfu / sfu_peak},
+            "hbm": {"bytes_per_row": MLP_BYTES_PER_ROW, "achieved_GBs": MLP_BYTES_PER_ROW * n / per_pass_s / 1e9}}
+    if rank == 0:
+        line = {"metric": "rows/s", "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+                "config": {"workload": case["workload"], "rows": n, "seed": 0, "lr": lr,
+                           "l2": "inputs (276 MB) larger than L2"},
+                "loss": loss, "inference": {"rows_per_s": n / (fms / 1e3), "us_per_pass": fms * 1e3},
+                "roofline": roof, "gpu_launches": 2 * args.steps, "clocks": clocks, "e2e": e2e}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = mlp_cpu_baseline()
+        print(json.dumps(line))
+    m.close()
 
 
 def workload_config(c: dict, name: str) -> dict:
@@ -436,6 +577,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     case = make_workload(args.workload)
     if args.impl == "reference":
+        if "mlp" in case:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned warm start: "
+                                  "its Newton always starts from the previous stage's pressure"}))
+            return
         if "batch" in case:
             run_reference_batch(args, case, rank)
             return
@@ -443,7 +589,9 @@ def main():
         return
     dist = dist_init(world, local_rank)
     try:
-        if "batch" in case:
+        if "mlp" in case:
+            run_mlp(args, case, rank, world, local_rank, dist)
+        elif "batch" in case:
             run_batch(args, case, rank, world, local_rank, dist)
         else:
             run_ours(args, case, rank, world, local_rank, dist)

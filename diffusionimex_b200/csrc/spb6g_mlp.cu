@@ -8,19 +8,30 @@
 // of the two guesses gives the smaller residual norm, and Newton then converges
 // to the same tolerance either way.
 //
-// Kernels (one CTA of 128 threads per SM, one sample per thread, tiles of 128
-// samples = the MMA's M):
+// Kernels (tiles of 128 samples = the MMA's M; sample i of a tile in TMEM lane i):
 //   k_mlp_forward  inference: three M=128, N=64, K=64 GEMMs (X W1^T, H1 W2^T,
 //                  H2 W3^T) with bias + SiLU between them, last layer a 64-term
-//                  FP32 dot product per thread;
+//                  FP32 dot product per sample;
 //   k_mlp_grad     one training pass over a batch: the same forward, then the
 //                  backward GEMMs dH = dZ W (M=128, N=64, K=64) and the weight
-//                  gradients dW^T... = dZ^T [H | 1] (M=128 of which 64 rows
-//                  used, N=80 = 64 inputs + the bias column, K=128 samples)
-//                  accumulated in tensor memory across every tile the CTA
-//                  processes; one FP32 partial per CTA;
-//   k_mlp_adam     folds the per-CTA partials in CTA order (deterministic) and
-//                  applies Adam to the FP32 master weights.
+//                  gradients dW^T = [H | 1]^T dZ (M=128: the 64 inputs, the bias
+//                  row and zero rows; N=64; K=128 samples) accumulated in tensor
+//                  memory across every tile the CTA processes; one FP32 partial
+//                  per CTA;
+//   k_mlp_adam     folds the per-CTA partials in CTA order (deterministic),
+//                  applies Adam to the FP32 master weights and rewrites their
+//                  BF16 operand images.
+//
+// Every operand is a BF16 tile with 128-byte rows (64 values) in the 128-byte
+// swizzled layout: the feature rows arrive by TMA straight into it, the
+// epilogues write 16-byte vectors into it, and the transposed operands of the
+// backward GEMMs are the same tiles read through MN-major descriptors, so no
+// transposed copy is ever written.  Feature tiles are double-buffered (the TMA
+// load of a later tile runs while the current one is computed), and the CTA's
+// warpgroups split the 64 columns of every epilogue between them.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -33,51 +44,50 @@ namespace mlp {
 
 using namespace tc;
 
-constexpr int TILE = 128;  // samples per tile (MMA M)
-constexpr int F = 64;      // padded input width and hidden width
-constexpr int NB = 80;     // weight-gradient N: 64 inputs, the bias column, zero padding
+constexpr int TILE = 128;         // samples per tile (MMA M)
+constexpr int F = 64;             // padded input width and hidden width
+constexpr uint32_t TB = 16384;    // bytes of a 128 x 64 BF16 tile
+constexpr uint32_t WB = 8192;     // bytes of a 64 x 64 BF16 weight image
 // parameter offsets (FP32 master copy; W[n][k], n = output, k = input)
 constexpr int OW1 = 0, OB1 = 4096, OW2 = 4160, OB2 = 8256, OW3 = 8320, OB3 = 12416, OW4 = 12480, OB4 = 12544;
 constexpr int NPARAM = 12545;
 constexpr int PSTRIDE = 12608;  // per-CTA partial record: gradients + loss at NPARAM
+constexpr int LSTRIDE = OW2 - OW1;  // distance between the hidden layers' parameter blocks
+static_assert(OB1 == OW1 + F * F && OB2 == OB1 + LSTRIDE && OW3 == OW2 + LSTRIDE && OB3 == OB2 + LSTRIDE && OW4 == OB3 + F &&
+                  OB4 == OW4 + F && NPARAM == OB4 + 1 && PSTRIDE > NPARAM,
+              "parameter layout");
 constexpr long long WAIT_CYCLES = 2000000000LL;  // about one second at 1.9 GHz
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
+// SiLU(z) = z s(z) with the logistic function s(z) = 1 / (1 + e^-z) = 1 / (1 + 2^(-z log2 e)),
+// evaluated with the approximate base-2 exponential and reciprocal instructions (one
+// special-function operation each); SiLU'(z) = s (1 + z (1 - s)).
+constexpr float NEG_LOG2E = -1.44269504088896340736f;
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
-__device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
-    *(__nv_bfloat16*)(base + off) = __float2bfloat16_rn(v);
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float logistic(float z) { return rcp_approx(1.0f + ex2_approx(z * NEG_LOG2E)); }
+__device__ __forceinline__ float dsilu(float z, float s) { return s * __fmaf_rn(z, 1.0f - s, 1.0f); }
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *(const uint32_t*)&v;
 }
 
-// Weights into K-major BF16 operands (and optionally their transposes).
-__device__ void load_weight(unsigned char* dst, const float* W, bool transpose) {
-    for (int e = threadIdx.x; e < F * F; e += blockDim.x) {
-        const int n = e / F, k = e % F;
-        if (!transpose) st_bf16(dst, kmajor_off(n, k, F), W[e]);   // row n, column k
-        else st_bf16(dst, kmajor_off(k, n, F), W[e]);              // row k, column n
-    }
-}
+// All threads: a CTA-wide vote, so that every thread takes the same branch after a
+// bounded wait (one thread's timeout stops the whole CTA).
+__device__ __forceinline__ bool vote_ok(bool mine) { return !__syncthreads_or(!mine); }
 
-struct Sync {
-    uint64_t* bar;
-    uint32_t phase;
-    bool ok;
-    // all threads: wait for the last commit, then order TMEM reads after it; the
-    // outcome is the same in every thread (a CTA-wide vote), so callers may branch on it
-    __device__ bool wait() {
-        const bool mine = mbar_wait(bar, phase, WAIT_CYCLES);
-        phase ^= 1u;
-        ok = !__syncthreads_or(!(ok && mine));
-        fence_after();
-        return ok;
-    }
-};
 // Operands written by the threads become visible to the tensor cores, and every
 // earlier TMEM read of the CTA is complete, before thread 0 issues more MMAs.
 __device__ __forceinline__ void publish() {
     tmem_wait_ld();
+    tmem_wait_st();
     fence_async_smem();
     fence_before();
     __syncthreads();
@@ -92,314 +102,476 @@ __device__ __forceinline__ unsigned char* align_smem(unsigned char* raw) {
     return raw + ((1024u - (smem_u32(raw) & 1023u)) & 1023u);
 }
 
-// --------------------------------------------------------------------------- inference
-constexpr size_t FWD_SMEM = 3 * 8192 + 2 * 16384 + 1024;
+// CW columns of this thread's TMEM lane starting at column `col` (CW a multiple of 16).
+template <int CW>
+__device__ __forceinline__ void tmem_load(uint32_t tb, int col, float* v) {
+#pragma unroll
+    for (int c = 0; c < CW; c += 16) tmem_ld16(tmem_lane_addr(tb, col + c), v + c);
+}
 
-__global__ void __launch_bounds__(TILE, 1) k_mlp_forward(const float* __restrict__ P, const __nv_bfloat16* __restrict__ X, int n,
-                                                          float* __restrict__ y, int* err) {
+// Hidden-layer epilogue for CW columns from c0 of sample `row`: zz = z + bias, h = SiLU(zz)
+// as BF16 into `tile` (16-byte stores); with DERIV also SiLU'(zz) into d.
+template <int CW, bool DERIV>
+__device__ __forceinline__ void hidden_epilogue(unsigned char* tile, int row, int c0, const float* z, const float* bias,
+                                                float* d) {
+#pragma unroll
+    for (int c = 0; c < CW; c += 8) {
+        const float4 ba = *(const float4*)(bias + c0 + c), bb = *(const float4*)(bias + c0 + c + 4);
+        const float b8[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+        float h[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const float zz = z[c + q] + b8[q], sg = logistic(zz);
+            h[q] = zz * sg;
+            if (DERIV) d[c + q] = dsilu(zz, sg);
+        }
+        *(uint4*)(tile + sw128_off(row, c0 + c)) =
+            make_uint4(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]), pack_bf16(h[4], h[5]), pack_bf16(h[6], h[7]));
+    }
+}
+// CW columns from this thread's registers into its TMEM lane (CW a multiple of 16).
+template <int CW>
+__device__ __forceinline__ void tmem_store(uint32_t tb, int col, const float* v) {
+#pragma unroll
+    for (int c = 0; c < CW; c += 16) tmem_st16(tmem_lane_addr(tb, col + c), v + c);
+}
+
+// The three hidden layers' weights as BF16 operand images into shared memory, the
+// biases (and w4, b4) as FP32.
+__device__ __forceinline__ void load_params(unsigned char* wdst, const uint4* __restrict__ Wimg, const float* __restrict__ P,
+                                            float* bias) {
+    for (int e = threadIdx.x; e < (int)(3 * WB / 16); e += blockDim.x) ((uint4*)wdst)[e] = Wimg[e];
+    for (int e = threadIdx.x; e < 4 * F; e += blockDim.x) {
+        const int l = e / F, j = e % F;
+        bias[e] = l < 3 ? P[OB1 + l * LSTRIDE + j] : P[OW4 + j];
+    }
+    if (threadIdx.x == 0) bias[4 * F] = P[OB4];
+}
+
+// --------------------------------------------------------------------------- inference
+constexpr uint32_t F_W = 0, F_X = 3 * WB, F_H = F_X + TB, F_END = F_H + TB;
+constexpr size_t FWD_SMEM = F_END + 1024;
+constexpr int FWD_NWG = 2;   // warpgroups per CTA
+constexpr int FWD_CTAS = 3;  // resident CTAs per SM (each with its own tile chain)
+
+template <int NWG>
+__global__ void __launch_bounds__(128 * NWG, FWD_CTAS) k_mlp_forward(const __grid_constant__ CUtensorMap xmap,
+                                                                      const float* __restrict__ P, const uint4* __restrict__ Wimg,
+                                                                      int n, float* __restrict__ y, int* err) {
+    constexpr int CW = F / NWG;
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* sm = align_smem(smraw);
-    __shared__ uint64_t bar;
+    __shared__ uint64_t barx, barm;
     __shared__ uint32_t tbase;
-    __shared__ float bias[3 * F + F + 1];
-    unsigned char* W1s = sm;
-    unsigned char* W2s = sm + 8192;
-    unsigned char* W3s = sm + 16384;
-    unsigned char* Xs = sm + 24576;
-    unsigned char* Hs = sm + 40960;
-    const int t = threadIdx.x;
-    load_weight(W1s, P + OW1, false);
-    load_weight(W2s, P + OW2, false);
-    load_weight(W3s, P + OW3, false);
-    for (int e = t; e < F; e += TILE) {
-        bias[e] = P[OB1 + e]; bias[F + e] = P[OB2 + e]; bias[2 * F + e] = P[OB3 + e]; bias[3 * F + e] = P[OW4 + e];
+    __shared__ __align__(16) float bias[4 * F + 4];
+    __shared__ float ypart[NWG][TILE];
+    const int t = threadIdx.x, row = t & (TILE - 1), g = t >> 7, c0 = g * CW;
+    const int ntiles = (n + TILE - 1) / TILE;
+    if (t == 0) {
+        mbar_init(&barx, 1);
+        mbar_init(&barm, 1);
+        tma_prefetch_map(&xmap);
     }
-    if (t == 0) { bias[4 * F] = P[OB4]; mbar_init(&bar, 1); }
-    if (t < 32) tmem_alloc(&tbase, 256);
+    load_params(sm + F_W, Wimg, P, bias);
+    if (t < 32) tmem_alloc(&tbase, 64);
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tb = tbase;
-    Sync sy{&bar, 0u, true};
-    const uint32_t id64 = idesc_bf16(TILE, F);
-    const int ntiles = (n + TILE - 1) / TILE;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long row = (long)tile * TILE + t;
-        const bool valid = row < n;
-        {   // X row -> operand
-            const uint4* src = (const uint4*)(X + row * F);
-#pragma unroll
-            for (int c = 0; c < F / 8; c++) {
-                const uint4 v = valid ? src[c] : make_uint4(0, 0, 0, 0);
-                *(uint4*)(Xs + kmajor_off(t, c * 8, F)) = v;
-            }
-        }
-        publish();
-        const unsigned char* Ain = Xs;
-        float acc = 0.0f;
-        for (int layer = 0; layer < 3; layer++) {
-            const unsigned char* Wl = layer == 0 ? W1s : (layer == 1 ? W2s : W3s);
+    int issued = 0, used = 0;  // TMA loads of feature tiles (thread 0's count)
+    if (t == 0 && (int)blockIdx.x < ntiles) {
+        mbar_expect_tx(&barx, TB);
+        tma_load_2d(sm + F_X, &xmap, 0, blockIdx.x * TILE, &barx);
+        issued++;
+    }
+    const uint32_t tb = tbase, id = idesc_bf16(TILE, F);
+    const uint32_t xa = smem_u32(sm + F_X), ha = smem_u32(sm + F_H);
+    uint32_t pm = 0;
+    bool ok = true;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        ok = vote_ok(mbar_wait(&barx, (uint32_t)it & 1u, WAIT_CYCLES));
+        if (!ok) break;
+        used++;
+        float yp = 0.0f;
+        for (int l = 0; l < 3; l++) {
             if (t == 0) {
-                mma_chain(tb + layer * F, smem_u32(Ain), F, smem_u32(Wl), F, F, id64, 0);
-                mma_commit(&bar);
-            }
-            if (!sy.wait()) break;
-            for (int c = 0; c < F; c += 16) {
-                float z[16];
-                tmem_ld16(tmem_lane_addr(tb, layer * F + c), z);
-                tmem_wait_ld();
+                const uint32_t a = l == 0 ? xa : ha, w = smem_u32(sm + F_W + l * WB);
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const float h = silu(z[q] + bias[layer * F + c + q]);
-                    if (layer < 2) st_bf16(Hs, kmajor_off(t, c + q, F), h);
-                    else acc += bias[3 * F + c + q] * h;
+                for (int s = 0; s < F / 16; s++) mma_bf16(tb, desc_sw128_k(a, s), desc_sw128_k(w, s), id, s > 0);
+                mma_commit(&barm);
+            }
+            ok = vote_ok(mbar_wait(&barm, pm, WAIT_CYCLES));
+            pm ^= 1u;
+            fence_after();
+            if (!ok) break;
+            if (l == 0 && t == 0) {  // the feature tile has been consumed: load the next one into it
+                const int next = tile + gridDim.x;
+                if (next < ntiles) {
+                    mbar_expect_tx(&barx, TB);
+                    tma_load_2d(sm + F_X, &xmap, 0, next * TILE, &barx);
+                    issued++;
                 }
             }
-            if (layer < 2) {
+            float z[CW];
+            tmem_load<CW>(tb, c0, z);
+            tmem_wait_ld();
+            if (l < 2) {
+                hidden_epilogue<CW, false>(sm + F_H, row, c0, z, bias + l * F, nullptr);
                 publish();
-                Ain = Hs;
+            } else {
+#pragma unroll
+                for (int c = 0; c < CW; c += 4) {
+                    const float4 b = *(const float4*)(bias + 2 * F + c0 + c), w = *(const float4*)(bias + 3 * F + c0 + c);
+                    const float zz[4] = {z[c] + b.x, z[c + 1] + b.y, z[c + 2] + b.z, z[c + 3] + b.w};
+                    const float w4[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) yp = __fmaf_rn(w4[q], zz[q] * logistic(zz[q]), yp);
+                }
             }
         }
-        if (!sy.ok) { if (t == 0) atomicExch(err, 1); break; }
-        if (valid) y[row] = acc + bias[4 * F];
+        if (!ok) break;
+        ypart[g][row] = yp;
         fence_before();
-        __syncthreads();
+        __syncthreads();  // TMEM reads done before the next tile's MMA; partial sums visible
         fence_after();
+        if (g == 0) {
+            const long r = (long)tile * TILE + row;
+            if (r < n) {
+                float s = bias[4 * F];
+#pragma unroll
+                for (int q = 0; q < NWG; q++) s += ypart[q][row];
+                y[r] = s;
+            }
+        }
+    }
+    if (t == 0) {
+        // only after a timeout can a load still be in flight: wait for it (bounded)
+        if (issued > used) mbar_wait(&barx, (uint32_t)used & 1u, WAIT_CYCLES);
+        if (!ok) atomicExch(err, 1);
     }
     fence_before();
     __syncthreads();
-    if (t < 32) tmem_free(tb, 256);
+    if (t < 32) tmem_free(tbase, 64);
 }
 
 // --------------------------------------------------------------------------- training pass
-// shared memory map (bytes)
-constexpr int S_W1 = 0, S_W2 = 8192, S_W3 = 16384, S_W2T = 24576, S_W3T = 32768;
-constexpr int S_X = 40960;            // 128 x 64   (layer-1 A)
-constexpr int S_XT = S_X + 16384;     // 80 x 128   (dW1 B: features, ones row, zero rows)
-constexpr int S_H1 = S_XT + 20480;    // 128 x 64
-constexpr int S_H1T = S_H1 + 16384;   // 80 x 128
-constexpr int S_H2 = S_H1T + 20480;   // 128 x 64
-constexpr int S_H2T = S_H2 + 16384;   // 80 x 128
-constexpr int S_DZ = S_H2T + 20480;   // 128 x 64   (dH A)
-constexpr int S_DZT = S_DZ + 16384;   // 128 x 128  (dW A: rows n < 64, zero rows 64..127)
-constexpr size_t GRAD_SMEM = S_DZT + 32768 + 1024;
-// TMEM columns
-constexpr int T_Z3 = 128, T_DH = 192,  // Z1, Z2 at 0, 64 (layer * F)
-              T_DW1 = 256, T_DW2 = 336, T_DW3 = 416;
+// shared memory map (bytes from the 1024-aligned base)
+constexpr uint32_t G_W = 0, G_X = 3 * WB, G_H1 = G_X + 2 * TB, G_H2 = G_H1 + TB, G_DZ = G_H2 + TB, G_ONE = G_DZ + TB,
+                   G_END = G_ONE + TB;
+constexpr size_t GRAD_SMEM = G_END + 1024;
+constexpr int GRAD_NWG = 4;
+// TMEM columns: Z1, Z2, Z3 (then dH2, dH1), dW1^T, dW2^T, dW3^T
+constexpr int T_Z1 = 0, T_Z2 = 64, T_Z3 = 128, T_DW = 192;
 
-__global__ void __launch_bounds__(TILE, 1) k_mlp_grad(const float* __restrict__ P, const __nv_bfloat16* __restrict__ X,
-                                                       const float* __restrict__ target, int n, float dscale,
-                                                       float* __restrict__ part, int* err) {
+// dW_l^T (+)= [A | 1]^T dZ over the tile's 128 samples: A (128 samples x 64) read MN-major
+// with the constant block `one` (column 0 = 1, rest 0) as its second 64-wide block, so TMEM
+// lane k < 64 gets the weight gradient of input k and lane 64 the bias gradient.
+__device__ __forceinline__ void mma_weight_grad(uint32_t tmem, uint32_t a, uint32_t one, uint32_t dz, int accumulate) {
+    const uint32_t id = idesc_bf16(TILE, F, 1, 1);
+#pragma unroll
+    for (int s = 0; s < TILE / 16; s++)
+        mma_bf16(tmem, desc_sw128_mn(a, s, one - a), desc_sw128_mn(dz, s, TB), id, (s > 0 || accumulate) ? 1 : 0);
+}
+// dH = dZ W: A = dZ (K-major over the 64 outputs), B = W read MN-major (its rows are K).
+__device__ __forceinline__ void mma_input_grad(uint32_t tmem, uint32_t dz, uint32_t w) {
+    const uint32_t id = idesc_bf16(TILE, F, 0, 1);
+#pragma unroll
+    for (int s = 0; s < F / 16; s++) mma_bf16(tmem, desc_sw128_k(dz, s), desc_sw128_mn(w, s, WB), id, s > 0);
+}
+
+template <int NWG>
+__global__ void __launch_bounds__(128 * NWG, 1) k_mlp_grad(const __grid_constant__ CUtensorMap xmap, const float* __restrict__ P,
+                                                            const uint4* __restrict__ Wimg, const float* __restrict__ target,
+                                                            int n, float dscale, float* __restrict__ part, int* err) {
+    constexpr int CW = F / NWG;
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* sm = align_smem(smraw);
-    __shared__ uint64_t bar;
+    __shared__ uint64_t barx[2], barm;
     __shared__ uint32_t tbase;
-    __shared__ float bias[3 * F + F + 1];
-    __shared__ float w4acc[4][F + 1];  // per-warp partial of dL/dw4 (and dL/db4 at F)
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    load_weight(sm + S_W1, P + OW1, false);
-    load_weight(sm + S_W2, P + OW2, false);
-    load_weight(sm + S_W3, P + OW3, false);
-    load_weight(sm + S_W2T, P + OW2, true);
-    load_weight(sm + S_W3T, P + OW3, true);
-    for (int e = t; e < F; e += TILE) {
-        bias[e] = P[OB1 + e]; bias[F + e] = P[OB2 + e]; bias[2 * F + e] = P[OB3 + e]; bias[3 * F + e] = P[OW4 + e];
+    __shared__ __align__(16) float bias[4 * F + 4];
+    __shared__ float ypart[NWG][TILE];
+    __shared__ float red[4 * NWG][CW + 2];
+    const int t = threadIdx.x, row = t & (TILE - 1), g = t >> 7, c0 = g * CW, lane = t & 31, warp = t >> 5;
+    const int ntiles = (n + TILE - 1) / TILE;
+    if (t == 0) {
+        mbar_init(&barx[0], 1);
+        mbar_init(&barx[1], 1);
+        mbar_init(&barm, 1);
+        tma_prefetch_map(&xmap);
     }
-    for (int e = t; e < 4 * (F + 1); e += TILE) (&w4acc[0][0])[e] = 0.0f;
-    // constant parts: zero rows 64..79 of the transposed activations, zero rows 64..127 of dZ^T
-    for (int e = t; e < 16 * TILE; e += TILE) {
-        const int r = 64 + e / TILE, i = e % TILE;
-        st_bf16(sm + S_XT, kmajor_off(r, i, TILE), 0.0f);
-        st_bf16(sm + S_H1T, kmajor_off(r, i, TILE), 0.0f);
-        st_bf16(sm + S_H2T, kmajor_off(r, i, TILE), 0.0f);
+    load_params(sm + G_W, Wimg, P, bias);
+    // the constant block: BF16 1.0 in column 0 of every row, zeros elsewhere
+    for (int e = t; e < (int)(TB / 16); e += blockDim.x) {
+        const int r = e >> 3, ch = e & 7;
+        ((uint4*)(sm + G_ONE))[e] = make_uint4(ch == (r & 7) ? 0x3F80u : 0u, 0u, 0u, 0u);
     }
-    for (int e = t; e < 64 * TILE; e += TILE) st_bf16(sm + S_DZT, kmajor_off(64 + e / TILE, e % TILE, TILE), 0.0f);
-    if (t == 0) { bias[4 * F] = P[OB4]; mbar_init(&bar, 1); }
     if (t < 32) tmem_alloc(&tbase, 512);
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tb = tbase;
-    Sync sy{&bar, 0u, true};
-    const uint32_t id64 = idesc_bf16(TILE, F), id80 = idesc_bf16(TILE, NB);
-    const uint32_t aX = smem_u32(sm + S_X), aXT = smem_u32(sm + S_XT), aH1 = smem_u32(sm + S_H1), aH1T = smem_u32(sm + S_H1T);
-    const uint32_t aH2 = smem_u32(sm + S_H2), aH2T = smem_u32(sm + S_H2T), aDZ = smem_u32(sm + S_DZ), aDZT = smem_u32(sm + S_DZT);
-    const uint32_t aW1 = smem_u32(sm + S_W1), aW2 = smem_u32(sm + S_W2), aW3 = smem_u32(sm + S_W3);
-    const uint32_t aW2T = smem_u32(sm + S_W2T), aW3T = smem_u32(sm + S_W3T);
-    float loss = 0.0f;
-    int first = 1;
-    const int ntiles = (n + TILE - 1) / TILE;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long row = (long)tile * TILE + t;
-        const bool valid = row < n;
-        {
-            const uint4* src = (const uint4*)(X + row * F);
-#pragma unroll
-            for (int c = 0; c < F / 8; c++) {
-                const uint4 v = valid ? src[c] : make_uint4(0, 0, 0, 0);
-                *(uint4*)(sm + S_X + kmajor_off(t, c * 8, F)) = v;
-                const __nv_bfloat16* e = (const __nv_bfloat16*)&v;
-#pragma unroll
-                for (int q = 0; q < 8; q++) *(__nv_bfloat16*)(sm + S_XT + kmajor_off(c * 8 + q, t, TILE)) = e[q];
-            }
-            st_bf16(sm + S_XT, kmajor_off(64, t, TILE), valid ? 1.0f : 0.0f);
-        }
-        publish();
-        // forward
-        for (int layer = 0; layer < 3; layer++) {
-            if (t == 0) {
-                const uint32_t a = layer == 0 ? aX : (layer == 1 ? aH1 : aH2);
-                const uint32_t w = layer == 0 ? aW1 : (layer == 1 ? aW2 : aW3);
-                mma_chain(tb + layer * F, a, F, w, F, F, id64, 0);
-                mma_commit(&bar);
-            }
-            if (!sy.wait() || layer == 2) break;
-            unsigned char* Hn = sm + (layer == 0 ? S_H1 : S_H2);
-            unsigned char* HnT = sm + (layer == 0 ? S_H1T : S_H2T);
-            for (int c = 0; c < F; c += 16) {
-                float z[16];
-                tmem_ld16(tmem_lane_addr(tb, layer * F + c), z);
-                tmem_wait_ld();
-#pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const float h = valid ? silu(z[q] + bias[layer * F + c + q]) : 0.0f;
-                    st_bf16(Hn, kmajor_off(t, c + q, F), h);
-                    st_bf16(HnT, kmajor_off(c + q, t, TILE), h);
-                }
-            }
-            st_bf16(HnT, kmajor_off(64, t, TILE), valid ? 1.0f : 0.0f);
-            publish();
-        }
-        if (!sy.ok) break;
-        // output layer, loss, dL/dw4, dL/db4, dZ3
-        float yv = bias[4 * F];
-        for (int c = 0; c < F; c += 16) {
-            float z[16];
-            tmem_ld16(tmem_lane_addr(tb, T_Z3 + c), z);
-            tmem_wait_ld();
-#pragma unroll
-            for (int q = 0; q < 16; q++) yv += bias[3 * F + c + q] * silu(z[q] + bias[2 * F + c + q]);
-        }
-        const float r = valid ? yv - target[row] : 0.0f;
-        loss += r * r;
-        const float dy = 2.0f * r * dscale;
-        for (int c = 0; c < F; c += 16) {
-            float z[16];
-            tmem_ld16(tmem_lane_addr(tb, T_Z3 + c), z);
-            tmem_wait_ld();
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const float zz = z[q] + bias[2 * F + c + q];
-                float g = dy * silu(zz);  // dL/dw4 term
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
-                if (lane == 0) w4acc[warp][c + q] += g;
-                const float dz = dy * bias[3 * F + c + q] * dsilu(zz);
-                st_bf16(sm + S_DZ, kmajor_off(t, c + q, F), dz);
-                st_bf16(sm + S_DZT, kmajor_off(c + q, t, TILE), dz);
+    // TMA loads issued and consumed per feature buffer (thread 0's count; 16 bits each)
+    uint32_t issued = 0, used = 0;
+    if (t == 0) {
+        for (int b = 0; b < 2; b++) {
+            const int tile = blockIdx.x + b * gridDim.x;
+            if (tile < ntiles) {
+                mbar_expect_tx(&barx[b], TB);
+                tma_load_2d(sm + G_X + b * TB, &xmap, 0, tile * TILE, &barx[b]);
+                issued += 1u << (16 * b);
             }
         }
-        {
-            float g = dy;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
-            if (lane == 0) w4acc[warp][F] += g;
-        }
-        publish();
-        // dW3 += dZ3^T [H2 | 1];  dH2 = dZ3 W3
-        if (t == 0) {
-            mma_chain(tb + T_DW3, aDZT, TILE, aH2T, TILE, TILE, id80, !first);
-            mma_chain(tb + T_DH, aDZ, F, aW3T, F, F, id64, 0);
-            mma_commit(&bar);
-        }
-        if (!sy.wait()) break;
-        for (int layer = 1; layer >= 0; layer--) {
-            // dZ_l = dH_l * silu'(Z_l)
-            for (int c = 0; c < F; c += 16) {
-                float dh[16], z[16];
-                tmem_ld16(tmem_lane_addr(tb, T_DH + c), dh);
-                tmem_ld16(tmem_lane_addr(tb, layer * F + c), z);
-                tmem_wait_ld();
-#pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const float dz = valid ? dh[q] * dsilu(z[q] + bias[layer * F + c + q]) : 0.0f;
-                    if (layer == 1) st_bf16(sm + S_DZ, kmajor_off(t, c + q, F), dz);
-                    st_bf16(sm + S_DZT, kmajor_off(c + q, t, TILE), dz);
-                }
-            }
-            publish();
-            if (t == 0) {
-                if (layer == 1) {  // dW2 += dZ2^T [H1 | 1];  dH1 = dZ2 W2
-                    mma_chain(tb + T_DW2, aDZT, TILE, aH1T, TILE, TILE, id80, !first);
-                    mma_chain(tb + T_DH, aDZ, F, aW2T, F, F, id64, 0);
-                } else {           // dW1 += dZ1^T [X | 1]
-                    mma_chain(tb + T_DW1, aDZT, TILE, aXT, TILE, TILE, id80, !first);
-                }
-                mma_commit(&bar);
-            }
-            if (!sy.wait()) break;
-        }
-        if (!sy.ok) break;
-        first = 0;
     }
-    const bool ok = sy.ok;
-    if (!ok && t == 0) atomicExch(err, 1);
-    // per-CTA partial: rows n < 64 of the dW accumulators (column 64 = bias gradient)
-    float* out = part + (size_t)blockIdx.x * PSTRIDE;
-    if (t < F) {
-        const int offs[3][2] = {{OW1, OB1}, {OW2, OB2}, {OW3, OB3}};
-        const int cols[3] = {T_DW1, T_DW2, T_DW3};
-        for (int l = 0; l < 3; l++) {
-            for (int c = 0; c < NB; c += 16) {
-                float v[16];
-                if (!first && ok) {
-                    tmem_ld16(tmem_lane_addr(tb, cols[l] + c), v);
-                    tmem_wait_ld();
-                } else {
+    const uint32_t tb = tbase, id = idesc_bf16(TILE, F);
+    const uint32_t aH1 = smem_u32(sm + G_H1), aH2 = smem_u32(sm + G_H2), aDZ = smem_u32(sm + G_DZ), aONE = smem_u32(sm + G_ONE);
+    const uint32_t aW1 = smem_u32(sm + G_W), aW2 = aW1 + WB, aW3 = aW1 + 2 * WB;
+    uint32_t pm = 0;
+    bool ok = true;
+    float acc4[CW];  // this sample's share of dL/dw4, summed over the CTA's tiles
 #pragma unroll
-                    for (int q = 0; q < 16; q++) v[q] = 0.0f;
+    for (int c = 0; c < CW; c++) acc4[c] = 0.0f;
+    float loss = 0.0f, accb4 = 0.0f;
+    auto mma_wait = [&]() {
+        if (t == 0) mma_commit(&barm);
+        ok = vote_ok(mbar_wait(&barm, pm, WAIT_CYCLES));
+        pm ^= 1u;
+        fence_after();
+        return ok;
+    };
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int b = it & 1;
+        const long grow = (long)tile * TILE + row;
+        const bool valid = grow < n;
+        const float tgt = valid ? target[grow] : 0.0f;  // needed after the forward GEMMs
+        ok = vote_ok(mbar_wait(&barx[b], (uint32_t)(it >> 1) & 1u, WAIT_CYCLES));
+        if (!ok) break;
+        used += 1u << (16 * b);
+        const uint32_t aX = smem_u32(sm + G_X + b * TB);
+        // ---- forward
+        if (t == 0)
+            for (int s = 0; s < F / 16; s++) mma_bf16(tb + T_Z1, desc_sw128_k(aX, s), desc_sw128_k(aW1, s), id, s > 0);
+        if (!mma_wait()) break;
+        if (t == 0 && it > 0) {
+            // this wait also covered the previous tile's last MMA (dW1, which read the other
+            // feature buffer): load the next tile into that buffer
+            const int next = tile + gridDim.x;
+            if (next < ntiles) {
+                mbar_expect_tx(&barx[b ^ 1], TB);
+                tma_load_2d(sm + G_X + (b ^ 1) * TB, &xmap, 0, next * TILE, &barx[b ^ 1]);
+                issued += 1u << (16 * (b ^ 1));
+            }
+        }
+        {   // H1 = SiLU(Z1 + b1); SiLU' kept in TMEM over Z1 for the backward pass
+            float z[CW], d[CW];
+            tmem_load<CW>(tb, T_Z1 + c0, z);
+            tmem_wait_ld();
+            hidden_epilogue<CW, true>(sm + G_H1, row, c0, z, bias, d);
+            tmem_store<CW>(tb, T_Z1 + c0, d);
+        }
+        publish();
+        if (t == 0)
+            for (int s = 0; s < F / 16; s++) mma_bf16(tb + T_Z2, desc_sw128_k(aH1, s), desc_sw128_k(aW2, s), id, s > 0);
+        if (!mma_wait()) break;
+        {
+            float z[CW], d[CW];
+            tmem_load<CW>(tb, T_Z2 + c0, z);
+            tmem_wait_ld();
+            hidden_epilogue<CW, true>(sm + G_H2, row, c0, z, bias + F, d);
+            tmem_store<CW>(tb, T_Z2 + c0, d);
+        }
+        publish();
+        if (t == 0)
+            for (int s = 0; s < F / 16; s++) mma_bf16(tb + T_Z3, desc_sw128_k(aH2, s), desc_sw128_k(aW3, s), id, s > 0);
+        if (!mma_wait()) break;
+        // ---- output layer, loss, dL/dw4, dL/db4, dZ3
+        {
+            float z[CW], sg[CW];
+            tmem_load<CW>(tb, T_Z3 + c0, z);
+            tmem_wait_ld();
+            float yp = 0.0f;
+            float w4[CW];
+#pragma unroll
+            for (int c = 0; c < CW; c += 4) {
+                const float4 b = *(const float4*)(bias + 2 * F + c0 + c), w = *(const float4*)(bias + 3 * F + c0 + c);
+                z[c] += b.x; z[c + 1] += b.y; z[c + 2] += b.z; z[c + 3] += b.w;
+                w4[c] = w.x; w4[c + 1] = w.y; w4[c + 2] = w.z; w4[c + 3] = w.w;
+            }
+#pragma unroll
+            for (int c = 0; c < CW; c++) {
+                sg[c] = logistic(z[c]);
+                yp = __fmaf_rn(w4[c], z[c] * sg[c], yp);
+            }
+            ypart[g][row] = yp;
+            __syncthreads();
+            float yv = bias[4 * F];
+#pragma unroll
+            for (int q = 0; q < NWG; q++) yv += ypart[q][row];
+            const float r = valid ? yv - tgt : 0.0f;
+            const float dy = 2.0f * r * dscale;
+            if (g == 0) {
+                loss += r * r;
+                accb4 += dy;
+            }
+#pragma unroll
+            for (int c = 0; c < CW; c += 8) {
+                float d[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int j = c + q;
+                    acc4[j] = __fmaf_rn(dy, z[j] * sg[j], acc4[j]);
+                    d[q] = dy * w4[j] * dsilu(z[j], sg[j]);
                 }
+                *(uint4*)(sm + G_DZ + sw128_off(row, c0 + c)) =
+                    make_uint4(pack_bf16(d[0], d[1]), pack_bf16(d[2], d[3]), pack_bf16(d[4], d[5]), pack_bf16(d[6], d[7]));
+            }
+        }
+        publish();
+        // ---- dW3^T += [H2 | 1]^T dZ3;  dH2 = dZ3 W3 (over Z3, which is no longer needed)
+        if (t == 0) {
+            mma_weight_grad(tb + T_DW + 2 * F, aH2, aONE, aDZ, it > 0);
+            mma_input_grad(tb + T_Z3, aDZ, aW3);
+        }
+        if (!mma_wait()) break;
+        for (int l = 1; l >= 0; l--) {
+            {   // dZ_l = dH_l * SiLU'(Z_l) (the derivative stored by the forward epilogue)
+                float dh[CW], d[CW];
+                tmem_load<CW>(tb, T_Z3 + c0, dh);
+                tmem_load<CW>(tb, l * F + c0, d);
+                tmem_wait_ld();
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int k = c + q;
-                    if (k < F) out[offs[l][0] + t * F + k] = v[q];
-                    else if (k == F) out[offs[l][1] + t] = v[q];
+                for (int c = 0; c < CW; c += 8) {
+                    uint32_t pk[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        pk[q] = pack_bf16(dh[c + 2 * q] * d[c + 2 * q], dh[c + 2 * q + 1] * d[c + 2 * q + 1]);
+                    *(uint4*)(sm + G_DZ + sw128_off(row, c0 + c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 }
             }
+            publish();
+            if (t == 0) {
+                if (l == 1) {  // dW2^T += [H1 | 1]^T dZ2;  dH1 = dZ2 W2
+                    mma_weight_grad(tb + T_DW + F, aH1, aONE, aDZ, it > 0);
+                    mma_input_grad(tb + T_Z3, aDZ, aW2);
+                } else {       // dW1^T += [X | 1]^T dZ1 (completion awaited with the next tile's first GEMM)
+                    mma_weight_grad(tb + T_DW, aX, aONE, aDZ, it > 0);
+                }
+            }
+            if (l == 1 && !mma_wait()) break;
+        }
+        if (!ok) break;
+    }
+    if (ok && it > 0) mma_wait();  // the last dW1 MMAs
+    if (t == 0) {
+        for (int b = 0; b < 2; b++) {
+            const uint32_t ib = (issued >> (16 * b)) & 0xFFFFu, ub = (used >> (16 * b)) & 0xFFFFu;
+            if (ib > ub) mbar_wait(&barx[b], ub & 1u, WAIT_CYCLES);
+        }
+        if (!ok) atomicExch(err, 1);
+    }
+    // ---- per-CTA partial record
+    float* out = part + (size_t)blockIdx.x * PSTRIDE;
+    for (int l = 0; l < 3; l++) {
+        float v[CW];
+        tmem_load<CW>(tb, T_DW + l * F + c0, v);
+        tmem_wait_ld();
+        if (!ok || it == 0) {
+#pragma unroll
+            for (int c = 0; c < CW; c++) v[c] = 0.0f;
+        }
+        if (row < F) {  // lane k = input k: dW_l[n][k] for this warpgroup's outputs n
+#pragma unroll
+            for (int c = 0; c < CW; c++) out[OW1 + l * LSTRIDE + (c0 + c) * F + row] = v[c];
+        } else if (row == F) {  // the bias row
+#pragma unroll
+            for (int c = 0; c < CW; c++) out[OB1 + l * LSTRIDE + c0 + c] = v[c];
+        }
+    }
+    // dL/dw4 (this warpgroup's columns), dL/db4 and the loss: sums over the CTA's samples in
+    // a fixed order (lanes by shuffles, then the warps)
+#pragma unroll
+    for (int c = 0; c < CW; c++) {
+        float v = acc4[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][c] = v;
+    }
+    {
+        float l = loss, bb = accb4;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            l += __shfl_xor_sync(0xffffffffu, l, o);
+            bb += __shfl_xor_sync(0xffffffffu, bb, o);
+        }
+        if (lane == 0) {
+            red[warp][CW] = l;
+            red[warp][CW + 1] = bb;
         }
     }
     __syncthreads();
-    if (t <= F) out[(t < F ? OW4 + t : OB4)] = w4acc[0][t] + w4acc[1][t] + w4acc[2][t] + w4acc[3][t];
-    {
-        __shared__ float ls[4];
-        float l = loss;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-        if (lane == 0) ls[warp] = l;
-        __syncthreads();
-        if (t == 0) out[NPARAM] = ls[0] + ls[1] + ls[2] + ls[3];
+    if (row < CW) {  // one thread per column of each warpgroup
+        float s = 0.0f;
+        for (int w = 0; w < 4; w++) s += red[4 * g + w][row];
+        out[OW4 + c0 + row] = ok ? s : 0.0f;
+    }
+    if (t == 0) {
+        float l = 0.0f, bb = 0.0f;
+        for (int w = 0; w < 4; w++) {
+            l += red[w][CW];
+            bb += red[w][CW + 1];
+        }
+        out[NPARAM] = ok ? l : 0.0f;
+        out[OB4] = ok ? bb : 0.0f;
     }
     fence_before();
     __syncthreads();
-    if (t < 32) tmem_free(tb, 512);
+    if (t < 32) tmem_free(tbase, 512);
 }
 
-// Folds the CTA partials in CTA order; optionally applies Adam (step >= 1).
-__global__ void k_mlp_adam(const float* __restrict__ part, int G, float* __restrict__ grad, float* __restrict__ P,
-                           float* __restrict__ m, float* __restrict__ v, long step, float lr, float b1, float b2, float eps,
-                           float* loss) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e <= NPARAM; e += gridDim.x * blockDim.x) {
-        float g = 0.0f;
-        for (int b = 0; b < G; b++) g += part[(size_t)b * PSTRIDE + e];
-        if (e == NPARAM) { *loss = g; continue; }
-        grad[e] = g;
-        if (step < 1) continue;
-        const float mm = b1 * m[e] + (1.0f - b1) * g, vv = b2 * v[e] + (1.0f - b2) * g * g;
-        m[e] = mm;
-        v[e] = vv;
-        const float mh = mm / (1.0f - powf(b1, (float)step)), vh = vv / (1.0f - powf(b2, (float)step));
-        P[e] -= lr * mh / (sqrtf(vh) + eps);
+// BF16 operand image of weight element e of the hidden layers (e < 3 * 4096), or -1.
+__device__ __forceinline__ int image_index(int e) {
+    const int l = e / LSTRIDE, r = e - l * LSTRIDE;
+    if (l > 2 || r >= F * F) return -1;
+    return (int)((l * WB + sw128_off(r / F, r % F)) / 2);
+}
+
+__global__ void k_mlp_pack(const float* __restrict__ P, __nv_bfloat16* __restrict__ Wimg) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < OW4; e += gridDim.x * blockDim.x) {
+        const int i = image_index(e);
+        if (i >= 0) Wimg[i] = __float2bfloat16_rn(P[e]);
     }
+}
+
+// Folds the CTA partials in a fixed order (slice j of 8 sums CTAs j, j + 8, ..., then the
+// slices in order); optionally applies Adam (step >= 1) and rewrites the operand images.
+constexpr int ADAM_PARAMS = 32, ADAM_SLICES = 8;
+__global__ void __launch_bounds__(ADAM_PARAMS * ADAM_SLICES) k_mlp_adam(const float* __restrict__ part, int G, float* __restrict__ grad,
+                                                                       float* __restrict__ P, float* __restrict__ m, float* __restrict__ v,
+                                                                       __nv_bfloat16* __restrict__ Wimg, long step, float lr, float b1,
+                                                                       float b2, float eps, float* loss) {
+    __shared__ float red[ADAM_SLICES][ADAM_PARAMS];
+    const int p = threadIdx.x % ADAM_PARAMS, j = threadIdx.x / ADAM_PARAMS;
+    const int e = blockIdx.x * ADAM_PARAMS + p;
+    float g = 0.0f;
+    if (e <= NPARAM)
+        for (int b = j; b < G; b += ADAM_SLICES) g += part[(size_t)b * PSTRIDE + e];
+    red[j][p] = g;
+    __syncthreads();
+    if (j != 0 || e > NPARAM) return;
+    g = 0.0f;
+    for (int q = 0; q < ADAM_SLICES; q++) g += red[q][p];
+    if (e == NPARAM) { *loss = g; return; }
+    grad[e] = g;
+    if (step < 1) return;
+    const float mm = b1 * m[e] + (1.0f - b1) * g, vv = b2 * v[e] + (1.0f - b2) * g * g;
+    m[e] = mm;
+    v[e] = vv;
+    const float mh = mm / (1.0f - powf(b1, (float)step)), vh = vv / (1.0f - powf(b2, (float)step));
+    const float w = P[e] - lr * mh / (sqrtf(vh) + eps);
+    P[e] = w;
+    const int i = image_index(e);
+    if (i >= 0) Wimg[i] = __float2bfloat16_rn(w);
 }
 
 }  // namespace mlp
@@ -409,23 +581,68 @@ using namespace spb6g::mlp;
 
 struct spb6g_mlp {
     int device = 0;
-    int G = 0;
+    int G = 0;       // CTAs of a training pass (one per SM)
+    int Gf = 0;      // CTAs of an inference pass (resident CTAs per SM x SMs)
     long step = 0;
     cudaStream_t st = nullptr;
     float *P = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *part = nullptr, *loss = nullptr;
+    __nv_bfloat16* Wimg = nullptr;
     int* err = nullptr;
+    // feature-row tensor maps of the last calls
+    const void* fx = nullptr;
+    int fn = -1;
+    CUtensorMap fmap;
+    const void* gx = nullptr;
+    int gn = -1;
+    CUtensorMap gmap;
 };
 
 namespace {
-int mlp_prepare(int device) {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+// Rows of 64 BF16 (128 bytes), n rows; 128-row boxes in the 128-byte swizzle; rows past n read as zeros.
+int feature_map(CUtensorMap* map, const void* X, int n) {
+    const auto enc = encode_fn();
+    if (!enc || ((uintptr_t)X & 15u) || n <= 0) return -1;
+    const cuuint64_t dims[2] = {(cuuint64_t)F, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)F * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)F, (cuuint32_t)TILE};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(X), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+               ? 0
+               : -1;
+}
+int mlp_prepare(int device, int* fwd_per_sm) {
     static std::mutex mu;
     static unsigned done = 0;
+    static int per_sm[32] = {0};
     std::lock_guard<std::mutex> lk(mu);
-    if (device < 32 && (done >> device) & 1u) return 0;
-    if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GRAD_SMEM) != cudaSuccess)
+    if (device < 32 && (done >> device) & 1u) {
+        *fwd_per_sm = per_sm[device];
+        return 0;
+    }
+    if (cudaFuncSetAttribute(k_mlp_forward<FWD_NWG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_forward<FWD_NWG>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_grad<GRAD_NWG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GRAD_SMEM) != cudaSuccess)
         return -1;
-    if (device < 32) done |= 1u << device;
+    // the kernel's launch bounds, shared memory and 64 TMEM columns are sized for FWD_CTAS per SM
+    const int k = FWD_CTAS;
+    if (device < 32) {
+        done |= 1u << device;
+        per_sm[device] = k;
+    }
+    *fwd_per_sm = k;
     return 0;
 }
 int mlp_check(spb6g_mlp* h) {
@@ -433,7 +650,7 @@ int mlp_check(spb6g_mlp* h) {
     if (cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->st) != cudaSuccess) return SPB6G_CUDA_ERROR;
     if (cudaStreamSynchronize(h->st) != cudaSuccess) return SPB6G_CUDA_ERROR;
     if (e) {
-        fprintf(stderr, "spb6g_mlp: a tensor-core wait timed out\n");
+        fprintf(stderr, "spb6g_mlp: a tensor-core or TMA wait timed out\n");
         cudaMemsetAsync(h->err, 0, sizeof(int), h->st);
         return SPB6G_CUDA_ERROR;
     }
@@ -452,24 +669,31 @@ int spb6g_mlp_create(int device, spb6g_mlp** out) {
     int major = 0;
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
     if (major != 10) return SPB6G_UNSUPPORTED;
-    if (mlp_prepare(device)) return SPB6G_CUDA_ERROR;
+    if (!encode_fn()) return SPB6G_UNSUPPORTED;
+    int per_sm = 0;
+    if (mlp_prepare(device, &per_sm)) return SPB6G_CUDA_ERROR;
     spb6g_mlp* h = new spb6g_mlp();
     h->device = device;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     h->G = sms > 0 ? sms : 148;
-    bool ok = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) == cudaSuccess;
+    h->Gf = h->G * per_sm;
+    // a blocking stream: the handle's work orders itself after the caller's work on the
+    // legacy default stream (which produces X and the targets in the usual case)
+    bool ok = cudaStreamCreate(&h->st) == cudaSuccess;
     ok = ok && cudaMalloc(&h->P, NPARAM * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&h->m, NPARAM * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&h->v, NPARAM * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&h->grad, NPARAM * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&h->part, (size_t)h->G * PSTRIDE * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&h->loss, sizeof(float)) == cudaSuccess;
+    ok = ok && cudaMalloc(&h->Wimg, 3 * WB) == cudaSuccess;
     ok = ok && cudaMalloc(&h->err, sizeof(int)) == cudaSuccess;
     if (ok) {
         cudaMemsetAsync(h->P, 0, NPARAM * sizeof(float), h->st);
         cudaMemsetAsync(h->m, 0, NPARAM * sizeof(float), h->st);
         cudaMemsetAsync(h->v, 0, NPARAM * sizeof(float), h->st);
+        cudaMemsetAsync(h->Wimg, 0, 3 * WB, h->st);
         cudaMemsetAsync(h->err, 0, sizeof(int), h->st);
         ok = cudaStreamSynchronize(h->st) == cudaSuccess;
     }
@@ -482,7 +706,8 @@ void spb6g_mlp_destroy(spb6g_mlp* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
-    for (void* p : {(void*)h->P, (void*)h->m, (void*)h->v, (void*)h->grad, (void*)h->part, (void*)h->loss, (void*)h->err})
+    for (void* p : {(void*)h->P, (void*)h->m, (void*)h->v, (void*)h->grad, (void*)h->part, (void*)h->loss, (void*)h->Wimg,
+                    (void*)h->err})
         if (p) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
@@ -496,6 +721,8 @@ int spb6g_mlp_set_params(spb6g_mlp* h, const float* params) {
     if (cudaMemcpyAsync(h->P, params, NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->st) != cudaSuccess) return SPB6G_CUDA_ERROR;
     cudaMemsetAsync(h->m, 0, NPARAM * sizeof(float), h->st);
     cudaMemsetAsync(h->v, 0, NPARAM * sizeof(float), h->st);
+    k_mlp_pack<<<(OW4 + 255) / 256, 256, 0, h->st>>>(h->P, h->Wimg);
+    if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
     h->step = 0;
     return cudaStreamSynchronize(h->st) == cudaSuccess ? SPB6G_OK : SPB6G_CUDA_ERROR;
 }
@@ -508,30 +735,66 @@ int spb6g_mlp_get_params(spb6g_mlp* h, float* params) {
 }
 
 int spb6g_mlp_forward(spb6g_mlp* h, const void* X_dev, int n, float* y_dev, void* stream) {
-    if (!h || !X_dev || !y_dev || n < 0) return SPB6G_BAD_ARG;
+    if (!h || !X_dev || !y_dev || n < 0 || ((uintptr_t)X_dev & 15u)) return SPB6G_BAD_ARG;
     if (n == 0) return SPB6G_OK;
     cudaSetDevice(h->device);
+    if (X_dev != h->fx || n != h->fn) {
+        if (feature_map(&h->fmap, X_dev, n)) return SPB6G_CUDA_ERROR;
+        h->fx = X_dev;
+        h->fn = n;
+    }
     cudaStream_t st = stream ? (cudaStream_t)stream : h->st;
     const int ntiles = (n + TILE - 1) / TILE;
-    k_mlp_forward<<<ntiles < h->G ? ntiles : h->G, TILE, FWD_SMEM, st>>>(h->P, (const __nv_bfloat16*)X_dev, n, y_dev, h->err);
+    const int G = ntiles < h->Gf ? ntiles : h->Gf;
+    k_mlp_forward<FWD_NWG><<<G, 128 * FWD_NWG, FWD_SMEM, st>>>(h->fmap, h->P, (const uint4*)h->Wimg, n, y_dev, h->err);
     if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
     if (stream) return SPB6G_OK;
+    return mlp_check(h);
+}
+
+// One pass over the batch on `stream`, nothing read back: gradient of mean((y - target)^2)
+// into the handle, with lr > 0 also an Adam step.
+static int mlp_train_launch(spb6g_mlp* h, const void* X_dev, const float* target_dev, int n, float lr, cudaStream_t st) {
+    if (X_dev != h->gx || n != h->gn) {
+        if (feature_map(&h->gmap, X_dev, n)) return SPB6G_CUDA_ERROR;
+        h->gx = X_dev;
+        h->gn = n;
+    }
+    const int ntiles = (n + TILE - 1) / TILE;
+    const int G = ntiles < h->G ? ntiles : h->G;
+    k_mlp_grad<GRAD_NWG><<<G, 128 * GRAD_NWG, GRAD_SMEM, st>>>(h->gmap, h->P, (const uint4*)h->Wimg, target_dev, n, 1.0f / (float)n,
+                                                               h->part, h->err);
+    if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
+    const long step = lr > 0 ? ++h->step : 0;
+    k_mlp_adam<<<(NPARAM + ADAM_PARAMS) / ADAM_PARAMS, ADAM_PARAMS * ADAM_SLICES, 0, st>>>(
+        h->part, G, h->grad, h->P, h->m, h->v, h->Wimg, step, lr, 0.9f, 0.999f, 1e-8f, h->loss);
+    return cudaGetLastError() == cudaSuccess ? SPB6G_OK : SPB6G_CUDA_ERROR;
+}
+
+int spb6g_mlp_train_async(spb6g_mlp* h, const void* X_dev, const float* target_dev, int n, float lr, void* stream) {
+    if (!h || !X_dev || !target_dev || n <= 0 || ((uintptr_t)X_dev & 15u)) return SPB6G_BAD_ARG;
+    cudaSetDevice(h->device);
+    return mlp_train_launch(h, X_dev, target_dev, n, lr, stream ? (cudaStream_t)stream : h->st);
+}
+
+int spb6g_mlp_last_loss(spb6g_mlp* h, void* stream, float* loss_sum) {
+    if (!h || !loss_sum) return SPB6G_BAD_ARG;
+    cudaSetDevice(h->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->st;
+    float l = 0;
+    if (cudaMemcpyAsync(&l, h->loss, sizeof(float), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SPB6G_CUDA_ERROR;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SPB6G_CUDA_ERROR;
+    *loss_sum = l;
     return mlp_check(h);
 }
 
 // One pass over the batch: gradient of mean((y - target)^2); with lr > 0 also an Adam step.
 int spb6g_mlp_train_step(spb6g_mlp* h, const void* X_dev, const float* target_dev, int n, float lr, float* loss_out,
                          float* grad_host) {
-    if (!h || !X_dev || !target_dev || n <= 0) return SPB6G_BAD_ARG;
+    if (!h || !X_dev || !target_dev || n <= 0 || ((uintptr_t)X_dev & 15u)) return SPB6G_BAD_ARG;
     cudaSetDevice(h->device);
-    const int ntiles = (n + TILE - 1) / TILE;
-    const int G = ntiles < h->G ? ntiles : h->G;
-    k_mlp_grad<<<G, TILE, GRAD_SMEM, h->st>>>(h->P, (const __nv_bfloat16*)X_dev, target_dev, n, 1.0f / (float)n, h->part, h->err);
-    if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
-    const long step = lr > 0 ? ++h->step : 0;
-    k_mlp_adam<<<(NPARAM + 256) / 256, 256, 0, h->st>>>(h->part, G, h->grad, h->P, h->m, h->v, step, lr, 0.9f, 0.999f, 1e-8f,
-                                                         h->loss);
-    if (cudaGetLastError() != cudaSuccess) return SPB6G_CUDA_ERROR;
+    const int lrc = mlp_train_launch(h, X_dev, target_dev, n, lr, h->st);
+    if (lrc != SPB6G_OK) return lrc;
     float l = 0;
     if (cudaMemcpyAsync(&l, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->st) != cudaSuccess) return SPB6G_CUDA_ERROR;
     if (grad_host && cudaMemcpyAsync(grad_host, h->grad, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, h->st) != cudaSuccess)

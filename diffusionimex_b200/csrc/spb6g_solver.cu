@@ -828,6 +828,9 @@ int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capa
 }
 int spb6g_dump_count(spb6g_solver* s, int64_t* count) {
     if (!s || !count) return SPB6G_BAD_ARG;
+    // the rows counted are complete when the call returns (the caller reads them on its own stream)
+    cudaSetDevice(s->cfg.device);
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) return SPB6G_CUDA_ERROR;
     *count = s->dump_count;
     return SPB6G_OK;
 }

@@ -36,9 +36,50 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t base, int K, int s) {
            (1ull << 46);  // descriptor version 1 (Blackwell); base offset 0; no swizzle
 }
 
-// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D; A and B K-major unless
+// a_mn / b_mn (MN-major: the operand's M or N index runs along its rows).
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn = 0, int b_mn = 0) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// ---- 128-byte swizzled tiles: rows of 64 BF16 (128 bytes); the 16-byte chunk c of
+// row r sits at chunk position c ^ (r % 8), the pattern TMA's 128-byte swizzle
+// writes (tile base 1024-byte aligned).  One physical tile serves as either operand
+// form: K-major (rows = M or N, the 64 columns = K) or MN-major (rows = K, the 64
+// columns = M or N).
+__host__ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
+    return (uint32_t)(r * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2);
+}
+// K-major descriptor of the 16-wide K-slice `s`: the slice starts 32 bytes further
+// into each 128-byte row (the swizzle is applied by the hardware on the address),
+// 8-row groups 1024 bytes apart; the leading offset is unused (set to 16 bytes).
+__device__ __forceinline__ uint64_t desc_sw128_k(uint32_t base, int s) {
+    const uint32_t start = base + (uint32_t)s * 32u;
+    return (uint64_t)((start >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+// MN-major descriptor of the 16-wide K-slice `s` (16 rows = two 8-row groups of
+// 1024 bytes); `atom_stride` = byte distance to the next 64-wide block along M/N.
+__device__ __forceinline__ uint64_t desc_sw128_mn(uint32_t base, int s, uint32_t atom_stride) {
+    const uint32_t start = base + (uint32_t)s * 2048u;
+    return (uint64_t)((start >> 4) & 0x3FFFu) | ((uint64_t)((atom_stride >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// ---- TMA (no multicast) and transaction-count mbarriers
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Tile {x, y} of a 2D tensor map into shared memory; completion counted on `bar`.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"((uint64_t)tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_map(const void* tmap) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)tmap) : "memory");
 }
 
 // One MMA (issued by a single thread): D = A * B (+ D when accumulate).
@@ -109,6 +150,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
     for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 consecutive FP32 columns into this thread's TMEM lane.
+__device__ __forceinline__ void tmem_st16(uint32_t addr, const float* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(addr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 // TMEM address of column `col` for the lanes of this thread's warp.
 __device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, int col) {
     return base + ((uint32_t)((threadIdx.x >> 5) & 3) * 32u << 16) + (uint32_t)col;

@@ -114,6 +114,8 @@ def library() -> ctypes.CDLL:
         "spb6g_mlp_get_params": (I, [P, P]),
         "spb6g_mlp_forward": (I, [P, P, I, P, P]),
         "spb6g_mlp_train_step": (I, [P, P, P, I, ctypes.c_float, P, P]),
+        "spb6g_mlp_train_async": (I, [P, P, P, I, ctypes.c_float, P]),
+        "spb6g_mlp_last_loss": (I, [P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

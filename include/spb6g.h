@@ -165,8 +165,11 @@ int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int
  * starts a stage's Newton from the previous stage's pressure).  A small MLP,
  * 64 inputs (54 used) -> 64 -> 64 -> 64 -> 1 with SiLU, BF16 weights on the
  * tensor cores and FP32 accumulation, FP32 master weights trained with Adam.
- * Inputs are row-major BF16 feature rows of 64 values on the device; outputs
- * and targets FP32 on the device.  One handle per device and host thread. */
+ * Inputs are row-major BF16 feature rows of 64 values on the device (16-byte
+ * aligned: they are read by TMA); outputs and targets FP32 on the device.  Calls
+ * without a stream run on the handle's stream, which is ordered after the legacy
+ * default stream only: inputs written on any other stream must be complete
+ * before the call.  One handle per device and host thread. */
 int spb6g_mlp_create(int device, spb6g_mlp** out);
 void spb6g_mlp_destroy(spb6g_mlp* m);
 /* Number of FP32 parameters: W1[64][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4. */
@@ -179,6 +182,12 @@ int spb6g_mlp_forward(spb6g_mlp* m, const void* X_dev, int n, float* y_dev, void
  * loss to *loss_out; with lr > 0 also one Adam step (beta 0.9 / 0.999, eps 1e-8). */
 int spb6g_mlp_train_step(spb6g_mlp* m, const void* X_dev, const float* target_dev, int n, float lr, float* loss_out,
                          float* grad_host);
+/* The same pass launched on `stream` (NULL: the handle's stream) without waiting or reading
+ * anything back, for training loops that keep the device busy. */
+int spb6g_mlp_train_async(spb6g_mlp* m, const void* X_dev, const float* target_dev, int n, float lr, void* stream);
+/* Sum over the rows of (y - target)^2 of the last pass (waits for `stream`; reports a timed-out
+ * tensor-core wait of any earlier call as an error). */
+int spb6g_mlp_last_loss(spb6g_mlp* m, void* stream, float* loss_sum);
 
 /* Warm start on the solver (no counterpart in the reference).  norm: 19 doubles:
  * mean[6], std[6] of the centre values and std[6] of the neighbour differences of
