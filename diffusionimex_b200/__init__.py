@@ -6,6 +6,6 @@ this package holds the kernels (csrc/), the build recipe (build.py), the
 ctypes host layer (solver.py) and the initial-data generators (cases.py).
 """
 from . import cases
-from .solver import BatchSolver, Solver, SolverError, library
+from .solver import BatchSolver, Solver, SolverError, format_profile, library, run_main
 
-__all__ = ["BatchSolver", "Solver", "SolverError", "library", "cases"]
+__all__ = ["BatchSolver", "Solver", "SolverError", "cases", "format_profile", "library", "run_main"]

@@ -29,6 +29,7 @@ struct NewtonScalars {
     double pmin;   // min pbar (P_REF) / caldt rates
     double rate_x, rate_y;
     double E, sumb, bb;  // Jacobian sums for the BiCGStab set-up
+    double tmax[2];      // phase temperature maxima of the last final state (st_Tmax)
     int fail;            // a residual / closure evaluation failed
     int err;             // inadmissible state in the explicit part or stage prep
     int nstrong;         // strong-shock worklist length

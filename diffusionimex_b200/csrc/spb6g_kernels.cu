@@ -1408,7 +1408,7 @@ void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
 }
 
 // ============================================================ final state (:1056-1073) and H_s (:1363-1371)
-SPB6G_DEV void final_at(const Ctx& c, int x) {
+SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
     const Geom& g = c.g;
     {
         const int i = x % g.nx, j = x / g.nx;
@@ -1426,13 +1426,26 @@ SPB6G_DEV void final_at(const Ctx& c, int x) {
             c.Ust.v[k][x] = U[k];
             c.H[(size_t)k * c.n + x] = (U[k] - qs) / c.adt;
         }
+        if (tm) {  // st_Tmax (:1064-1065): the phase temperatures where the phase is present
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const double T = T_amp(c.phy, k, o.o.a[k], o.in.mtr[k], o.o.pbar);
+                if (o.o.a[k] > 1e-9 && isfinite(T)) tm[k] = SMAX(tm[k], T);
+            }
+        }
     }
 }
-__global__ void k_final(Ctx c) {
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) final_at(c, x);
+__global__ void __launch_bounds__(RED_THREADS) k_final(Ctx c) {
+    double m[2] = {0.0, 0.0};
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) final_at(c, x, m);
+    double tot[2];
+    if (grid_fold<RedMax, 2>(m, c.partials, &c.counters[12], tot) && threadIdx.x == 0) {
+        c.ns->tmax[0] = tot[0];
+        c.ns->tmax[1] = tot[1];
+    }
 }
 void launch_final(const Ctx& c, cudaStream_t st) {
-    k_final<<<blocks_for(c.n), TPB, 0, st>>>(c);
+    k_final<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c);
     count(c, 1);
 }
 

@@ -9,10 +9,12 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "../../include/spb6g.h"
 #include "spb6g_ctx.cuh"
+#include "spb6g_output.h"
 
 using namespace spb6g;
 
@@ -73,6 +75,15 @@ struct spb6g_solver {
     float* dumpT = nullptr;
     int64_t dump_cap = 0, dump_count = 0;
     bool dump_stage = false;
+    // output of main() (snap=, probe=, prec=, the final profile; :1325, :1380-1387)
+    std::string out_file;
+    std::vector<double> snaps;
+    size_t snapi = 0;
+    bool probe = false;
+    double probe_x = 0, probe_y = 0;
+    int prec = 16;
+    double M0[3] = {0, 0, 0};           // conserved totals at the start of the run (:1251)
+    std::vector<double> host_U;         // AoS staging of the state for the writers
 };
 
 namespace {
@@ -407,6 +418,7 @@ int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double
     if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
     if (s->pin->ns.fail) return SPB6G_NEWTON_FAIL;
     s->stats.stages++;
+    for (int k = 0; k < 2; k++) s->stats.tmax[k] = SMAX(s->stats.tmax[k], s->pin->ns.tmax[k]);  // st_Tmax (:1070)
     return SPB6G_OK;
 }
 
@@ -433,6 +445,7 @@ int do_step(spb6g_solver* s) {
         }
     }
     s->dt = SMIN(s->dt, cf.tend - s->t);
+    if (s->snapi < s->snaps.size() && s->t + s->dt > s->snaps[s->snapi]) s->dt = s->snaps[s->snapi] - s->t;
     if (!(s->dt > 1e-12 * cf.tend)) return SPB6G_DT_UNDERFLOW;
     bool done = false;
     double Ae[3][3], Ai[3][3];
@@ -604,6 +617,12 @@ int spb6g_destroy(spb6g_solver* s) {
     return SPB6G_OK;
 }
 
+static int copy_state(spb6g_solver* s, double* const* dev, double* host_dst, const double* host_src, int layout);
+// The current state in the AoS layout, in the handle's host staging buffer (for the writers).
+static int stage_host_state(spb6g_solver* s) {
+    s->host_U.resize((size_t)s->n * NV);
+    return copy_state(s, s->U, s->host_U.data(), nullptr, SPB6G_LAYOUT_AOS);
+}
 static int copy_state(spb6g_solver* s, double* const* dev, double* host_dst, const double* host_src, int layout) {
     const int n = s->n;
     std::vector<double> tmp;
@@ -660,6 +679,10 @@ int spb6g_init_pressure(spb6g_solver* s) {
     launch_pbar_init(s->c, s->st, u, pr, s->Pmain);
     CK(cudaStreamSynchronize(s->st));
     s->t = 0; s->dt = 0; s->dtprev = -1; s->startup = true;
+    // conserved totals of the initial state, the stats line's reference (:1251)
+    const int rc = stage_host_state(s);
+    if (rc != SPB6G_OK) return rc;
+    out::conserved_totals(s->cfg, s->host_U.data(), s->M0);
     return SPB6G_OK;
 }
 int spb6g_set_pressure(spb6g_solver* s, const double* P, double p_ref) {
@@ -687,6 +710,22 @@ int spb6g_step(spb6g_solver* s) {
     const int rc = do_step(s);
     s->stats.t = s->t;
     s->stats.dt = s->dt;
+    if (rc == SPB6G_OK && !s->out_file.empty()) {  // snapshot and probe after the accepted step (:1380-1381)
+        const bool snap = s->snapi < s->snaps.size() && s->t >= s->snaps[s->snapi] * (1 - 1e-12);
+        if (snap || s->probe) {
+            const int r = stage_host_state(s);
+            if (r != SPB6G_OK) return r;
+        }
+        if (snap) {
+            const int r = out::write_profile(s->cfg, s->host_U.data(), out::snap_name(s->out_file, s->snapi).c_str(), s->prec);
+            if (r != SPB6G_OK) return r;
+            s->snapi++;
+        }
+        if (s->probe) {
+            const int r = out::write_probe(s->cfg, s->host_U.data(), s->t, s->probe_x, s->probe_y, s->out_file + ".probe", false);
+            if (r != SPB6G_OK) return r;
+        }
+    }
     return rc;
 }
 int spb6g_advance(spb6g_solver* s, int nsteps) {
@@ -696,7 +735,77 @@ int spb6g_advance(spb6g_solver* s, int nsteps) {
         rc = spb6g_step(s);
         if (rc != SPB6G_OK) break;
     }
+    // the profile main() writes at the end of the run or when a step fails (:1326, :1379, :1388)
+    const bool failed = rc == SPB6G_STEP_FAILED || rc == SPB6G_DT_UNDERFLOW;
+    if (!s->out_file.empty() && (failed || (rc == SPB6G_OK && !(s->t < s->cfg.tend * (1 - 1e-12))))) {
+        const int r = spb6g_write_profile(s, s->out_file.c_str(), s->prec);
+        if (r != SPB6G_OK && rc == SPB6G_OK) rc = r;
+    }
     return rc;
+}
+
+int spb6g_set_output(spb6g_solver* s, const spb6g_output* o) {
+    if (!s) return SPB6G_BAD_ARG;
+    if (!o || !o->out_file || !o->out_file[0]) {
+        s->out_file.clear();
+        s->snaps.clear();
+        s->snapi = 0;
+        s->probe = false;
+        return SPB6G_OK;
+    }
+    if (o->nsnap < 0 || (o->nsnap > 0 && !o->snaps)) return SPB6G_BAD_ARG;
+    s->out_file = o->out_file;
+    s->snaps.assign(o->snaps, o->snaps + o->nsnap);
+    s->snapi = 0;
+    while (s->snapi < s->snaps.size() && s->t >= s->snaps[s->snapi] * (1 - 1e-12)) s->snapi++;  // times already passed
+    s->probe = o->probe != 0;
+    s->probe_x = o->probe_x;
+    s->probe_y = o->probe_y;
+    s->prec = o->prec > 0 ? o->prec : 16;
+    if (s->probe) {  // the first probe line, at the current state (:1306)
+        const int r = stage_host_state(s);
+        if (r != SPB6G_OK) return r;
+        return out::write_probe(s->cfg, s->host_U.data(), s->t, s->probe_x, s->probe_y, s->out_file + ".probe", true);
+    }
+    return SPB6G_OK;
+}
+
+int spb6g_format_profile(const spb6g_config* cfg, const double* U, const char* path, int prec) {
+    if (!cfg || !U || !path || prec < 0 || cfg->nx < 1 || cfg->ny < 1) return SPB6G_BAD_ARG;
+    return out::write_profile(*cfg, U, path, prec > 0 ? prec : 16);
+}
+
+int spb6g_write_profile(spb6g_solver* s, const char* path, int prec) {
+    if (!s || !path || prec < 0) return SPB6G_BAD_ARG;
+    const int r = stage_host_state(s);
+    if (r != SPB6G_OK) return r;
+    return out::write_profile(s->cfg, s->host_U.data(), path, prec > 0 ? prec : 16);
+}
+
+int spb6g_conserved_totals(spb6g_solver* s, double* M) {
+    if (!s || !M) return SPB6G_BAD_ARG;
+    const int r = stage_host_state(s);
+    if (r != SPB6G_OK) return r;
+    out::conserved_totals(s->cfg, s->host_U.data(), M);
+    return SPB6G_OK;
+}
+
+int spb6g_stats_line(spb6g_solver* s, int case_id, double wall_s, char* buf, size_t len) {
+    if (!s || !buf || len == 0) return SPB6G_BAD_ARG;
+    double M1[3];
+    const int r = spb6g_conserved_totals(s, M1);
+    if (r != SPB6G_OK) return r;
+    const spb6g_stats& q = s->stats;
+    const double* M0 = s->M0;
+    // st_cl_fail is never incremented by the reference's IMEX program, so its column is always 0;
+    // the reconstruction is always MUSCL (SpaceOrder 2)
+    std::snprintf(buf, len,
+                  "case %d mode 1 order %d rk %d N %d CFL %g | steps %ld (rk1 %ld) rejects %ld floor %ld | stages %ld newton it %ld "
+                  "(%.2f/stage) maxres %.2e Tmax %.4g %.4g | closure fails %ld | dM1/M %.2e dM2/M %.2e dE/E %.2e | wall %.2f s",
+                  case_id, 2, s->cfg.rk, s->cfg.nx, s->cfg.cfl, (long)q.steps, (long)q.rk1, (long)q.rejects, (long)q.floor_count,
+                  (long)q.stages, (long)q.newton_it, q.stages ? (double)q.newton_it / q.stages : 0.0, q.maxres, q.tmax[0], q.tmax[1],
+                  0L, (M1[0] - M0[0]) / M0[0], (M1[1] - M0[1]) / M0[1], (M1[2] - M0[2]) / M0[2], wall_s);
+    return SPB6G_OK;
 }
 int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double* ube_x, double* ube_y, double* phi_x,
                      double* phi_y) {

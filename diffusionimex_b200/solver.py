@@ -56,7 +56,14 @@ class Stats(ctypes.Structure):
         ("steps", ctypes.c_int64), ("rejects", ctypes.c_int64), ("rk1", ctypes.c_int64), ("stages", ctypes.c_int64),
         ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
         ("learned", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
-        ("p_ref", ctypes.c_double),
+        ("p_ref", ctypes.c_double), ("tmax", ctypes.c_double * 2),
+    ]
+
+
+class Output(ctypes.Structure):
+    _fields_ = [
+        ("out_file", ctypes.c_char_p), ("snaps", ctypes.c_void_p), ("nsnap", ctypes.c_int32), ("probe", ctypes.c_int32),
+        ("probe_x", ctypes.c_double), ("probe_y", ctypes.c_double), ("prec", ctypes.c_int32),
     ]
 
 
@@ -86,6 +93,11 @@ def library() -> ctypes.CDLL:
         "spb6g_advance": (I, [P, I]),
         "spb6g_stage_dump": (I, [P, D, P, P, P, P, P, P]),
         "spb6g_get_stats": (I, [P, P]),
+        "spb6g_set_output": (I, [P, P]),
+        "spb6g_write_profile": (I, [P, ctypes.c_char_p, I]),
+        "spb6g_format_profile": (I, [P, P, ctypes.c_char_p, I]),
+        "spb6g_conserved_totals": (I, [P, P]),
+        "spb6g_stats_line": (I, [P, I, D, ctypes.c_char_p, ctypes.c_size_t]),
         "spb6g_set_time": (I, [P, D, D, I]),
         "spb6g_timing_enable": (I, [P, I]),
         "spb6g_timing_get": (I, [P, P, P, I, P]),
@@ -145,6 +157,32 @@ def make_config(case: dict, device: int = 0) -> Config:
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def format_profile(case: dict, U: np.ndarray, path: str, prec: int = 16):
+    """The reference's 17-column profile of a host state U (ny, nx, 8) on the case's grid (host code)."""
+    lib = library()
+    cfg = make_config(case, 0)
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    rc = lib.spb6g_format_profile(ctypes.byref(cfg), _ptr(U), path.encode(), int(prec))
+    if rc != 0:
+        raise SolverError(rc, "spb6g_format_profile")
+
+
+def run_main(case: dict, out_file: str, snaps=(), probe=None, prec: int = 16, device: int = 0) -> str:
+    """The output sequence of the reference's main() (src/SPB6_PC_IMEX_omp.cpp:1305-1427) on one
+    case: probe line at t = 0, steps to t_end with snapshots and probe lines, final profile;
+    returns its end-of-run line (wall time of the time loop)."""
+    import time
+
+    s = Solver(case, device=device)
+    try:
+        s.set_output(out_file, snaps=snaps, probe=probe, prec=prec)
+        t0 = time.perf_counter()
+        s.advance(0)
+        return s.stats_line(int(case.get("case", 0)), time.perf_counter() - t0)
+    finally:
+        s.close()
 
 
 class Solver:
@@ -245,7 +283,38 @@ class Solver:
     def stats(self) -> dict:
         s = Stats()
         self._check(self.lib.spb6g_get_stats(self.h, ctypes.byref(s)), "spb6g_get_stats")
-        return {k: getattr(s, k) for k, _ in Stats._fields_ if k != "reserved"}
+        out = {}
+        for k, _ in Stats._fields_:
+            v = getattr(s, k)
+            out[k] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+    # ---- output of the reference's main() (profile, snapshots, probe, stats line)
+    def set_output(self, out_file: str | None, snaps=(), probe=None, prec: int = 16):
+        """Files main() writes: the final profile `out_file` (at t_end or when a step fails),
+        `<out>_s<k>.dat` at the snapshot times (the step size lands on them) and, with
+        probe=(x, y), `<out>.probe` with one line before the first step and one per step."""
+        if not out_file:
+            self._check(self.lib.spb6g_set_output(self.h, None), "set_output")
+            return
+        self._snaps = np.ascontiguousarray(snaps, dtype=np.float64)
+        o = Output(out_file.encode(), self._snaps.ctypes.data if len(self._snaps) else None, len(self._snaps),
+                   1 if probe is not None else 0, float(probe[0]) if probe is not None else 0.0,
+                   float(probe[1]) if probe is not None else 0.0, int(prec))
+        self._check(self.lib.spb6g_set_output(self.h, ctypes.byref(o)), "set_output")
+
+    def write_profile(self, path: str, prec: int = 16):
+        self._check(self.lib.spb6g_write_profile(self.h, path.encode(), int(prec)), "write_profile")
+
+    def conserved_totals(self):
+        M = np.empty(3)
+        self._check(self.lib.spb6g_conserved_totals(self.h, _ptr(M)), "conserved_totals")
+        return M
+
+    def stats_line(self, case_id: int, wall_s: float = 0.0) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        self._check(self.lib.spb6g_stats_line(self.h, int(case_id), float(wall_s), buf, len(buf)), "stats_line")
+        return buf.value.decode()
 
     def region_begin(self):
         self._check(self.lib.spb6g_region_begin(self.h), "region_begin")

@@ -79,6 +79,7 @@ typedef struct {
     int64_t steps, rejects, rk1, stages, newton_it, floor_count, bicg_it;
     int64_t learned;                /* stages whose Newton started from the learned guess */
     double t, dt, maxres, p_ref;
+    double tmax[2];                 /* max phase temperatures of the stages' final states (st_Tmax :96, :1070) */
 } spb6g_stats;
 
 typedef struct spb6g_solver spb6g_solver;
@@ -125,6 +126,39 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
 int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double* qph);
 
 int spb6g_get_stats(spb6g_solver* s, spb6g_stats* st);
+
+/* ---------------------------------------------------------------------------
+ * Output of the reference's main(): the 17-column profile (write_profile,
+ * :1083-1094: "# x y p u v rho alpha2 Y2 rho1 rho2 c_frozen c_wood T1 T2 p1 p2
+ * g1-g2", one line per interior cell, j outer, i inner), snapshots (snap=:
+ * the step size is cut to land on each time, physics :972, and the profile is
+ * written to <out>_s<k>.dat when t reaches it, :1380), the pressure probe
+ * (probe=x,y: "t p Y2 alpha2 T1" of the nearest cell before the first step
+ * and after every accepted step to <out>.probe, :1191-1197) and the final
+ * profile at t_end or when a step fails (:1326, :1379, :1388).  Cell
+ * diagnostics are evaluated on the host in FP64 with the reference's
+ * formulas, so a state equal to the reference's prints the same text. */
+typedef struct {
+    const char* out_file;           /* NULL or "": no files */
+    const double* snaps;            /* snapshot times, ascending (snap=) */
+    int32_t nsnap;
+    int32_t probe;                  /* 1: write the probe file (probe=) */
+    double probe_x, probe_y;
+    int32_t prec;                   /* significant digits of the profile columns (prec=, 0: 16) */
+} spb6g_output;
+/* Copies *o; with a probe, writes the probe file's first line at the current state. */
+int spb6g_set_output(spb6g_solver* s, const spb6g_output* o);
+/* The profile of the current state to `path` (prec 0: 16 digits). */
+int spb6g_write_profile(spb6g_solver* s, const char* path, int prec);
+/* The same profile of a host state (AoS layout) for the grid and phases of *cfg; host code only,
+ * needs no device. */
+int spb6g_format_profile(const spb6g_config* cfg, const double* U, const char* path, int prec);
+/* Sums of m1, m2 and E over the interior cells (conserved_totals, :1185-1188). */
+int spb6g_conserved_totals(spb6g_solver* s, double* M3);
+/* The reference's end-of-run line (:1425-1427) for this run: "case <id> mode 1 order 2 rk ...
+ * | dM1/M .. dM2/M .. dE/E .. | wall <wall_s> s" (no newline); conservation against the totals
+ * at spb6g_init_pressure. */
+int spb6g_stats_line(spb6g_solver* s, int case_id, double wall_s, char* buf, size_t len);
 /* Simulation time t (settable, e.g. when restarting from a dump). */
 int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup);
 

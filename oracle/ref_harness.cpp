@@ -260,15 +260,20 @@ int write_result(const char* path, const spb6_result& r, const std::vector<const
 }  // namespace
 
 int main(int argc, char** argv) {
-    if (argc >= 3 && std::string(argv[1]) == "--main") {
+    const bool main_files = argc >= 3 && std::string(argv[1]) == "--main-files";
+    if (argc >= 3 && (std::string(argv[1]) == "--main" || main_files)) {
         // The reference main() itself; the final state is captured through cell_diag.
+        // "--main-files" keeps main()'s own out= (profile, snapshots, probe files are
+        // written); the capture then keeps the cells of the last profile only.
         std::vector<char*> av;
         av.push_back(argv[0]);
         for (int a = 3; a < argc; a++) av.push_back(argv[a]);
         static char outarg[] = "out=/dev/null";
-        av.push_back(outarg);
+        if (!main_files) av.push_back(outarg);
         g_capture.clear();
         const int rc = ref_main((int)av.size(), av.data());
+        const size_t keep = (size_t)nxCells * nyCells * NUM_VARS;
+        if (main_files && g_capture.size() > keep) g_capture.erase(g_capture.begin(), g_capture.end() - keep);
         spb6_result r{};
         r.magic = SPB6_CASE_MAGIC; r.status = rc; r.nx = nxCells; r.ny = nyCells;
         r.steps = st_steps; r.rejects = st_reject; r.rk1 = st_rk1; r.stages = st_stage;

@@ -113,6 +113,27 @@ def run_ref_main(args: list[str], nx: int, ny: int = 1, timeout: float = 3600) -
             return parse_result(f.read(), nx, ny, MODE_STEPS)
 
 
+def run_ref_main_files(args: list[str], out_name: str = "run.dat", timeout: float = 3600, nx: int = 0,
+                       ny: int = 1) -> dict:
+    """Run the reference's own main() with out=<tmp>/<out_name> and the given key=value
+    arguments; returns {"files": {name: bytes} of every file it wrote, "stdout": text} and,
+    with nx given, "U": the state of the last profile it wrote."""
+    with tempfile.TemporaryDirectory() as d:
+        co = os.path.join(d, "result.bin")
+        r = subprocess.run([REF_BIN, "--main-files", co, f"out={os.path.join(d, out_name)}", *args], check=True,
+                           timeout=timeout, stdout=subprocess.PIPE, text=True)
+        files = {}
+        for name in sorted(os.listdir(d)):
+            if name != "result.bin":
+                with open(os.path.join(d, name), "rb") as f:
+                    files[name] = f.read()
+        out = {"files": files, "stdout": r.stdout}
+        if nx:
+            with open(co, "rb") as f:
+                out["U"] = parse_result(f.read(), nx, ny, MODE_STEPS)["U"]
+        return out
+
+
 _port = {}
 VARIANTS = {None: "libspb6_oracle.so", "ulp": "libspb6_oracle_ulp.so", "fd": "libspb6_oracle_fd.so"}
 

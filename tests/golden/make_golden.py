@@ -11,6 +11,10 @@ where the reference tree does not exist.
 Fixtures:
   ref_<name>.npz      U0 (initial state), U, P, p_ref and run counters of the
                       compiled reference on the case built by CASES[name]
+  ref_main_outputs.npz
+                      the files the reference's own main() writes (profile, snapshot
+                      profiles, probe) and its end-of-run line, for the runs in
+                      MAIN_RUNS, with the captured final state of each run
   archived_case5_N100.npz, archived_case87_N200.npz
                       columns x, p, u, rho, alpha2 of the reference's archived
                       profiles data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat
@@ -75,6 +79,31 @@ CASES = {
 }
 
 
+# reference main() runs with output: tag -> (case, N, key=value arguments besides case, N, out)
+MAIN_RUNS = {
+    "case5_N100": (5, 100, ["snap=8e-5,1.6e-4", "probe=0.6,0.5"]),
+    "case87_N200": (87, 200, ["snap=1e-4", "probe=0.5,0.5"]),
+}
+
+
+def main_outputs():
+    """Files and stdout of the reference main() for MAIN_RUNS, one compressed archive."""
+    import refio
+
+    out = {}
+    for tag, (case, n, args) in MAIN_RUNS.items():
+        r = refio.run_ref_main_files([f"case={case}", f"N={n}", *args], out_name="run.dat", nx=n)
+        res = refio.run_ref_main_files([f"case={case}", f"N={n}", *args], out_name="run.dat")
+        assert r["files"] == res["files"], "the reference main() is not deterministic"
+        for name, data in r["files"].items():
+            out[f"{tag}/{name}"] = np.frombuffer(data, dtype=np.uint8)
+        out[f"{tag}/stdout"] = np.frombuffer(r["stdout"].encode(), dtype=np.uint8)
+        out[f"{tag}/args"] = np.frombuffer(json.dumps([case, n, args]).encode(), dtype=np.uint8)
+        out[f"{tag}/U"] = r["U"]
+        print(tag, {k: len(v) for k, v in r["files"].items()}, r["stdout"].strip()[:80])
+    np.savez_compressed(os.path.join(HERE, "ref_main_outputs.npz"), **out)
+
+
 def build_case(name):
     fn, mode, nsteps, over = CASES[name]
     c = fn()
@@ -99,6 +128,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), U0=c["U"], U=r["U"], P=r["P"],
                             meta=json.dumps(meta), **extra)
         print(name, meta)
+    main_outputs()
     for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
                       ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):
         d = np.loadtxt(os.path.join(REF_TREE, path))
