@@ -61,6 +61,16 @@ def _nasg(n):
     return next(c for c in b if c["nasg"])
 
 
+def _bc(c, bc, bcu=(0.0, 0.0, 0.0, 0.0), bcp=(0.0, 0.0, 0.0, 0.0)):
+    """Boundary variant of a case: kinds left, right, bottom, top (cases.BC_*), wall velocities
+    (piston) and outlet pressures."""
+    c = dict(c)
+    c.update(bc=list(bc), bcu=list(bcu), bcp=list(bcp))
+    return c
+
+
+T, W, PER, PRES = cases.BC_TRANS, cases.BC_WALL, cases.BC_PERIODIC, cases.BC_PRES
+
 # name -> (builder, mode, nsteps, overrides)
 CASES = {
     "case87_N200_tend": (lambda: cases.reference_case(87, 200), "tend", 0, {}),
@@ -76,6 +86,16 @@ CASES = {
     "shock64x32_stage": (lambda: _shock(64, 32), "stage", 0, {"dtfix": 5e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "shock64x32_3steps": (lambda: _shock(64, 32), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "nasg256_20steps": (lambda: _nasg(256), "steps", 20, {}),
+    # boundary variants (bc_apply physics :982-1013, M_P :709-718, residual_at :728-729)
+    "tube_walls_N200_20steps": (lambda: _bc(_tube(200), (W, W, T, T)), "steps", 20, {}),
+    "tube_piston_N200_20steps": (lambda: _bc(_tube(200), (W, W, T, T), bcu=(50.0, -20.0, 0, 0)), "steps", 20, {}),
+    "tube_outlet_N200_20steps": (lambda: _bc(_tube(200), (T, PRES, T, T), bcp=(0, 2e5, 0, 0)), "steps", 20, {}),
+    "tube_periodic_N200_10steps": (lambda: _bc(_tube(200), (PER, PER, T, T)), "steps", 10,
+                                   {"bicg_tol": 1e-13}),
+    "bubble_walls32_3steps": (lambda: _bc(_bubble(32), (W, W, W, W), bcu=(0, 0, 5.0, 0)), "steps", 3,
+                              {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "bubble_outlet32_3steps": (lambda: _bc(_bubble(32), (PRES, PRES, W, W), bcp=(1.2e7, 0.8e7, 0, 0)), "steps", 3,
+                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
 }
 
 
@@ -117,7 +137,8 @@ def main():
     if not refio.ref_available():
         raise SystemExit("oracle/_ref/spb6_ref is missing: run `make -C oracle ref` first")
     modes = {"tend": refio.MODE_TEND, "steps": refio.MODE_STEPS, "stage": refio.MODE_STAGE}
-    for name in CASES:
+    only = sys.argv[1:]
+    for name in (only or CASES):
         c, mode, nsteps = build_case(name)
         r = refio.run_ref(c, mode=modes[mode], nsteps=nsteps)
         meta = {k: r[k] for k in ("status", "steps", "rejects", "rk1", "stages", "newton_it", "floor_count", "t", "dt",
@@ -128,6 +149,8 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), U0=c["U"], U=r["U"], P=r["P"],
                             meta=json.dumps(meta), **extra)
         print(name, meta)
+    if only:
+        return
     main_outputs()
     for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
                       ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):

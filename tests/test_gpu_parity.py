@@ -109,6 +109,8 @@ def test_1d_tube_one_step_bitwise():
 
 
 @pytest.mark.parametrize("name", ["case87_N200_tend", "case5_N100_tend", "tube_N1000_tend", "nasg256_20steps",
+                                  "tube_walls_N200_20steps", "tube_piston_N200_20steps", "tube_outlet_N200_20steps",
+                                  "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps",
                                   "case83_N200_10steps"])
 def test_runs_match_reference_in_l1(name):
     """Whole runs in L1: within 1e-6 of the field maximum, or within 10x the reference's own L1

@@ -14,7 +14,10 @@ from helpers import golden_case, load_golden, mixture_pressure
 from diffusionimex_b200 import cases
 
 FIXTURES = ["case87_N200_tend", "case5_N100_tend", "case83_N200_10steps", "tube_N1000_1step", "tube_N200_stage",
-            "bubble48_stage", "bubble48_4steps", "lowmach32_3steps", "shock64x32_3steps", "nasg256_20steps"]
+            "bubble48_stage", "bubble48_4steps", "lowmach32_3steps", "shock64x32_3steps", "nasg256_20steps",
+            # boundary variants: walls, pistons, pressure outlets, 1D periodic (cyclic matrix on BiCGStab)
+            "tube_walls_N200_20steps", "tube_piston_N200_20steps", "tube_outlet_N200_20steps",
+            "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps"]
 MODES = {"tend": refio.MODE_TEND, "steps": refio.MODE_STEPS, "stage": refio.MODE_STAGE}
 
 
