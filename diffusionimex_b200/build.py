@@ -3,7 +3,11 @@
     python -m diffusionimex_b200.build [--force]
 
 nvcc compiles every csrc/*.cu into one shared library with a plain C ABI
-(include/spb6g.h).  FP64 multiply-add contraction is disabled (-fmad=false)
+(include/spb6g.h).  The kernel sources that evaluate the equations of state
+(MG_VARIANT_SOURCES) are compiled twice: as they are (stiffened gas / NASG
+phases) and with SPB6G_MG = 1 into namespace spb6g_mg (Mie-Grueneisen phases);
+the first build's launchers forward to the second for a configuration with a
+Mie-Grueneisen phase.  FP64 multiply-add contraction is disabled (-fmad=false)
 so the device arithmetic rounds exactly like the reference CPU build (gcc -O2
 on x86-64 emits no FMA); FP64 division and sqrt are IEEE on the device.
 """
@@ -28,6 +32,9 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
     "-Xptxas", "-warn-spills",
 ]
+
+
+MG_VARIANT_SOURCES = ("spb6g_kernels.cu", "spb6g_flux.cu")
 
 
 def _nvcc() -> str:
@@ -56,9 +63,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
-    for src in sources():
-        obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-dc", "-c", src, "-o", obj]
+    jobs = [(src, os.path.join(objdir, os.path.basename(src) + ".o"), []) for src in sources()]
+    jobs += [(src, os.path.join(objdir, os.path.basename(src) + ".mg.o"), ["-DSPB6G_MG=1", "-Dspb6g=spb6g_mg"])
+             for src in sources() if os.path.basename(src) in MG_VARIANT_SOURCES]
+    for src, obj, defs in jobs:
+        cmd = [_nvcc(), *NVCC_FLAGS, *defs, "-I", INCLUDE, "-dc", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -29,6 +29,13 @@ BC_TRANS, BC_WALL, BC_PERIODIC, BC_PRES = 0, 1, 2, 3
 
 WATER_SG = dict(g=4.4, pinf=6e8, q=0.0, qp=0.0, cv=1000.0, b=0.0)
 AIR_SG = dict(g=1.4, pinf=0.0, q=0.0, qp=0.0, cv=1000.0, b=0.0)
+# Mie-Grueneisen phases of the reference's cases 60, 61, 73 (src/spb6_physics_omp.h:1047-1070):
+# kind 1 Cochran-Chan, kind 2 JWL; fields besides G, rr, c1, c2, e1, e2, e0 as Phase{} leaves them
+NITROMETHANE_CC = dict(g=2.19, pinf=0.0, q=0.0, qp=0.0, cv=0.0, b=0.0, kind=1, G=1.19, rr=1134.0, c1=0.819181e9,
+                       c2=1.50835e9, e1=4.52969, e2=1.42144, e0=0.0)
+DETONATION_JWL = dict(g=1.25, pinf=0.0, q=0.0, qp=0.0, cv=0.0, b=0.0, kind=2, G=0.25, rr=1840.0, c1=854.5e9, c2=20.5e9,
+                      e1=4.6, e2=1.35, e0=0.0)
+WATER_NASG = dict(g=1.187, pinf=7028e5, q=-1177788.0, qp=0.0, cv=3610.0, b=6.61e-4)
 
 
 def default_settings() -> dict:
@@ -43,8 +50,28 @@ def default_settings() -> dict:
     )
 
 
+def mg_ref(ph: dict, r: float):
+    """Mie-Grueneisen reference curves pr, pr', er at density r (src/spb6_physics_omp.h:60-69),
+    with the C library's pow / exp as the reference calls them."""
+    if ph["kind"] == 1:
+        x = r / ph["rr"]
+        t1, t2 = ph["c1"] * math.pow(x, ph["e1"]), ph["c2"] * math.pow(x, ph["e2"])
+        return t1 - t2, (ph["e1"] * t1 - ph["e2"] * t2) / r, (t1 / (ph["e1"] - 1.0) - t2 / (ph["e2"] - 1.0)) / r
+    t1, t2 = ph["c1"] * math.exp(-ph["e1"] * ph["rr"] / r), ph["c2"] * math.exp(-ph["e2"] * ph["rr"] / r)
+    return (t1 + t2, (ph["e1"] * t1 + ph["e2"] * t2) * ph["rr"] / (r * r),
+            t1 / (ph["e1"] * ph["rr"]) + t2 / (ph["e2"] * ph["rr"]) - ph["e0"])
+
+
 def eps_amp(ph: dict, a, m, p):
-    """Phase internal energy per unit volume (SG/NASG), src/spb6_physics_omp.h:71-73."""
+    """Phase internal energy per unit volume, src/spb6_physics_omp.h:71-73: SG/NASG, or
+    Mie-Grueneisen m er(m/a) + a (p - pr(m/a)) / G (cell by cell, scalar libm)."""
+    if ph.get("kind", 0):
+        a, m, p = np.broadcast_arrays(np.asarray(a, np.float64), np.asarray(m, np.float64), np.asarray(p, np.float64))
+        out = np.empty(a.shape)
+        for i in np.ndindex(a.shape):
+            pr, _, er = mg_ref(ph, float(m[i]) / float(a[i]))
+            out[i] = float(m[i]) * er + float(a[i]) * (float(p[i]) - pr) / ph["G"]
+        return out
     return (p + ph["g"] * ph["pinf"]) * (a - m * ph["b"]) / (ph["g"] - 1.0) + m * ph["q"]
 
 
@@ -80,8 +107,9 @@ def cell_centres(cfg: dict):
 # Reference cases (test_setup / test_state, src/spb6_physics_omp.h:1017-1157)
 # --------------------------------------------------------------------------------------------
 def reference_case(case: int, nx: int | None = None) -> dict:
-    """A subset of the reference's 1D SG cases: 4 (interface advection), 5 (SPB 4.3.1
-    water-air), 80-88 (Schropff 2026 Riemann problems)."""
+    """A subset of the reference's 1D cases: 4 (interface advection), 5 (SPB 4.3.1 water-air),
+    80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes 60 (SPB 4.2
+    nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG water)."""
     c = default_settings()
     air, water = dict(AIR_SG), dict(WATER_SG)
     if case == 4:
@@ -97,6 +125,10 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         c.update(phases=[water, air], nx=1000, tend=0.25 if case == 86 else 241e-6)
     elif case == 88:
         c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=1000, tend=30e-6)
+    elif case == 60:  # SPB 4.2 nitromethane shock tube, Cochran-Chan for both phases
+        c.update(phases=[dict(NITROMETHANE_CC), dict(NITROMETHANE_CC)], nx=500, tend=67e-6)
+    elif case == 61:  # Pelanti 8.1.1 detonation gas (JWL) - water (NASG) shock tube on [-10, 10] m
+        c.update(phases=[dict(DETONATION_JWL), dict(WATER_NASG)], nx=500, tend=0.9e-3, x0=-10.0, x1=10.0)
     else:
         raise ValueError(f"reference case {case} is not restated here")
     if nx is not None:
@@ -130,9 +162,17 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         L = x < (0.25 if adv else 0.7)
         p = np.full_like(x, 1e5) if adv else np.where(L, 1e9, 1e5)
         U = prim2cell(ph, np.where(L, 1 - 1e-7, 1e-7), 1000.0, 0.01 if adv else 50.0, 1.0 if adv else 0.0, 0.0, p, p)
-    else:  # 88
+    elif case == 88:
         p = np.where(x < 0.6, 1e10, 1e5)
         U = prim2cell(ph, np.full_like(x, 0.5954), 1185.0, 3622.0, 0.0, 0.0, p, p)
+    elif case == 60:
+        L = x < 0.5
+        p = np.where(L, 20e9, 0.2e6)
+        U = prim2cell(ph, np.where(L, 1 - 1e-8, 1e-8), 1134.0, 1200.0, 0.0, 0.0, p, p)
+    else:  # 61
+        L = x < 0.0
+        p = np.where(L, 4.6406e10, 1e5)
+        U = prim2cell(ph, np.where(L, 1 - 1e-8, 1e-8), 2000.0, 1044.0, 0.0, 0.0, p, p)
     c["U"] = U.reshape(1, c["nx"], NUM_VARS)
     return c
 
@@ -290,3 +330,20 @@ def riemann_batch(count: int = 512, seed: int = 0, nmin: int = 256, nmax: int = 
         c.update(steps=steps, instance=k, nasg=nasg)
         out.append(c)
     return out
+
+
+def underwater_explosion(nx: int = 361, ny: int = 200) -> dict:
+    """The reference's case 73 geometry (Pelanti 8.1.2, src/spb6_physics_omp.h:1067-1069, :1112-1113):
+    a JWL detonation-gas bubble (radius 0.05 m, centre (0, -0.32) m, 4.6406e10 Pa) in NASG water at
+    1e5 Pa on [-1.35, 1.35] x [-1.5, 0] m, a wall at y = 0, transmissive elsewhere; cell-centre
+    values (the reference averages 4 x 4 sub-points per cell)."""
+    c = default_settings()
+    c.update(nx=nx, ny=ny, x0=-1.35, x1=1.35, y0=-1.5, y1=0.0, tend=0.4e-3,
+             phases=[dict(DETONATION_JWL), dict(WATER_NASG)], bc=[BC_TRANS, BC_TRANS, BC_TRANS, BC_WALL], case=73)
+    x, y, _, _ = cell_centres(c)
+    X, Y = np.meshgrid(x, y)
+    inside = X * X + (Y + 0.32) * (Y + 0.32) < 0.05 * 0.05
+    p = np.where(inside, 4.6406e10, 1e5)
+    c["U"] = prim2cell(c["phases"], np.where(inside, 1 - 1e-6, 1e-6), 2000.0, 1044.0, 0.0, 0.0, p, p)
+    c["workload"] = f"underwater explosion (JWL gas bubble in NASG water) 2D, {nx}x{ny} cells"
+    return c

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "../../include/spb6g.h"
 #include "spb6g_common.cuh"
 
 namespace spb6g {
@@ -35,6 +36,23 @@ struct NewtonScalars {
     int nstrong;         // strong-shock worklist length
     int pad;
 };
+
+// Phases and scheme switches of a configuration (host side).
+inline void phys_from_config(const spb6g_config* cfg, Phys& P) {
+    P = Phys{};
+    for (int k = 0; k < 2; k++) {
+        PhaseD& h = P.ph[k];
+        h.g = cfg->gamma[k]; h.pi = cfg->pinf[k]; h.q = cfg->q[k];
+        h.qp = cfg->qp[k]; h.cv = cfg->cv[k]; h.b = cfg->b[k];
+        h.kind = cfg->kind[k];
+        h.G = cfg->mg_G[k]; h.rr = cfg->mg_rr[k]; h.c1 = cfg->mg_c1[k]; h.c2 = cfg->mg_c2[k];
+        h.e1 = cfg->mg_e1[k]; h.e2 = cfg->mg_e2[k]; h.e0 = cfg->mg_e0[k];
+    }
+    P.share_mode = cfg->share_mode;
+    P.limiter = cfg->limiter;
+    P.rus_local = cfg->rus_local;
+    P.mg = cfg->kind[0] != 0 || cfg->kind[1] != 0;
+}
 
 struct Ctx {
     Phys phy;

@@ -15,6 +15,7 @@
 // cell one layer around the tile, every face flux of the tile once, and the
 // update of the tile's cells.
 #include "spb6g_ctx.cuh"
+#include "spb6g_mgfwd.cuh"
 
 namespace spb6g {
 
@@ -62,7 +63,7 @@ SPB6G_DEV bool frozen_cf(const Phys& P, const double* Q, double& cf) {
     if (!(a1 > 0 && a2 > 0 && m1 > 0 && m2 > 0)) return false;
     const double rho = m1 + m2, r1 = m1 / a1, r2 = m2 / a2;
     const double p1 = p_ame(P, 0, a1, m1, Q[IE1]), p2 = p_ame(P, 1, a2, m2, Q[IE2]);
-    if (!(p_admissible(P, 0, p1) && p_admissible(P, 1, p2))) return false;
+    if (!(p_admissible(P, 0, a1, m1, p1) && p_admissible(P, 1, a2, m2, p2))) return false;
     cf = sqrt((m1 * c2_rp(P, 0, r1, p1) + m2 * c2_rp(P, 1, r2, p2)) / rho);
     return true;
 }
@@ -108,6 +109,7 @@ SPB6G_DEV void recon3(const Phys& P, const R* Ua, const R* Uc, const R* Ub, R vs
     if (P.limiter && phi > R(0.0)) {
 #pragma unroll
         for (int ph = 0; ph < 2; ph++) {
+            if (SPB6G_MG && P.ph[ph].kind) continue;  // the face-admissibility bound is for NASG / SG phases (:419)
             R L1[3], L2[3];
             if constexpr (sizeof(R) == sizeof(double)) {
                 const R* cs[3] = {Ua, Uc, Ub};
@@ -420,6 +422,7 @@ size_t flux_tile_bytes_1d(int tx) {
 }
 
 void launch_flux(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_flux, mg_view(c), st);
     if (c.prec) {  // precision form: reconstruction and fluxes in FP32
         if (c.g.ny > 1) launch_tile<float, 32, 8, true>(c, st);
         else launch_tile<float, 256, 1, false>(c, st);

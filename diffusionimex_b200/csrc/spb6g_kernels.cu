@@ -7,6 +7,7 @@
 
 #include "../../include/spb6g.h"
 #include "spb6g_ctx.cuh"
+#include "spb6g_mgfwd.cuh"
 
 namespace spb6g {
 
@@ -39,7 +40,7 @@ SPB6G_DEV double cfz(const Phys& P, const double* X, double a2) {
     const double a1 = X[IA1], m1 = X[IM1], m2 = X[IM2];
     if (!(a1 > 0 && a2 > 0 && m1 > 0 && m2 > 0)) return INFINITY;
     const double p1 = p_ame(P, 0, a1, m1, X[IE1]), p2 = p_ame(P, 1, a2, m2, X[IE2]);
-    if (!(p_admissible(P, 0, p1) && p_admissible(P, 1, p2))) return INFINITY;
+    if (!(p_admissible(P, 0, a1, m1, p1) && p_admissible(P, 1, a2, m2, p2))) return INFINITY;
     const double c21 = c2_rp(P, 0, m1 / a1, p1), c22 = c2_rp(P, 1, m2 / a2, p2);
     const double c2 = (m1 * c21 + m2 * c22) / (m1 + m2);
     return c2 > 0 ? sqrt(c2) : INFINITY;
@@ -87,15 +88,15 @@ SPB6G_DEV void prep_cell_at(const Ctx& c, long t) {
         double K = SMAX(c.phy.ph[0].pi, c.phy.ph[1].pi), PE = 0.0;
         if (a1 > 0 && a2 > 0 && m1 > 0 && m2 > 0) {
             const double p1 = p_ame(c.phy, 0, a1, m1, X[IE1]), p2 = p_ame(c.phy, 1, a2, m2, X[IE2]);
-            if (p_admissible(c.phy, 0, p1) && p_admissible(c.phy, 1, p2))
+            if (p_admissible(c.phy, 0, a1, m1, p1) && p_admissible(c.phy, 1, a2, m2, p2))
                 K = 1.0 / ((a1 / sa) / (m1 / a1 * c2_rp(c.phy, 0, m1 / a1, p1)) + (a2 / sa) / (m2 / a2 * c2_rp(c.phy, 1, m2 / a2, p2)));
             const double dd = dedp_am(c.phy, 0, a1, m1) + dedp_am(c.phy, 1, a2, m2);
-            if (dd > 0) PE = (fabs(X[IE1]) + eps_round(c.phy, 0, m1) + fabs(X[IE2]) + eps_round(c.phy, 1, m2)) / dd;
+            if (dd > 0) PE = (fabs(X[IE1]) + eps_round(c.phy, 0, a1, m1) + fabs(X[IE2]) + eps_round(c.phy, 1, a2, m2)) / dd;
         }
         c.kw[x] = K + PE;
     }
 }
-__global__ void k_prep_cell(Ctx c) {
+__global__ void __launch_bounds__(TPB, 3) k_prep_cell(Ctx c) {
     const long tot = prep_cells(c.g);
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) prep_cell_at(c, t);
 }
@@ -179,6 +180,7 @@ __global__ void k_prep_fy(Ctx c) {
     }
 }
 void launch_prep(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_prep, mg_view(c), st);
     const long pad = (long)(c.g.nx + 4) * (c.g.ny > 1 ? c.g.ny + 4 : 1);
     k_prep_cell<<<blocks_for(pad), TPB, 0, st>>>(c);
     k_prep_fx<<<blocks_for((long)(c.g.nx + 1) * c.g.ny), TPB, 0, st>>>(c);
@@ -254,10 +256,12 @@ __global__ void k_shock_strong(Ctx c) {
 // Weak-shock cells are finished in place; strong-shock cells (Kapila profile
 // shooting, 6-9 RK45 integrations each) go through a compacted worklist.
 void launch_shock_weak(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_shock_weak, mg_view(c), st);
     k_shock_weak<<<blocks_for(c.n), TPB, 0, st>>>(c);
     count(c, 1);
 }
 void launch_shock_strong(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_shock_strong, mg_view(c), st);
     k_shock_strong<<<(c.n + 31) / 32, 32, 0, st>>>(c);
     count(c, 1);
 }
@@ -442,6 +446,7 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_residual(Ctx c, int mode, do
     if (grid_fold<RedMax, 1>(m, c.partials, &c.counters[0], tot) && threadIdx.x == 0) c.ns->res = tot[0];
 }
 void launch_residual(const Ctx& c, cudaStream_t st, int mode, double lam, int skip_strong) {
+    SPB6G_MG_FORWARD(launch_residual, mg_view(c), st, mode, lam, skip_strong);
     k_residual<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, mode, lam, skip_strong);
     count(c, 1);
 }
@@ -466,6 +471,7 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_residual_strong(Ctx c) {
     if (grid_fold<RedMax, 1>(m, c.partials, &c.counters[10], tot) && threadIdx.x == 0) c.ns->res = SMAX(c.ns->res, tot[0]);
 }
 void launch_residual_strong(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_residual_strong, mg_view(c), st);
     k_residual_strong<<<148 * 2, RED_THREADS, 0, st>>>(c);
     count(c, 1);
 }
@@ -541,11 +547,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_jac_finish(Ctx c) {
     }
 }
 void launch_jac_entries(const Ctx& c, cudaStream_t st, int skip_strong) {
+    SPB6G_MG_FORWARD(launch_jac_entries, mg_view(c), st, skip_strong);
     const int nw = c.g.ny > 1 ? 5 : 3;
     k_jac_entries<<<nw * ((c.n + RED_THREADS - 1) / RED_THREADS), RED_THREADS, 0, st>>>(c, skip_strong);
     count(c, 1);
 }
 void launch_jac_strong(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_jac_strong, mg_view(c), st);
     k_jac_strong<<<148 * 4, RED_THREADS, 0, st>>>(c);
     count(c, 1);
 }
@@ -554,6 +562,7 @@ void launch_jac_finish(const Ctx& c, cudaStream_t st) {
     count(c, 1);
 }
 void launch_jacobian(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_jacobian, mg_view(c), st);
     launch_jac_entries(c, st, 0);
     launch_jac_finish(c, st);
 }
@@ -1310,6 +1319,7 @@ __global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X)
     }
 }
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X) {
+    SPB6G_MG_FORWARD(launch_features, mg_view(c), st, mg_view(nm), X);
     k_features<<<blocks_for(c.n), TPB, 0, st>>>(c, nm, (__nv_bfloat16*)X);
     count(c, 1);
 }
@@ -1403,6 +1413,7 @@ __global__ void k_floor(Ctx c, double tol) {
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) floor_at(c, x, tol);
 }
 void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
+    SPB6G_MG_FORWARD(launch_floor, mg_view(c), st, tol);
     k_floor<<<blocks_for(c.n), TPB, 0, st>>>(c, tol);
     count(c, 1);
 }
@@ -1435,7 +1446,7 @@ SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
         }
     }
 }
-__global__ void __launch_bounds__(RED_THREADS) k_final(Ctx c) {
+__global__ void __launch_bounds__(RED_THREADS, 2) k_final(Ctx c) {
     double m[2] = {0.0, 0.0};
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) final_at(c, x, m);
     double tot[2];
@@ -1445,12 +1456,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_final(Ctx c) {
     }
 }
 void launch_final(const Ctx& c, cudaStream_t st) {
+    SPB6G_MG_FORWARD(launch_final, mg_view(c), st);
     k_final<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c);
     count(c, 1);
 }
 
 // ============================================================ caldt (:502-514) and P_REF (:1309-1312)
-__global__ void __launch_bounds__(RED_THREADS) k_caldt(Ctx c, CState U, int acoustic) {
+__global__ void __launch_bounds__(RED_THREADS, 3) k_caldt(Ctx c, CState U, int acoustic) {
     double m[2] = {0.0, 0.0};
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         double q[NV];
@@ -1469,6 +1481,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_caldt(Ctx c, CState U, int acou
     }
 }
 void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic) {
+    SPB6G_MG_FORWARD(launch_caldt, mg_view(c), st, mg_view(U), acoustic);
     k_caldt<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U, acoustic);
     count(c, 1);
 }
@@ -1484,6 +1497,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_pbar_min(Ctx c, CState U) {
     if (grid_fold<RedMin, 1>(m, c.partials, &c.counters[9], tot) && threadIdx.x == 0) c.ns->pmin = tot[0];
 }
 void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U) {
+    SPB6G_MG_FORWARD(launch_pbar_min, mg_view(c), st, mg_view(U));
     k_pbar_min<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U);
     count(c, 1);
 }
@@ -1496,6 +1510,7 @@ __global__ void k_pbar_init(Ctx c, CState U, double p_ref, double* P) {
     }
 }
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P) {
+    SPB6G_MG_FORWARD(launch_pbar_init, mg_view(c), st, mg_view(U), p_ref, P);
     k_pbar_init<<<blocks_for(c.n), TPB, 0, st>>>(c, U, p_ref, P);
     count(c, 1);
 }

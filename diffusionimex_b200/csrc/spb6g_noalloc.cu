@@ -25,6 +25,7 @@
 
 #include "../../include/spb6g.h"
 #include "spb6g_common.cuh"
+#include "spb6g_ctx.cuh"
 
 using namespace spb6g;
 
@@ -75,6 +76,7 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_caldt_noalloc(Phys P, int n
 extern "C" int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
                                    double* inv_rate) {
     if (!cfg || !U_dev || !inv_rate || cfg->nx < 1 || cfg->ny < 1) return SPB6G_BAD_ARG;
+    if (cfg->kind[0] != 0 || cfg->kind[1] != 0) return SPB6G_UNSUPPORTED;  // stiffened gas / NASG phases only
     for (int k = 0; k < NV; k++)
         if (!U_dev[k]) return SPB6G_BAD_ARG;
     const long long n = (long long)cfg->nx * cfg->ny;
@@ -100,14 +102,8 @@ extern "C" int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const*
     }
     const NoallocSymbols& sy = g_syms[dev];
     cudaStream_t st = (cudaStream_t)stream;
-    Phys P{};
-    for (int k = 0; k < 2; k++) {
-        P.ph[k].g = cfg->gamma[k]; P.ph[k].pi = cfg->pinf[k]; P.ph[k].q = cfg->q[k];
-        P.ph[k].qp = cfg->qp[k]; P.ph[k].cv = cfg->cv[k]; P.ph[k].b = cfg->b[k];
-    }
-    P.share_mode = cfg->share_mode;
-    P.limiter = cfg->limiter;
-    P.rus_local = cfg->rus_local;
+    Phys P;
+    phys_from_config(cfg, P);
     CState U;
     for (int k = 0; k < NV; k++) U.v[k] = U_dev[k];
     double host[2];

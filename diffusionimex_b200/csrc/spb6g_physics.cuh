@@ -1,6 +1,7 @@
 // Per-cell physics of the SPB 6+1-equation model on the device: stiffened-gas /
-// NASG equations of state, the mechanical (p) relaxation closure, the shock
-// dissipation budget and the primitive-variable map.
+// NASG and Mie-Grueneisen (Cochran-Chan, JWL) equations of state, the
+// mechanical (p) relaxation closure, the shock dissipation budget and the
+// primitive-variable map.
 //
 // Each function follows the reference line for line in operation order
 // (src/spb6_physics_omp.h, cited per function); the library is compiled with
@@ -12,6 +13,12 @@
 #include <cstdint>
 
 #define SPB6G_DEV __device__ __forceinline__
+// SPB6G_MG = 1 compiles the Mie-Grueneisen branches in.  The library builds the kernels twice:
+// with SPB6G_MG = 0 they are exactly the stiffened-gas / NASG kernels, and a configuration with a
+// Mie-Grueneisen phase runs the second build (namespace spb6g_mg) instead.
+#ifndef SPB6G_MG
+#define SPB6G_MG 0
+#endif
 #define SMAX(a, b) ((a) < (b) ? (b) : (a))
 #define SMIN(a, b) ((b) < (a) ? (b) : (a))
 
@@ -20,8 +27,14 @@ namespace spb6g {
 enum { IA1 = 0, IM1, IM2, IMU, IMV, IE1, IE2, IEN, NV = 8 };
 enum { BC_TRANS = 0, BC_WALL = 1, BC_PERIODIC = 2, BC_PRES = 3 };
 
+// A phase: stiffened gas / NASG (kind 0: g, pi, q, qp, cv, b; b = 0 is stiffened gas), or
+// Mie-Grueneisen p = G rho (e - er(rho)) + pr(rho) with constant G and er' = pr / rho^2
+// (physics :51-56): Cochran-Chan (kind 1) or JWL (kind 2), reference curve parameters rr,
+// c1, c2, e1, e2, e0; cv > 0 gives the temperature (e - er) / cv (output only).
 struct PhaseD {
     double g, pi, q, qp, cv, b;
+    int kind, pad;
+    double G, rr, c1, c2, e1, e2, e0;
 };
 
 // Phases and scheme switches shared by every kernel (passed by value).
@@ -30,28 +43,80 @@ struct Phys {
     int share_mode;  // SHARE_MODE, src/spb6_physics_omp.h:436
     int limiter;     // LIMITER, :969
     int rus_local;   // RUS_LOCAL, src/SPB6_PC_IMEX_omp.cpp:93
-    int pad;
+    int mg;          // a Mie-Grueneisen phase is present (mg_any, :58)
 };
 
-// ------------------------------------------------------------ EOS, src/spb6_physics_omp.h:71-111
+// ------------------------------------------------------------ EOS, src/spb6_physics_omp.h:60-111
+// Mie-Grueneisen reference curves pr(rho), pr'(rho), er(rho) (mg_ref :60-69): Cochran-Chan
+// pr = c1 x^e1 - c2 x^e2 with x = rho / rr; JWL pr = c1 exp(-e1 rr / rho) + c2 exp(-e2 rr / rho).
+// The Mie-Grueneisen routines are kept out of line and take their arguments by value: the
+// SG / NASG kernels then carry only a call in a branch they never take, with no pow / exp in
+// their register allocation and no kernel parameter copied to local memory.
+struct MgRef {
+    double pr, dpr, er;
+};
+static __device__ __noinline__ MgRef mg_curve(int kind, double rr, double c1, double c2, double e1, double e2, double e0,
+                                              double r) {
+    MgRef o;
+    if (kind == 1) {
+        const double x = r / rr, t1 = c1 * pow(x, e1), t2 = c2 * pow(x, e2);
+        o.pr = t1 - t2;
+        o.dpr = (e1 * t1 - e2 * t2) / r;
+        o.er = (t1 / (e1 - 1.0) - t2 / (e2 - 1.0)) / r;
+    } else {
+        const double t1 = c1 * exp(-e1 * rr / r), t2 = c2 * exp(-e2 * rr / r);
+        o.pr = t1 + t2;
+        o.dpr = (e1 * t1 + e2 * t2) * rr / (r * r);
+        o.er = t1 / (e1 * rr) + t2 / (e2 * rr) - e0;
+    }
+    return o;
+}
+SPB6G_DEV void mg_ref(const PhaseD& h, double r, double& pr, double& dpr, double& er) {
+    const MgRef o = mg_curve(h.kind, h.rr, h.c1, h.c2, h.e1, h.e2, h.e0, r);
+    pr = o.pr;
+    dpr = o.dpr;
+    er = o.er;
+}
 SPB6G_DEV double eps_amp(const Phys& P, int k, double a, double m, double p) {
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) {
+        double pr, dpr, er;
+        mg_ref(h, m / a, pr, dpr, er);
+        return m * er + a * (p - pr) / h.G;
+    }
     return (p + h.g * h.pi) * (a - m * h.b) / (h.g - 1.0) + m * h.q;
 }
 SPB6G_DEV double p_ame(const Phys& P, int k, double a, double m, double e) {
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) {
+        double pr, dpr, er;
+        mg_ref(h, m / a, pr, dpr, er);
+        return h.G * (e - m * er) / a + pr;
+    }
     return (e - m * h.q) * (h.g - 1.0) / (a - m * h.b) - h.g * h.pi;
 }
 SPB6G_DEV double c2_rp(const Phys& P, int k, double r, double p) {
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) {
+        double pr, dpr, er;
+        mg_ref(h, r, pr, dpr, er);
+        return (h.G + 1.0) * (p - pr) / r + dpr;
+    }
     return h.g * (p + h.pi) / (r * (1.0 - r * h.b));
 }
 SPB6G_DEV double dedp_am(const Phys& P, int k, double a, double m) {
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) return a / h.G;
     return (a - m * h.b) / (h.g - 1.0);
 }
 SPB6G_DEV double T_amp(const Phys& P, int k, double a, double m, double p) {
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) {
+        if (!(h.cv > 0)) return NAN;
+        double pr, dpr, er;
+        mg_ref(h, m / a, pr, dpr, er);
+        return (a * (p - pr) / (h.G * m)) / h.cv;
+    }
     return (a / m - h.b) * (p + h.pi) / ((h.g - 1.0) * h.cv);
 }
 SPB6G_DEV double p_mix(const Phys& P, double a1, double m1, double m2, double rhoe) {
@@ -59,13 +124,31 @@ SPB6G_DEV double p_mix(const Phys& P, double a1, double m1, double m2, double rh
     double num = rhoe, den = 0.0;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-        num -= m[k] * P.ph[k].q + P.ph[k].g * P.ph[k].pi * dedp_am(P, k, a[k], m[k]);
+        if (SPB6G_MG && P.ph[k].kind) {  // (A2.7)
+            double pr, dpr, er;
+            mg_ref(P.ph[k], m[k] / a[k], pr, dpr, er);
+            num -= m[k] * er - a[k] * pr / P.ph[k].G;
+        } else {
+            num -= m[k] * P.ph[k].q + P.ph[k].g * P.ph[k].pi * dedp_am(P, k, a[k], m[k]);
+        }
         den += dedp_am(P, k, a[k], m[k]);
     }
     return num / den;
 }
-SPB6G_DEV bool p_admissible(const Phys& P, int k, double p) { return p + P.ph[k].pi > 0; }
-SPB6G_DEV double eps_round(const Phys& P, int k, double m) { return fabs(m * P.ph[k].q); }
+// Admissible phase state (:103-106): NASG p + pi > 0; Mie-Grueneisen c^2 > 0.
+SPB6G_DEV bool p_admissible(const Phys& P, int k, double a, double m, double p) {
+    if (SPB6G_MG && P.ph[k].kind) return isfinite(p) && c2_rp(P, k, m / a, p) > 0;
+    return p + P.ph[k].pi > 0;
+}
+// Round-off scale of eps_k besides |eps_k| (:108-111): NASG |m q|; MG |m er| + |alpha pr / G|.
+SPB6G_DEV double eps_round(const Phys& P, int k, double a, double m) {
+    if (SPB6G_MG && P.ph[k].kind) {
+        double pr, dpr, er;
+        mg_ref(P.ph[k], m / a, pr, dpr, er);
+        return fabs(m * er) + fabs(a * pr / P.ph[k].G);
+    }
+    return fabs(m * P.ph[k].q);
+}
 
 // ------------------------------------------------------------ closure, :229-243, :430-548, :842-866
 struct ClIn {
@@ -76,6 +159,12 @@ struct ClOut {
 };
 
 SPB6G_DEV double E_above(const Phys& P, const ClIn& in, int k) {  // :430-433
+    if (SPB6G_MG && P.ph[k].kind) {  // thermal energy above the cold curve, eps_k - m_k er
+        if (!(in.atr[k] > 0 && in.mtr[k] > 0)) return 0.0;
+        double pr, dpr, er;
+        mg_ref(P.ph[k], in.mtr[k] / in.atr[k], pr, dpr, er);
+        return SMAX(0.0, in.etr[k] - in.mtr[k] * er);
+    }
     const double v = in.etr[k] - in.mtr[k] * P.ph[k].q - (in.atr[k] - in.mtr[k] * P.ph[k].b) * P.ph[k].pi;
     return SMAX(0.0, v);
 }
@@ -130,6 +219,177 @@ SPB6G_DEV double PhiD(const Phys& P, const ClIn& in, const ClPre& pr, double p, 
     }
     return f - 1.0;
 }
+// alpha_k(p) of a Mie-Grueneisen phase (alpha_mg :552-584): the root of
+// f(a) = m er(m/a) + a (p - pr)/G + p a - A - B p on the branch where f' = rho c^2 / G > 0;
+// the bracket grows from the guess (moved up first if the guess lies where c^2 <= 0), then a
+// safeguarded Newton.  Kept out of line: the SG/NASG kernels do not carry its registers.
+static __device__ __noinline__ bool alpha_mg(const PhaseD& h, double m, double A, double B, double p, double guess, double& al,
+                                      double& dal) {
+    auto F = [&](double a, double& df) {
+        double pr, dpr, er;
+        const double r = m / a;
+        mg_ref(h, r, pr, dpr, er);
+        df = ((h.G + 1.0) * (p - pr) + r * dpr) / h.G;
+        return m * er + a * (p - pr) / h.G + p * a - A - B * p;
+    };
+    double lo = guess, hi = guess, d;
+    double flo = F(lo, d), fhi = flo;
+    if (!isfinite(flo)) return false;
+    if (!(d > 0)) {
+        for (int it = 0; it < 200 && !(d > 0); it++) {
+            guess *= 2.0;
+            flo = F(guess, d);
+            if (!isfinite(flo)) return false;
+        }
+        if (!(d > 0)) return false;
+        lo = hi = guess;
+        fhi = flo;
+    }
+    if (flo < 0) {
+        for (int it = 0; it < 200 && fhi < 0; it++) {
+            lo = hi; flo = fhi; hi *= 2.0;
+            fhi = F(hi, d);
+            if (!isfinite(fhi)) return false;
+        }
+        if (fhi < 0) return false;
+    } else {
+        for (int it = 0; it < 200 && flo > 0; it++) {
+            hi = lo; fhi = flo; lo *= 0.5;
+            flo = F(lo, d);
+            if (!isfinite(flo)) return false;
+            if (d <= 0) {  // past the c^2 = 0 point: bisect [lo, hi] for F <= 0 on the admissible branch
+                bool found = false;
+                for (int b = 0; b < 200; b++) {
+                    const double mid = sqrt(lo * hi);
+                    double dm;
+                    const double fm = F(mid, dm);
+                    if (!isfinite(fm)) return false;
+                    if (!(dm > 0)) lo = mid;
+                    else if (fm > 0) { hi = mid; fhi = fm; }
+                    else { lo = mid; flo = fm; found = true; break; }
+                    if (hi - lo <= 1e-15 * hi) break;
+                }
+                if (!found) return false;
+                break;
+            }
+        }
+        if (flo > 0) return false;
+    }
+    double a = (flo == 0) ? lo : (fhi == 0 ? hi : (guess >= lo && guess <= hi ? guess : sqrt(lo * hi)));
+    for (int it = 0; it < 200; it++) {
+        double df;
+        const double fa = F(a, df);
+        if (fa == 0) break;
+        if (fa < 0) lo = a; else hi = a;
+        double an = (df > 0) ? a - fa / df : -1.0;
+        if (an > 0 && fabs(an - a) <= 4e-16 * a) { a = an; break; }
+        if (!(an > lo && an < hi)) an = sqrt(lo * hi);
+        if (fabs(an - a) <= 4e-16 * a || hi - lo <= 4e-16 * hi) { a = an; break; }
+        a = an;
+    }
+    double df;
+    F(a, df);
+    if (!(df > 0)) return false;
+    al = a;
+    dal = -(a / h.G + a - B) / df;
+    return true;
+}
+// The p-closure with a Mie-Grueneisen phase (closure_p_mg :585-629): the defect split's
+// segment is taken at the guess; Phi(p) = sum_k alpha_k(p) - 1 with alpha_mg for MG phases and
+// the closed form (B6.2) for NASG ones; bracket grown from the guess, then bracketed Newton.
+struct ClMg {
+    ClOut o;
+    int ok;
+};
+static __device__ __noinline__ ClMg closure_p_mg(const Phys P, const ClIn in) {
+    ClMg res;
+    res.ok = 0;
+    ClOut& o = res.o;
+    if (!(in.mtr[0] + in.mtr[1] > 0)) return res;  // p_coef's failure condition
+    ClPre pr;
+    closure_pre(P, in, pr);
+    double lam[2], ex[2], A[2], B[2], N[2];
+    seg_lambda(in, pr, in.pguess, lam, ex);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        A[k] = pr.A0[k] + lam[k] * pr.D0 + ex[k];
+        B[k] = in.atr[k] + lam[k] * in.s;
+        N[k] = A[k] - (B[k] - in.mtr[k] * P.ph[k].b) * P.ph[k].pi;
+    }
+    double ag[2] = {in.atr[0] / (in.atr[0] + in.atr[1]), in.atr[1] / (in.atr[0] + in.atr[1])};
+    auto Phi = [&](double p, double& dPhi, bool upd) -> double {  // NaN: a phase has no solution at this p
+        double s = -1.0, an[2];
+        dPhi = 0.0;
+        for (int k = 0; k < 2; k++) {
+            const PhaseD& h = P.ph[k];
+            double a, da;
+            if (SPB6G_MG && h.kind) {
+                if (!alpha_mg(h, in.mtr[k], A[k], B[k], p, ag[k], a, da)) return NAN;
+            } else {
+                if (!(p + h.pi > 0) || !(N[k] > 0)) return NAN;
+                a = ((h.g - 1.0) * (A[k] + B[k] * p) + (p + h.g * h.pi) * in.mtr[k] * h.b) / (h.g * (p + h.pi));
+                da = -(h.g - 1.0) * N[k] / (h.g * (p + h.pi) * (p + h.pi));
+            }
+            an[k] = a;
+            s += a;
+            dPhi += da;
+        }
+        if (upd) { ag[0] = an[0]; ag[1] = an[1]; }
+        return s;
+    };
+    double p = in.pguess, d;
+    const double f = Phi(p, d, true);
+    double scale = 1e-6 * (fabs(p) + 1e5);
+    double lo, hi, flo, fhi;
+    if (!isfinite(f) || f > 0) {  // p too low: search upwards for Phi < 0
+        lo = p; flo = f; hi = p;
+        for (int it = 0; it < 300; it++) {
+            hi = p + scale;
+            fhi = Phi(hi, d, false);
+            if (isfinite(fhi) && fhi <= 0) break;
+            if (isfinite(fhi)) { lo = hi; flo = fhi; }
+            scale *= 2.0;
+        }
+        if (!(isfinite(fhi) && fhi <= 0)) return res;
+    } else {
+        hi = p; fhi = f; lo = p;
+        for (int it = 0; it < 300; it++) {
+            lo = p - scale;
+            flo = Phi(lo, d, false);
+            if (isfinite(flo) && flo >= 0) break;
+            if (!isfinite(flo)) {
+                scale *= 0.5;
+                if (scale < 1e-300) return res;
+                continue;
+            }
+            hi = lo; fhi = flo; scale *= 2.0;
+        }
+        if (!(isfinite(flo) && flo >= 0)) return res;
+    }
+    p = (isfinite(f) && in.pguess >= lo && in.pguess <= hi) ? in.pguess : 0.5 * (lo + hi);
+    for (int it = 0; it < 300; it++) {
+        double df;
+        const double fp = Phi(p, df, true);
+        if (fp == 0.0) break;
+        if (!isfinite(fp) || fp > 0) lo = p; else hi = p;
+        double pn = (isfinite(fp) && df < 0) ? p - fp / df : 0.5 * (lo + hi);
+        if (isfinite(fp) && df < 0 && fabs(pn - p) <= 2e-16 * (fabs(p) + fabs(pn))) { p = pn; break; }
+        if (!(pn > lo && pn < hi)) pn = 0.5 * (lo + hi);
+        if (fabs(pn - p) <= 2e-16 * (fabs(p) + fabs(pn)) || hi - lo <= 4e-16 * (fabs(hi) + fabs(lo))) { p = pn; break; }
+        p = pn;
+    }
+    double df;
+    if (!isfinite(Phi(p, df, true))) return res;
+    for (int k = 0; k < 2; k++) {
+        o.a[k] = ag[k];
+        if (!p_admissible(P, k, o.a[k], in.mtr[k], p)) return res;
+        o.e[k] = eps_amp(P, k, o.a[k], in.mtr[k], p);
+    }
+    o.pbar = p;
+    res.ok = isfinite(p) ? 1 : 0;
+    return res;
+}
+
 // Bracketed safeguarded Newton on Phi (closure_p, :472-548), preceded by the
 // admissibility checks of closure() (:842-866).  At most 400 iterations.
 SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
@@ -137,6 +397,11 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
     for (int k = 0; k < 2; k++)
         if (!(in.atr[k] > 0) || !(in.mtr[k] > 0) || !isfinite(in.etr[k])) return false;
     if (!isfinite(in.rhoeC) || !isfinite(in.s)) return false;
+    if (SPB6G_MG && P.mg) {
+        const ClMg r = closure_p_mg(P, in);
+        o = r.o;
+        return r.ok && isfinite(o.pbar);
+    }
     if (!(in.mtr[0] + in.mtr[1] > 0)) return false;
     const double plo = SMAX(-P.ph[0].pi, -P.ph[1].pi);
     ClPre pr;
@@ -177,6 +442,7 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
 }
 // Round-off floor of the closure pressure (SPB6_PC_IMEX_omp.cpp:657-664, via p_coef :453-464).
 SPB6G_DEV double closure_roundoff(const Phys& P, const ClIn& in, double p) {
+    if (SPB6G_MG && P.mg) return 0.0;  // no floor with a Mie-Grueneisen phase (:658)
     if (!(in.mtr[0] + in.mtr[1] > 0)) return 0.0;
     const double D0 = in.rhoeC - in.etr[0] - in.etr[1];
     // defect_split (:438-449) at delta = D0 + p s
@@ -221,7 +487,7 @@ SPB6G_DEV bool prim_of(const Phys& P, const double* Q, Prim& w) {
     w.u = Q[IMU] / w.rho;
     w.v = Q[IMV] / w.rho;
     const double p1 = p_ame(P, 0, a1, m1, Q[IE1]), p2 = p_ame(P, 1, a2, m2, Q[IE2]);
-    if (!(p_admissible(P, 0, p1) && p_admissible(P, 1, p2))) return false;
+    if (!(p_admissible(P, 0, a1, m1, p1) && p_admissible(P, 1, a2, m2, p2))) return false;
     w.cf = sqrt((m1 * c2_rp(P, 0, r1, p1) + m2 * c2_rp(P, 1, r2, p2)) / w.rho);
     return true;
 }
@@ -231,20 +497,54 @@ SPB6G_DEV double pbar_of(const Phys& P, const double* Q) {
 }
 
 // ------------------------------------------------------------ shock budget, :267-428
-SPB6G_DEV bool eos_ok(const Phys& P, int k, double p, double v) {
+template <bool MG = true>
+SPB6G_DEV bool eos_ok(const Phys& P, int k, double p, double v) {  // :273-277
     if (!(v > 0) || !isfinite(p)) return false;
+    if (MG && SPB6G_MG && P.ph[k].kind) return c2_rp(P, k, 1.0 / v, p) > 0;
     return v > P.ph[k].b && p + P.ph[k].pi > 0;
+}
+// Mie-Grueneisen Hugoniot from (p0, v0) to p1 (:285-292): bisection on (0, v0].
+static __device__ __noinline__ double hug_v_mg(const PhaseD h, double p0, double p1, double v0) {
+    auto e_pv = [&](double p, double v) {
+        double pr, dpr, er;
+        mg_ref(h, 1.0 / v, pr, dpr, er);
+        return er + v * (p - pr) / h.G;
+    };
+    const double e0 = e_pv(p0, v0);
+    auto g = [&](double v) { return e_pv(p1, v) - e0 + 0.5 * (p0 + p1) * (v - v0); };
+    double hi = v0, lo = v0, gl = g(v0);
+    if (!(gl > 0)) return v0;
+    for (int it = 0; it < 80 && gl > 0; it++) {
+        hi = lo;
+        lo *= 0.9;
+        gl = g(lo);
+        if (!isfinite(gl)) return NAN;
+    }
+    if (gl > 0) return NAN;
+    for (int it = 0; it < 100; it++) {
+        const double m = 0.5 * (lo + hi), gm = g(m);
+        if (gm > 0) hi = m; else lo = m;
+        if (hi - lo <= 1e-14 * v0) break;
+    }
+    return 0.5 * (lo + hi);
 }
 SPB6G_DEV double hug_v(const Phys& P, int k, double p0, double p1, double v0) {  // NASG closed form, :279-284
     const PhaseD& h = P.ph[k];
+    if (SPB6G_MG && h.kind) return hug_v_mg(h, p0, p1, v0);
     const double x0 = p0 + h.pi, x1 = p1 + h.pi;
     return h.b + (v0 - h.b) * ((h.g - 1.0) * x1 + (h.g + 1.0) * x0) / ((h.g + 1.0) * x1 + (h.g - 1.0) * x0);
 }
 SPB6G_DEV void K_G(const Phys& P, int k, double p, double v, double& K, double& Gm) {  // :296-301
     K = c2_rp(P, k, 1.0 / v, p) / v;
+    if (SPB6G_MG && P.ph[k].kind) {  // MG: dK/dp along the isentrope dv = -v dp / K by a difference
+        const double dp = 1e-6 * K, K2 = c2_rp(P, k, 1.0 / (v * (1.0 - dp / K)), p + dp) / (v * (1.0 - dp / K));
+        Gm = 0.5 * (1.0 + (K2 - K) / dp);
+        return;
+    }
     Gm = 0.5 * (P.ph[k].g + 1.0);
     if (P.ph[k].b != 0.0) Gm *= v / (v - P.ph[k].b);
 }
+
 // Per-cell constants of the profile ODE: 1/Y_2 and, per phase, 1/(g-1) and g/(g-1); lamY
 // holds lambda_k / Y_k for the integration's c.  The right-hand side below is the
 // reference's (:304-312) with these reciprocals hoisted: 3 divisions per evaluation
@@ -263,9 +563,55 @@ SPB6G_DEV void prof_consts(const Phys& P, ShockProf& S) {
         S.ggm[k] = P.ph[k].g * S.ig1[k];
     }
 }
+// The right-hand side with a Mie-Grueneisen phase, in the reference's own form (:304-312 with
+// eos_ep_ev :268-272).
+struct ProfRhs {
+    double dy[3];
+    int ok;
+};
+static __device__ __noinline__ ProfRhs prof_rhs_mg(const Phys P, const ShockProf S, double v, double y0, double y1) {
+    ProfRhs res;
+    res.ok = 0;
+    double* dy = res.dy;
+    const double p = y0, v1 = y1, v2 = (v - S.Y[0] * v1) / S.Y[1], Pr = S.p0 + S.j2 * (S.v0 - v);
+    if (!eos_ok(P, 0, p, v1) || !eos_ok(P, 1, p, v2)) return res;
+    const double vk[2] = {v1, v2};
+    double num = -1.0, den = 0.0, r[2], ep[2], evp[2];
+    for (int k = 0; k < 2; k++) {
+        const PhaseD& h = P.ph[k];
+        if (SPB6G_MG && h.kind) {
+            double pr, dpr, er;
+            const double rr = 1.0 / vk[k];
+            mg_ref(h, rr, pr, dpr, er);
+            ep[k] = vk[k] / h.G;
+            evp[k] = (p - pr) * (1.0 + 1.0 / h.G) + rr * dpr / h.G;
+        } else {
+            ep[k] = (vk[k] - h.b) / (h.g - 1.0);
+            evp[k] = h.g * (p + h.pi) / (h.g - 1.0);
+        }
+        r[k] = S.lamY[k] * (p - Pr);
+        num += S.Y[k] * r[k] / evp[k];
+        den += S.Y[k] * ep[k] / evp[k];
+    }
+    dy[0] = num / den;
+    dy[1] = (r[0] - ep[0] * dy[0]) / evp[0];
+    dy[2] = p - Pr;
+    res.ok = isfinite(dy[0]) && isfinite(dy[1]);
+    return res;
+}
+// MG: the strong-shock routine is instantiated twice, and the SG / NASG instantiation makes no
+// Mie-Grueneisen call inside its integration loop.
+template <bool MG>
 SPB6G_DEV bool prof_rhs(const Phys& P, const ShockProf& S, double v, const double* y, double* dy) {  // :304-312
+    if constexpr (MG) {
+        const ProfRhs r = prof_rhs_mg(P, S, v, y[0], y[1]);
+        dy[0] = r.dy[0];
+        dy[1] = r.dy[1];
+        dy[2] = r.dy[2];
+        return r.ok;
+    }
     const double p = y[0], v1 = y[1], v2 = (v - S.Y[0] * v1) * S.iY1, Pr = S.p0 + S.j2 * (S.v0 - v);
-    if (!eos_ok(P, 0, p, v1) || !eos_ok(P, 1, p, v2)) return false;
+    if (!eos_ok<false>(P, 0, p, v1) || !eos_ok<false>(P, 1, p, v2)) return false;
     const double vk[2] = {v1, v2}, dp = p - Pr;
     double num = -1.0, den = 0.0, r[2], ep[2], iev[2];
 #pragma unroll
@@ -284,6 +630,7 @@ SPB6G_DEV bool prof_rhs(const Phys& P, const ShockProf& S, double v, const doubl
 }
 // Kapila shock profile integrated with the adaptive Cash-Karp embedded RK4(5)
 // pair (Cash & Karp 1990), :313-343.  At most 4000 steps.
+template <bool MG>
 SPB6G_DEV bool prof_integrate(const Phys& P, ShockProf& S, double c, double& v1end, double& qend) {
     S.lamY[0] = c / S.Y[0];
     S.lamY[1] = (1.0 - c) / S.Y[1];
@@ -310,7 +657,7 @@ SPB6G_DEV bool prof_integrate(const Phys& P, ShockProf& S, double c, double& v1e
                 yt[n] = y[n];
                 for (int q = 0; q < st; q++) yt[n] += h * B[st][q] * k[q][n];
             }
-            ok = prof_rhs(P, S, v + A[st] * h, yt, k[st]);
+            ok = prof_rhs<MG>(P, S, v + A[st] * h, yt, k[st]);
         }
         double err = 0.0, y5[3];
         if (ok)
@@ -332,10 +679,11 @@ SPB6G_DEV bool prof_integrate(const Phys& P, ShockProf& S, double c, double& v1e
     }
     return false;
 }
+template <bool MG>
 SPB6G_DEV double shoot_F(const Phys& P, ShockProf& S, const double vH[2], const double vpre[2], double t, double& qq) {
     const double c = 1.0 / (1.0 + exp(-t));
     double v1e;
-    if (!prof_integrate(P, S, c, v1e, qq)) return NAN;
+    if (!prof_integrate<MG>(P, S, c, v1e, qq)) return NAN;
     return (v1e - vH[0]) / vpre[0];
 }
 // Weak-shock analytic share; returns false and sets `strong` when the profile
@@ -361,7 +709,8 @@ SPB6G_DEV bool shock_share_weak(const Phys& P, const double Y[2], const double v
     return false;
 }
 // Strong-shock branch of shock_share (:356-392): Illinois false position on logit(c).
-SPB6G_DEV bool shock_share_strong(const Phys& P, const double Y[2], const double vpre[2], double p0, double p1,
+template <bool MG>
+SPB6G_DEV bool shock_share_strong_t(const Phys& P, const double Y[2], const double vpre[2], double p0, double p1,
                                   const double K[2], const double Gm[2], double lam[2], double& q) {
     const double dp = p1 - p0;
     ShockProf S;
@@ -386,18 +735,18 @@ SPB6G_DEV bool shock_share_strong(const Phys& P, const double Y[2], const double
         t0 = isfinite(c0) ? log(c0 / (1.0 - c0)) : 0.0;
     }
     double ta = SMAX(-40.0, t0 - 1.0), tb = SMIN(40.0, t0 + 1.0), qa = 0, qb = 0;
-    double fa = shoot_F(P, S, vH, vpre, ta, qa), fb = shoot_F(P, S, vH, vpre, tb, qb);
+    double fa = shoot_F<MG>(P, S, vH, vpre, ta, qa), fb = shoot_F<MG>(P, S, vH, vpre, tb, qb);
     if (!isfinite(fa) || !isfinite(fb)) return false;
     for (double st = 2.0; fa >= 0 && ta > -40.0; st *= 2.0) {
         tb = ta; fb = fa; qb = qa;
         ta = SMAX(-40.0, ta - st);
-        fa = shoot_F(P, S, vH, vpre, ta, qa);
+        fa = shoot_F<MG>(P, S, vH, vpre, ta, qa);
         if (!isfinite(fa)) return false;
     }
     for (double st = 2.0; fb <= 0 && tb < 40.0; st *= 2.0) {
         ta = tb; fa = fb; qa = qb;
         tb = SMIN(40.0, tb + st);
-        fb = shoot_F(P, S, vH, vpre, tb, qb);
+        fb = shoot_F<MG>(P, S, vH, vpre, tb, qb);
         if (!isfinite(fb)) return false;
     }
     double t, qt;
@@ -409,7 +758,7 @@ SPB6G_DEV bool shock_share_strong(const Phys& P, const double Y[2], const double
         for (int it = 0; it < 100; it++) {
             t = (ta * fb - tb * fa) / (fb - fa);
             if (!(t > ta && t < tb)) t = 0.5 * (ta + tb);
-            const double ft = shoot_F(P, S, vH, vpre, t, qt);
+            const double ft = shoot_F<MG>(P, S, vH, vpre, t, qt);
             if (!isfinite(ft)) return false;
             if (fabs(ft) < 1e-10 || tb - ta < 1e-10) break;
             if (ft < 0) { ta = t; fa = ft; if (side == -1) fb *= 0.5; side = -1; }
@@ -422,6 +771,29 @@ SPB6G_DEV bool shock_share_strong(const Phys& P, const double Y[2], const double
     q = qt;
     return q > 0;
 }
+struct ShockShare {
+    double lam[2], q;
+    int ok;
+};
+static __device__ __noinline__ ShockShare shock_share_strong_mg(const Phys P, const double Y0, const double Y1, const double v0,
+                                                                const double v1, double p0, double p1, double K0, double K1,
+                                                                double G0, double G1) {
+    ShockShare r;
+    const double Y[2] = {Y0, Y1}, vpre[2] = {v0, v1}, K[2] = {K0, K1}, Gm[2] = {G0, G1};
+    r.ok = shock_share_strong_t<true>(P, Y, vpre, p0, p1, K, Gm, r.lam, r.q) ? 1 : 0;
+    return r;
+}
+SPB6G_DEV bool shock_share_strong(const Phys& P, const double Y[2], const double vpre[2], double p0, double p1,
+                                  const double K[2], const double Gm[2], double lam[2], double& q) {
+    if (SPB6G_MG && P.mg) {
+        const ShockShare r = shock_share_strong_mg(P, Y[0], Y[1], vpre[0], vpre[1], p0, p1, K[0], K[1], Gm[0], Gm[1]);
+        lam[0] = r.lam[0];
+        lam[1] = r.lam[1];
+        q = r.q;
+        return r.ok != 0;
+    }
+    return shock_share_strong_t<false>(P, Y, vpre, p0, p1, K, Gm, lam, q);
+}
 // stencil_state (:395-400): {a1, a2, m1, m2, p, u, v}; p = NaN when inadmissible.
 SPB6G_DEV void stencil_state(const Phys& P, const double* c, double* st) {
     const double a1 = c[IA1], m1 = c[IM1], m2 = c[IM2], r = m1 + m2;
@@ -430,7 +802,7 @@ SPB6G_DEV void stencil_state(const Phys& P, const double* c, double* st) {
     st[6] = r > 0 ? c[IMV] / r : 0.0;
     if (a1 > 0 && a1 < 1 && m1 > 0 && m2 > 0) {
         const double p = p_mix(P, a1, m1, m2, c[IE1] + c[IE2]);
-        if (p_admissible(P, 0, p) && p_admissible(P, 1, p)) st[4] = p;
+        if (p_admissible(P, 0, a1, m1, p) && p_admissible(P, 1, 1.0 - a1, m2, p)) st[4] = p;
     }
 }
 

@@ -506,19 +506,17 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if ((cfg->bc[0] == SPB6G_BC_PERIODIC) != (cfg->bc[1] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if ((cfg->bc[2] == SPB6G_BC_PERIODIC) != (cfg->bc[3] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if (cfg->rus_local != 1) return SPB6G_UNSUPPORTED;
+    for (int k = 0; k < 2; k++) {
+        if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
+        if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return SPB6G_NO_DEVICE;
     spb6g_solver* s = new (std::nothrow) spb6g_solver();
     if (!s) return SPB6G_BAD_ARG;
     s->cfg = *cfg;
-    for (int k = 0; k < 2; k++) {
-        s->P.ph[k].g = cfg->gamma[k]; s->P.ph[k].pi = cfg->pinf[k]; s->P.ph[k].q = cfg->q[k];
-        s->P.ph[k].qp = cfg->qp[k]; s->P.ph[k].cv = cfg->cv[k]; s->P.ph[k].b = cfg->b[k];
-    }
-    s->P.share_mode = cfg->share_mode;
-    s->P.limiter = cfg->limiter;
-    s->P.rus_local = cfg->rus_local;
+    phys_from_config(cfg, s->P);
     s->g.nx = cfg->nx; s->g.ny = cfg->ny;
     for (int q = 0; q < 4; q++) { s->g.bcs[q] = cfg->bc[q]; s->g.bcu[q] = cfg->bcu[q]; s->g.bcp[q] = cfg->bcp[q]; }
     s->g.dx = (cfg->x1 - cfg->x0) / cfg->nx;
@@ -1038,7 +1036,9 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     if (!cfgs || !out || count < 1) return SPB6G_BAD_ARG;
     *out = nullptr;
     for (int i = 0; i < count; i++)
-        if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device) return SPB6G_UNSUPPORTED;
+        if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
+            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0)  // the batched kernel: stiffened gas / NASG phases
+            return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;
     for (int i = 0; i < count; i++) {

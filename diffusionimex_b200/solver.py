@@ -47,7 +47,11 @@ class Config(ctypes.Structure):
         ("dtfix", ctypes.c_double), ("rus_local", ctypes.c_int32), ("limiter", ctypes.c_int32), ("acdt", ctypes.c_int32),
         ("newton_tol", ctypes.c_double), ("newton_iter", ctypes.c_int32), ("bicg_tol", ctypes.c_double),
         ("bicg_iter", ctypes.c_int32), ("share_mode", ctypes.c_int32), ("tend", ctypes.c_double),
-        ("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
+        ("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("kind", ctypes.c_int32 * 2),
+        ("reserved", ctypes.c_int32 * 4),
+        ("mg_G", ctypes.c_double * 2), ("mg_rr", ctypes.c_double * 2), ("mg_c1", ctypes.c_double * 2),
+        ("mg_c2", ctypes.c_double * 2), ("mg_e1", ctypes.c_double * 2), ("mg_e2", ctypes.c_double * 2),
+        ("mg_e0", ctypes.c_double * 2),
     ]
 
 
@@ -150,6 +154,9 @@ def make_config(case: dict, device: int = 0) -> Config:
     for k in range(2):
         ph = case["phases"][k]
         c.gamma[k], c.pinf[k], c.q[k], c.qp[k], c.cv[k], c.b[k] = ph["g"], ph["pinf"], ph["q"], ph["qp"], ph["cv"], ph["b"]
+        c.kind[k] = int(ph.get("kind", 0))
+        for f in ("G", "rr", "c1", "c2", "e1", "e2", "e0"):
+            getattr(c, "mg_" + f)[k] = float(ph.get(f, 0.0))
     c.device = device
     c.precision = int(case.get("precision", 0))
     return c

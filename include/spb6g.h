@@ -71,7 +71,13 @@ typedef struct {
     int32_t precision;              /* 0: FP64 throughout; 1: precision form -- FP32 reconstruction,
                                        Rusanov fluxes and SpMV, FP64 EOS inversion, relaxation Newton,
                                        BiCGStab reductions and residuals (no counterpart in the reference) */
-    int32_t reserved[6];
+    int32_t kind[2];                /* 0 SG / NASG; Mie-Grueneisen p = G rho (e - er(rho)) + pr(rho):
+                                       1 Cochran-Chan pr = c1 x^e1 - c2 x^e2, x = rho / rr;
+                                       2 JWL pr = c1 exp(-e1 rr / rho) + c2 exp(-e2 rr / rho), er - e0
+                                       (Phase.kind, physics :51-69); MG phases use only G, rr, c1, c2,
+                                       e1, e2, e0 and cv (temperature output) */
+    int32_t reserved[4];
+    double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
 } spb6g_config;
 
 /* Run statistics: the counters of the reference's stats line (:98-99, :1425). */

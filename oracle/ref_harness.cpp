@@ -86,7 +86,9 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
         PH[k] = Phase{};
         PH[k].g = c.g[k]; PH[k].pi = c.pinf[k]; PH[k].q = c.q[k];
         PH[k].qp = c.qp[k]; PH[k].cv = c.cv[k]; PH[k].b = c.b[k];
-        PH[k].kind = 0;
+        PH[k].kind = c.kind[k];
+        PH[k].G = c.mg_G[k]; PH[k].rr = c.mg_rr[k]; PH[k].c1 = c.mg_c1[k]; PH[k].c2 = c.mg_c2[k];
+        PH[k].e1 = c.mg_e1[k]; PH[k].e2 = c.mg_e2[k]; PH[k].e0 = c.mg_e0[k];
     }
     RELAX_LEVEL = 0;
     theta_rate = 0.0;

@@ -30,7 +30,10 @@ CASE_DT = np.dtype([
     ("g", "<f8", 2), ("pinf", "<f8", 2), ("q", "<f8", 2), ("qp", "<f8", 2), ("cv", "<f8", 2), ("b", "<f8", 2),
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
     ("budget_s", "<f8"), ("warmup", "<i4"), ("inject_qph", "<i4"),
+    ("kind", "<i4", 2), ("mg_G", "<f8", 2), ("mg_rr", "<f8", 2), ("mg_c1", "<f8", 2), ("mg_c2", "<f8", 2),
+    ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2),
 ])
+MG_KEYS = ("G", "rr", "c1", "c2", "e1", "e2", "e0")
 RESULT_DT = np.dtype([
     ("magic", "<u4"), ("status", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
     ("steps", "<i8"), ("rejects", "<i8"), ("rk1", "<i8"), ("stages", "<i8"), ("newton_it", "<i8"),
@@ -42,7 +45,7 @@ RESULT_DT = np.dtype([
 def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, warmup: int = 0,
                 budget_s: float = 0.0) -> np.ndarray:
     r = np.zeros((), CASE_DT)
-    r["magic"], r["version"] = MAGIC, 1
+    r["magic"], r["version"] = MAGIC, 2
     for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
         r[k] = int(cfg[k])
     r["bc"] = cfg["bc"]
@@ -53,6 +56,9 @@ def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int
     r["bcu"], r["bcp"] = cfg["bcu"], cfg["bcp"]
     for f in ("g", "pinf", "q", "qp", "cv", "b"):
         r[f] = [cfg["phases"][0][f], cfg["phases"][1][f]]
+    r["kind"] = [int(cfg["phases"][k].get("kind", 0)) for k in range(2)]
+    for f in MG_KEYS:
+        r["mg_" + f] = [float(cfg["phases"][k].get(f, 0.0)) for k in range(2)]
     return r
 
 

@@ -20,7 +20,7 @@
 #include <stdint.h>
 
 #define SPB6_CASE_MAGIC 0x36425053u /* "SPB6" */
-#define SPB6_CASE_VERSION 1
+#define SPB6_CASE_VERSION 2
 
 enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2 };
 enum { SPB6_BC_TRANS = 0, SPB6_BC_WALL = 1, SPB6_BC_PERIODIC = 2, SPB6_BC_PRES = 3 };
@@ -40,6 +40,9 @@ typedef struct {
     double budget_s;   /* > 0: stop stepping once the timed steps have used this much wall time */
     int32_t warmup;    /* steps run before the timed region (wall_s counts the rest) */
     int32_t inject_qph; /* stage mode, C restatement only: U0 is followed by Q_1, Q_2 (2 x nx*ny) */
+    int32_t kind[2];    /* 0 SG / NASG, 1 Cochran-Chan, 2 JWL (reference harness only; the C restatement
+                           runs SG / NASG phases) */
+    double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
 } spb6_case;
 
 typedef struct {

@@ -94,6 +94,11 @@ CASES = {
                                    {"bicg_tol": 1e-13}),
     "bubble_walls32_3steps": (lambda: _bc(_bubble(32), (W, W, W, W), bcu=(0, 0, 5.0, 0)), "steps", 3,
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # Mie-Grueneisen phases (physics :51-111, closure_p_mg :585-629, hug_v / K_G :279-301)
+    "nm_N200_20steps": (lambda: cases.reference_case(60, 200), "steps", 20, {}),
+    "jwl_N200_20steps": (lambda: cases.reference_case(61, 200), "steps", 20, {}),
+    "undex120x80_3steps": (lambda: cases.underwater_explosion(120, 80), "steps", 3,
+                           {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "bubble_outlet32_3steps": (lambda: _bc(_bubble(32), (PRES, PRES, W, W), bcp=(1.2e7, 0.8e7, 0, 0)), "steps", 3,
                                {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
 }
