@@ -11,18 +11,63 @@ namespace {
 
 enum { IA1 = 0, IM1 = 1, IM2 = 2, IMU = 3, IMV = 4, IE1 = 5, IE2 = 6, IEN = 7 };
 
-// Stiffened gas / NASG relations of phase k (physics :71-89, :103-106), as the reference writes them.
+// Relations of phase k (physics :60-106), as the reference writes them: stiffened gas / NASG, or
+// Mie-Grueneisen with the Cochran-Chan (kind 1) or JWL (kind 2) reference curves.
 struct PhaseH {
     double g, pi, q, qp, cv, b;
+    int kind;
+    double G, rr, c1, c2, e1, e2, e0;
 };
-PhaseH phase(const spb6g_config& cf, int k) { return {cf.gamma[k], cf.pinf[k], cf.q[k], cf.qp[k], cf.cv[k], cf.b[k]}; }
-double p_ame(const PhaseH& P, double a, double m, double e) { return (e - m * P.q) * (P.g - 1.0) / (a - m * P.b) - P.g * P.pi; }
-double T_amp(const PhaseH& P, double a, double m, double p) { return (a / m - P.b) * (p + P.pi) / ((P.g - 1.0) * P.cv); }
+PhaseH phase(const spb6g_config& cf, int k) {
+    return {cf.gamma[k], cf.pinf[k], cf.q[k], cf.qp[k], cf.cv[k], cf.b[k], cf.kind[k],
+            cf.mg_G[k], cf.mg_rr[k], cf.mg_c1[k], cf.mg_c2[k], cf.mg_e1[k], cf.mg_e2[k], cf.mg_e0[k]};
+}
+void mg_ref(const PhaseH& P, double r, double& pr, double& dpr, double& er) {  // :60-69
+    if (P.kind == 1) {
+        const double x = r / P.rr, t1 = P.c1 * std::pow(x, P.e1), t2 = P.c2 * std::pow(x, P.e2);
+        pr = t1 - t2;
+        dpr = (P.e1 * t1 - P.e2 * t2) / r;
+        er = (t1 / (P.e1 - 1.0) - t2 / (P.e2 - 1.0)) / r;
+    } else {
+        const double t1 = P.c1 * std::exp(-P.e1 * P.rr / r), t2 = P.c2 * std::exp(-P.e2 * P.rr / r);
+        pr = t1 + t2;
+        dpr = (P.e1 * t1 + P.e2 * t2) * P.rr / (r * r);
+        er = t1 / (P.e1 * P.rr) + t2 / (P.e2 * P.rr) - P.e0;
+    }
+}
+double p_ame(const PhaseH& P, double a, double m, double e) {
+    if (P.kind) {
+        double pr, dpr, er;
+        mg_ref(P, m / a, pr, dpr, er);
+        return P.G * (e - m * er) / a + pr;
+    }
+    return (e - m * P.q) * (P.g - 1.0) / (a - m * P.b) - P.g * P.pi;
+}
+double T_amp(const PhaseH& P, double a, double m, double p) {
+    if (P.kind) {
+        if (!(P.cv > 0)) return NAN;
+        double pr, dpr, er;
+        mg_ref(P, m / a, pr, dpr, er);
+        return (a * (p - pr) / (P.G * m)) / P.cv;
+    }
+    return (a / m - P.b) * (p + P.pi) / ((P.g - 1.0) * P.cv);
+}
 double s_pT(const PhaseH& P, double p, double T) {
     return P.cv * (P.g * std::log(T) - (P.g - 1.0) * std::log(p + P.pi)) + P.qp;
 }
 double g_pT(const PhaseH& P, double p, double T) { return P.g * P.cv * T + P.b * p + P.q - T * s_pT(P, p, T); }
-double c2_rp(const PhaseH& P, double r, double p) { return P.g * (p + P.pi) / (r * (1.0 - r * P.b)); }
+double c2_rp(const PhaseH& P, double r, double p) {
+    if (P.kind) {
+        double pr, dpr, er;
+        mg_ref(P, r, pr, dpr, er);
+        return (P.G + 1.0) * (p - pr) / r + dpr;
+    }
+    return P.g * (p + P.pi) / (r * (1.0 - r * P.b));
+}
+bool p_admissible(const PhaseH& P, double a, double m, double p) {  // :103-106
+    if (P.kind) return std::isfinite(p) && c2_rp(P, m / a, p) > 0;
+    return p + P.pi > 0;
+}
 
 struct Prim {
     double a1, r1, r2, u, v, p1, p2, rho, cf;
@@ -39,7 +84,7 @@ bool prim_of(const PhaseH (&ph)[2], const double* Q, Prim& w) {
     w.v = Q[IMV] / w.rho;
     w.p1 = p_ame(ph[0], a1, m1, Q[IE1]);
     w.p2 = p_ame(ph[1], a2, m2, Q[IE2]);
-    if (!(w.p1 + ph[0].pi > 0 && w.p2 + ph[1].pi > 0)) return false;
+    if (!(p_admissible(ph[0], a1, m1, w.p1) && p_admissible(ph[1], a2, m2, w.p2))) return false;
     w.cf = std::sqrt((m1 * c2_rp(ph[0], w.r1, w.p1) + m2 * c2_rp(ph[1], w.r2, w.p2)) / w.rho);
     return true;
 }
@@ -57,7 +102,7 @@ void cell_diag(const spb6g_config& cf, const double* Q, double* o) {
         cw = std::sqrt(1.0 / (rho * (a1 / (w.r1 * c2_rp(ph[0], w.r1, w.p1)) + (1 - a1) / (w.r2 * c2_rp(ph[1], w.r2, w.p2)))));
         T1 = T_amp(ph[0], a1, m1, w.p1);
         T2 = T_amp(ph[1], 1 - a1, m2, w.p2);
-        if (T1 > 0 && T2 > 0 && ph[0].cv > 0) dg = g_pT(ph[0], w.p1, T1) - g_pT(ph[1], w.p2, T2);
+        if (T1 > 0 && T2 > 0 && ph[0].cv > 0 && !ph[0].kind && !ph[1].kind) dg = g_pT(ph[0], w.p1, T1) - g_pT(ph[1], w.p2, T2);
     }
     o[0] = ok ? a1 * w.p1 + (1 - a1) * w.p2 : NAN;
     o[1] = ok ? w.u : NAN;

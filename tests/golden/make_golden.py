@@ -108,6 +108,7 @@ CASES = {
 MAIN_RUNS = {
     "case5_N100": (5, 100, ["snap=8e-5,1.6e-4", "probe=0.6,0.5"]),
     "case87_N200": (87, 200, ["snap=1e-4", "probe=0.5,0.5"]),
+    "case60_N100": (60, 100, ["snap=3e-5", "probe=0.6,0.5"]),  # Mie-Grueneisen (Cochran-Chan) phases
 }
 
 
