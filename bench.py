@@ -67,7 +67,7 @@ def parse():
     p.add_argument("--workload", default="bubbles1024",
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
-                        "mlp (learned warm-start network)")
+                        "undex361x200 (Mie-Grueneisen phases), mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -92,6 +92,8 @@ def make_workload(name: str):
         c = make_workload(name[:-len("-mixed")])
         c["precision"] = 1
         c["workload"] = c.get("workload", name) + " (precision form)"
+    elif name == "undex361x200":
+        c = cases.underwater_explosion(361, 200)
     elif name == "riemann512":
         return {"batch": cases.riemann_batch(count=512, seed=0), "workload": "512 1D Riemann problems, 256-4096 cells"}
     elif name == "mlp":
