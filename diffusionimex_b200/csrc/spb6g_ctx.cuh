@@ -52,11 +52,14 @@ inline void phys_from_config(const spb6g_config* cfg, Phys& P) {
     P.limiter = cfg->limiter;
     P.rus_local = cfg->rus_local;
     P.mg = cfg->kind[0] != 0 || cfg->kind[1] != 0;
+    P.relax = cfg->relax;
+    P.eps_i = cfg->eps_i;
 }
 
 struct Ctx {
     Phys phy;
     Geom g;
+    unsigned char* ctype;  // per-cell closure type of the step (p-pT relaxation only)
     int n;
     int prec;  // 1: precision form (FP32 reconstruction, fluxes and SpMV), 0: FP64
     double tau, rx, ry, p_ref, adt;
@@ -174,6 +177,7 @@ void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);
 void launch_floor(const Ctx& c, cudaStream_t st, double tol);
 void launch_final(const Ctx& c, cudaStream_t st);
+void launch_relax_activate(const Ctx& c, cudaStream_t st, State U);
 void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic);
 void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U);
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P);

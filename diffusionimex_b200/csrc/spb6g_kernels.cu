@@ -376,6 +376,7 @@ SPB6G_DEV bool cell_residual(const Ctx& c, int i, int j, double Pc, double PW, d
     in.pguess = c.p_ref + Pc;
     in.Qph[0] = c.qph0[x];
     in.Qph[1] = c.qph1[x];
+    in.type = (SPB6G_MG && c.phy.relax) ? (int)c.ctype[x] : CL_P;  // S.type (:695), frozen per step
     ClOut o;
     if (!closure(c.phy, in, o)) return false;
     Gr = (o.pbar - c.p_ref) - Pc;
@@ -1419,6 +1420,48 @@ void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
 }
 
 // ============================================================ final state (:1056-1073) and H_s (:1363-1371)
+// RelaxationActivation (:563-586) for p-pT relaxation (RELAX_LEVEL 1): every cell of the interface
+// zone eps_I <= alpha1 <= 1 - eps_I gets the pT closure for the step (closure_type_of :870-886 with
+// the thermal rate infinite) and U^n is projected on its manifold (project_cell :549-561: the same
+// closure at s = 0 from the conservative state; alpha and the phase energies change, masses,
+// momentum and E do not); a cell whose projection has no solution keeps the p closure.
+#if SPB6G_MG
+__global__ void k_relax_activate(Ctx c, State U) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+        const double a1 = U.v[IA1][x];
+        unsigned char ty = CL_P;
+        if (a1 >= c.phy.eps_i && a1 <= 1.0 - c.phy.eps_i) {
+            const double m1 = U.v[IM1][x], m2 = U.v[IM2][x], mu = U.v[IMU][x], mv = U.v[IMV][x];
+            const double rho = m1 + m2;
+            ClIn in;
+            in.atr[0] = a1; in.atr[1] = 1.0 - a1; in.mtr[0] = m1; in.mtr[1] = m2;
+            in.etr[0] = U.v[IE1][x]; in.etr[1] = U.v[IE2][x];
+            in.s = 0.0;
+            in.rhoeC = U.v[IEN][x] - 0.5 * (mu * mu + mv * mv) / rho;
+            in.pguess = SMAX(p_mix(c.phy, in.atr[0], in.mtr[0], in.mtr[1], in.rhoeC), 1.0);
+            in.Qph[0] = in.Qph[1] = 0.0;
+            in.type = CL_PT;
+            ClOut o;
+            if (closure(c.phy, in, o)) {
+                ty = CL_PT;
+                U.v[IA1][x] = o.a[0];
+                U.v[IE1][x] = o.e[0];
+                U.v[IE2][x] = o.e[1];
+            }
+        }
+        c.ctype[x] = ty;
+    }
+}
+#endif
+void launch_relax_activate(const Ctx& c, cudaStream_t st, State U) {
+#if SPB6G_MG
+    k_relax_activate<<<blocks_for(c.n), TPB, 0, st>>>(c, U);
+    count(c, 1);
+#else
+    spb6g_mg::launch_relax_activate(mg_view(c), st, mg_view(U));
+#endif
+}
+
 SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
     const Geom& g = c.g;
     {

@@ -1,7 +1,8 @@
-// The launchers of the Mie-Grueneisen build of the kernels: the same sources compiled a second
-// time with SPB6G_MG = 1 into namespace spb6g_mg.  The default (stiffened-gas / NASG) launchers
-// of every kernel that evaluates the equations of state forward to them when the configuration
-// has a Mie-Grueneisen phase, so the default kernels carry no Mie-Grueneisen code at all.  The
+// The launchers of the extended-physics build of the kernels: the same sources compiled a second
+// time with SPB6G_MG = 1 into namespace spb6g_mg (Mie-Grueneisen phases, p-pT relaxation).  The
+// default (stiffened-gas / NASG, mechanical relaxation) launchers of every kernel that evaluates
+// the equations of state forward to them when the configuration needs either, so the default
+// kernels carry none of that code.  The
 // two builds' types are the same source, hence the same layout.
 #pragma once
 #include <cuda_runtime.h>
@@ -13,6 +14,10 @@ struct FeatureNorm;
 struct CState {
     const double* v[8];
 };
+struct State {
+    double* v[8];
+};
+void launch_relax_activate(const Ctx& c, cudaStream_t st, State U);
 void launch_flux(const Ctx& c, cudaStream_t st);
 void launch_prep(const Ctx& c, cudaStream_t st);
 void launch_shock_weak(const Ctx& c, cudaStream_t st);
@@ -33,6 +38,11 @@ void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, dou
 namespace spb6g {
 inline const spb6g_mg::Ctx& mg_view(const Ctx& c) { return reinterpret_cast<const spb6g_mg::Ctx&>(c); }
 inline const spb6g_mg::FeatureNorm& mg_view(const FeatureNorm& f) { return reinterpret_cast<const spb6g_mg::FeatureNorm&>(f); }
+inline spb6g_mg::State mg_view(const State& u) {
+    spb6g_mg::State o;
+    for (int k = 0; k < 8; k++) o.v[k] = u.v[k];
+    return o;
+}
 inline spb6g_mg::CState mg_view(const CState& u) {
     spb6g_mg::CState o;
     for (int k = 0; k < 8; k++) o.v[k] = u.v[k];
@@ -42,7 +52,7 @@ inline spb6g_mg::CState mg_view(const CState& u) {
 // First statement of a default launcher: run the Mie-Grueneisen build's launcher instead.
 #define SPB6G_MG_FORWARD(name, ...)                      \
     do {                                                 \
-        if (c.phy.mg) {                                  \
+        if (c.phy.mg || c.phy.relax) {                   \
             spb6g_mg::name(__VA_ARGS__);                 \
             return;                                      \
         }                                                \

@@ -44,7 +44,13 @@ struct Phys {
     int limiter;     // LIMITER, :969
     int rus_local;   // RUS_LOCAL, src/SPB6_PC_IMEX_omp.cpp:93
     int mg;          // a Mie-Grueneisen phase is present (mg_any, :58)
+    int relax;       // RELAX_LEVEL (:39): 0 mechanical relaxation only, 1 p-pT (instantaneous thermal
+                     // relaxation in the interface zone)
+    int pad;
+    double eps_i;    // EPS_I (:40): interface zone eps_I <= alpha1 <= 1 - eps_I
 };
+// Closure types (ClosureType :228) built here: p (mechanical) and pT (instantaneous thermal).
+enum { CL_P = 0, CL_PT = 2 };
 
 // ------------------------------------------------------------ EOS, src/spb6_physics_omp.h:60-111
 // Mie-Grueneisen reference curves pr(rho), pr'(rho), er(rho) (mg_ref :60-69): Cochran-Chan
@@ -153,6 +159,7 @@ SPB6G_DEV double eps_round(const Phys& P, int k, double a, double m) {
 // ------------------------------------------------------------ closure, :229-243, :430-548, :842-866
 struct ClIn {
     double atr[2], mtr[2], etr[2], s, rhoeC, pguess, Qph[2];
+    int type;  // CL_P or CL_PT, frozen per step by the activation
 };
 struct ClOut {
     double a[2], e[2], pbar;
@@ -390,6 +397,113 @@ static __device__ __noinline__ ClMg closure_p_mg(const Phys P, const ClIn in) {
     return res;
 }
 
+// ---- instantaneous thermal relaxation (pT closure, B6.3), built with the extended physics
+// Brent's bracketed root search (brent :183-205): f(a), f(b) of opposite signs.
+template <class Fn>
+SPB6G_DEV bool brent(Fn f, double a, double b, double fa, double fb, double tol, double& root) {
+    if (!(fa * fb <= 0)) return false;
+    if (fa == 0) { root = a; return true; }
+    if (fb == 0) { root = b; return true; }
+    double c = a, fc = fa, d = b - a, e = d;
+    for (int it = 0; it < 200; it++) {
+        if (fb * fc > 0) { c = a; fc = fa; d = b - a; e = d; }
+        if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+        const double tol1 = 2.0 * 1e-16 * fabs(b) + 0.5 * tol, xm = 0.5 * (c - b);
+        if (fabs(xm) <= tol1 || fb == 0) { root = b; return true; }
+        if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+            double s = fb / fa, p, q;
+            if (a == c) { p = 2 * xm * s; q = 1 - s; }
+            else {
+                const double qq = fa / fc, r = fb / fc;
+                p = s * (2 * xm * qq * (qq - r) - (b - a) * (r - 1));
+                q = (qq - 1) * (r - 1) * (s - 1);
+            }
+            if (p > 0) q = -q;
+            p = fabs(p);
+            if (2 * p < SMIN(3 * xm * q - fabs(tol1 * q), fabs(e * q))) { e = d; d = p / q; }
+            else { d = xm; e = d; }
+        } else { d = xm; e = d; }
+        a = b; fa = fb;
+        b += (fabs(d) > tol1) ? d : (xm > 0 ? tol1 : -tol1);
+        fb = f(b);
+        if (!isfinite(fb)) return false;
+    }
+    root = b;
+    return true;
+}
+// Root of f on (plo, inf) through y = ln(p - plo): a sign change bracketed from the guess, then
+// Brent (root_above :207-225); f is positive (or undefined) just above plo and negative at inf.
+template <class Fn>
+SPB6G_DEV bool root_above(Fn f, double plo, double guess, double& root) {
+    auto F = [&](double y) { return f(plo + exp(y)); };
+    const double y0 = log(SMAX(guess - plo, 1e-6 * (fabs(plo) + 1.0) + 1e-12));
+    const double f0 = F(y0);
+    if (f0 == 0.0) { root = plo + exp(y0); return true; }
+    double ya = y0, yb = y0, fa = f0, fb = f0, st = 0.1;
+    if (!isfinite(f0)) {  // upwards to a feasible point
+        for (int k = 0; k < 200 && !isfinite(fb); k++) { yb += 1.0; fb = F(yb); }
+        if (!isfinite(fb)) return false;
+        ya = yb; fa = fb;
+    }
+    if (fa > 0) {
+        for (int k = 0; k < 400 && !(fb < 0); k++) {
+            ya = yb; fa = fb; yb += st; st *= 1.6;
+            fb = F(yb);
+            if (!isfinite(fb)) return false;
+        }
+    } else {
+        for (int k = 0; k < 400 && !(fa > 0); k++) {
+            yb = ya; fb = fa; ya -= st; st *= 1.6;
+            fa = F(ya);
+            if (!isfinite(fa)) {
+                ya = yb; fa = fb;
+                for (int q = 0; q < 60; q++) {
+                    const double ym = ya - st / ldexp(1.0, q + 1), fm = F(ym);
+                    if (isfinite(fm) && fm > 0) { ya = ym; fa = fm; break; }
+                }
+                break;
+            }
+        }
+    }
+    if (fa == 0.0) { root = plo + exp(ya); return true; }
+    if (fb == 0.0) { root = plo + exp(yb); return true; }
+    if (!(fa > 0 && fb < 0)) return false;
+    double y;
+    if (!brent(F, ya, yb, fa, fb, 1e-15, y)) return false;
+    root = plo + exp(y);
+    return true;
+}
+// pT closure (closure_pT :716-726): common p and T with T(p) explicit from the energy and
+// sum_k m_k v_k(p, T) = 1 (SG / NASG v_pT, e_pT :80-81).
+static __device__ __noinline__ ClMg closure_pT(const Phys P, double m0, double m1, double rhoeC, double pguess) {
+    ClMg res;
+    res.ok = 0;
+    const double m[2] = {m0, m1};
+    const double Eth = rhoeC - m[0] * P.ph[0].q - m[1] * P.ph[1].q;
+    if (!(Eth > 0)) return res;
+    auto Tof = [&](double p) {
+        double d = 0;
+        for (int k = 0; k < 2; k++) d += m[k] * P.ph[k].cv * (p + P.ph[k].g * P.ph[k].pi) / (p + P.ph[k].pi);
+        return Eth / d;
+    };
+    auto v_pT = [&](int k, double p, double T) { return (P.ph[k].g - 1.0) * P.ph[k].cv * T / (p + P.ph[k].pi) + P.ph[k].b; };
+    auto e_pT = [&](int k, double p, double T) { return P.ph[k].cv * T * (p + P.ph[k].g * P.ph[k].pi) / (p + P.ph[k].pi) + P.ph[k].q; };
+    auto Phi = [&](double p) {
+        const double T = Tof(p);
+        return m[0] * v_pT(0, p, T) + m[1] * v_pT(1, p, T) - 1.0;
+    };
+    double p;
+    if (!root_above(Phi, SMAX(-P.ph[0].pi, -P.ph[1].pi), pguess, p)) return res;
+    const double T = Tof(p);
+    for (int k = 0; k < 2; k++) {
+        res.o.a[k] = m[k] * v_pT(k, p, T);
+        res.o.e[k] = m[k] * e_pT(k, p, T);
+    }
+    res.o.pbar = p;
+    res.ok = T > 0;
+    return res;
+}
+
 // Bracketed safeguarded Newton on Phi (closure_p, :472-548), preceded by the
 // admissibility checks of closure() (:842-866).  At most 400 iterations.
 SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
@@ -397,6 +511,12 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
     for (int k = 0; k < 2; k++)
         if (!(in.atr[k] > 0) || !(in.mtr[k] > 0) || !isfinite(in.etr[k])) return false;
     if (!isfinite(in.rhoeC) || !isfinite(in.s)) return false;
+    if (SPB6G_MG && in.type != CL_P) {  // the thermal closure; Mie-Grueneisen phases relax mechanically only (:846)
+        if (P.mg) return false;
+        const ClMg r = closure_pT(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
+        o = r.o;
+        return r.ok && isfinite(o.pbar);
+    }
     if (SPB6G_MG && P.mg) {
         const ClMg r = closure_p_mg(P, in);
         o = r.o;
@@ -442,7 +562,7 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
 }
 // Round-off floor of the closure pressure (SPB6_PC_IMEX_omp.cpp:657-664, via p_coef :453-464).
 SPB6G_DEV double closure_roundoff(const Phys& P, const ClIn& in, double p) {
-    if (SPB6G_MG && P.mg) return 0.0;  // no floor with a Mie-Grueneisen phase (:658)
+    if (SPB6G_MG && (P.mg || in.type != CL_P)) return 0.0;  // floor of the p-closure without MG phases only (closure_roundoff :657-658)
     if (!(in.mtr[0] + in.mtr[1] > 0)) return 0.0;
     const double D0 = in.rhoeC - in.etr[0] - in.etr[1];
     // defect_split (:438-449) at delta = D0 + p s

@@ -454,6 +454,11 @@ int do_step(spb6g_solver* s) {
         const int rk = first_order ? 1 : cf.rk;
         if (rk == 1) s->stats.rk1++;
         set_tab(rk, Ae, Ai);
+        if (cf.relax) {  // RelaxationActivation at every attempt (:1333): closure types, U^n projected
+            State u;
+            for (int k = 0; k < NV; k++) u.v[k] = s->U[k];
+            launch_relax_activate(s->c, s->st, u);
+        }
         if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
         bool ok = true;
         for (int rks = 0; rks < rk && ok; rks++) {
@@ -491,6 +496,7 @@ void spb6g_default_config(spb6g_config* cfg) {
     cfg->x0 = 0; cfg->x1 = 1; cfg->y0 = 0; cfg->y1 = 1;
     cfg->gamma[0] = 4.4; cfg->pinf[0] = 6e8; cfg->gamma[1] = 1.4; cfg->pinf[1] = 0;
     cfg->cv[0] = cfg->cv[1] = 1000.0;
+    cfg->eps_i = 1e-4;
     cfg->rk = 2; cfg->cfl = 0.2; cfg->cfl_ac = 0.4; cfg->ramp = 1; cfg->rus_local = 1; cfg->limiter = 1;
     cfg->newton_tol = 1e-13; cfg->newton_iter = 60; cfg->bicg_tol = 1e-13; cfg->bicg_iter = 4000;
     cfg->tend = 240e-6;
@@ -510,6 +516,9 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
     }
+    if (cfg->relax < 0 || cfg->relax > 3) return SPB6G_BAD_ARG;
+    if (cfg->relax > 1 || (cfg->relax && (cfg->kind[0] || cfg->kind[1]))) return SPB6G_UNSUPPORTED;
+    if (cfg->relax && !(cfg->eps_i >= 0 && cfg->eps_i < 0.5)) return SPB6G_BAD_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return SPB6G_NO_DEVICE;
@@ -561,6 +570,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.fxd = A(10 * nfx); c.fyd = A(10 * nfy);
     c.strong_list = (int*)A(n / 2 + 1);
     c.smask = (unsigned char*)A(n / 8 + 1);
+    c.ctype = cfg->relax ? (unsigned char*)A(n / 8 + 1) : nullptr;  // n bytes
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
     c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
     c.prec = cfg->precision ? 1 : 0;
@@ -736,6 +746,11 @@ int spb6g_advance(spb6g_solver* s, int nsteps) {
     // the profile main() writes at the end of the run or when a step fails (:1326, :1379, :1388)
     const bool failed = rc == SPB6G_STEP_FAILED || rc == SPB6G_DT_UNDERFLOW;
     if (!s->out_file.empty() && (failed || (rc == SPB6G_OK && !(s->t < s->cfg.tend * (1 - 1e-12))))) {
+        if (rc == SPB6G_OK && s->cfg.relax) {  // the activation projection before the final profile (:1388)
+            State u;
+            for (int k = 0; k < NV; k++) u.v[k] = s->U[k];
+            launch_relax_activate(s->c, s->st, u);
+        }
         const int r = spb6g_write_profile(s, s->out_file.c_str(), s->prec);
         if (r != SPB6G_OK && rc == SPB6G_OK) rc = r;
     }
@@ -1037,7 +1052,7 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     *out = nullptr;
     for (int i = 0; i < count; i++)
         if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
-            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0)  // the batched kernel: stiffened gas / NASG phases
+            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0)  // the batched kernel: SG / NASG, p
             return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;

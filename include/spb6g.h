@@ -76,8 +76,12 @@ typedef struct {
                                        2 JWL pr = c1 exp(-e1 rr / rho) + c2 exp(-e2 rr / rho), er - e0
                                        (Phase.kind, physics :51-69); MG phases use only G, rr, c1, c2,
                                        e1, e2, e0 and cv (temperature output) */
-    int32_t reserved[4];
+    int32_t relax;                  /* RELAX_LEVEL (physics :39): 0 mechanical relaxation; 1 p-pT, instantaneous
+                                       thermal relaxation in the interface zone (2 and 3, chemical relaxation,
+                                       and finite rates are not built: SPB6G_UNSUPPORTED) */
+    int32_t reserved[3];
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
+    double eps_i;                   /* EPS_I (physics :40): interface zone eps_I <= alpha1 <= 1 - eps_I (1e-4) */
 } spb6g_config;
 
 /* Run statistics: the counters of the reference's stats line (:98-99, :1425). */

@@ -90,9 +90,13 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
         PH[k].G = c.mg_G[k]; PH[k].rr = c.mg_rr[k]; PH[k].c1 = c.mg_c1[k]; PH[k].c2 = c.mg_c2[k];
         PH[k].e1 = c.mg_e1[k]; PH[k].e2 = c.mg_e2[k]; PH[k].e0 = c.mg_e0[k];
     }
-    RELAX_LEVEL = 0;
-    theta_rate = 0.0;
-    nu_rate = 0.0;
+    // relaxation level and interface zone; the rates as main() defaults them (:1233-1234)
+    RELAX_LEVEL = c.relax;
+    EPS_I = c.eps_i;
+    mu_rate = INF;
+    theta_rate = RELAX_LEVEL >= 1 ? INF : 0.0;
+    nu_rate = (RELAX_LEVEL == 2 || RELAX_LEVEL == 3) ? INF : 0.0;
+    STEP_TYPE.clear();
     SHARE_MODE = c.share_mode;
     RKs = c.rk;
     CFL = c.cfl;
@@ -174,6 +178,7 @@ int step(Harness& H) {
         const int rk = first_order ? 1 : RKs;
         if (rk == 1) st_rk1++;
         set_tab(H, rk);
+        if (RELAX_LEVEL > 0) RelaxationActivation(u_con);  // :1333
         copy(u_con_n, u_con);
         H.Pst = H.P;
         bool ok = true;

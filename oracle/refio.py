@@ -31,7 +31,8 @@ CASE_DT = np.dtype([
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
     ("budget_s", "<f8"), ("warmup", "<i4"), ("inject_qph", "<i4"),
     ("kind", "<i4", 2), ("mg_G", "<f8", 2), ("mg_rr", "<f8", 2), ("mg_c1", "<f8", 2), ("mg_c2", "<f8", 2),
-    ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2),
+    ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2), ("relax", "<i4"), ("pad2", "<i4"),
+    ("eps_i", "<f8"),
 ])
 MG_KEYS = ("G", "rr", "c1", "c2", "e1", "e2", "e0")
 RESULT_DT = np.dtype([
@@ -45,7 +46,7 @@ RESULT_DT = np.dtype([
 def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, warmup: int = 0,
                 budget_s: float = 0.0) -> np.ndarray:
     r = np.zeros((), CASE_DT)
-    r["magic"], r["version"] = MAGIC, 2
+    r["magic"], r["version"] = MAGIC, 3
     for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
         r[k] = int(cfg[k])
     r["bc"] = cfg["bc"]
@@ -59,6 +60,8 @@ def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int
     r["kind"] = [int(cfg["phases"][k].get("kind", 0)) for k in range(2)]
     for f in MG_KEYS:
         r["mg_" + f] = [float(cfg["phases"][k].get(f, 0.0)) for k in range(2)]
+    r["relax"] = int(cfg.get("relax", 0))
+    r["eps_i"] = float(cfg.get("eps_i", 1e-4))
     return r
 
 

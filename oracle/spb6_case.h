@@ -20,7 +20,7 @@
 #include <stdint.h>
 
 #define SPB6_CASE_MAGIC 0x36425053u /* "SPB6" */
-#define SPB6_CASE_VERSION 2
+#define SPB6_CASE_VERSION 3
 
 enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2 };
 enum { SPB6_BC_TRANS = 0, SPB6_BC_WALL = 1, SPB6_BC_PERIODIC = 2, SPB6_BC_PRES = 3 };
@@ -43,6 +43,8 @@ typedef struct {
     int32_t kind[2];    /* 0 SG / NASG, 1 Cochran-Chan, 2 JWL (reference harness only; the C restatement
                            runs SG / NASG phases) */
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
+    int32_t relax, pad2;  /* RELAX_LEVEL (reference harness only; the C restatement has relax 0) */
+    double eps_i;
 } spb6_case;
 
 typedef struct {

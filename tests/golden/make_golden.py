@@ -99,6 +99,11 @@ CASES = {
     "jwl_N200_20steps": (lambda: cases.reference_case(61, 200), "steps", 20, {}),
     "undex120x80_3steps": (lambda: cases.underwater_explosion(120, 80), "steps", 3,
                            {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # p-pT relaxation: instantaneous thermal relaxation in the interface zone (RELAX_LEVEL 1;
+    # closure_type_of :870-886, closure_pT :716-726, RelaxationActivation :563-586)
+    "tube_relax_N200_20steps": (lambda: dict(_tube(200), relax=1, eps_i=1e-4), "steps", 20, {}),
+    "bubble_relax32_3steps": (lambda: dict(_bubble(32), relax=1, eps_i=1e-4), "steps", 3,
+                              {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "bubble_outlet32_3steps": (lambda: _bc(_bubble(32), (PRES, PRES, W, W), bcp=(1.2e7, 0.8e7, 0, 0)), "steps", 3,
                                {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
 }
@@ -109,6 +114,7 @@ MAIN_RUNS = {
     "case5_N100": (5, 100, ["snap=8e-5,1.6e-4", "probe=0.6,0.5"]),
     "case87_N200": (87, 200, ["snap=1e-4", "probe=0.5,0.5"]),
     "case60_N100": (60, 100, ["snap=3e-5", "probe=0.6,0.5"]),  # Mie-Grueneisen (Cochran-Chan) phases
+    "case5_relax_N100": (5, 100, ["relax=1", "snap=1.2e-4", "probe=0.75,0.5"]),  # p-pT relaxation
 }
 
 

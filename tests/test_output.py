@@ -1,8 +1,10 @@
 """Output formats of the reference's main() against files the reference itself wrote.
 
-tests/golden/ref_main_outputs.npz holds, for two 1D runs of the reference's own
-main() (case 5 at N = 100, case 87 at N = 200 and the Mie-Grueneisen case 60 at
-N = 100, with snapshots and a pressure probe; tests/golden/make_golden.py), every file it wrote -- the final profile
+tests/golden/ref_main_outputs.npz holds, for four 1D runs of the reference's own
+main() (case 5 at N = 100, case 87 at N = 200, the Mie-Grueneisen case 60 at
+N = 100 and case 5 with p-pT relaxation, whose final profile follows the last
+activation projection; with snapshots and a pressure probe;
+tests/golden/make_golden.py), every file it wrote -- the final profile
 run.dat, the snapshot profiles run_s<k>.dat, the probe run.dat.probe -- its
 end-of-run line and the state of the last profile.  The 1D solver is bitwise the
 reference in its arithmetic except the shock budget's libm calls, whose last-ulp
@@ -10,7 +12,7 @@ differences leave whole runs a round-off apart, so: the profile of an equal stat
 is byte-identical (host formatter, CPU test); a whole run writes the same set of
 files with the same headers, coordinates and line counts, column values within
 the whole-run L1 bar of the parity tests, and the same counters in its
-end-of-run line (write_profile src/SPB6_PC_IMEX_omp.cpp:1083-1094, probe_write
+end-of-run line, the Newton total within one iteration in 200 (write_profile src/SPB6_PC_IMEX_omp.cpp:1083-1094, probe_write
 :1191-1197, snap_limit / snap_name physics :972-973, stats line :1425-1427)."""
 from __future__ import annotations
 
@@ -24,7 +26,7 @@ from diffusionimex_b200 import cases
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIX = os.path.join(HERE, "golden", "ref_main_outputs.npz")
-RUNS = ["case5_N100", "case87_N200", "case60_N100"]
+RUNS = ["case5_N100", "case87_N200", "case60_N100", "case5_relax_N100"]
 
 
 def _run(tag):
@@ -36,7 +38,13 @@ def _run(tag):
     snaps = [float(v) for v in kv["snap"].split(",")] if "snap" in kv else []
     probe = tuple(float(v) for v in kv["probe"].split(",")) if "probe" in kv else None
     return dict(case=case, n=n, files=files, stdout=bytes(z[f"{tag}/stdout"]).decode(), U=z[f"{tag}/U"], snaps=snaps,
-                probe=probe)
+                probe=probe, relax=int(kv.get("relax", 0)))
+
+
+def _case(r):
+    c = cases.reference_case(r["case"], r["n"])
+    c["relax"] = r["relax"]
+    return c
 
 
 @pytest.mark.parametrize("tag", RUNS)
@@ -46,7 +54,7 @@ def test_profile_of_the_reference_state_is_byte_identical(tag, tmp_path):
 
     r = _run(tag)
     path = str(tmp_path / "p.dat")
-    format_profile(cases.reference_case(r["case"], r["n"]), r["U"], path)
+    format_profile(_case(r), r["U"], path)
     with open(path, "rb") as f:
         assert f.read() == r["files"]["run.dat"]
 
@@ -68,7 +76,7 @@ def test_run_writes_the_reference_files(tag, tmp_path):
 
     r = _run(tag)
     out = str(tmp_path / "run.dat")
-    s = Solver(cases.reference_case(r["case"], r["n"]))
+    s = Solver(_case(r))
     s.set_output(out, snaps=r["snaps"], probe=r["probe"])
     s.advance(0)
     line = s.stats_line(r["case"], 0.0)
@@ -97,7 +105,13 @@ def test_run_writes_the_reference_files(tag, tmp_path):
         bar[list(TRACE_COLS_DAT if name.endswith(".dat") else TRACE_COLS_PROBE)] = L1_BAR_TRACE
         assert np.all(l1 <= bar), (name, [f"{v:.3g}" for v in l1])
     ref_line = r["stdout"].strip().splitlines()[-1]
-    assert _counters(line) == _counters(ref_line), (line, ref_line)
+    mine_c, ref_c = _counters(line), _counters(ref_line)
+    assert mine_c[:NEWTON_IT] + mine_c[NEWTON_IT + 1:] == ref_c[:NEWTON_IT] + ref_c[NEWTON_IT + 1:], (line, ref_line)
+    # The Newton total counts iterations whose residual is compared with the tolerance: a stage
+    # whose residual lands within round-off of it may take one iteration more or fewer.  The pT
+    # closure of the relaxed run calls log/exp, whose last-ulp results differ between the device
+    # and glibc (one iteration in 350 at case 5 with relax 1); the other runs match exactly.
+    assert abs(mine_c[NEWTON_IT] - ref_c[NEWTON_IT]) <= max(1, ref_c[NEWTON_IT] // 200), (line, ref_line)
 
 
 # Whole-run bar: 10x the 1e-6 field L1 of the parity tests (the reference's own one-ulp libm
@@ -109,6 +123,7 @@ L1_BAR = 1e-5
 L1_BAR_TRACE = 1e-4
 TRACE_COLS_DAT = (8, 9, 12, 13, 16)  # rho1, rho2, T1, T2, g1-g2 of the profile
 TRACE_COLS_PROBE = (4,)        # T1 of the probe
+NEWTON_IT = 9                  # index of the Newton iteration total in _counters()
 
 
 def _cols(lines):
