@@ -67,7 +67,8 @@ def parse():
     p.add_argument("--workload", default="bubbles1024",
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
-                        "undex361x200 (Mie-Grueneisen phases), mlp (learned warm-start network)")
+                        "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
+                        "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -94,6 +95,10 @@ def make_workload(name: str):
         c["workload"] = c.get("workload", name) + " (precision form)"
     elif name == "undex361x200":
         c = cases.underwater_explosion(361, 200)
+    elif name == "bubbles1024-relax":
+        c = cases.bubble_field(1024, seed=0, nbub=8)
+        c.update(relax=1, eps_i=1e-4)
+        c["workload"] += ", p-pT relaxation in the interface zone (relax 1, eps_I 1e-4)"
     elif name == "riemann512":
         return {"batch": cases.riemann_batch(count=512, seed=0), "workload": "512 1D Riemann problems, 256-4096 cells"}
     elif name == "mlp":
@@ -333,6 +338,7 @@ def run_mlp(args, case, rank: int, world: int, local_rank: int, dist):
 def workload_config(c: dict, name: str) -> dict:
     return {"workload": c.get("workload", name), "nx": c["nx"], "ny": c["ny"], "fp": "fp64",
             "newton_tol": c["newton_tol"], "bicg_tol": c["bicg_tol"], "cfl": c["cfl"], "seed": c.get("seed", 0),
+            "relax": c.get("relax", 0),
             "l2": "working set > L2 (no flush needed)"}
 
 

@@ -422,7 +422,7 @@ size_t flux_tile_bytes_1d(int tx) {
 }
 
 void launch_flux(const Ctx& c, cudaStream_t st) {
-    SPB6G_MG_FORWARD(launch_flux, mg_view(c), st);
+    SPB6G_MG_FORWARD_EOS(launch_flux, mg_view(c), st);
     if (c.prec) {  // precision form: reconstruction and fluxes in FP32
         if (c.g.ny > 1) launch_tile<float, 32, 8, true>(c, st);
         else launch_tile<float, 256, 1, false>(c, st);

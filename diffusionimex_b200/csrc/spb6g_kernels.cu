@@ -180,7 +180,7 @@ __global__ void k_prep_fy(Ctx c) {
     }
 }
 void launch_prep(const Ctx& c, cudaStream_t st) {
-    SPB6G_MG_FORWARD(launch_prep, mg_view(c), st);
+    SPB6G_MG_FORWARD_EOS(launch_prep, mg_view(c), st);
     const long pad = (long)(c.g.nx + 4) * (c.g.ny > 1 ? c.g.ny + 4 : 1);
     k_prep_cell<<<blocks_for(pad), TPB, 0, st>>>(c);
     k_prep_fx<<<blocks_for((long)(c.g.nx + 1) * c.g.ny), TPB, 0, st>>>(c);
@@ -256,12 +256,12 @@ __global__ void k_shock_strong(Ctx c) {
 // Weak-shock cells are finished in place; strong-shock cells (Kapila profile
 // shooting, 6-9 RK45 integrations each) go through a compacted worklist.
 void launch_shock_weak(const Ctx& c, cudaStream_t st) {
-    SPB6G_MG_FORWARD(launch_shock_weak, mg_view(c), st);
+    SPB6G_MG_FORWARD_EOS(launch_shock_weak, mg_view(c), st);
     k_shock_weak<<<blocks_for(c.n), TPB, 0, st>>>(c);
     count(c, 1);
 }
 void launch_shock_strong(const Ctx& c, cudaStream_t st) {
-    SPB6G_MG_FORWARD(launch_shock_strong, mg_view(c), st);
+    SPB6G_MG_FORWARD_EOS(launch_shock_strong, mg_view(c), st);
     k_shock_strong<<<(c.n + 31) / 32, 32, 0, st>>>(c);
     count(c, 1);
 }
@@ -1524,7 +1524,7 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_caldt(Ctx c, CState U, int a
     }
 }
 void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic) {
-    SPB6G_MG_FORWARD(launch_caldt, mg_view(c), st, mg_view(U), acoustic);
+    SPB6G_MG_FORWARD_EOS(launch_caldt, mg_view(c), st, mg_view(U), acoustic);
     k_caldt<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U, acoustic);
     count(c, 1);
 }
@@ -1540,7 +1540,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_pbar_min(Ctx c, CState U) {
     if (grid_fold<RedMin, 1>(m, c.partials, &c.counters[9], tot) && threadIdx.x == 0) c.ns->pmin = tot[0];
 }
 void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U) {
-    SPB6G_MG_FORWARD(launch_pbar_min, mg_view(c), st, mg_view(U));
+    SPB6G_MG_FORWARD_EOS(launch_pbar_min, mg_view(c), st, mg_view(U));
     k_pbar_min<<<red_blocks(c.n), RED_THREADS, 0, st>>>(c, U);
     count(c, 1);
 }
@@ -1553,7 +1553,7 @@ __global__ void k_pbar_init(Ctx c, CState U, double p_ref, double* P) {
     }
 }
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P) {
-    SPB6G_MG_FORWARD(launch_pbar_init, mg_view(c), st, mg_view(U), p_ref, P);
+    SPB6G_MG_FORWARD_EOS(launch_pbar_init, mg_view(c), st, mg_view(U), p_ref, P);
     k_pbar_init<<<blocks_for(c.n), TPB, 0, st>>>(c, U, p_ref, P);
     count(c, 1);
 }

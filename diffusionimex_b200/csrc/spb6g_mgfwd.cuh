@@ -49,7 +49,12 @@ inline spb6g_mg::CState mg_view(const CState& u) {
     return o;
 }
 }  // namespace spb6g
-// First statement of a default launcher: run the Mie-Grueneisen build's launcher instead.
+// First statement of a default launcher: run the extended build's launcher instead.
+// SPB6G_MG_FORWARD: kernels that evaluate the closure (its type is per cell under p-pT
+// relaxation) and so need the extended build for a Mie-Grueneisen phase or for relax > 0.
+// SPB6G_MG_FORWARD_EOS: kernels that evaluate the equations of state but never the closure;
+// with stiffened-gas / NASG phases they are the same in both builds, so only a
+// Mie-Grueneisen phase sends them to the extended build.
 #define SPB6G_MG_FORWARD(name, ...)                      \
     do {                                                 \
         if (c.phy.mg || c.phy.relax) {                   \
@@ -57,8 +62,18 @@ inline spb6g_mg::CState mg_view(const CState& u) {
             return;                                      \
         }                                                \
     } while (0)
+#define SPB6G_MG_FORWARD_EOS(name, ...)                  \
+    do {                                                 \
+        if (c.phy.mg) {                                  \
+            spb6g_mg::name(__VA_ARGS__);                 \
+            return;                                      \
+        }                                                \
+    } while (0)
 #else
 #define SPB6G_MG_FORWARD(name, ...) \
     do {                            \
+    } while (0)
+#define SPB6G_MG_FORWARD_EOS(name, ...) \
+    do {                                \
     } while (0)
 #endif
