@@ -68,6 +68,7 @@ def parse():
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
                         "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
+                        "<2D workload>-rus0 (grid-wide Rusanov speed), "
                         "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -89,6 +90,10 @@ def make_workload(name: str):
         c = cases.lowmach_bubbles(2048, seed=0)
     elif name == "shock2048x1024":
         c = cases.shock_bubble(2048, 1024)
+    elif name.endswith("-rus0"):  # the same workload with the grid-wide Rusanov speed (rus_local = 0)
+        c = make_workload(name[:-len("-rus0")])
+        c["rus_local"] = 0
+        c["workload"] = c.get("workload", name) + ", grid-wide Rusanov speed (rus 0)"
     elif name in ("bubbles2048-mixed", "shock2048x1024-mixed"):
         c = make_workload(name[:-len("-mixed")])
         c["precision"] = 1
@@ -338,7 +343,7 @@ def run_mlp(args, case, rank: int, world: int, local_rank: int, dist):
 def workload_config(c: dict, name: str) -> dict:
     return {"workload": c.get("workload", name), "nx": c["nx"], "ny": c["ny"], "fp": "fp64",
             "newton_tol": c["newton_tol"], "bicg_tol": c["bicg_tol"], "cfl": c["cfl"], "seed": c.get("seed", 0),
-            "relax": c.get("relax", 0),
+            "relax": c.get("relax", 0), "rus_local": c.get("rus_local", 1),
             "l2": "working set > L2 (no flush needed)"}
 
 

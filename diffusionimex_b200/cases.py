@@ -108,8 +108,10 @@ def cell_centres(cfg: dict):
 # --------------------------------------------------------------------------------------------
 def reference_case(case: int, nx: int | None = None) -> dict:
     """A subset of the reference's 1D cases: 4 (interface advection), 5 (SPB 4.3.1 water-air),
-    80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes 60 (SPB 4.2
-    nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG water)."""
+    12 and 13 (SPB 5.1 / 5.2 epoxy-spinel mixture; 13 takes the grid-wide Rusanov speed,
+    rus_local = 0), 80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes 60
+    (SPB 4.2 nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG
+    water)."""
     c = default_settings()
     air, water = dict(AIR_SG), dict(WATER_SG)
     if case == 4:
@@ -125,6 +127,13 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         c.update(phases=[water, air], nx=1000, tend=0.25 if case == 86 else 241e-6)
     elif case == 88:
         c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=1000, tend=30e-6)
+    elif case in (12, 13):  # test_setup physics :1029-1032
+        c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=500,
+                 tend=80e-6 if case == 12 else 34e-6)
+        if case == 12:
+            c["cfl"] = 0.05
+        else:
+            c["rus_local"] = 0
     elif case == 60:  # SPB 4.2 nitromethane shock tube, Cochran-Chan for both phases
         c.update(phases=[dict(NITROMETHANE_CC), dict(NITROMETHANE_CC)], nx=500, tend=67e-6)
     elif case == 61:  # Pelanti 8.1.1 detonation gas (JWL) - water (NASG) shock tube on [-10, 10] m
@@ -162,8 +171,8 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         L = x < (0.25 if adv else 0.7)
         p = np.full_like(x, 1e5) if adv else np.where(L, 1e9, 1e5)
         U = prim2cell(ph, np.where(L, 1 - 1e-7, 1e-7), 1000.0, 0.01 if adv else 50.0, 1.0 if adv else 0.0, 0.0, p, p)
-    elif case == 88:
-        p = np.where(x < 0.6, 1e10, 1e5)
+    elif case in (12, 13, 88):
+        p = np.where(x < 0.6, 2e11 if case == 13 else 1e10, 1e5)
         U = prim2cell(ph, np.full_like(x, 0.5954), 1185.0, 3622.0, 0.0, 0.0, p, p)
     elif case == 60:
         L = x < 0.5

@@ -31,6 +31,7 @@ struct NewtonScalars {
     double rate_x, rate_y;
     double E, sumb, bb;  // Jacobian sums for the BiCGStab set-up
     double tmax[2];      // phase temperature maxima of the last final state (st_Tmax)
+    unsigned long long rus_v[2];  // RUS_LOCAL = 0: bits of the grid-wide speeds vx_max, vy_max (:92)
     int fail;            // a residual / closure evaluation failed
     int err;             // inadmissible state in the explicit part or stage prep
     int nstrong;         // strong-shock worklist length
@@ -142,7 +143,7 @@ int red_blocks(int n, int threads = RED_THREADS);
 void launch_flux(const Ctx& c, cudaStream_t st);
 // the fused explicit kernel's tile as a block-level device function (spb6g_flux.cu), and the
 // shared-memory bytes of a 1D tile of width tx (128 or 256)
-template <class R, int TX, int TY, bool TWO_D>
+template <class R, int TX, int TY, bool TWO_D, bool SPEED = false>
 __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_bytes, int tid, int nth);
 size_t flux_tile_bytes_1d(int tx);
 void launch_prep(const Ctx& c, cudaStream_t st);

@@ -174,23 +174,34 @@ SPB6G_DEV void face_value(const R* Ua, const R* Uc, const R* Ub, R vcu, R vcv, R
 }
 
 // Rusanov flux (RusanovC_x/y :237-259); returns the normal face-state velocities, which are
-// also the terms of the face velocity ube (Update :283-294).
+// also the terms of the face velocity ube (Update :283-294).  The dissipation speed is the face's
+// max(|vL|, |vR|) (RUS_LOCAL = 1) or, for aglob >= 0, the grid-wide maximum aglob (RUS_LOCAL = 0).
 template <class R>
-SPB6G_DEV void rusanov_flux(const R* QL, const R* QR, int d, R* flux, R& vL, R& vR) {
+SPB6G_DEV void rusanov_flux(const R* QL, const R* QR, int d, R aglob, R* flux, R& vL, R& vR) {
     const int km = d == 0 ? IMU : IMV;
     vL = QL[km] / (QL[IM1] + QL[IM2]);
     vR = QR[km] / (QR[IM1] + QR[IM2]);
-    const R a = SMAX(fabs(vL), fabs(vR));
+    const R a = aglob >= R(0) ? aglob : SMAX(fabs(vL), fabs(vR));
 #pragma unroll
     for (int k = 0; k < NV; k++) flux[k] = R(0.5) * (QL[k] * vL + QR[k] * vR) - R(0.5) * a * (QR[k] - QL[k]);
 }
 
 }  // namespace
 
+// Non-negative doubles order as their bit patterns: the grid-wide maxima are reduced with an
+// integer atomicMax on the bits.
+SPB6G_DEV void atomic_max_nonneg(unsigned long long* dst, double v) {
+    atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+}
+
 // One TX x TY tile (tile coordinates bx, by) computed by `nth` threads of a block
 // (thread index tid); `smem_bytes` holds FluxTile<...>::BYTES.  Used by k_flux
 // (one tile per block) and by the batched driver (a block walks its instance's tiles).
-template <class R, int TX, int TY, bool TWO_D>
+// SPEED = true is the pre-pass of RUS_LOCAL = 0: the same reconstruction and face states,
+// reduced to the grid-wide dissipation speeds a_x, a_y of Update :266-298 (max of |u|, |v| over
+// the interior cells of Qe, then over the normal velocities of every face state) in
+// c.ns->rus_v; it writes nothing else.
+template <class R, int TX, int TY, bool TWO_D, bool SPEED>
 __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_bytes, int tid, int nth) {
     using T = FluxTile<R, TX, TY, TWO_D>;
     constexpr bool MIXED = sizeof(R) != sizeof(double);
@@ -217,6 +228,8 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
         return gi >= -2 && gi <= g.nx + 1 && (TWO_D ? (gj >= -2 && gj <= g.ny + 1) : true);
     };
 
+    double smax_x = 0.0, smax_y = 0.0;  // SPEED: this thread's maxima
+
     // 1. Qe of the tile and its halo; per-cell scales
     for (int t = tid; t < NLX * NLY; t += nth) {
         const int lx = t % NLX, ly = t / NLX;
@@ -226,6 +239,11 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
         load_qe(c, gi, gj, q);
 #pragma unroll
         for (int k = 0; k < NV; k++) Q(k, ly, lx) = (R)q[k];
+        if (SPEED && gi >= i0 && gi < i0 + TX && gi < g.nx && (!TWO_D || (gj >= j0 && gj < j0 + TY && gj < g.ny))) {
+            const double rho = q[IM1] + q[IM2];
+            smax_x = fmax(smax_x, fabs(q[IMU] / rho));
+            smax_y = fmax(smax_y, fabs(q[IMV] / rho));
+        }
         double vs, es;
         scales_of(c.phy, q, vs, es);
         VS[ly * NLX + lx] = (R)vs;
@@ -265,7 +283,7 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
         RX[(1 * TY + ry) * NRX + rx] = slu;
         RX[(2 * TY + ry) * NRX + rx] = slv;
         const bool own = (gi >= i0 && gi < i0 + TX) || gi == -1 || gi == g.nx;
-        if (own) c.phis_x[rxi(g, gi, gj)] = (double)phis;
+        if (own && !SPEED) c.phis_x[rxi(g, gi, gj)] = (double)phis;
     }
     if (TWO_D) {
         for (int t = tid; t < TX * NRY; t += nth) {
@@ -285,13 +303,18 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
             RY[(1 * NRY + ry) * TX + rx] = slu;
             RY[(2 * NRY + ry) * TX + rx] = slv;
             const bool own = (gj >= j0 && gj < j0 + TY) || gj == -1 || gj == g.ny;
-            if (own) c.phis_y[ryi(g, gi, gj)] = (double)phis;
+            if (own && !SPEED) c.phis_y[ryi(g, gi, gj)] = (double)phis;
         }
     }
     __syncthreads();
 
     // 3. face fluxes, face velocities ube and donors, once per face
     const size_t nfx = (size_t)(g.nx + 1) * g.ny, nfy = (size_t)g.nx * (g.ny + 1);
+    R ax = R(-1), ay = R(-1);  // local dissipation speeds unless RUS_LOCAL = 0
+    if (!SPEED && !c.phy.rus_local) {
+        ax = (R)__longlong_as_double((long long)c.ns->rus_v[0]);
+        ay = (R)__longlong_as_double((long long)c.ns->rus_v[1]);
+    }
     for (int t = tid; t < NFX * TY; t += nth) {
         const int f = t % NFX, ry = t / NFX;  // face between cells i0 - 1 + f and i0 + f
         const int gl = i0 - 1 + f, gj = j0 + ry;
@@ -309,7 +332,11 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
         face_value(Ua, Uc, Ub, VU[ly * NLX + la + 1], VV[ly * NLX + la + 1], RX[(0 * TY + ry) * NRX + f + 1],
                    RX[(1 * TY + ry) * NRX + f + 1], RX[(2 * TY + ry) * NRX + f + 1], false, wL);
         R uL, uR;
-        rusanov_flux<R>(wR, wL, 0, fl, uL, uR);
+        rusanov_flux<R>(wR, wL, 0, ax, fl, uL, uR);
+        if (SPEED) {
+            smax_x = fmax(smax_x, fmax(fabs((double)uL), fabs((double)uR)));
+            continue;
+        }
         const R ube = R(0.5) * (uL + uR);
 #pragma unroll
         for (int k = 0; k < NV; k++) FX[(k * TY + ry) * NFX + f] = fl[k];
@@ -341,7 +368,11 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
             face_value(Ua, Uc, Ub, VU[(la + 1) * NLX + lx], VV[(la + 1) * NLX + lx], RY[(0 * NRY + f + 1) * TX + rx],
                        RY[(1 * NRY + f + 1) * TX + rx], RY[(2 * NRY + f + 1) * TX + rx], false, wL);
             R vL, vR;
-            rusanov_flux<R>(wR, wL, 1, fl, vL, vR);
+            rusanov_flux<R>(wR, wL, 1, ay, fl, vL, vR);
+            if (SPEED) {
+                smax_y = fmax(smax_y, fmax(fabs((double)vL), fabs((double)vR)));
+                continue;
+            }
             const R ube = R(0.5) * (vL + vR);
 #pragma unroll
             for (int k = 0; k < NV; k++) FY[(k * NFY + f) * TX + rx] = fl[k];
@@ -357,6 +388,18 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
                 }
             }
         }
+    }
+    if (SPEED) {  // warp maxima, one atomic per warp and direction
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            smax_x = fmax(smax_x, __shfl_xor_sync(0xffffffffu, smax_x, o));
+            smax_y = fmax(smax_y, __shfl_xor_sync(0xffffffffu, smax_y, o));
+        }
+        if ((tid & 31) == 0) {
+            atomic_max_nonneg(&c.ns->rus_v[0], smax_x);
+            atomic_max_nonneg(&c.ns->rus_v[1], smax_y);
+        }
+        return;
     }
     __syncthreads();
 
@@ -390,15 +433,15 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
     }
 }
 
-template __device__ void flux_tile<double, 128, 1, false>(const Ctx&, int, int, unsigned char*, int, int);
-template __device__ void flux_tile<double, 256, 1, false>(const Ctx&, int, int, unsigned char*, int, int);
+template __device__ void flux_tile<double, 128, 1, false, false>(const Ctx&, int, int, unsigned char*, int, int);
+template __device__ void flux_tile<double, 256, 1, false, false>(const Ctx&, int, int, unsigned char*, int, int);
 
 namespace {
 
-template <class R, int TX, int TY, bool TWO_D>
+template <class R, int TX, int TY, bool TWO_D, bool SPEED>
 __global__ void __launch_bounds__(TX * TY) k_flux(Ctx c) {
     extern __shared__ __align__(16) unsigned char flux_smem[];
-    flux_tile<R, TX, TY, TWO_D>(c, blockIdx.x, blockIdx.y, flux_smem, threadIdx.x, TX * TY);
+    flux_tile<R, TX, TY, TWO_D, SPEED>(c, blockIdx.x, blockIdx.y, flux_smem, threadIdx.x, TX * TY);
 }
 
 template <class R, int TX, int TY, bool TWO_D>
@@ -408,11 +451,17 @@ void launch_tile(const Ctx& c, cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !(configured & (1ull << dev))) {
-        cudaFuncSetAttribute(k_flux<R, TX, TY, TWO_D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
+        cudaFuncSetAttribute(k_flux<R, TX, TY, TWO_D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
+        cudaFuncSetAttribute(k_flux<R, TX, TY, TWO_D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::BYTES);
         configured |= 1ull << dev;
     }
     const dim3 grid((unsigned)((c.g.nx + TX - 1) / TX), TWO_D ? (unsigned)((c.g.ny + TY - 1) / TY) : 1u);
-    k_flux<R, TX, TY, TWO_D><<<grid, TX * TY, T::BYTES, st>>>(c);
+    if (!c.phy.rus_local) {  // RUS_LOCAL = 0: the grid-wide speeds first (Update :266-298)
+        cudaMemsetAsync(c.ns->rus_v, 0, sizeof(c.ns->rus_v), st);
+        k_flux<R, TX, TY, TWO_D, true><<<grid, TX * TY, T::BYTES, st>>>(c);
+        if (c.nlaunch) *c.nlaunch += 1;
+    }
+    k_flux<R, TX, TY, TWO_D, false><<<grid, TX * TY, T::BYTES, st>>>(c);
 }
 
 }  // namespace

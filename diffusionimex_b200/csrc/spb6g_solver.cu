@@ -511,7 +511,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         if (cfg->bc[q] < 0 || cfg->bc[q] > 3) return SPB6G_BAD_ARG;
     if ((cfg->bc[0] == SPB6G_BC_PERIODIC) != (cfg->bc[1] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if ((cfg->bc[2] == SPB6G_BC_PERIODIC) != (cfg->bc[3] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
-    if (cfg->rus_local != 1) return SPB6G_UNSUPPORTED;
+    if (cfg->rus_local != 0 && cfg->rus_local != 1) return SPB6G_BAD_ARG;
     for (int k = 0; k < 2; k++) {
         if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
@@ -1052,7 +1052,8 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     *out = nullptr;
     for (int i = 0; i < count; i++)
         if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
-            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0)  // the batched kernel: SG / NASG, p
+            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0 ||
+            cfgs[i].rus_local != 1)  // the batched kernel: SG / NASG, p, per-face Rusanov speed
             return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;

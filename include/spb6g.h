@@ -58,7 +58,8 @@ typedef struct {
     double cfl, cfl_ac;             /* material CFL, start-up acoustic CFL (:71-72) */
     int32_t ramp;                   /* start-up ramp (RAMP, :75) */
     double dtfix;                   /* > 0: fixed step (DTFIX, :77) */
-    int32_t rus_local;              /* RUS_LOCAL (:93); only 1 is implemented */
+    int32_t rus_local;              /* RUS_LOCAL (:93): 1 per-face max(|u_L|, |u_R|), 0 the grid-wide
+                                       maximum over cells and face states (batched form: 1 only) */
     int32_t limiter;                /* LIMITER (physics :969) */
     int32_t acdt;                   /* 1: acoustic CFL every step (caltimestep = Fullydt, :55) */
     double newton_tol;              /* NewtonTol (:79) */

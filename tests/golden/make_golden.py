@@ -106,6 +106,12 @@ CASES = {
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "bubble_outlet32_3steps": (lambda: _bc(_bubble(32), (PRES, PRES, W, W), bcp=(1.2e7, 0.8e7, 0, 0)), "steps", 3,
                                {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)
+    "case13_N200_20steps": (lambda: cases.reference_case(13, 200), "steps", 20, {}),
+    "lowmach_rus0_32_stage": (lambda: dict(_lowmach(32), rus_local=0), "stage", 0,
+                              {"dtfix": 2e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "lowmach_rus0_32_3steps": (lambda: dict(_lowmach(32), rus_local=0), "steps", 3,
+                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
 }
 
 

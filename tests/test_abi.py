@@ -53,7 +53,21 @@ def test_bad_arguments_rejected_before_device_use():
     lib.spb6g_default_config(ctypes.byref(c))
     c.bc[0] = 2  # periodic on one side only
     assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 7
+    lib.spb6g_default_config(ctypes.byref(c))
+    c.rus_local = 2
+    assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 7
     assert lib.spb6g_destroy(None) == 7
+
+
+def test_batched_form_takes_the_per_face_rusanov_speed_only():
+    """The batched kernel has no grid-wide speed pass: rus_local = 0 is refused before any
+    device use."""
+    lib = solver.library()
+    c = solver.Config()
+    lib.spb6g_default_config(ctypes.byref(c))
+    c.rus_local = 0
+    b = ctypes.c_void_p()
+    assert lib.spb6g_batch_create(ctypes.byref(c), 1, ctypes.byref(b)) == 8  # SPB6G_UNSUPPORTED
 
 
 def test_no_device_reported_on_cpu_host():

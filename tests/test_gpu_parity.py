@@ -111,7 +111,7 @@ def test_1d_tube_one_step_bitwise():
 @pytest.mark.parametrize("name", ["case87_N200_tend", "case5_N100_tend", "tube_N1000_tend", "nasg256_20steps",
                                   "tube_walls_N200_20steps", "tube_piston_N200_20steps", "tube_outlet_N200_20steps",
                                   "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps",
-                                  "case83_N200_10steps"])
+                                  "case83_N200_10steps", "case13_N200_20steps", "lowmach_rus0_32_3steps"])
 def test_runs_match_reference_in_l1(name):
     """Whole runs in L1: within 1e-6 of the field maximum, or within 10x the reference's own L1
     change under round-off perturbations (one-ulp libm, FD step 1.01e-7) where that is larger --
@@ -186,7 +186,7 @@ STAGE_KEYS = ["Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y", "fx_ubs", "fx_kp"
               "fy_ubs", "fy_kp", "fy_wl", "fy_pv", "kw"]
 
 
-@pytest.mark.parametrize("name", ["lowmach32_stage", "shock64x32_stage", "bubble48_stage"])
+@pytest.mark.parametrize("name", ["lowmach32_stage", "shock64x32_stage", "bubble48_stage", "lowmach_rus0_32_stage"])
 def test_stage_data_matches_restatement(name):
     """Every array one stage produces -- explicit predictor, face coefficients of the implicit
     face velocity/pressure, residual scale, shock budget -- against the C restatement, then the

@@ -17,7 +17,9 @@ FIXTURES = ["case87_N200_tend", "case5_N100_tend", "case83_N200_10steps", "tube_
             "bubble48_stage", "bubble48_4steps", "lowmach32_3steps", "shock64x32_3steps", "nasg256_20steps",
             # boundary variants: walls, pistons, pressure outlets, 1D periodic (cyclic matrix on BiCGStab)
             "tube_walls_N200_20steps", "tube_piston_N200_20steps", "tube_outlet_N200_20steps",
-            "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps"]
+            "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps",
+            # grid-wide Rusanov dissipation speed (rus_local = 0)
+            "case13_N200_20steps", "lowmach_rus0_32_stage", "lowmach_rus0_32_3steps"]
 MODES = {"tend": refio.MODE_TEND, "steps": refio.MODE_STEPS, "stage": refio.MODE_STAGE}
 
 
@@ -75,3 +77,14 @@ def test_oracle_vs_archived_profiles(golden_dir, tag, case, n, tmean, tmax):
     for a, b, s in ((p, z["p"], scale_p), (u, z["u"], scale_u), (rho, z["rho"], scale_r)):
         assert np.abs(a - b).mean() / s < tmean
         assert np.abs(a - b).max() / s < tmax
+
+
+def test_epoxy_spinel_initial_states_are_the_reference():
+    """Cases 12 and 13 (SPB 5.1 / 5.2; case 13 with the grid-wide Rusanov speed) as the
+    reference's own u_initialization builds them, where the compiled reference exists."""
+    if not refio.ref_available():
+        pytest.skip("compiled reference not available")
+    for case in (12, 13):
+        r = refio.run_ref_main_files([f"case={case}", "N=200", "init=1"], nx=200)
+        assert np.array_equal(r["U"], cases.reference_case(case, 200)["U"])
+    assert cases.reference_case(13)["rus_local"] == 0 and cases.reference_case(12)["rus_local"] == 1
