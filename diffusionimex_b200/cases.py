@@ -36,6 +36,29 @@ NITROMETHANE_CC = dict(g=2.19, pinf=0.0, q=0.0, qp=0.0, cv=0.0, b=0.0, kind=1, G
 DETONATION_JWL = dict(g=1.25, pinf=0.0, q=0.0, qp=0.0, cv=0.0, b=0.0, kind=2, G=0.25, rr=1840.0, c1=854.5e9, c2=20.5e9,
                       e1=4.6, e2=1.35, e0=0.0)
 WATER_NASG = dict(g=1.187, pinf=7028e5, q=-1177788.0, qp=0.0, cv=3610.0, b=6.61e-4)
+# Liquid / vapour pairs of the reference's phase-transition cases (test_setup, physics :1019-1064;
+# set_SG(k, g, pi, q, qp, cv)): water SG (P-S 2014), dodecane SG (P-S 2014), water NASG (Pelanti
+# 2022 8.2.1), dodecane NASG (Pelanti 8.2.2), water NASG 350-550 K (Pelanti 8.2.4, Bartak)
+WATER_LIQ_SG = dict(g=2.35, pinf=1e9, q=-1167e3, qp=0.0, cv=1816.0, b=0.0)
+WATER_VAP_SG = dict(g=1.43, pinf=0.0, q=2030e3, qp=-23.4e3, cv=1040.0, b=0.0)
+DODECANE_LIQ_SG = dict(g=2.35, pinf=4e8, q=-775.269e3, qp=0.0, cv=1077.7, b=0.0)
+DODECANE_VAP_SG = dict(g=1.025, pinf=0.0, q=-237.547e3, qp=-24.4e3, cv=1956.45, b=0.0)
+WATER_LIQ_NASG = dict(WATER_NASG)
+WATER_VAP_NASG = dict(g=1.467, pinf=0.0, q=2077616.0, qp=14317.0, cv=955.0, b=0.0)
+DODECANE_LIQ_NASG = dict(g=1.206, pinf=1681e5, q=-996054.0, qp=0.0, cv=2532.0, b=7.51e-4)
+DODECANE_VAP_NASG = dict(g=1.021, pinf=0.0, q=-384592.0, qp=-4301.0, cv=2274.0, b=0.0)
+WATER_LIQ_BARTAK = dict(g=1.387, pinf=8899e5, q=-1244191.0, qp=0.0, cv=3202.0, b=4.78e-4)
+WATER_VAP_BARTAK = dict(g=1.954, pinf=0.0, q=2287484.0, qp=6417.0, cv=462.0, b=0.0)
+
+
+def v_pT(ph: dict, p, T):
+    """Specific volume of a SG / NASG phase at (p, T) (v_pT, physics :80)."""
+    return (ph["g"] - 1.0) * ph["cv"] * T / (p + ph["pinf"]) + ph["b"]
+
+
+def rho_pT(ph: dict, p, T):
+    """rho_pT (physics :1015)."""
+    return 1.0 / v_pT(ph, p, T)
 
 
 def default_settings() -> dict:
@@ -109,9 +132,14 @@ def cell_centres(cfg: dict):
 def reference_case(case: int, nx: int | None = None) -> dict:
     """A subset of the reference's 1D cases: 4 (interface advection), 5 (SPB 4.3.1 water-air),
     12 and 13 (SPB 5.1 / 5.2 epoxy-spinel mixture; 13 takes the grid-wide Rusanov speed,
-    rus_local = 0), 80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes 60
-    (SPB 4.2 nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG
-    water)."""
+    rus_local = 0), the liquid-vapour cases of phase transition -- 1, 2 (P-S 2014 5.1 water
+    cavitation tube, +-2 and +-500 m/s), 3 (P-S 5.2 dodecane shock tube, SG), 30 (Pelanti 2022
+    8.2.1 water cavitation, NASG), 31 (Pelanti 8.2.2 dodecane, NASG), 32 (Pelanti 8.2.4 Bartak
+    depressurisation: pressure outlet left, wall right, relax 2), 40, 41 (uniform non-equilibrium
+    states, periodic) -- 80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes
+    60 (SPB 4.2 nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG
+    water).  The relaxation level is the case's own (32: 2; the others 0); set "relax" to run one
+    with thermal or chemical relaxation."""
     c = default_settings()
     air, water = dict(AIR_SG), dict(WATER_SG)
     if case == 4:
@@ -127,6 +155,20 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         c.update(phases=[water, air], nx=1000, tend=0.25 if case == 86 else 241e-6)
     elif case == 88:
         c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=1000, tend=30e-6)
+    elif case in (1, 2):  # physics :1021-1023
+        c.update(phases=[dict(WATER_LIQ_SG), dict(WATER_VAP_SG)], nx=5000, tend=3.2e-3 if case == 1 else 0.58e-3)
+    elif case in (3, 31):  # :1024-1025, :1036
+        pair = (DODECANE_LIQ_SG, DODECANE_VAP_SG) if case == 3 else (DODECANE_LIQ_NASG, DODECANE_VAP_NASG)
+        c.update(phases=[dict(pair[0]), dict(pair[1])], nx=2000, tend=473e-6)
+        if case == 3:
+            c["cfl"] = 0.05
+    elif case == 30:  # :1035
+        c.update(phases=[dict(WATER_LIQ_NASG), dict(WATER_VAP_NASG)], nx=5000, tend=3e-3)
+    elif case == 32:  # :1037-1039
+        c.update(phases=[dict(WATER_LIQ_BARTAK), dict(WATER_VAP_BARTAK)], x0=0.0, x1=1.7, tend=17.5e-3, nx=1000,
+                 relax=2, bc=[BC_PRES, BC_WALL, BC_TRANS, BC_TRANS], bcp=[1e5, 0.0, 0.0, 0.0])
+    elif case in (40, 41):  # :1040
+        c.update(phases=[dict(WATER_LIQ_SG), dict(WATER_VAP_SG)], tend=1e-4, bc=[BC_PERIODIC, BC_PERIODIC, BC_TRANS, BC_TRANS])
     elif case in (12, 13):  # test_setup physics :1029-1032
         c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=500,
                  tend=80e-6 if case == 12 else 34e-6)
@@ -171,6 +213,24 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         L = x < (0.25 if adv else 0.7)
         p = np.full_like(x, 1e5) if adv else np.where(L, 1e9, 1e5)
         U = prim2cell(ph, np.where(L, 1 - 1e-7, 1e-7), 1000.0, 0.01 if adv else 50.0, 1.0 if adv else 0.0, 0.0, p, p)
+    elif case in (1, 2, 30):  # test_state :1090-1092, :1141
+        T0 = 353.0 if case == 30 else 354.728
+        U0 = 500.0 if case == 2 else 2.0
+        u = np.where(x < 0.5, -U0, U0)
+        U = prim2cell(ph, np.full_like(x, 1 - 1e-2), rho_pT(ph[0], 1e5, T0), rho_pT(ph[1], 1e5, T0), u, 0.0, 1e5, 1e5)
+    elif case in (3, 31):  # :1095
+        L = x < 0.75
+        p = np.where(L, 1e8, 1e5)
+        U = prim2cell(ph, np.where(L, 1 - 1e-8, 1e-8), 500.0, 2.0, 0.0, 0.0, p, p)
+    elif case == 32:  # :1093-1094
+        p, T = 12.5e6, 563.15
+        U = prim2cell(ph, np.full_like(x, 1 - 1e-3), rho_pT(ph[0], p, T), rho_pT(ph[1], p, T), 0.0, 0.0, p, p)
+    elif case == 40:  # :1143
+        T1, T2, p1, p2 = 350.0, 380.0, 1.2e5, 0.8e5
+        U = prim2cell(ph, np.full_like(x, 1 - 0.2), rho_pT(ph[0], p1, T1), rho_pT(ph[1], p2, T2), 0.0, 0.0, p1, p2)
+    elif case == 41:  # :1142
+        T0, p0 = 380.0, 0.8e5
+        U = prim2cell(ph, np.full_like(x, 1 - 0.2), rho_pT(ph[0], p0, T0), rho_pT(ph[1], p0, T0), 0.0, 0.0, p0, p0)
     elif case in (12, 13, 88):
         p = np.where(x < 0.6, 2e11 if case == 13 else 1e10, 1e5)
         U = prim2cell(ph, np.full_like(x, 0.5954), 1185.0, 3622.0, 0.0, 0.0, p, p)
@@ -339,6 +399,32 @@ def riemann_batch(count: int = 512, seed: int = 0, nmin: int = 256, nmax: int = 
         c.update(steps=steps, instance=k, nasg=nasg)
         out.append(c)
     return out
+
+
+def bubble_compression(nx: int = 200, ny: int = 200) -> dict:
+    """The reference's case 72 (P-S 2014 5.4, src/spb6_physics_omp.h:1062-1064, :1115-1117): a
+    dodecane vapour bubble (radius 0.2 m, centred) in liquid dodecane at 1e5 Pa and 600 K on the
+    unit square, walls all round, the left wall a piston at 100 m/s; p-pT-pTg relaxation
+    (relax 2), the grid-wide Rusanov speed (rus_local 0).  Cell values are the reference's
+    averages over 4 x 4 sub-points (u_initialization :482-487, summed in its order)."""
+    c = default_settings()
+    c.update(nx=nx, ny=ny, tend=1.2e-3, phases=[dict(DODECANE_LIQ_SG), dict(DODECANE_VAP_SG)],
+             bc=[BC_WALL] * 4, bcu=[100.0, 0.0, 0.0, 0.0], relax=2, rus_local=0, case=72)
+    x, y, dx, dy = cell_centres(c)
+    X, Y = np.meshgrid(x, y)
+    ph = c["phases"]
+    r1, r2 = rho_pT(ph[0], 1e5, 600.0), rho_pT(ph[1], 1e5, 600.0)
+    sub = 4
+    U = np.zeros((ny, nx, NUM_VARS))
+    for a in range(sub):
+        for b in range(sub):
+            xs = X + ((a + 0.5) / sub - 0.5) * dx
+            ys = Y + ((b + 0.5) / sub - 0.5) * dy
+            inside = (xs - 0.5) * (xs - 0.5) + (ys - 0.5) * (ys - 0.5) < 0.04
+            U = U + prim2cell(ph, np.where(inside, 1e-6, 1 - 1e-6), r1, r2, 0.0, 0.0, 1e5, 1e5) / (sub * sub)
+    c["U"] = U
+    c["workload"] = f"piston-compressed dodecane vapour bubble 2D, {nx}x{ny} cells, relax 2"
+    return c
 
 
 def underwater_explosion(nx: int = 361, ny: int = 200) -> dict:

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "../../include/spb6g.h"
 #include "spb6g_common.cuh"
 
@@ -179,6 +181,8 @@ void launch_apply_step(const Ctx& c, cudaStream_t st);
 void launch_floor(const Ctx& c, cudaStream_t st, double tol);
 void launch_final(const Ctx& c, cudaStream_t st);
 void launch_relax_activate(const Ctx& c, cudaStream_t st, State U);
+// Host: the packed saturation table of cfg's phases (spb6g_saturation.cu).
+std::vector<double> saturation_table(const spb6g_config* cfg);
 void launch_caldt(const Ctx& c, cudaStream_t st, CState U, int acoustic);
 void launch_pbar_min(const Ctx& c, cudaStream_t st, CState U);
 void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, double* P);

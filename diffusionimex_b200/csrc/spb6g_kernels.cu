@@ -1420,17 +1420,21 @@ void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
 }
 
 // ============================================================ final state (:1056-1073) and H_s (:1363-1371)
-// RelaxationActivation (:563-586) for p-pT relaxation (RELAX_LEVEL 1): every cell of the interface
-// zone eps_I <= alpha1 <= 1 - eps_I gets the pT closure for the step (closure_type_of :870-886 with
-// the thermal rate infinite) and U^n is projected on its manifold (project_cell :549-561: the same
-// closure at s = 0 from the conservative state; alpha and the phase energies change, masses,
-// momentum and E do not); a cell whose projection has no solution keeps the p closure.
+// RelaxationActivation (:563-586) with the rates infinite: the closure type of every cell for the
+// step (closure_type_of :870-886).  Outside the interface zone eps_I <= alpha1 <= 1 - eps_I, and
+// for RELAX_LEVEL 0, the p closure.  In the zone: level 1 pT; level 2 pT, or pTg where the pT
+// state's temperature is above Tsat(p); level 3 pTg where a phase temperature of the p closure
+// without the energy defect is above Tsat(p), else p.  U^n of a pT / pTg cell is projected on that
+// manifold (project_cell :549-561: the closure at s = 0 from the conservative state; alpha, the
+// phase masses and energies change, the momentum and E do not); a cell whose projection has no
+// solution takes the p closure.  The level-2 test's pT state is the pT projection itself (the
+// same closure of the same input).
 #if SPB6G_MG
 __global__ void k_relax_activate(Ctx c, State U) {
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double a1 = U.v[IA1][x];
         unsigned char ty = CL_P;
-        if (a1 >= c.phy.eps_i && a1 <= 1.0 - c.phy.eps_i) {
+        if (c.phy.relax > 0 && a1 >= c.phy.eps_i && a1 <= 1.0 - c.phy.eps_i) {
             const double m1 = U.v[IM1][x], m2 = U.v[IM2][x], mu = U.v[IMU][x], mv = U.v[IMV][x];
             const double rho = m1 + m2;
             ClIn in;
@@ -1440,13 +1444,36 @@ __global__ void k_relax_activate(Ctx c, State U) {
             in.rhoeC = U.v[IEN][x] - 0.5 * (mu * mu + mv * mv) / rho;
             in.pguess = SMAX(p_mix(c.phy, in.atr[0], in.mtr[0], in.mtr[1], in.rhoeC), 1.0);
             in.Qph[0] = in.Qph[1] = 0.0;
-            in.type = CL_PT;
             ClOut o;
-            if (closure(c.phy, in, o)) {
+            bool have = false;  // o holds the projection of type ty
+            if (c.phy.relax == 3) {
+                in.type = CL_PND;
+                if (closure(c.phy, in, o)) {
+                    const double p = o.pbar, Ts = sat_temperature(c.phy, p);
+                    if (isfinite(Ts) && (T_amp(c.phy, 0, o.a[0], m1, p) > Ts || T_amp(c.phy, 1, o.a[1], m2, p) > Ts))
+                        ty = CL_PTG;
+                }
+            } else {
                 ty = CL_PT;
+                in.type = CL_PT;
+                have = closure(c.phy, in, o);
+                if (c.phy.relax == 2 && have) {
+                    const double Ts = sat_temperature(c.phy, o.pbar);
+                    if (isfinite(Ts) && o.T > Ts) { ty = CL_PTG; have = false; }
+                }
+            }
+            if (ty != CL_P && !have) {
+                in.type = ty;
+                have = closure(c.phy, in, o);
+            }
+            if (ty != CL_P && have) {
                 U.v[IA1][x] = o.a[0];
+                U.v[IM1][x] = o.m[0];
+                U.v[IM2][x] = o.m[1];
                 U.v[IE1][x] = o.e[0];
                 U.v[IE2][x] = o.e[1];
+            } else {
+                ty = CL_P;
             }
         }
         c.ctype[x] = ty;
@@ -1470,8 +1497,11 @@ SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
         double Gr;
         CellRes o;
         if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 8); return; }
+        // a pTg cell exchanges mass: its phase masses are the closure's (:1063)
+        const int ty = (SPB6G_MG && c.phy.relax) ? (int)c.ctype[x] : CL_P;
+        const double mk[2] = {ty == CL_PTG ? o.o.m[0] : o.in.mtr[0], ty == CL_PTG ? o.o.m[1] : o.in.mtr[1]};
         double U[NV];
-        U[IA1] = o.o.a[0]; U[IM1] = o.in.mtr[0]; U[IM2] = o.in.mtr[1]; U[IMU] = o.mx; U[IMV] = o.my;
+        U[IA1] = o.o.a[0]; U[IM1] = mk[0]; U[IM2] = mk[1]; U[IMU] = o.mx; U[IMV] = o.my;
         U[IE1] = o.o.e[0]; U[IE2] = o.o.e[1]; U[IEN] = o.E;
 #pragma unroll
         for (int k = 0; k < NV; k++) {
@@ -1482,8 +1512,8 @@ SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
         }
         if (tm) {  // st_Tmax (:1064-1065): the phase temperatures where the phase is present
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const double T = T_amp(c.phy, k, o.o.a[k], o.in.mtr[k], o.o.pbar);
+            for (int k = 0; k < 2; k++) {  // pT / pTg cells: the common temperature of the closure
+                const double T = ty != CL_P ? o.o.T : T_amp(c.phy, k, o.o.a[k], mk[k], o.o.pbar);
                 if (o.o.a[k] > 1e-9 && isfinite(T)) tm[k] = SMAX(tm[k], T);
             }
         }

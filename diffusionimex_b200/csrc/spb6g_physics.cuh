@@ -44,13 +44,18 @@ struct Phys {
     int limiter;     // LIMITER, :969
     int rus_local;   // RUS_LOCAL, src/SPB6_PC_IMEX_omp.cpp:93
     int mg;          // a Mie-Grueneisen phase is present (mg_any, :58)
-    int relax;       // RELAX_LEVEL (:39): 0 mechanical relaxation only, 1 p-pT (instantaneous thermal
-                     // relaxation in the interface zone)
+    int relax;       // RELAX_LEVEL (:39): 0 mechanical relaxation only; in the interface zone 1 p-pT
+                     // (instantaneous thermal relaxation), 2 p-pT-pTg and 3 p-pTg (instantaneous
+                     // chemical relaxation where a phase is above the saturation temperature)
     int pad;
     double eps_i;    // EPS_I (:40): interface zone eps_I <= alpha1 <= 1 - eps_I
+    const double* sat;  // relax >= 2: the saturation table (SatTable :114), packed as n, pcrit, vcrit,
+                        // pmin, ln p[n], Tsat[n]
 };
-// Closure types (ClosureType :228) built here: p (mechanical) and pT (instantaneous thermal).
-enum { CL_P = 0, CL_PT = 2 };
+// Closure types (ClosureType :228) built here: p (mechanical), pT (instantaneous thermal) and pTg
+// (instantaneous thermal and chemical).  CL_PND is internal: the p closure without the energy
+// defect (ClIn::nodelta :236), the prediction of the p-pTg activation test (:878).
+enum { CL_P = 0, CL_PT = 2, CL_PTG = 5, CL_PND = 6 };
 
 // ------------------------------------------------------------ EOS, src/spb6_physics_omp.h:60-111
 // Mie-Grueneisen reference curves pr(rho), pr'(rho), er(rho) (mg_ref :60-69): Cochran-Chan
@@ -163,6 +168,7 @@ struct ClIn {
 };
 struct ClOut {
     double a[2], e[2], pbar;
+    double m[2], T;  // pT / pTg closures: phase masses (pTg moves mass) and the common temperature
 };
 
 SPB6G_DEV double E_above(const Phys& P, const ClIn& in, int k) {  // :430-433
@@ -182,7 +188,7 @@ struct ClPre {
     bool byMass;
 };
 SPB6G_DEV void closure_pre(const Phys& P, const ClIn& in, ClPre& pr) {
-    pr.D0 = in.rhoeC - in.etr[0] - in.etr[1];
+    pr.D0 = (SPB6G_MG && in.type == CL_PND) ? 0.0 : in.rhoeC - in.etr[0] - in.etr[1];
     const double sm = in.mtr[0] + in.mtr[1];
     pr.byMass = P.share_mode == 2;
     double E[2], sE = 0.0;
@@ -498,9 +504,102 @@ static __device__ __noinline__ ClMg closure_pT(const Phys P, double m0, double m
     for (int k = 0; k < 2; k++) {
         res.o.a[k] = m[k] * v_pT(k, p, T);
         res.o.e[k] = m[k] * e_pT(k, p, T);
+        res.o.m[k] = m[k];
     }
     res.o.pbar = p;
+    res.o.T = T;
     res.ok = T > 0;
+    return res;
+}
+
+// ---- instantaneous chemical relaxation (pTg closure, B6.6), built with the extended physics
+// Specific volume, energy, entropy and Gibbs function of a SG / NASG phase at (p, T) (:80-83).
+SPB6G_DEV double v_pT(const PhaseD& h, double p, double T) { return (h.g - 1.0) * h.cv * T / (p + h.pi) + h.b; }
+SPB6G_DEV double e_pT(const PhaseD& h, double p, double T) { return h.cv * T * (p + h.g * h.pi) / (p + h.pi) + h.q; }
+SPB6G_DEV double s_pT(const PhaseD& h, double p, double T) {
+    return h.cv * (h.g * log(T) - (h.g - 1.0) * log(p + h.pi)) + h.qp;
+}
+SPB6G_DEV double g_pT(const PhaseD& h, double p, double T) { return h.g * h.cv * T + h.b * p + h.q - T * s_pT(h, p, T); }
+// Saturation temperature of pressure p, the root of g_1 - g_2 on the physical branch (Tsat
+// :155-163): a first guess interpolated linearly in ln p from the table, then Newton with the
+// step held within [T/2, 2T] (sat_newton :116-126); NaN off the table's range (p <= 0 or at or
+// above the critical pressure) or where Newton does not converge.
+SPB6G_DEV double sat_temperature(const Phys& P, double p) {
+    const double* S = P.sat;
+    const int n = (int)S[0];
+    if (!(p > 0) || !(p < S[1]) || n < 1) return NAN;
+    const double* lp = S + 4;
+    const double* Tt = lp + n;
+    const double l = log(p);
+    double T;
+    if (l <= lp[0]) T = Tt[0];
+    else if (l >= lp[n - 1]) T = Tt[n - 1];
+    else {
+        const double h = lp[1] - lp[0];
+        const int i = SMIN((int)((l - lp[0]) / h), n - 2);
+        const double w = (l - lp[i]) / h;
+        T = (1 - w) * Tt[i] + w * Tt[i + 1];
+    }
+    const PhaseD &h0 = P.ph[0], &h1 = P.ph[1];
+    for (int it = 0; it < 60; it++) {
+        const double f = g_pT(h0, p, T) - g_pT(h1, p, T), d = s_pT(h1, p, T) - s_pT(h0, p, T);
+        if (!(d > 0) || !isfinite(f)) return NAN;
+        double Tn = T - f / d;
+        if (Tn < 0.5 * T) Tn = 0.5 * T;
+        if (Tn > 2.0 * T) Tn = 2.0 * T;
+        if (fabs(Tn - T) < 1e-14 * T) return Tn;
+        T = Tn;
+    }
+    return fabs(g_pT(h0, p, T) - g_pT(h1, p, T)) < 1e-8 * fabs(g_pT(h0, p, T)) + 1e-8 ? T : NAN;
+}
+// Temperature of the mixture at pressure p, vapour mass fraction Y and specific energy eC
+// (T_from_energy :766-769).
+SPB6G_DEV double T_of_energy(const Phys& P, double p, double Y, double eC) {
+    const PhaseD &h0 = P.ph[0], &h1 = P.ph[1];
+    const double d = (1 - Y) * h0.cv * (p + h0.g * h0.pi) / (p + h0.pi) + Y * h1.cv * (p + h1.g * h1.pi) / (p + h1.pi);
+    return (eC - (1 - Y) * h0.q - Y * h1.q) / d;
+}
+constexpr double Y_MIN = 1e-10;  // YMIN :245: the mass fractions stay within [Y_MIN, 1 - Y_MIN]
+// pTg closure (closure_pTg :825-834 with pTg_state :811-824): at pressure p the temperature is
+// Tsat(p) and Y follows from the energy, clamped to [Y_MIN, 1 - Y_MIN] (then T from the energy);
+// at or above the critical pressure one phase by v against the critical volume; p solves
+// rho ((1 - Y) v_1 + Y v_2) = 1 by root_above.
+static __device__ __noinline__ ClMg closure_pTg(const Phys P, double m0, double m1, double rhoeC, double pguess) {
+    ClMg res;
+    res.ok = 0;
+    const double rho = m0 + m1, eC = rhoeC / rho;
+    auto state = [&](double p, double& Y, double& T) -> bool {
+        const double Ts = sat_temperature(P, p);
+        if (isfinite(Ts)) {
+            const double el = e_pT(P.ph[0], p, Ts), ev = e_pT(P.ph[1], p, Ts);
+            Y = (eC - el) / (ev - el);
+            if (Y > Y_MIN && Y < 1 - Y_MIN) { T = Ts; return true; }
+            Y = SMIN(SMAX(Y, Y_MIN), 1 - Y_MIN);
+        } else {
+            if (!(p >= P.sat[1])) return false;
+            Y = (1.0 / rho < P.sat[2]) ? Y_MIN : 1 - Y_MIN;
+        }
+        T = T_of_energy(P, p, Y, eC);
+        return T > 0;
+    };
+    auto Phi = [&](double p) {
+        double Y, T;
+        if (!state(p, Y, T)) return (double)NAN;
+        return rho * ((1 - Y) * v_pT(P.ph[0], p, T) + Y * v_pT(P.ph[1], p, T)) - 1.0;
+    };
+    double p;
+    if (!root_above(Phi, SMAX(-P.ph[0].pi, -P.ph[1].pi), pguess, p)) return res;
+    double Y, T;
+    if (!state(p, Y, T)) return res;
+    res.o.m[0] = rho * (1 - Y);
+    res.o.m[1] = rho * Y;
+    for (int k = 0; k < 2; k++) {
+        res.o.a[k] = res.o.m[k] * v_pT(P.ph[k], p, T);
+        res.o.e[k] = res.o.m[k] * e_pT(P.ph[k], p, T);
+    }
+    res.o.pbar = p;
+    res.o.T = T;
+    res.ok = 1;
     return res;
 }
 
@@ -511,9 +610,10 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
     for (int k = 0; k < 2; k++)
         if (!(in.atr[k] > 0) || !(in.mtr[k] > 0) || !isfinite(in.etr[k])) return false;
     if (!isfinite(in.rhoeC) || !isfinite(in.s)) return false;
-    if (SPB6G_MG && in.type != CL_P) {  // the thermal closure; Mie-Grueneisen phases relax mechanically only (:846)
-        if (P.mg) return false;
-        const ClMg r = closure_pT(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
+    if (SPB6G_MG && in.type != CL_P && in.type != CL_PND) {  // thermal / chemical closures; Mie-Grueneisen
+        if (P.mg) return false;                              // phases relax mechanically only (:846)
+        const ClMg r = in.type == CL_PTG ? closure_pTg(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess)
+                                         : closure_pT(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
         o = r.o;
         return r.ok && isfinite(o.pbar);
     }

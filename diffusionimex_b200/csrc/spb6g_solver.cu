@@ -517,7 +517,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
     }
     if (cfg->relax < 0 || cfg->relax > 3) return SPB6G_BAD_ARG;
-    if (cfg->relax > 1 || (cfg->relax && (cfg->kind[0] || cfg->kind[1]))) return SPB6G_UNSUPPORTED;
+    if (cfg->relax && (cfg->kind[0] || cfg->kind[1])) return SPB6G_UNSUPPORTED;
     if (cfg->relax && !(cfg->eps_i >= 0 && cfg->eps_i < 0.5)) return SPB6G_BAD_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;
@@ -571,6 +571,13 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.strong_list = (int*)A(n / 2 + 1);
     c.smask = (unsigned char*)A(n / 8 + 1);
     c.ctype = cfg->relax ? (unsigned char*)A(n / 8 + 1) : nullptr;  // n bytes
+    if (cfg->relax >= 2) {  // the saturation line (build_sat, physics :127-153; main :1236)
+        const std::vector<double> sat = saturation_table(cfg);
+        double* d = A(sat.size());
+        if (d && cudaMemcpy(d, sat.data(), sat.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) ok = false;
+        c.phy.sat = d;
+        s->P.sat = d;
+    }
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
     c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
     c.prec = cfg->precision ? 1 : 0;

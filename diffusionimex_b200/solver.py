@@ -112,6 +112,7 @@ def library() -> ctypes.CDLL:
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
         "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
+        "spb6g_saturation_table": (I, [P, P, I, P]),
         "spb6g_batch_create": (I, [P, I, P]),
         "spb6g_batch_destroy": (None, [P]),
         "spb6g_batch_instance": (P, [P, I]),
@@ -166,6 +167,25 @@ def make_config(case: dict, device: int = 0) -> Config:
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def saturation_table(case: dict) -> dict:
+    """The saturation line of the case's two phases as chemical relaxation uses it (host only):
+    n points ln p, Tsat(p), the critical pressure and volume and the lowest tabulated pressure
+    (build_sat, src/spb6_physics_omp.h:127-153)."""
+    lib = library()
+    cfg = make_config(case)
+    n = ctypes.c_int()
+    rc = lib.spb6g_saturation_table(ctypes.byref(cfg), None, 0, ctypes.byref(n))
+    if rc != 0:
+        raise SolverError(rc, "spb6g_saturation_table")
+    buf = np.empty(n.value, dtype=np.float64)
+    rc = lib.spb6g_saturation_table(ctypes.byref(cfg), _ptr(buf), n.value, ctypes.byref(n))
+    if rc != 0:
+        raise SolverError(rc, "spb6g_saturation_table")
+    k = int(buf[0])
+    return {"raw": buf, "n": k, "pcrit": buf[1], "vcrit": buf[2], "pmin": buf[3], "lp": buf[4:4 + k],
+            "T": buf[4 + k:4 + 2 * k]}
 
 
 def format_profile(case: dict, U: np.ndarray, path: str, prec: int = 16):

@@ -38,7 +38,8 @@ typedef enum {
     SPB6G_BAD_ARG = 7,
     SPB6G_UNSUPPORTED = 8,
     SPB6G_NO_DEVICE = 9,
-    SPB6G_TOO_LARGE = 10        /* grid larger than spb6g_caldt_noalloc's fixed scratch */
+    SPB6G_TOO_LARGE = 10        /* grid larger than spb6g_caldt_noalloc's fixed scratch, or an
+                                   output buffer too small */
 } spb6g_status;
 
 enum { SPB6G_BC_TRANS = 0, SPB6G_BC_WALL = 1, SPB6G_BC_PERIODIC = 2, SPB6G_BC_PRES = 3 };
@@ -77,9 +78,11 @@ typedef struct {
                                        2 JWL pr = c1 exp(-e1 rr / rho) + c2 exp(-e2 rr / rho), er - e0
                                        (Phase.kind, physics :51-69); MG phases use only G, rr, c1, c2,
                                        e1, e2, e0 and cv (temperature output) */
-    int32_t relax;                  /* RELAX_LEVEL (physics :39): 0 mechanical relaxation; 1 p-pT, instantaneous
-                                       thermal relaxation in the interface zone (2 and 3, chemical relaxation,
-                                       and finite rates are not built: SPB6G_UNSUPPORTED) */
+    int32_t relax;                  /* RELAX_LEVEL (physics :39): 0 mechanical relaxation; in the interface zone
+                                       1 p-pT (instantaneous thermal relaxation), 2 p-pT-pTg and 3 p-pTg
+                                       (instantaneous chemical relaxation above the saturation temperature);
+                                       SG / NASG phases only (SPB6G_UNSUPPORTED with a Mie-Grueneisen phase);
+                                       the rates are infinite (finite rates are not built) */
     int32_t reserved[3];
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
     double eps_i;                   /* EPS_I (physics :40): interface zone eps_I <= alpha1 <= 1 - eps_I (1e-4) */
@@ -112,6 +115,12 @@ int spb6g_init_pressure(spb6g_solver* s);
 /* The pressure unknown P - P_REF (PField, :172), nx*ny doubles. */
 int spb6g_set_pressure(spb6g_solver* s, const double* P, double p_ref);
 int spb6g_get_pressure(spb6g_solver* s, double* P, double* p_ref);
+
+/* The saturation table of cfg's two SG / NASG phases (build_sat, physics :127-153), host only:
+ * n, pcrit, vcrit, pmin, then ln p[n] and Tsat[n] -- 4 + 2n doubles, the count in *len.  With
+ * out == NULL only *len is set; SPB6G_TOO_LARGE if cap < *len.  Solvers with relax >= 2 build and
+ * keep it on the device themselves. */
+int spb6g_saturation_table(const spb6g_config* cfg, double* out, int cap, int* len);
 
 /* caldt (:502-514): returns 1 / (a_x/dx + a_y/dy) (INFINITY if the rate is 0). */
 int spb6g_caldt(spb6g_solver* s, int acoustic, double* inv_rate);

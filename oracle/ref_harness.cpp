@@ -97,6 +97,8 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
     theta_rate = RELAX_LEVEL >= 1 ? INF : 0.0;
     nu_rate = (RELAX_LEVEL == 2 || RELAX_LEVEL == 3) ? INF : 0.0;
     STEP_TYPE.clear();
+    // the saturation table of these phases, built before any parallel loop as main() does (:1236)
+    if (RELAX_LEVEL > 0 && !mg_any()) build_sat();
     SHARE_MODE = c.share_mode;
     RKs = c.rk;
     CFL = c.cfl;
@@ -308,7 +310,12 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     int rc = 0;
     long timed_steps = 0;
-    if (c.mode == SPB6_MODE_STAGE) {
+    if (c.mode == SPB6_MODE_SAT) {  // the saturation table of the phases (build_sat :127-153)
+        if (!SAT.built) build_sat();
+        extra = {(double)SAT.lp.size(), SAT.pcrit, SAT.vcrit, SAT.pmin};
+        extra.insert(extra.end(), SAT.lp.begin(), SAT.lp.end());
+        extra.insert(extra.end(), SAT.T.begin(), SAT.T.end());
+    } else if (c.mode == SPB6_MODE_STAGE) {
         rc = stage_dump(H, c.dtfix, extra);
     } else {
         const bool to_end = c.mode == SPB6_MODE_TEND;

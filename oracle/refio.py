@@ -17,9 +17,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "spb6_ref")
+REF_BIN_ULP = os.path.join(HERE, "_ref", "spb6_ref_ulp")  # log / exp / pow one ulp up (ulp_libm.c)
 PORT_LIB = os.path.join(HERE, "_build", "libspb6_oracle.so")
 MAGIC = 0x36425053
-MODE_STEPS, MODE_TEND, MODE_STAGE = 0, 1, 2
+MODE_STEPS, MODE_TEND, MODE_STAGE, MODE_SAT = 0, 1, 2, 3
 
 CASE_DT = np.dtype([
     ("magic", "<u4"), ("version", "<i4"), ("nx", "<i4"), ("ny", "<i4"), ("bc", "<i4", 4),
@@ -73,6 +74,9 @@ def parse_result(buf: bytes, nx: int, ny: int, mode: int) -> dict:
     o = 0
     out["U"] = arr[o:o + n * 8].reshape(ny, nx, 8).copy(); o += n * 8
     out["P"] = arr[o:o + n].reshape(ny, nx).copy() if arr.size >= o + n else None; o += n
+    if mode == MODE_SAT:  # n, pcrit, vcrit, pmin, ln p[n], Tsat[n]
+        out["sat"] = arr[o:].copy()
+        return out
     if mode == MODE_STAGE and arr.size > o:
         out["Xs"] = arr[o:o + n * 8].reshape(ny, nx, 8).copy(); o += n * 8
         out["a2s"] = arr[o:o + n].reshape(ny, nx).copy(); o += n
@@ -95,9 +99,10 @@ def ref_available() -> bool:
 
 
 def run_ref(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, timeout: float = 3600,
-            warmup: int = 0, budget_s: float = 0.0) -> dict:
+            warmup: int = 0, budget_s: float = 0.0, variant: str | None = None) -> dict:
     """Run the reference solver (compiled from its sources) on cfg['U'].  With `warmup`, the first
-    steps are excluded from wall_s; with `budget_s`, stepping stops once the timed steps used it."""
+    steps are excluded from wall_s; with `budget_s`, stepping stops once the timed steps used it.
+    variant "ulp" / "ulpdown": the reference with its log / exp / pow results one ulp up / down."""
     U = np.ascontiguousarray(cfg["U"], dtype="<f8")
     with tempfile.TemporaryDirectory() as d:
         ci, co = os.path.join(d, "case.bin"), os.path.join(d, "out.bin")
@@ -107,7 +112,10 @@ def run_ref(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
-        subprocess.run([REF_BIN, ci, co], check=True, timeout=timeout, env=env)
+        if variant == "ulpdown":
+            env["SPB6_ULP_DOWN"] = "1"
+        subprocess.run([REF_BIN_ULP if variant in ("ulp", "ulpdown") else REF_BIN, ci, co], check=True,
+                       timeout=timeout, env=env)
         with open(co, "rb") as f:
             return parse_result(f.read(), cfg["nx"], cfg["ny"], mode)
 

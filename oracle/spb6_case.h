@@ -22,7 +22,7 @@
 #define SPB6_CASE_MAGIC 0x36425053u /* "SPB6" */
 #define SPB6_CASE_VERSION 3
 
-enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2 };
+enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2, SPB6_MODE_SAT = 3 };
 enum { SPB6_BC_TRANS = 0, SPB6_BC_WALL = 1, SPB6_BC_PERIODIC = 2, SPB6_BC_PRES = 3 };
 
 typedef struct {

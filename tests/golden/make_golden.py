@@ -11,6 +11,8 @@ where the reference tree does not exist.
 Fixtures:
   ref_<name>.npz      U0 (initial state), U, P, p_ref and run counters of the
                       compiled reference on the case built by CASES[name]
+  ref_sat_tables.npz  the reference's saturation tables (SAT after build_sat) of the
+                      liquid / vapour pairs in SAT_CASES
   ref_main_outputs.npz
                       the files the reference's own main() writes (profile, snapshot
                       profiles, probe) and its end-of-run line, for the runs in
@@ -33,6 +35,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.dirname(HERE))  # tests/helpers.py
 
 from diffusionimex_b200 import cases  # noqa: E402
 
@@ -106,6 +109,21 @@ CASES = {
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "bubble_outlet32_3steps": (lambda: _bc(_bubble(32), (PRES, PRES, W, W), bcp=(1.2e7, 0.8e7, 0, 0)), "steps", 3,
                                {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # chemical relaxation (RELAX_LEVEL 2 p-pT-pTg, 3 p-pTg; closure_pTg :811-834, Tsat :114-163,
+    # closure_type_of :870-886) on the reference's liquid-vapour cases
+    "dodecane_relax2_N200_20steps": (lambda: dict(cases.reference_case(3, 200), relax=2), "steps", 20, {}),
+    "dodecane_relax3_N200_20steps": (lambda: dict(cases.reference_case(3, 200), relax=3), "steps", 20, {}),
+    "cavitation_relax2_N200_20steps": (lambda: dict(cases.reference_case(1, 200), relax=2), "steps", 20, {}),
+    "bartak_N200_20steps": (lambda: cases.reference_case(32, 200), "steps", 20, {}),
+    "chem0d_N16_10steps": (lambda: dict(cases.reference_case(41, 16), relax=2), "steps", 10, {"bicg_tol": 1e-13}),
+    "bubblecomp32_3steps": (lambda: cases.bubble_compression(32, 32), "steps", 3,
+                            {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # the same before their first round-off type decision (pTg already active, noise < 1e-12)
+    "dodecane_relax2_N200_2steps": (lambda: dict(cases.reference_case(3, 200), relax=2), "steps", 2, {}),
+    "dodecane_relax3_N200_2steps": (lambda: dict(cases.reference_case(3, 200), relax=3), "steps", 2, {}),
+    "bartak_N200_5steps": (lambda: cases.reference_case(32, 200), "steps", 5, {}),
+    "bubblecomp32_1step": (lambda: cases.bubble_compression(32, 32), "steps", 1,
+                           {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)
     "case13_N200_20steps": (lambda: cases.reference_case(13, 200), "steps", 20, {}),
     "lowmach_rus0_32_stage": (lambda: dict(_lowmach(32), rus_local=0), "stage", 0,
@@ -142,6 +160,23 @@ def main_outputs():
     np.savez_compressed(os.path.join(HERE, "ref_main_outputs.npz"), **out)
 
 
+# liquid / vapour pairs whose saturation tables (build_sat, physics :127-153) are pinned
+SAT_CASES = (1, 3, 30, 31, 32)
+
+
+def sat_tables():
+    """The reference's own saturation table (its global SAT after build_sat) for the phase pairs of
+    SAT_CASES, one archive: n, pcrit, vcrit, pmin, ln p[n], Tsat[n] per case."""
+    import refio
+
+    out = {}
+    for case in SAT_CASES:
+        c = dict(cases.reference_case(case, 16), relax=2)
+        out[f"case{case}"] = refio.run_ref(c, mode=refio.MODE_SAT)["sat"]
+        print("sat table", case, int(out[f"case{case}"][0]), "points")
+    np.savez_compressed(os.path.join(HERE, "ref_sat_tables.npz"), **out)
+
+
 def build_case(name):
     fn, mode, nsteps, over = CASES[name]
     c = fn()
@@ -156,6 +191,9 @@ def main():
         raise SystemExit("oracle/_ref/spb6_ref is missing: run `make -C oracle ref` first")
     modes = {"tend": refio.MODE_TEND, "steps": refio.MODE_STEPS, "stage": refio.MODE_STAGE}
     only = sys.argv[1:]
+    if only == ["sat"]:
+        sat_tables()
+        return
     for name in (only or CASES):
         c, mode, nsteps = build_case(name)
         r = refio.run_ref(c, mode=modes[mode], nsteps=nsteps)
@@ -164,12 +202,20 @@ def main():
         extra = {}
         if mode == "stage":
             extra = {k: r[k] for k in ("Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y")}
+        if c.get("relax", 0) >= 2:  # the reference's own one-ulp libm noise (its type decisions at
+            # T = Tsat(p) are round-off decisions): per-field L1 of the ulp-up / ulp-down runs
+            from helpers import fieldwise_l1
+
+            extra["noise"] = np.maximum(*[fieldwise_l1(refio.run_ref(c, mode=modes[mode], nsteps=nsteps,
+                                                                     variant=v)["U"], r["U"])
+                                          for v in ("ulp", "ulpdown")])
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), U0=c["U"], U=r["U"], P=r["P"],
                             meta=json.dumps(meta), **extra)
         print(name, meta)
     if only:
         return
     main_outputs()
+    sat_tables()
     for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
                       ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):
         d = np.loadtxt(os.path.join(REF_TREE, path))
