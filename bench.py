@@ -68,7 +68,8 @@ def parse():
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
                         "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
-                        "<2D workload>-rus0 (grid-wide Rusanov speed), "
+                        "<2D workload>-rus0 (grid-wide Rusanov speed), bubblecomp200 (chemical relaxation, "
+                        "case 72), "
                         "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -100,6 +101,8 @@ def make_workload(name: str):
         c["workload"] = c.get("workload", name) + " (precision form)"
     elif name == "undex361x200":
         c = cases.underwater_explosion(361, 200)
+    elif name == "bubblecomp200":  # the reference's case 72 at its own 200 x 200 grid
+        c = cases.bubble_compression(200, 200)
     elif name == "bubbles1024-relax":
         c = cases.bubble_field(1024, seed=0, nbub=8)
         c.update(relax=1, eps_i=1e-4)
