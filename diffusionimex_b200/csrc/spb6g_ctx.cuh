@@ -57,12 +57,26 @@ inline void phys_from_config(const spb6g_config* cfg, Phys& P) {
     P.mg = cfg->kind[0] != 0 || cfg->kind[1] != 0;
     P.relax = cfg->relax;
     P.eps_i = cfg->eps_i;
+    // rates as main() resolves them (:1233-1235)
+    P.mu_rate = cfg->mu_rate;
+    P.theta_rate = cfg->theta_rate < 0 ? (cfg->relax >= 1 ? INFINITY : 0.0) : cfg->theta_rate;
+    P.nu_rate = cfg->nu_rate < 0 ? ((cfg->relax == 2 || cfg->relax == 3) ? INFINITY : 0.0) : cfg->nu_rate;
+    if (cfg->nu_law) P.nu_rate = 0.0;
+    P.nu_cr = cfg->nu_cr;
+    P.nu_pc = cfg->nu_pc;
+    P.relax_form = cfg->relax_form;
+    P.unify = cfg->unify;
+    P.unify_proj = cfg->unify_proj;
+    P.nu_law = cfg->nu_law;
+    P.mech = isinf(cfg->mu_rate) ? CL_P : CL_MU;
+    P.rates = (!isinf(cfg->mu_rate) || cfg->unify == 1) ? 1 : 0;
 }
 
 struct Ctx {
     Phys phy;
     Geom g;
-    unsigned char* ctype;  // per-cell closure type of the step (p-pT relaxation only)
+    unsigned char* ctype;
+    double* step_nu;  // nu law: each cell's mass transfer rate for the step (STEP_NU :175), else null  // per-cell closure type of the step (p-pT relaxation only)
     int n;
     int prec;  // 1: precision form (FP32 reconstruction, fluxes and SpMV), 0: FP64
     double tau, rx, ry, p_ref, adt;

@@ -376,7 +376,19 @@ SPB6G_DEV bool cell_residual(const Ctx& c, int i, int j, double Pc, double PW, d
     in.pguess = c.p_ref + Pc;
     in.Qph[0] = c.qph0[x];
     in.Qph[1] = c.qph1[x];
-    in.type = (SPB6G_MG && c.phy.relax) ? (int)c.ctype[x] : CL_P;  // S.type (:695), frozen per step
+    // S.type (:695): the activation's type, frozen per step; without relaxation the mechanical one
+    in.type = SPB6G_MG ? (c.phy.relax ? (int)c.ctype[x] : c.phy.mech) : CL_P;
+    in.tau = c.tau;
+    in.Z[0] = in.Z[1] = 1.0;
+    in.nu = (SPB6G_MG && c.step_nu) ? c.step_nu[x] : -1.0;
+    if (SPB6G_MG && in.type == CL_MU) {  // impedances of the stage's unit contents X* / (a1 + a2) (:1036-1037)
+        const double sa = c.Xs.v[IA1][x] + c.a2s[x];
+        for (int k = 0; k < 2; k++) {
+            const double a = (k == 0 ? c.Xs.v[IA1][x] : c.a2s[x]) / sa, m = c.Xs.v[k == 0 ? IM1 : IM2][x] / sa;
+            const double pk = p_ame(c.phy, k, a, m, c.Xs.v[k == 0 ? IE1 : IE2][x] / sa), r = m / a;
+            in.Z[k] = r * sqrt(SMAX(c2_rp(c.phy, k, r, pk), 1e-30));
+        }
+    }
     ClOut o;
     if (!closure(c.phy, in, o)) return false;
     Gr = (o.pbar - c.p_ref) - Pc;
@@ -1431,10 +1443,13 @@ void launch_floor(const Ctx& c, cudaStream_t st, double tol) {
 // same closure of the same input).
 #if SPB6G_MG
 __global__ void k_relax_activate(Ctx c, State U) {
+    const Phys& P = c.phy;
+    const int therm = isinf(P.theta_rate) ? CL_PT : CL_THETA, chem = isinf(P.nu_rate) ? CL_PTG : CL_NU;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double a1 = U.v[IA1][x];
-        unsigned char ty = CL_P;
-        if (c.phy.relax > 0 && a1 >= c.phy.eps_i && a1 <= 1.0 - c.phy.eps_i) {
+        int ty = P.mech;
+        double nu = 0.0;
+        if (P.relax > 0 && a1 >= P.eps_i && a1 <= 1.0 - P.eps_i) {
             const double m1 = U.v[IM1][x], m2 = U.v[IM2][x], mu = U.v[IMU][x], mv = U.v[IMV][x];
             const double rho = m1 + m2;
             ClIn in;
@@ -1442,41 +1457,51 @@ __global__ void k_relax_activate(Ctx c, State U) {
             in.etr[0] = U.v[IE1][x]; in.etr[1] = U.v[IE2][x];
             in.s = 0.0;
             in.rhoeC = U.v[IEN][x] - 0.5 * (mu * mu + mv * mv) / rho;
-            in.pguess = SMAX(p_mix(c.phy, in.atr[0], in.mtr[0], in.mtr[1], in.rhoeC), 1.0);
+            in.pguess = SMAX(p_mix(P, in.atr[0], in.mtr[0], in.mtr[1], in.rhoeC), 1.0);
             in.Qph[0] = in.Qph[1] = 0.0;
+            in.tau = 0.0;
+            in.Z[0] = in.Z[1] = 1.0;
+            in.nu = -1.0;
             ClOut o;
-            bool have = false;  // o holds the projection of type ty
-            if (c.phy.relax == 3) {
+            if (P.relax == 3) {  // a phase above Tsat in the p closure without the energy defect
                 in.type = CL_PND;
-                if (closure(c.phy, in, o)) {
-                    const double p = o.pbar, Ts = sat_temperature(c.phy, p);
-                    if (isfinite(Ts) && (T_amp(c.phy, 0, o.a[0], m1, p) > Ts || T_amp(c.phy, 1, o.a[1], m2, p) > Ts))
-                        ty = CL_PTG;
+                if (closure(P, in, o)) {
+                    const double p = o.pbar, Ts = sat_temperature(P, p);
+                    if (isfinite(Ts) && (T_amp(P, 0, o.a[0], m1, p) > Ts || T_amp(P, 1, o.a[1], m2, p) > Ts)) ty = chem;
                 }
-            } else {
-                ty = CL_PT;
-                in.type = CL_PT;
-                have = closure(c.phy, in, o);
-                if (c.phy.relax == 2 && have) {
-                    const double Ts = sat_temperature(c.phy, o.pbar);
-                    if (isfinite(Ts) && o.T > Ts) { ty = CL_PTG; have = false; }
+            } else {  // levels 1, 2: thermal, or chemical where the pT state is above Tsat (level 2)
+                ty = therm;
+                if (P.relax == 2) {
+                    const ClMg r = closure_pT(P, m1, m2, in.rhoeC, in.pguess);
+                    if (r.ok) {
+                        const double Ts = sat_temperature(P, r.o.pbar);
+                        if (isfinite(Ts) && r.o.Tk[0] > Ts) ty = chem;
+                    }
                 }
             }
-            if (ty != CL_P && !have) {
+            if (ty == CL_PT || ty == CL_PTG) {  // project_cell: the closure is also the feasibility test
                 in.type = ty;
-                have = closure(c.phy, in, o);
+                if (!closure(P, in, o)) {
+                    ty = P.mech;
+                } else if (P.unify_proj) {
+                    U.v[IA1][x] = o.a[0];
+                    U.v[IM1][x] = o.m[0];
+                    U.v[IM2][x] = o.m[1];
+                    U.v[IE1][x] = o.e[0];
+                    U.v[IE2][x] = o.e[1];
+                }
             }
-            if (ty != CL_P && have) {
-                U.v[IA1][x] = o.a[0];
-                U.v[IM1][x] = o.m[0];
-                U.v[IM2][x] = o.m[1];
-                U.v[IE1][x] = o.e[0];
-                U.v[IE2][x] = o.e[1];
-            } else {
-                ty = CL_P;
+            if (P.nu_law && ty == CL_NU) {  // the rate at the cell's pT state (no mass transfer), :574-581
+                in.atr[0] = U.v[IA1][x]; in.atr[1] = 1.0 - in.atr[0];
+                in.mtr[0] = U.v[IM1][x]; in.mtr[1] = U.v[IM2][x];
+                in.etr[0] = U.v[IE1][x]; in.etr[1] = U.v[IE2][x];
+                in.pguess = SMAX(p_mix(P, in.atr[0], in.mtr[0], in.mtr[1], in.rhoeC), 1.0);
+                in.type = CL_PT;
+                if (closure(P, in, o)) nu = nu_law(P, o.pbar, o.Tk[0], o.a[1]);
             }
         }
-        c.ctype[x] = ty;
+        c.ctype[x] = (unsigned char)ty;
+        if (c.step_nu) c.step_nu[x] = nu;
     }
 }
 #endif
@@ -1497,9 +1522,10 @@ SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
         double Gr;
         CellRes o;
         if (!residual_at(c, i, j, p, 0, -1, 0, Gr, &o)) { atomicOr(&c.ns->fail, 8); return; }
-        // a pTg cell exchanges mass: its phase masses are the closure's (:1063)
-        const int ty = (SPB6G_MG && c.phy.relax) ? (int)c.ctype[x] : CL_P;
-        const double mk[2] = {ty == CL_PTG ? o.o.m[0] : o.in.mtr[0], ty == CL_PTG ? o.o.m[1] : o.in.mtr[1]};
+        // the phase masses are the closure's (:1063): pTg and nu cells exchange mass
+        const int ty = o.in.type;
+        const bool xm = SPB6G_MG && (ty == CL_PTG || ty == CL_NU || (ty == CL_PT && c.phy.unify == 1));
+        const double mk[2] = {xm ? o.o.m[0] : o.in.mtr[0], xm ? o.o.m[1] : o.in.mtr[1]};
         double U[NV];
         U[IA1] = o.o.a[0]; U[IM1] = mk[0]; U[IM2] = mk[1]; U[IMU] = o.mx; U[IMV] = o.my;
         U[IE1] = o.o.e[0]; U[IE2] = o.o.e[1]; U[IEN] = o.E;
@@ -1512,8 +1538,9 @@ SPB6G_DEV void final_at(const Ctx& c, int x, double* tm = nullptr) {
         }
         if (tm) {  // st_Tmax (:1064-1065): the phase temperatures where the phase is present
 #pragma unroll
-            for (int k = 0; k < 2; k++) {  // pT / pTg cells: the common temperature of the closure
-                const double T = ty != CL_P ? o.o.T : T_amp(c.phy, k, o.o.a[k], mk[k], o.o.pbar);
+            for (int k = 0; k < 2; k++) {  // the closure's phase temperatures (o.cl.T :1066-1067)
+                const bool own = SPB6G_MG && (ty != CL_P || c.phy.unify == 1);
+                const double T = own ? o.o.Tk[k] : T_amp(c.phy, k, o.o.a[k], mk[k], o.o.pbar);
                 if (o.o.a[k] > 1e-9 && isfinite(T)) tm[k] = SMAX(tm[k], T);
             }
         }

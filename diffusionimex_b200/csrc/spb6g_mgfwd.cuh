@@ -50,14 +50,14 @@ inline spb6g_mg::CState mg_view(const CState& u) {
 }
 }  // namespace spb6g
 // First statement of a default launcher: run the extended build's launcher instead.
-// SPB6G_MG_FORWARD: kernels that evaluate the closure (its type is per cell under p-pT
-// relaxation) and so need the extended build for a Mie-Grueneisen phase or for relax > 0.
+// SPB6G_MG_FORWARD: kernels that evaluate the closure (its type is per cell under relaxation)
+// and so need the extended build for a Mie-Grueneisen phase, relax > 0, a finite mu or unify = 1.
 // SPB6G_MG_FORWARD_EOS: kernels that evaluate the equations of state but never the closure;
 // with stiffened-gas / NASG phases they are the same in both builds, so only a
 // Mie-Grueneisen phase sends them to the extended build.
 #define SPB6G_MG_FORWARD(name, ...)                      \
     do {                                                 \
-        if (c.phy.mg || c.phy.relax) {                   \
+        if (c.phy.mg || c.phy.relax || c.phy.rates) {    \
             spb6g_mg::name(__VA_ARGS__);                 \
             return;                                      \
         }                                                \

@@ -51,11 +51,18 @@ struct Phys {
     double eps_i;    // EPS_I (:40): interface zone eps_I <= alpha1 <= 1 - eps_I
     const double* sat;  // relax >= 2: the saturation table (SatTable :114), packed as n, pcrit, vcrit,
                         // pmin, ln p[n], Tsat[n]
+    // relaxation rates (mu_rate, theta_rate, nu_rate :35; INFINITY instantaneous; theta and nu
+    // resolved to the level's defaults, nu 0 under the nu law), the nu law's coefficient and
+    // pressure (NU_CR, NU_PC :38), RELAX_FORM (:42), UNIFY, UNIFY_PROJ (:45), NU_LAW (:37)
+    double mu_rate, theta_rate, nu_rate, nu_cr, nu_pc;
+    int relax_form, unify, unify_proj, nu_law;
+    int mech;  // the mechanical closure type: CL_P (mu = inf) or CL_MU
+    int rates; // a finite mu or unify = 1: closure kernels take the extended build even at relax 0
 };
-// Closure types (ClosureType :228) built here: p (mechanical), pT (instantaneous thermal) and pTg
-// (instantaneous thermal and chemical).  CL_PND is internal: the p closure without the energy
-// defect (ClIn::nodelta :236), the prediction of the p-pTg activation test (:878).
-enum { CL_P = 0, CL_PT = 2, CL_PTG = 5, CL_PND = 6 };
+// Closure types (ClosureType :228): p, finite mu, pT, finite theta, finite nu, pTg.  CL_PND is
+// internal: the p closure without the energy defect (ClIn::nodelta :236), the prediction of the
+// p-pTg activation test (:878).
+enum { CL_P = 0, CL_MU = 1, CL_PT = 2, CL_THETA = 3, CL_NU = 4, CL_PTG = 5, CL_PND = 6 };
 
 // ------------------------------------------------------------ EOS, src/spb6_physics_omp.h:60-111
 // Mie-Grueneisen reference curves pr(rho), pr'(rho), er(rho) (mg_ref :60-69): Cochran-Chan
@@ -164,11 +171,14 @@ SPB6G_DEV double eps_round(const Phys& P, int k, double a, double m) {
 // ------------------------------------------------------------ closure, :229-243, :430-548, :842-866
 struct ClIn {
     double atr[2], mtr[2], etr[2], s, rhoeC, pguess, Qph[2];
-    int type;  // CL_P or CL_PT, frozen per step by the activation
+    int type;     // closure type, frozen per step by the activation
+    double tau;   // finite rates: the stage's implicit step a_ii dt (0 at activation)
+    double Z[2];  // finite mu: the phases' acoustic impedances, frozen per stage (1 otherwise)
+    double nu;    // finite nu: the cell's rate under the nu law, < 0 for nu_rate
 };
 struct ClOut {
     double a[2], e[2], pbar;
-    double m[2], T;  // pT / pTg closures: phase masses (pTg moves mass) and the common temperature
+    double m[2], Tk[2];  // closures other than p: phase masses (pTg and nu move mass) and temperatures
 };
 
 SPB6G_DEV double E_above(const Phys& P, const ClIn& in, int k) {  // :430-433
@@ -505,9 +515,9 @@ static __device__ __noinline__ ClMg closure_pT(const Phys P, double m0, double m
         res.o.a[k] = m[k] * v_pT(k, p, T);
         res.o.e[k] = m[k] * e_pT(k, p, T);
         res.o.m[k] = m[k];
+        res.o.Tk[k] = T;
     }
     res.o.pbar = p;
-    res.o.T = T;
     res.ok = T > 0;
     return res;
 }
@@ -596,12 +606,316 @@ static __device__ __noinline__ ClMg closure_pTg(const Phys P, double m0, double 
     for (int k = 0; k < 2; k++) {
         res.o.a[k] = res.o.m[k] * v_pT(P.ph[k], p, T);
         res.o.e[k] = res.o.m[k] * e_pT(P.ph[k], p, T);
+        res.o.Tk[k] = T;
     }
     res.o.pbar = p;
-    res.o.T = T;
     res.ok = 1;
     return res;
 }
+
+// ---- finite relaxation rates (B6.2, B6.4, B6.5), built with the extended physics
+// Finite pressure relaxation (closure_mu :636-714): the volume transfer R of phase 1 over the
+// stage, with (p1, p2)(R) from the 2 x 2 linear energy system (pressure work at the interface
+// pressure weighted by the impedances Z), solves F(R) = R - tau mu (p1 - p2) = 0 (backward
+// Euler) between 0 and the sign change of F, bracketed outwards and refined by Brent.  For
+// tau mu = inf, or the exponential form (relaxform 1), it first solves p1 = p2 (R_eq, bracketed
+// from the acoustic linearisation, not across the system's singularity); the exponential form
+// then takes R = R_eq (1 - exp(-tau mu D)) with the secant D = dp(0) / R_eq.
+static __device__ __noinline__ ClMg closure_mu(const Phys P, const ClIn in, double mrate) {
+    ClMg res;
+    res.ok = 0;
+    const PhaseD &h0 = P.ph[0], &h1 = P.ph[1];
+    const double sa = in.atr[0] + in.atr[1];
+    const double om[2] = {in.atr[0] / sa, in.atr[1] / sa};
+    const double ak[2] = {in.atr[0] / sa, in.atr[1] / sa};
+    ClPre pr;
+    closure_pre(P, in, pr);
+    const double D0 = pr.D0;
+    double lam[2], ex[2];
+    seg_lambda(in, pr, in.pguess, lam, ex);
+    const double w1 = in.Z[0] + in.Z[1] > 0 ? in.Z[1] / (in.Z[0] + in.Z[1]) : 0.5, w2 = 1.0 - w1;
+    const double tm = isinf(mrate) ? INFINITY : in.tau * mrate;
+    double det = 0.0;
+    auto solve = [&](double R, double& p1, double& p2) -> bool {
+        const double a1 = ak[0] + R, a2 = ak[1] - R;
+        const double C1 = dedp_am(P, 0, a1, in.mtr[0]) + om[0] * in.s, C2 = dedp_am(P, 1, a2, in.mtr[1]) + om[1] * in.s;
+        const double M11 = C1 + R * w1 - lam[0] * in.s * om[0], M12 = R * w2 - lam[0] * in.s * om[1];
+        const double M21 = -R * w1 - lam[1] * in.s * om[0], M22 = C2 - R * w2 - lam[1] * in.s * om[1];
+        const double r1 = in.etr[0] - in.mtr[0] * h0.q - h0.g * h0.pi * dedp_am(P, 0, a1, in.mtr[0]) + lam[0] * D0 + ex[0];
+        const double r2 = in.etr[1] - in.mtr[1] * h1.q - h1.g * h1.pi * dedp_am(P, 1, a2, in.mtr[1]) + lam[1] * D0 + ex[1];
+        det = M11 * M22 - M12 * M21;
+        if (!(fabs(det) > 0)) return false;
+        p1 = (r1 * M22 - M12 * r2) / det;
+        p2 = (M11 * r2 - M21 * r1) / det;
+        return isfinite(p1) && isfinite(p2);
+    };
+    double R = 0.0, p1, p2;
+    const bool eq = P.relax_form == 1 || isinf(tm);
+    if (tm > 0) {
+        double det0 = 0.0, r0 = 0.0;  // r0: start of the bracket, inside the admissible volumes for R_eq
+        if (eq) {
+            const double Rlo = in.mtr[0] * h0.b - ak[0], Rhi = ak[1] - in.mtr[1] * h1.b;
+            if (!(Rlo < Rhi)) return res;
+            if (!(Rlo < 0.0 && 0.0 < Rhi)) r0 = Rlo >= 0.0 ? Rlo + 1e-9 * (Rhi - Rlo) : Rhi - 1e-9 * (Rhi - Rlo);
+        }
+        auto Fa = [&](double r, double& f) -> bool {
+            double q1, q2;
+            if (!solve(r, q1, q2)) return false;
+            const double a1 = ak[0] + r, a2 = ak[1] - r;
+            if (!(a1 > in.mtr[0] * h0.b && a2 > in.mtr[1] * h1.b)) return false;
+            if (eq) {
+                if (r != r0 && !(det * det0 > 0)) return false;  // not across the singularity
+            } else if (!(q1 + h0.pi > 0 && q2 + h1.pi > 0)) {
+                return false;
+            }
+            f = eq ? q2 - q1 : r - tm * (q1 - q2);
+            return isfinite(f);
+        };
+        double f0;
+        if (!Fa(r0, f0)) return res;
+        det0 = det;
+        if (eq && fabs(f0) <= 1e-13 * (fabs(in.pguess) + h0.g * fabs(h0.pi) + h1.g * fabs(h1.pi))) f0 = 0.0;
+        R = r0;
+        if (f0 != 0.0) {
+            double hi = -f0;
+            if (eq) {  // acoustic linearisation, else half the compressed phase's compressible volume
+                double q[2], k = 0.0;
+                solve(r0, q[0], q[1]);
+                for (int j = 0; j < 2; j++) {
+                    const double a = ak[j] + (j == 0 ? r0 : -r0), r = in.mtr[j] / a;
+                    k += r * c2_rp(P, j, r, q[j]) / a;
+                }
+                hi = -f0 / k;
+                if (!(isfinite(hi) && hi * -f0 > 0))
+                    hi = f0 < 0 ? 0.5 * (ak[1] - r0 - in.mtr[1] * h1.b) : -0.5 * (ak[0] + r0 - in.mtr[0] * h0.b);
+                hi += r0;
+            }
+            double lo = r0, flo = f0, fhi = NAN;
+            bool ok = false, exact = false;
+            for (int it = 0; it < 200; it++) {
+                if (Fa(hi, fhi)) {
+                    if (eq && fhi == 0.0) { ok = exact = true; break; }
+                    if (fhi * flo < 0) { ok = true; break; }
+                    lo = hi;
+                    flo = fhi;
+                    hi = lo + (lo - r0 == 0 ? -f0 : (lo - r0));
+                } else {
+                    hi = 0.5 * (lo + hi);
+                }
+            }
+            if (!ok) return res;
+            auto F = [&](double r) {
+                double f;
+                return Fa(r, f) ? f : (double)NAN;
+            };
+            if (exact) R = hi;
+            else if (!brent(F, SMIN(lo, hi), SMAX(lo, hi), lo < hi ? flo : fhi, lo < hi ? fhi : flo,
+                            1e-16 * (fabs(lo) + fabs(hi)) + 1e-300, R))
+                return res;
+        }
+        if (P.relax_form == 1 && !isinf(tm)) {
+            const double D = R != 0.0 && r0 == 0.0 ? -f0 / R : 0.0;
+            if (D > 0 && isfinite(D)) R = -R * expm1(-tm * D);
+        }
+    }
+    if (!solve(R, p1, p2)) return res;
+    const double pp[2] = {p1, p2};
+    for (int k = 0; k < 2; k++) {
+        res.o.a[k] = ak[k] + (k == 0 ? R : -R);
+        res.o.m[k] = in.mtr[k];
+        if (!(res.o.a[k] > res.o.m[k] * P.ph[k].b) || !(pp[k] + P.ph[k].pi > 0)) return res;
+        res.o.e[k] = eps_amp(P, k, res.o.a[k], res.o.m[k], pp[k]);
+        res.o.Tk[k] = T_amp(P, k, res.o.a[k], res.o.m[k], pp[k]);
+    }
+    res.o.pbar = res.o.a[0] * p1 + res.o.a[1] * p2;
+    res.ok = 1;
+    return res;
+}
+
+// Finite heat exchange at mu = inf (closure_theta :732-764): at fixed p each phase's temperature is
+// linear in the heat dQ moved, so dQ has a closed form -- backward Euler tt (T2 - T1) / (1 + tt S)
+// or the exponential (T2 - T1)(1 - exp(-tt S)) / S, tt = tau theta, S = 1/Cp1 + 1/Cp2 -- and p
+// solves sum_k alpha_k(p, dQ(p)) = 1 by root_above.
+static __device__ __noinline__ ClMg closure_theta(const Phys P, const ClIn in, double th) {
+    ClMg res;
+    res.ok = 0;
+    if (!(in.mtr[0] + in.mtr[1] > 0)) return res;
+    ClPre pr;
+    closure_pre(P, in, pr);
+    double lam[2], ex[2];
+    seg_lambda(in, pr, in.pguess, lam, ex);
+    double A[2], B[2], N[2];  // p_coef (:452-465)
+    for (int k = 0; k < 2; k++) {
+        A[k] = in.etr[k] - in.mtr[k] * P.ph[k].q + lam[k] * pr.D0 + ex[k];
+        B[k] = in.atr[k] + lam[k] * in.s;
+        N[k] = A[k] - (B[k] - in.mtr[k] * P.ph[k].b) * P.ph[k].pi;
+    }
+    const double tt = isinf(th) ? INFINITY : in.tau * th;
+    if (tt > 0 && !isinf(tt))
+        for (int k = 0; k < 2; k++)
+            if (!(N[k] > 0)) return res;
+    const double Cp[2] = {P.ph[0].g * P.ph[0].cv * in.mtr[0], P.ph[1].g * P.ph[1].cv * in.mtr[1]};
+    const double S = 1.0 / Cp[0] + 1.0 / Cp[1];
+    auto eval = [&](double p, double a[2]) {
+        double a0[2], T0[2];
+        for (int k = 0; k < 2; k++) {  // alpha_p (:466)
+            const PhaseD& h = P.ph[k];
+            a0[k] = ((h.g - 1.0) * (A[k] + B[k] * p) + (p + h.g * h.pi) * in.mtr[k] * h.b) / (h.g * (p + h.pi));
+            T0[k] = T_amp(P, k, a0[k], in.mtr[k], p);
+        }
+        double dQ;
+        if (P.relax_form == 1) dQ = (T0[1] - T0[0]) * (-expm1(-tt * S)) / S;
+        else if (isinf(tt)) dQ = (T0[1] - T0[0]) / S;
+        else dQ = tt * (T0[1] - T0[0]) / (1.0 + tt * (1.0 / Cp[0] + 1.0 / Cp[1]));
+        a[0] = a0[0] + (P.ph[0].g - 1.0) * dQ / (P.ph[0].g * (p + P.ph[0].pi));
+        a[1] = a0[1] - (P.ph[1].g - 1.0) * dQ / (P.ph[1].g * (p + P.ph[1].pi));
+    };
+    auto Phi = [&](double p) {
+        double a[2];
+        eval(p, a);
+        return a[0] + a[1] - 1.0;
+    };
+    double p;
+    if (!root_above(Phi, SMAX(-P.ph[0].pi, -P.ph[1].pi), in.pguess, p)) return res;
+    double a[2];
+    eval(p, a);
+    for (int k = 0; k < 2; k++) {
+        res.o.a[k] = a[k];
+        res.o.m[k] = in.mtr[k];
+        if (!(res.o.a[k] > res.o.m[k] * P.ph[k].b)) return res;
+        res.o.e[k] = eps_amp(P, k, res.o.a[k], res.o.m[k], p);
+        res.o.Tk[k] = T_amp(P, k, res.o.a[k], res.o.m[k], p);
+    }
+    res.o.pbar = p;
+    res.ok = 1;
+    return res;
+}
+
+// Finite mass transfer at mu = theta = inf (closure_nu :771-809): at each trial p the vapour
+// fraction Y solves rho Y - m2 + tau nu (g2 - g1)(p, T(p, Y)) = 0 (backward Euler; Brent on the
+// admissible interval, clamped to its end where it has no root), or for the exponential form Y =
+// Y_eq + (Y0 - Y_eq) exp(-tau nu D / rho) with the secant D through Y_eq and the transported Y0;
+// p solves rho ((1 - Y) v1 + Y v2) = 1 by root_above.
+static __device__ __noinline__ ClMg closure_nu(const Phys P, const ClIn in, double nr) {
+    ClMg res;
+    res.ok = 0;
+    const double rho = in.mtr[0] + in.mtr[1], eC = in.rhoeC / rho;
+    const double tn = isinf(nr) ? INFINITY : in.tau * nr;
+    const double Y0 = in.mtr[1] / rho;
+    const PhaseD &h0 = P.ph[0], &h1 = P.ph[1];
+    auto Yof = [&](double p, double& Y, double& T) -> bool {
+        auto G = [&](double y) {
+            const double TT = T_of_energy(P, p, y, eC);
+            if (!(TT > 0)) return (double)NAN;
+            return g_pT(h1, p, TT) - g_pT(h0, p, TT);
+        };
+        auto Rf = [&](double y) {
+            if (P.relax_form == 1 || isinf(tn)) return G(y);
+            const double TT = T_of_energy(P, p, y, eC);
+            if (!(TT > 0)) return (double)NAN;
+            return rho * y - in.mtr[1] + tn * (g_pT(h1, p, TT) - g_pT(h0, p, TT));
+        };
+        double ya = Y_MIN, yb = 1.0 - Y_MIN;  // T(p, y) > 0 bounds y on the side of the larger q
+        const double dq = h1.q - h0.q, yT = dq != 0.0 ? (eC - h0.q) / dq : INFINITY;
+        if (dq > 0) yb = SMIN(yb, yT * (1.0 - 1e-12));
+        else if (dq < 0) ya = SMAX(ya, yT * (1.0 + 1e-12));
+        if (!(ya < yb)) return false;
+        if (P.relax_form == 1 && tn == 0.0) {
+            Y = SMIN(SMAX(Y0, ya), yb);
+            T = T_of_energy(P, p, Y, eC);
+            return T > 0;
+        }
+        const double Ra = Rf(ya), Rb = Rf(yb);
+        if (!isfinite(Ra) || !isfinite(Rb)) return false;
+        if (Ra >= 0) Y = ya;
+        else if (Rb <= 0) Y = yb;
+        else if (!brent(Rf, ya, yb, Ra, Rb, 1e-16, Y)) return false;
+        if (P.relax_form == 1 && !isinf(tn)) {  // Y is Y_eq(p)
+            const double Yeq = Y, Ys = SMIN(SMAX(Y0, ya), yb);
+            const double D = Ys != Yeq ? G(Ys) / (Ys - Yeq) : 0.0;
+            if (D > 0 && isfinite(D)) {
+                Y = SMIN(SMAX(Yeq + (Y0 - Yeq) * exp(-(tn * D) / rho), ya), yb);
+            } else if (fabs(Ys - Yeq) <= 1e-14) {
+                Y = Yeq;
+            } else {  // G not monotone: the backward-Euler root
+                auto Rbe = [&](double y) {
+                    const double gg = G(y);
+                    return isfinite(gg) ? rho * y - in.mtr[1] + tn * gg : (double)NAN;
+                };
+                const double ra = Rbe(ya), rb = Rbe(yb);
+                if (!isfinite(ra) || !isfinite(rb)) return false;
+                if (ra >= 0) Y = ya;
+                else if (rb <= 0) Y = yb;
+                else if (!brent(Rbe, ya, yb, ra, rb, 1e-16, Y)) return false;
+            }
+        }
+        T = T_of_energy(P, p, Y, eC);
+        return T > 0;
+    };
+    auto Phi = [&](double p) {
+        double Y, T;
+        if (!Yof(p, Y, T)) return (double)NAN;
+        return rho * ((1 - Y) * v_pT(h0, p, T) + Y * v_pT(h1, p, T)) - 1.0;
+    };
+    double p;
+    if (!root_above(Phi, SMAX(-h0.pi, -h1.pi), in.pguess, p)) return res;
+    double Y, T;
+    if (!Yof(p, Y, T)) return res;
+    res.o.m[0] = rho * (1 - Y);
+    res.o.m[1] = rho * Y;
+    for (int k = 0; k < 2; k++) {
+        res.o.a[k] = res.o.m[k] * v_pT(P.ph[k], p, T);
+        res.o.e[k] = res.o.m[k] * e_pT(P.ph[k], p, T);
+        res.o.Tk[k] = T;
+    }
+    res.o.pbar = p;
+    res.ok = 1;
+    return res;
+}
+
+// Every closure but p for SG / NASG phases (closure :842-866): the instantaneous pT and pTg, the
+// finite-rate mu, theta and nu, and under unify = 1 the instantaneous p, pT and pTg as the mu,
+// theta and nu closures at rate = inf (closure_rate_inf :836-841).
+static __device__ __noinline__ ClMg closure_relaxed(const Phys P, const ClIn in) {
+    const bool inst = in.type == CL_P || in.type == CL_PT || in.type == CL_PTG;
+    if (P.unify == 1 && inst) {
+        if (in.type == CL_P) return closure_mu(P, in, INFINITY);
+        if (in.type == CL_PT) return closure_theta(P, in, INFINITY);
+        return closure_nu(P, in, INFINITY);
+    }
+    switch (in.type) {
+        case CL_MU: return closure_mu(P, in, P.mu_rate);
+        case CL_PT: return closure_pT(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
+        case CL_THETA: return closure_theta(P, in, P.theta_rate);
+        case CL_NU: return closure_nu(P, in, in.nu >= 0 ? in.nu : P.nu_rate);
+        default: return closure_pTg(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
+    }
+}
+
+// Saturation pressure of temperature T, the inverse of Tsat by bisection in ln p over the table's
+// range (psat :165-172): 0 below it, INFINITY above.
+SPB6G_DEV double sat_pressure(const Phys& P, double T) {
+    if ((int)P.sat[0] < 1) return NAN;
+    double a = P.sat[3], b = P.sat[1] * (1 - 1e-12);
+    const double Ta = sat_temperature(P, a), Tb = sat_temperature(P, b);
+    if (!(T > Ta)) return 0.0;
+    if (!(T < Tb)) return INFINITY;
+    for (int it = 0; it < 80; it++) {
+        const double c = sqrt(a * b);
+        if (sat_temperature(P, c) < T) a = c;
+        else b = c;
+        if (b / a - 1 < 1e-14) break;
+    }
+    return sqrt(a * b);
+}
+// The mass transfer rate of a cell (nu_law :174-179, Pelanti 2022 (84)): nu_cr alpha_v^0.6
+// ((psat(T) - p) / (nu_pc - psat(T)))^1.76 for superheated liquid (p < psat(T)), else 0.
+SPB6G_DEV double nu_law(const Phys& P, double p, double T, double av) {
+    const double ps = sat_pressure(P, T);
+    if (!isfinite(ps) || !(ps > p) || !(ps < P.nu_pc) || !(av > 0)) return 0.0;
+    return P.nu_cr * pow(av, 0.6) * pow((ps - p) / (P.nu_pc - ps), 1.76);
+}
+
 
 // Bracketed safeguarded Newton on Phi (closure_p, :472-548), preceded by the
 // admissibility checks of closure() (:842-866).  At most 400 iterations.
@@ -610,12 +924,13 @@ SPB6G_DEV bool closure(const Phys& P, const ClIn& in, ClOut& o) {
     for (int k = 0; k < 2; k++)
         if (!(in.atr[k] > 0) || !(in.mtr[k] > 0) || !isfinite(in.etr[k])) return false;
     if (!isfinite(in.rhoeC) || !isfinite(in.s)) return false;
-    if (SPB6G_MG && in.type != CL_P && in.type != CL_PND) {  // thermal / chemical closures; Mie-Grueneisen
-        if (P.mg) return false;                              // phases relax mechanically only (:846)
-        const ClMg r = in.type == CL_PTG ? closure_pTg(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess)
-                                         : closure_pT(P, in.mtr[0], in.mtr[1], in.rhoeC, in.pguess);
-        o = r.o;
-        return r.ok && isfinite(o.pbar);
+    if (SPB6G_MG && in.type != CL_PND) {
+        if (P.mg && in.type != CL_P) return false;  // Mie-Grueneisen phases relax mechanically only (:846)
+        if (!P.mg && (in.type != CL_P || P.unify == 1)) {
+            const ClMg r = closure_relaxed(P, in);
+            o = r.o;
+            return r.ok && isfinite(o.pbar);
+        }
     }
     if (SPB6G_MG && P.mg) {
         const ClMg r = closure_p_mg(P, in);

@@ -497,6 +497,15 @@ void spb6g_default_config(spb6g_config* cfg) {
     cfg->gamma[0] = 4.4; cfg->pinf[0] = 6e8; cfg->gamma[1] = 1.4; cfg->pinf[1] = 0;
     cfg->cv[0] = cfg->cv[1] = 1000.0;
     cfg->eps_i = 1e-4;
+    cfg->mu_rate = INFINITY;
+    cfg->theta_rate = -1.0;
+    cfg->nu_rate = -1.0;
+    cfg->nu_cr = 1.0;
+    cfg->nu_pc = 22.064e6;
+    cfg->relax_form = 0;
+    cfg->unify = 0;
+    cfg->unify_proj = 1;
+    cfg->nu_law = 0;
     cfg->rk = 2; cfg->cfl = 0.2; cfg->cfl_ac = 0.4; cfg->ramp = 1; cfg->rus_local = 1; cfg->limiter = 1;
     cfg->newton_tol = 1e-13; cfg->newton_iter = 60; cfg->bicg_tol = 1e-13; cfg->bicg_iter = 4000;
     cfg->tend = 240e-6;
@@ -517,7 +526,12 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
     }
     if (cfg->relax < 0 || cfg->relax > 3) return SPB6G_BAD_ARG;
-    if (cfg->relax && (cfg->kind[0] || cfg->kind[1])) return SPB6G_UNSUPPORTED;
+    if (!(cfg->mu_rate >= 0) || !(cfg->nu_cr >= 0) || !(cfg->nu_pc > 0) || cfg->relax_form < 0 || cfg->relax_form > 1 ||
+        cfg->unify < 0 || cfg->unify > 2 || cfg->unify_proj < 0 || cfg->unify_proj > 1 || cfg->nu_law < 0 || cfg->nu_law > 1)
+        return SPB6G_BAD_ARG;
+    // Mie-Grueneisen phases relax mechanically and instantaneously only (closure :846)
+    if ((cfg->relax || !std::isinf(cfg->mu_rate) || cfg->unify == 1) && (cfg->kind[0] || cfg->kind[1]))
+        return SPB6G_UNSUPPORTED;
     if (cfg->relax && !(cfg->eps_i >= 0 && cfg->eps_i < 0.5)) return SPB6G_BAD_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;
@@ -571,6 +585,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.strong_list = (int*)A(n / 2 + 1);
     c.smask = (unsigned char*)A(n / 8 + 1);
     c.ctype = cfg->relax ? (unsigned char*)A(n / 8 + 1) : nullptr;  // n bytes
+    c.step_nu = (cfg->relax && cfg->nu_law) ? A(n) : nullptr;
     if (cfg->relax >= 2) {  // the saturation line (build_sat, physics :127-153; main :1236)
         const std::vector<double> sat = saturation_table(cfg);
         double* d = A(sat.size());
@@ -1060,7 +1075,8 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     for (int i = 0; i < count; i++)
         if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
             cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0 ||
-            cfgs[i].rus_local != 1)  // the batched kernel: SG / NASG, p, per-face Rusanov speed
+            cfgs[i].rus_local != 1 || !std::isinf(cfgs[i].mu_rate) ||
+            cfgs[i].unify == 1)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov speed
             return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;

@@ -52,7 +52,11 @@ class Config(ctypes.Structure):
         ("mg_G", ctypes.c_double * 2), ("mg_rr", ctypes.c_double * 2), ("mg_c1", ctypes.c_double * 2),
         ("mg_c2", ctypes.c_double * 2), ("mg_e1", ctypes.c_double * 2), ("mg_e2", ctypes.c_double * 2),
         ("mg_e0", ctypes.c_double * 2), ("eps_i", ctypes.c_double),
+        ("mu_rate", ctypes.c_double), ("theta_rate", ctypes.c_double), ("nu_rate", ctypes.c_double),
+        ("nu_cr", ctypes.c_double), ("nu_pc", ctypes.c_double), ("relax_form", ctypes.c_int32),
+        ("unify", ctypes.c_int32), ("unify_proj", ctypes.c_int32), ("nu_law", ctypes.c_int32),
     ]
+RATE_KEYS = ("mu_rate", "theta_rate", "nu_rate", "nu_cr", "nu_pc", "relax_form", "unify", "unify_proj", "nu_law")
 
 
 class Stats(ctypes.Structure):
@@ -162,6 +166,9 @@ def make_config(case: dict, device: int = 0) -> Config:
     c.precision = int(case.get("precision", 0))
     c.relax = int(case.get("relax", 0))
     c.eps_i = float(case.get("eps_i", 1e-4))
+    for k in RATE_KEYS:  # absent keys keep spb6g_default_config's values
+        if k in case:
+            setattr(c, k, type(getattr(c, k))(case[k]))
     return c
 
 

@@ -86,6 +86,18 @@ typedef struct {
     int32_t reserved[3];
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
     double eps_i;                   /* EPS_I (physics :40): interface zone eps_I <= alpha1 <= 1 - eps_I (1e-4) */
+    /* Relaxation rates (physics :34-46; mu=, theta=, nu=, relaxform=, unify=, unifyproj=, nulaw=,
+     * nucr=, nupc= arguments).  A rate of INFINITY is instantaneous; a finite rate turns the p, pT or
+     * pTg closure of a cell into its finite-rate form (closure_mu, closure_theta, closure_nu). */
+    double mu_rate;                 /* pressure relaxation rate (INFINITY) */
+    double theta_rate;              /* heat exchange rate; < 0: INFINITY for relax >= 1, else 0 (-1) */
+    double nu_rate;                 /* mass transfer rate; < 0: INFINITY for relax 2, 3, else 0 (-1) */
+    double nu_cr, nu_pc;            /* nu law (physics :36-38): coefficient (1) and pressure (22.064e6) */
+    int32_t relax_form;             /* RELAX_FORM: 0 backward Euler over the stage step, 1 exponential (0) */
+    int32_t unify;                  /* UNIFY: 1 the instantaneous closures as their rate = inf forms (0) */
+    int32_t unify_proj;             /* UNIFY_PROJ: 0 no projection of the step's state at activation (1) */
+    int32_t nu_law;                 /* NU_LAW: 1 the mass transfer rate of each cell from nu_law at the
+                                       step start (0) */
 } spb6g_config;
 
 /* Run statistics: the counters of the reference's stats line (:98-99, :1425). */

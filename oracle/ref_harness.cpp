@@ -93,10 +93,21 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
     // relaxation level and interface zone; the rates as main() defaults them (:1233-1234)
     RELAX_LEVEL = c.relax;
     EPS_I = c.eps_i;
-    mu_rate = INF;
-    theta_rate = RELAX_LEVEL >= 1 ? INF : 0.0;
-    nu_rate = (RELAX_LEVEL == 2 || RELAX_LEVEL == 3) ? INF : 0.0;
+    // the rates and forms as main() sets them from its arguments (:1211-1214, :1233-1235)
+    mu_rate = c.mu_rate;
+    theta_rate = c.theta_rate;
+    nu_rate = c.nu_rate;
+    NU_CR = c.nu_cr;
+    NU_PC = c.nu_pc;
+    RELAX_FORM = c.relax_form;
+    UNIFY = c.unify;
+    UNIFY_PROJ = c.unify_proj;
+    NU_LAW = c.nu_law;
+    if (theta_rate < 0) theta_rate = RELAX_LEVEL >= 1 ? INF : 0.0;
+    if (nu_rate < 0) nu_rate = (RELAX_LEVEL == 2 || RELAX_LEVEL == 3) ? INF : 0.0;
+    if (NU_LAW) nu_rate = 0.0;
     STEP_TYPE.clear();
+    STEP_NU.clear();
     // the saturation table of these phases, built before any parallel loop as main() does (:1236)
     if (RELAX_LEVEL > 0 && !mg_any()) build_sat();
     SHARE_MODE = c.share_mode;

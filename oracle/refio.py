@@ -34,7 +34,12 @@ CASE_DT = np.dtype([
     ("kind", "<i4", 2), ("mg_G", "<f8", 2), ("mg_rr", "<f8", 2), ("mg_c1", "<f8", 2), ("mg_c2", "<f8", 2),
     ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2), ("relax", "<i4"), ("pad2", "<i4"),
     ("eps_i", "<f8"),
+    ("mu_rate", "<f8"), ("theta_rate", "<f8"), ("nu_rate", "<f8"), ("nu_cr", "<f8"), ("nu_pc", "<f8"),
+    ("relax_form", "<i4"), ("unify", "<i4"), ("unify_proj", "<i4"), ("nu_law", "<i4"),
 ])
+# relaxation-rate settings of a case and their defaults (the reference's, physics :34-46)
+RATE_DEFAULTS = {"mu_rate": float("inf"), "theta_rate": -1.0, "nu_rate": -1.0, "nu_cr": 1.0, "nu_pc": 22.064e6,
+                 "relax_form": 0, "unify": 0, "unify_proj": 1, "nu_law": 0}
 MG_KEYS = ("G", "rr", "c1", "c2", "e1", "e2", "e0")
 RESULT_DT = np.dtype([
     ("magic", "<u4"), ("status", "<i4"), ("nx", "<i4"), ("ny", "<i4"),
@@ -47,7 +52,7 @@ RESULT_DT = np.dtype([
 def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int = 0, warmup: int = 0,
                 budget_s: float = 0.0) -> np.ndarray:
     r = np.zeros((), CASE_DT)
-    r["magic"], r["version"] = MAGIC, 3
+    r["magic"], r["version"] = MAGIC, 4
     for k in ("nx", "ny", "rk", "ramp", "rus_local", "limiter", "acdt", "newton_iter", "bicg_iter", "share_mode"):
         r[k] = int(cfg[k])
     r["bc"] = cfg["bc"]
@@ -63,6 +68,8 @@ def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int
         r["mg_" + f] = [float(cfg["phases"][k].get(f, 0.0)) for k in range(2)]
     r["relax"] = int(cfg.get("relax", 0))
     r["eps_i"] = float(cfg.get("eps_i", 1e-4))
+    for k, v in RATE_DEFAULTS.items():
+        r[k] = type(v)(cfg.get(k, v))
     return r
 
 

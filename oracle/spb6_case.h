@@ -20,7 +20,7 @@
 #include <stdint.h>
 
 #define SPB6_CASE_MAGIC 0x36425053u /* "SPB6" */
-#define SPB6_CASE_VERSION 3
+#define SPB6_CASE_VERSION 4
 
 enum { SPB6_MODE_STEPS = 0, SPB6_MODE_TEND = 1, SPB6_MODE_STAGE = 2, SPB6_MODE_SAT = 3 };
 enum { SPB6_BC_TRANS = 0, SPB6_BC_WALL = 1, SPB6_BC_PERIODIC = 2, SPB6_BC_PRES = 3 };
@@ -45,6 +45,10 @@ typedef struct {
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
     int32_t relax, pad2;  /* RELAX_LEVEL (reference harness only; the C restatement has relax 0) */
     double eps_i;
+    /* relaxation rates (reference harness only; the C restatement has the defaults): mu_rate, and
+       theta_rate / nu_rate < 0 for the level's default, nu law coefficient and pressure */
+    double mu_rate, theta_rate, nu_rate, nu_cr, nu_pc;
+    int32_t relax_form, unify, unify_proj, nu_law;
 } spb6_case;
 
 typedef struct {

@@ -31,14 +31,19 @@ RELAX_FIXTURES = ["tube_relax_N200_20steps", "bubble_relax32_3steps",
                   "dodecane_relax2_N200_20steps", "dodecane_relax3_N200_20steps", "cavitation_relax2_N200_20steps",
                   "bartak_N200_20steps", "chem0d_N16_10steps", "bubblecomp32_3steps",
                   "dodecane_relax2_N200_2steps", "dodecane_relax3_N200_2steps", "bartak_N200_5steps",
-                  "bubblecomp32_1step"]
+                  "bubblecomp32_1step",
+                  # finite rates: mu, theta, nu in both forms, all three at once, unify = 1, the nu law
+                  "mu0d_N4_10steps", "mu0d_expo_N4_10steps", "theta0d_N4_10steps", "theta0d_expo_N4_10steps",
+                  "nu0d_N4_10steps", "nu0d_expo_N4_10steps", "dodecane_rates_N200_2steps",
+                  "dodecane_rates_N200_20steps", "dodecane_unify_N200_2steps", "bartak_nulaw_N200_5steps",
+                  "bartak_nulaw_N200_20steps", "bubble_theta32_3steps"]
 SAT_FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_sat_tables.npz")
 
 
 @pytest.mark.parametrize("name", RELAX_FIXTURES)
 def test_case_builders_reproduce_the_fixture_states(name):
     c, _, _ = golden_case(name)
-    assert c["relax"] >= 1 and np.array_equal(c["U"], load_golden(name)["U0"])
+    assert (c.get("relax", 0) >= 1 or "mu_rate" in c) and np.array_equal(c["U"], load_golden(name)["U0"])
 
 
 @pytest.mark.parametrize("case", [1, 3, 30, 31, 32])
