@@ -94,7 +94,7 @@ CASES = {
     "tube_piston_N200_20steps": (lambda: _bc(_tube(200), (W, W, T, T), bcu=(50.0, -20.0, 0, 0)), "steps", 20, {}),
     "tube_outlet_N200_20steps": (lambda: _bc(_tube(200), (T, PRES, T, T), bcp=(0, 2e5, 0, 0)), "steps", 20, {}),
     "tube_periodic_N200_10steps": (lambda: _bc(_tube(200), (PER, PER, T, T)), "steps", 10,
-                                   {"bicg_tol": 1e-13, "dtfix": 1e-5}),
+                                   {"bicg_tol": 1e-13}),
     "bubble_walls32_3steps": (lambda: _bc(_bubble(32), (W, W, W, W), bcu=(0, 0, 5.0, 0)), "steps", 3,
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # Mie-Grueneisen phases (physics :51-111, closure_p_mg :585-629, hug_v / K_G :279-301)
@@ -201,6 +201,21 @@ def sat_tables():
     np.savez_compressed(os.path.join(HERE, "ref_sat_tables.npz"), **out)
 
 
+def case_settings(c: dict) -> dict:
+    """The scalar settings and phases of a case (everything but its state), as JSON values."""
+    def plain(v):
+        if isinstance(v, dict):
+            return {k: plain(x) for k, x in v.items()}
+        if isinstance(v, (list, tuple)):
+            return [plain(x) for x in v]
+        if isinstance(v, (np.floating, float)):
+            return float(v) if np.isfinite(v) else repr(float(v))
+        if isinstance(v, (np.integer, int, bool, str)):
+            return v if isinstance(v, (bool, str)) else int(v)
+        return None
+    return {k: plain(v) for k, v in c.items() if not isinstance(v, np.ndarray) and plain(v) is not None}
+
+
 def build_case(name):
     fn, mode, nsteps, over = CASES[name]
     c = fn()
@@ -223,6 +238,7 @@ def main():
         r = refio.run_ref(c, mode=modes[mode], nsteps=nsteps)
         meta = {k: r[k] for k in ("status", "steps", "rejects", "rk1", "stages", "newton_it", "floor_count", "t", "dt",
                                   "maxres", "p_ref")}
+        meta["config"] = case_settings(c)
         extra = {}
         if mode == "stage":
             extra = {k: r[k] for k in ("Xs", "a2s", "ube_x", "ube_y", "phi_x", "phi_y")}

@@ -13,6 +13,8 @@ import refio
 from helpers import golden_case, load_golden, mixture_pressure
 from diffusionimex_b200 import cases
 
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
 FIXTURES = ["case87_N200_tend", "case5_N100_tend", "case83_N200_10steps", "tube_N1000_1step", "tube_N200_stage",
             "bubble48_stage", "bubble48_4steps", "lowmach32_3steps", "shock64x32_3steps", "nasg256_20steps",
             # boundary variants: walls, pistons, pressure outlets, 1D periodic (cyclic matrix on BiCGStab)
@@ -88,3 +90,24 @@ def test_epoxy_spinel_initial_states_are_the_reference():
         r = refio.run_ref_main_files([f"case={case}", "N=200", "init=1"], nx=200)
         assert np.array_equal(r["U"], cases.reference_case(case, 200)["U"])
     assert cases.reference_case(13)["rus_local"] == 0 and cases.reference_case(12)["rus_local"] == 1
+
+
+def test_fixture_builders_keep_their_settings():
+    """Every fixture's case builder still produces the settings the fixture was made with (a
+    changed tolerance, step size or rate would leave U0 alone but the run different)."""
+    import glob
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN_DIR, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    names = [os.path.basename(f)[4:-4] for f in sorted(glob.glob(os.path.join(GOLDEN_DIR, "ref_*.npz")))]
+    checked = 0
+    for name in names:
+        if name not in mg.CASES:
+            continue
+        meta = load_golden(name)["meta"]
+        c, _, _ = mg.build_case(name)
+        assert mg.case_settings(c) == meta["config"], name
+        checked += 1
+    assert checked == len(mg.CASES)
