@@ -69,7 +69,7 @@ def parse():
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
                         "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
                         "<2D workload>-rus0 (grid-wide Rusanov speed), bubblecomp200 (chemical relaxation, "
-                        "case 72), "
+                        "case 72), dodecane2000-rates (finite relaxation rates, case 3), "
                         "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -103,6 +103,11 @@ def make_workload(name: str):
         c = cases.underwater_explosion(361, 200)
     elif name == "bubblecomp200":  # the reference's case 72 at its own 200 x 200 grid
         c = cases.bubble_compression(200, 200)
+    elif name == "dodecane2000-rates":  # the reference's case 3 at its own 2000 cells, finite rates
+        c = cases.reference_case(3)
+        c.update(relax=2, mu_rate=1e-2, theta_rate=1e5, nu_rate=1e3)
+        c["workload"] = ("dodecane liquid-vapour shock tube 1D, 2000 cells, relax 2 with finite rates "
+                         "mu 1e-2, theta 1e5, nu 1e3")
     elif name == "bubbles1024-relax":
         c = cases.bubble_field(1024, seed=0, nbub=8)
         c.update(relax=1, eps_i=1e-4)
@@ -347,6 +352,7 @@ def workload_config(c: dict, name: str) -> dict:
     return {"workload": c.get("workload", name), "nx": c["nx"], "ny": c["ny"], "fp": "fp64",
             "newton_tol": c["newton_tol"], "bicg_tol": c["bicg_tol"], "cfl": c["cfl"], "seed": c.get("seed", 0),
             "relax": c.get("relax", 0), "rus_local": c.get("rus_local", 1),
+            **{k: c[k] for k in ("mu_rate", "theta_rate", "nu_rate") if k in c},
             "l2": "working set > L2 (no flush needed)"}
 
 

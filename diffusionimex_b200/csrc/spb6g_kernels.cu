@@ -1388,8 +1388,74 @@ __global__ void k_thomas(Ctx c) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     thomas_solve(c);
 }
+// The same elimination with the rows staged in shared memory: every thread of the block forms the
+// rows' coefficients and right-hand sides (coalesced loads), one thread runs the two sweeps with
+// the next row's operands already in registers -- the chain is then the divisions' latency, not
+// a global-memory round trip per row -- and the block writes dP back.  The arithmetic and its
+// order are thomas_solve's, so the result is bitwise the same.
+constexpr int THOMAS_THREADS = 512;
+constexpr int THOMAS_SMEM_MAX_ROWS = (224 * 1024) / (4 * (int)sizeof(double));  // lo, di, up/cp, rhs/dp/x
+__global__ void __launch_bounds__(THOMAS_THREADS) k_thomas_smem(Ctx c) {
+    extern __shared__ __align__(16) double tsm[];
+    const Geom& g = c.g;
+    const int n = g.nx;
+    double* lo = tsm;
+    double* di = lo + n;
+    double* up = di + n;   // becomes cp
+    double* rhs = up + n;  // becomes dp, then the solution
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        double l = 0, d = 0, u = 0;
+        d += c.aC[r];
+        const int cw = mp_index(g, r - 1, 0), ce = mp_index(g, r + 1, 0);
+        const double vw = c.aW[r], ve = c.aE[r];
+        if (cw == r) d += vw; else if (cw == r - 1) l = vw; else if (cw == r + 1) u = vw;
+        if (ce == r) d += ve; else if (ce == r - 1) l = ve; else if (ce == r + 1) u = ve;
+        lo[r] = l;
+        di[r] = d;
+        up[r] = u;
+        rhs[r] = c.G[r];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double cpv = up[0] / di[0], dpv = -rhs[0] / di[0];
+        up[0] = cpv;
+        rhs[0] = dpv;
+        double ln = n > 1 ? lo[1] : 0.0, dn = n > 1 ? di[1] : 0.0, un = n > 1 ? up[1] : 0.0, gn = n > 1 ? rhs[1] : 0.0;
+        for (int r = 1; r < n; r++) {
+            const double l = ln, d = dn, u = un, gr = gn;
+            if (r + 1 < n) { ln = lo[r + 1]; dn = di[r + 1]; un = up[r + 1]; gn = rhs[r + 1]; }
+            const double m = d - l * cpv;
+            cpv = u / m;
+            dpv = (-gr - l * dpv) / m;
+            up[r] = cpv;
+            rhs[r] = dpv;
+        }
+        double xv = rhs[n - 1];
+        double cn = n > 1 ? up[n - 2] : 0.0, pn = n > 1 ? rhs[n - 2] : 0.0;
+        for (int r = n - 2; r >= 0; r--) {
+            const double cr = cn, pr = pn;
+            if (r > 0) { cn = up[r - 1]; pn = rhs[r - 1]; }
+            xv = pr - cr * xv;
+            rhs[r] = xv;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) c.dP[r] = rhs[r];
+}
 void launch_thomas(const Ctx& c, cudaStream_t st) {
-    k_thomas<<<1, 32, 0, st>>>(c);
+    const int n = c.g.nx;
+    if (n <= THOMAS_SMEM_MAX_ROWS) {
+        static unsigned long long configured = 0;  // one bit per device: the attribute is per device
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 64 && !(configured & (1ull << dev))) {
+            cudaFuncSetAttribute(k_thomas_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, 224 * 1024);
+            configured |= 1ull << dev;
+        }
+        k_thomas_smem<<<1, THOMAS_THREADS, (size_t)n * 4 * sizeof(double), st>>>(c);
+    } else {
+        k_thomas<<<1, 32, 0, st>>>(c);
+    }
     count(c, 1);
 }
 
