@@ -1190,6 +1190,13 @@ int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup) {
     s->t = t; s->dtprev = dtprev; s->startup = startup != 0;
     return SPB6G_OK;
 }
+int spb6g_get_time(const spb6g_solver* s, double* t, double* dtprev, int* startup) {
+    if (!s) return SPB6G_BAD_ARG;
+    if (t) *t = s->t;
+    if (dtprev) *dtprev = s->dtprev;
+    if (startup) *startup = s->startup ? 1 : 0;
+    return SPB6G_OK;
+}
 int spb6g_timing_enable(spb6g_solver* s, int on) {
     if (!s) return SPB6G_BAD_ARG;
     cudaStreamSynchronize(s->st);

@@ -107,6 +107,7 @@ def library() -> ctypes.CDLL:
         "spb6g_conserved_totals": (I, [P, P]),
         "spb6g_stats_line": (I, [P, I, D, ctypes.c_char_p, ctypes.c_size_t]),
         "spb6g_set_time": (I, [P, D, D, I]),
+        "spb6g_get_time": (I, [P, P, P, P]),
         "spb6g_timing_enable": (I, [P, I]),
         "spb6g_timing_get": (I, [P, P, P, I, P]),
         "spb6g_timing_name": (ctypes.c_char_p, [I]),
@@ -280,6 +281,25 @@ class Solver:
     def set_pressure(self, P: np.ndarray, p_ref: float):
         P = np.ascontiguousarray(P, dtype=np.float64)
         self._check(self.lib.spb6g_set_pressure(self.h, _ptr(P), float(p_ref)), "spb6g_set_pressure")
+
+    def time_state(self) -> tuple[float, float, bool]:
+        """(t, dtprev, startup): with the state and the pressure, a restart point."""
+        t, dtp, su = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        self._check(self.lib.spb6g_get_time(self.h, ctypes.byref(t), ctypes.byref(dtp), ctypes.byref(su)), "get_time")
+        return t.value, dtp.value, bool(su.value)
+
+    def set_time(self, t: float, dtprev: float, startup: bool):
+        self._check(self.lib.spb6g_set_time(self.h, float(t), float(dtprev), int(startup)), "set_time")
+
+    def restart_point(self) -> dict:
+        """Everything the next step depends on (state, pressure unknown, time-loop state)."""
+        P, pref = self.pressure()
+        return {"U": self.state(), "P": P, "p_ref": pref, "time": self.time_state()}
+
+    def restore(self, rp: dict):
+        self.upload(rp["U"])
+        self.set_pressure(rp["P"], rp["p_ref"])
+        self.set_time(*rp["time"])
 
     # reference driver entry points --------------------------------------------------------
     def caldt(self, acoustic: bool = False) -> float:

@@ -193,6 +193,10 @@ int spb6g_conserved_totals(spb6g_solver* s, double* M3);
 int spb6g_stats_line(spb6g_solver* s, int case_id, double wall_s, char* buf, size_t len);
 /* Simulation time t (settable, e.g. when restarting from a dump). */
 int spb6g_set_time(spb6g_solver* s, double t, double dtprev, int startup);
+/* The time-loop state spb6g_set_time restores: t, the last accepted step (dtprev) and whether the
+ * start-up ramp still runs (startup).  With spb6g_download_state and spb6g_get_pressure it is
+ * everything the next step depends on -- a restart point. */
+int spb6g_get_time(const spb6g_solver* s, double* t, double* dtprev, int* startup);
 
 /* Per-kernel-group device time (ms, CUDA events on the solver's stream)
  * accumulated since timing was enabled; spb6g_timing_name(g) names group g. */
