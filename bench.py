@@ -13,8 +13,8 @@ max over ranks).  The working set (~1 GB) is far larger than L2.
 
 metric: cell-updates/s = interior cells x accepted steps / device time.
 
-Multi-GPU: the path is one grid per GPU (north_star is single-GPU), so N > 1
-runs N independent replicas ("scaling": "weak"); value is the total over ranks.
+Multi-GPU: the measured path solves one grid on one GPU, so N > 1 runs N independent
+replicas ("scaling": "weak"); value is the total over ranks.
 
 --impl reference times the reference's own CPU solver (oracle/_ref, compiled from
 its sources) on the same workload on all host cores; rank 0 only.
