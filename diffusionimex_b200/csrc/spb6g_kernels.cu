@@ -1359,30 +1359,59 @@ void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itsca
 
 // ============================================================ Thomas (1D non-periodic, :858-863)
 SPB6G_DEV void thomas_solve(const Ctx& c) {
+    // One thread; the loads of row r + 2 are issued while row r is eliminated (the pointers do not
+    // alias), so the division chain, not a memory round trip, sets the pace.  Same arithmetic as
+    // the sweep re-reading cp, dp and dP from memory.
     const Geom& g = c.g;
     const int n = g.nx;
-    double* cp = c.tcp;
-    double* dp = c.tdp;
-    auto coef = [&](int r, double& lo, double& di, double& up) {
+    double* __restrict__ cp = c.tcp;
+    double* __restrict__ dp = c.tdp;
+    double* __restrict__ x = c.dP;
+    const double* __restrict__ aC = c.aC;
+    const double* __restrict__ aW = c.aW;
+    const double* __restrict__ aE = c.aE;
+    const double* __restrict__ G = c.G;
+    struct Row {
+        double c, w, e, g;
+    };
+    auto load = [&](int r) { return r < n ? Row{aC[r], aW[r], aE[r], G[r]} : Row{0.0, 0.0, 0.0, 0.0}; };
+    auto coef = [&](int r, const Row& q, double& lo, double& di, double& up) {
         lo = up = di = 0;
-        di += c.aC[r];
+        di += q.c;
         const int cw = mp_index(g, r - 1, 0), ce = mp_index(g, r + 1, 0);
-        const double vw = c.aW[r], ve = c.aE[r];
+        const double vw = q.w, ve = q.e;
         if (cw == r) di += vw; else if (cw == r - 1) lo = vw; else if (cw == r + 1) up = vw;
         if (ce == r) di += ve; else if (ce == r - 1) lo = ve; else if (ce == r + 1) up = ve;
     };
     double lo, di, up;
-    coef(0, lo, di, up);
-    cp[0] = up / di;
-    dp[0] = -c.G[0] / di;
+    Row q0 = load(0), q1 = load(1), q2 = load(2);
+    coef(0, q0, lo, di, up);
+    double cpv = up / di, dpv = -q0.g / di;
+    cp[0] = cpv;
+    dp[0] = dpv;
     for (int r = 1; r < n; r++) {
-        coef(r, lo, di, up);
-        const double m = di - lo * cp[r - 1];
-        cp[r] = up / m;
-        dp[r] = (-c.G[r] - lo * dp[r - 1]) / m;
+        const Row q = q1;
+        q1 = q2;
+        q2 = load(r + 2);
+        coef(r, q, lo, di, up);
+        const double m = di - lo * cpv;
+        cpv = up / m;
+        dpv = (-q.g - lo * dpv) / m;
+        cp[r] = cpv;
+        dp[r] = dpv;
     }
-    c.dP[n - 1] = dp[n - 1];
-    for (int r = n - 2; r >= 0; r--) c.dP[r] = dp[r] - cp[r] * c.dP[r + 1];
+    double xv = dpv;  // dp[n - 1]
+    x[n - 1] = xv;
+    double c1 = n > 1 ? cp[n - 2] : 0.0, d1 = n > 1 ? dp[n - 2] : 0.0;
+    double c2 = n > 2 ? cp[n - 3] : 0.0, d2 = n > 2 ? dp[n - 3] : 0.0;
+    for (int r = n - 2; r >= 0; r--) {
+        const double cr = c1, dr = d1;
+        c1 = c2;
+        d1 = d2;
+        if (r >= 2) { c2 = cp[r - 2]; d2 = dp[r - 2]; }
+        xv = dr - cr * xv;
+        x[r] = xv;
+    }
 }
 __global__ void k_thomas(Ctx c) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
