@@ -146,6 +146,10 @@ CASES = {
     "dodecane_unify_N200_2steps": (lambda: dict(cases.reference_case(3, 200), relax=2, unify=1), "steps", 2, {}),
     "bartak_nulaw_N200_5steps": (lambda: dict(cases.reference_case(32, 200), nu_law=1), "steps", 5, {}),
     "bartak_nulaw_N200_20steps": (lambda: dict(cases.reference_case(32, 200), nu_law=1), "steps", 20, {}),
+    "dodecane_unifyproj0_N200_2steps": (lambda: dict(cases.reference_case(3, 200), relax=2, unify_proj=0), "steps", 2,
+                                        {}),
+    "dodecane_relax3_nulaw_N200_5steps": (lambda: dict(cases.reference_case(3, 200), relax=3, nu_law=1), "steps", 5,
+                                          {}),
     "bubble_theta32_3steps": (lambda: dict(_bubble(32), relax=1, theta_rate=1e3, mu_rate=1e-4), "steps", 3,
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)

@@ -36,7 +36,8 @@ RELAX_FIXTURES = ["tube_relax_N200_20steps", "bubble_relax32_3steps",
                   "mu0d_N4_10steps", "mu0d_expo_N4_10steps", "theta0d_N4_10steps", "theta0d_expo_N4_10steps",
                   "nu0d_N4_10steps", "nu0d_expo_N4_10steps", "dodecane_rates_N200_2steps",
                   "dodecane_rates_N200_20steps", "dodecane_unify_N200_2steps", "bartak_nulaw_N200_5steps",
-                  "bartak_nulaw_N200_20steps", "bubble_theta32_3steps"]
+                  "bartak_nulaw_N200_20steps", "bubble_theta32_3steps", "dodecane_unifyproj0_N200_2steps",
+                  "dodecane_relax3_nulaw_N200_5steps"]
 SAT_FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_sat_tables.npz")
 
 
