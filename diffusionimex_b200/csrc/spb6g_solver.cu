@@ -97,6 +97,35 @@ namespace {
         }                                                                                            \
     } while (0)
 
+// Keep [p, p + bytes) in the persisting part of L2 for the solver's kernels: the set-aside is the
+// smaller of the block and the device's maximum (a limit of this process's context, gone with
+// it), the window covers as much of the block as one window may, and its hit ratio is the part
+// of the window the set-aside holds.  Without persisting L2 the accesses stay normal.
+static void persist_in_l2(spb6g_solver* s, void* p, size_t bytes) {
+    int dev = 0, max_persist = 0, max_window = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
+        max_persist <= 0 || max_window <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    const size_t set_aside = bytes < (size_t)max_persist ? bytes : (size_t)max_persist;
+    const size_t window = bytes < (size_t)max_window ? bytes : (size_t)max_window;
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, set_aside) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaStreamAttrValue a = {};
+    a.accessPolicyWindow.base_ptr = p;
+    a.accessPolicyWindow.num_bytes = window;
+    a.accessPolicyWindow.hitRatio = (float)((double)set_aside / (double)window < 1.0 ? (double)set_aside / (double)window : 1.0);
+    a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    for (cudaStream_t st : {s->st, s->st2})
+        if (st && cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &a) != cudaSuccess) cudaGetLastError();
+}
+
 double* dalloc(spb6g_solver* s, size_t count) {
     void* p = nullptr;
     if (cudaMalloc(&p, (count ? count : 1) * sizeof(double)) != cudaSuccess) return nullptr;
@@ -594,7 +623,15 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         s->P.sat = d;
     }
     c.G = A(n); c.Gn = A(n); c.sc = A(n); c.scn = A(n); c.dP = A(n);
-    c.aC = A(n); c.aW = A(n); c.aE = A(n); c.aS = A(n); c.aN = A(n); c.A1 = A(n); c.dinv = A(n);
+    {  // the five diagonals, A 1 and D^-1 -- what every BiCGStab pass re-reads -- in one block
+        const size_t stride = (n + 31) & ~(size_t)31;
+        double* mb = A(7 * stride);
+        if (mb) {
+            c.aC = mb; c.aW = mb + stride; c.aE = mb + 2 * stride; c.aS = mb + 3 * stride; c.aN = mb + 4 * stride;
+            c.A1 = mb + 5 * stride; c.dinv = mb + 6 * stride;
+            if (ny > 1) persist_in_l2(s, mb, 7 * stride * sizeof(double));
+        }
+    }
     c.prec = cfg->precision ? 1 : 0;
     if (c.prec) {
         auto Af = [&](size_t cnt) { return (float*)A(cnt / 2 + 1); };
