@@ -629,7 +629,9 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
         if (mb) {
             c.aC = mb; c.aW = mb + stride; c.aE = mb + 2 * stride; c.aS = mb + 3 * stride; c.aN = mb + 4 * stride;
             c.A1 = mb + 5 * stride; c.dinv = mb + 6 * stride;
-            if (ny > 1) persist_in_l2(s, mb, 7 * stride * sizeof(double));
+            // the diagonals only: also holding A 1 and D^-1 gained nothing in the solve and cost
+            // the state-streaming kernels more L2
+            if (ny > 1) persist_in_l2(s, mb, 5 * stride * sizeof(double));
         }
     }
     c.prec = cfg->precision ? 1 : 0;
