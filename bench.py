@@ -68,7 +68,8 @@ def parse():
                    help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
                         "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
-                        "<2D workload>-rus0 (grid-wide Rusanov speed), bubblecomp200 (chemical relaxation, "
+                        "<2D workload>-rus0 (grid-wide Rusanov speed), <workload>-jreuse (modified Newton), "
+                        "bubblecomp200 (chemical relaxation, "
                         "case 72), dodecane2000-rates (finite relaxation rates, case 3), "
                         "mlp (learned warm-start network)")
     p.add_argument("--no-e2e", action="store_true")
@@ -91,6 +92,10 @@ def make_workload(name: str):
         c = cases.lowmach_bubbles(2048, seed=0)
     elif name == "shock2048x1024":
         c = cases.shock_bubble(2048, 1024)
+    elif name.endswith("-jreuse"):  # the same workload with the modified Newton (jreuse = 1)
+        c = make_workload(name[:-len("-jreuse")])
+        c["jreuse"] = 1
+        c["workload"] = c.get("workload", name) + ", modified Newton (jreuse 1)"
     elif name.endswith("-rus0"):  # the same workload with the grid-wide Rusanov speed (rus_local = 0)
         c = make_workload(name[:-len("-rus0")])
         c["rus_local"] = 0
@@ -351,7 +356,7 @@ def run_mlp(args, case, rank: int, world: int, local_rank: int, dist):
 def workload_config(c: dict, name: str) -> dict:
     return {"workload": c.get("workload", name), "nx": c["nx"], "ny": c["ny"], "fp": "fp64",
             "newton_tol": c["newton_tol"], "bicg_tol": c["bicg_tol"], "cfl": c["cfl"], "seed": c.get("seed", 0),
-            "relax": c.get("relax", 0), "rus_local": c.get("rus_local", 1),
+            "relax": c.get("relax", 0), "rus_local": c.get("rus_local", 1), "jreuse": c.get("jreuse", 0),
             **{k: c[k] for k in ("mu_rate", "theta_rate", "nu_rate") if k in c},
             "l2": "working set > L2 (no flush needed)"}
 

@@ -42,6 +42,7 @@ struct spb6g_solver {
     double* Hs = nullptr;  // 3 stages x 8 x n
     double* Pbuf[3] = {nullptr, nullptr, nullptr};
     double* Pmain = nullptr;  // accepted pressure unknown; the other two buffers hold the Newton iterate and trial
+    double* sc_build = nullptr;  // jreuse: the row scales s_q of the last Jacobian build (:831-836)
     Ctx c{};
     Pinned* pin = nullptr;
     // time state
@@ -299,17 +300,29 @@ int newton(spb6g_solver* s, double& resfinal) {
         }
         if (reset_fail(s)) return SPB6G_CUDA_ERROR;
     }
+    // jreuse (modified Newton, :826-830, :887): the Jacobian is rebuilt at the first iteration, after
+    // a damped step or a contraction above 0.25 (fresh_ok :797), and when the kept one lets the
+    // line search fail; the step criterion meanwhile uses the scales of the last build
+    const bool jreuse = s->cfg.jreuse != 0;
+    double ratio = 1.0, lamprev = 1.0;
+    bool fresh = false;
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
         if (res < tol) return SPB6G_OK;
+        const bool build = !jreuse || it == 0 || !(lamprev == 1.0 && ratio <= 0.25);
         tbegin(s, TG_JACOBIAN);
-        if (it == 0 && ahead) {  // the rows formed ahead stand; add the worklist rows
+        if (!build) {  // the kept diagonals; the BiCGStab set-up sums of the new right-hand side
+            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+            launch_jac_finish(c, s->st);
+        } else if (it == 0 && ahead) {  // the rows formed ahead stand; add the worklist rows
             launch_jac_strong(c, s->st);
             launch_jac_finish(c, s->st);
         } else {
             if (reset_fail(s)) return SPB6G_CUDA_ERROR;
             launch_jacobian(c, s->st);
         }
+        if (jreuse && build) CK(cudaMemcpyAsync(s->sc_build, c.sc, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        fresh = build;
         tend_(s, TG_JACOBIAN);
         tbegin(s, TG_LINEAR);
         if (tri) {
@@ -352,7 +365,11 @@ int newton(spb6g_solver* s, double& resfinal) {
         // step criterion (:870-879) and the first line-search trial (lam = 1) in one sync
         if (reset_fail(s)) return SPB6G_CUDA_ERROR;
         tbegin(s, TG_RESIDUAL);
-        launch_stepnorm(c, s->st);
+        {
+            Ctx cs = c;  // the scales of the last build (the current ones unless the Jacobian is kept)
+            if (jreuse) cs.sc = s->sc_build;
+            launch_stepnorm(cs, s->st);
+        }
         launch_residual(c, s->st, 1, 1.0);
         tend_(s, TG_RESIDUAL);
         if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
@@ -370,6 +387,7 @@ int newton(spb6g_solver* s, double& resfinal) {
         }
         double lam = 1.0;
         bool acc = false;
+        const double res0 = res;
         for (int ls = 0; ls < 40; ls++) {
             if (ls > 0) {
                 if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -384,6 +402,13 @@ int newton(spb6g_solver* s, double& resfinal) {
             }
             lam *= 0.5;
         }
+        if (!acc && !fresh) {  // a kept Jacobian that does not descend: rebuild at the same P (:887)
+            ratio = 1.0;
+            lamprev = 0.0;
+            continue;
+        }
+        ratio = res / res0;
+        lamprev = lam;
         if (!acc) {  // round-off floor acceptance (:890-899)
             resfinal = res;
             if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -550,6 +575,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if ((cfg->bc[0] == SPB6G_BC_PERIODIC) != (cfg->bc[1] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if ((cfg->bc[2] == SPB6G_BC_PERIODIC) != (cfg->bc[3] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if (cfg->rus_local != 0 && cfg->rus_local != 1) return SPB6G_BAD_ARG;
+    if (cfg->jreuse != 0 && cfg->jreuse != 1) return SPB6G_BAD_ARG;
     for (int k = 0; k < 2; k++) {
         if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
@@ -615,6 +641,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.smask = (unsigned char*)A(n / 8 + 1);
     c.ctype = cfg->relax ? (unsigned char*)A(n / 8 + 1) : nullptr;  // n bytes
     c.step_nu = (cfg->relax && cfg->nu_law) ? A(n) : nullptr;
+    s->sc_build = cfg->jreuse ? A(n) : nullptr;
     if (cfg->relax >= 2) {  // the saturation line (build_sat, physics :127-153; main :1236)
         const std::vector<double> sat = saturation_table(cfg);
         double* d = A(sat.size());
@@ -1114,8 +1141,9 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     for (int i = 0; i < count; i++)
         if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
             cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0 ||
-            cfgs[i].rus_local != 1 || !std::isinf(cfgs[i].mu_rate) ||
-            cfgs[i].unify == 1)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov speed
+            cfgs[i].rus_local != 1 || !std::isinf(cfgs[i].mu_rate) || cfgs[i].unify == 1 ||
+            cfgs[i].jreuse != 0)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov
+                                  // speed, a fresh Jacobian every Newton iteration
             return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;

@@ -92,6 +92,7 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
     }
     // relaxation level and interface zone; the rates as main() defaults them (:1233-1234)
     RELAX_LEVEL = c.relax;
+    JREUSE = c.jreuse;
     EPS_I = c.eps_i;
     // the rates and forms as main() sets them from its arguments (:1211-1214, :1233-1235)
     mu_rate = c.mu_rate;
@@ -125,7 +126,6 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
     recon = Minmod;
     SpaceOrder = 2;
     caltimestep = c.acdt ? Fullydt : IMEXdt;
-    JREUSE = 0;
     x_0 = c.x0; x_1 = c.x1; y_0 = c.y0; y_1 = c.y1;
     time_stop = c.tend;
     // apply_bc_setup (physics :974-979) with the per-side codes given directly

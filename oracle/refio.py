@@ -32,7 +32,7 @@ CASE_DT = np.dtype([
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
     ("budget_s", "<f8"), ("warmup", "<i4"), ("inject_qph", "<i4"),
     ("kind", "<i4", 2), ("mg_G", "<f8", 2), ("mg_rr", "<f8", 2), ("mg_c1", "<f8", 2), ("mg_c2", "<f8", 2),
-    ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2), ("relax", "<i4"), ("pad2", "<i4"),
+    ("mg_e1", "<f8", 2), ("mg_e2", "<f8", 2), ("mg_e0", "<f8", 2), ("relax", "<i4"), ("jreuse", "<i4"),
     ("eps_i", "<f8"),
     ("mu_rate", "<f8"), ("theta_rate", "<f8"), ("nu_rate", "<f8"), ("nu_cr", "<f8"), ("nu_pc", "<f8"),
     ("relax_form", "<i4"), ("unify", "<i4"), ("unify_proj", "<i4"), ("nu_law", "<i4"),
@@ -67,6 +67,7 @@ def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int
     for f in MG_KEYS:
         r["mg_" + f] = [float(cfg["phases"][k].get(f, 0.0)) for k in range(2)]
     r["relax"] = int(cfg.get("relax", 0))
+    r["jreuse"] = int(cfg.get("jreuse", 0))
     r["eps_i"] = float(cfg.get("eps_i", 1e-4))
     for k, v in RATE_DEFAULTS.items():
         r[k] = type(v)(cfg.get(k, v))

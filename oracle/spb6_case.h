@@ -43,7 +43,8 @@ typedef struct {
     int32_t kind[2];    /* 0 SG / NASG, 1 Cochran-Chan, 2 JWL (reference harness only; the C restatement
                            runs SG / NASG phases) */
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
-    int32_t relax, pad2;  /* RELAX_LEVEL (reference harness only; the C restatement has relax 0) */
+    int32_t relax;        /* RELAX_LEVEL (reference harness only; the C restatement has relax 0) */
+    int32_t jreuse;       /* JREUSE (reference harness only; the C restatement has 0) */
     double eps_i;
     /* relaxation rates (reference harness only; the C restatement has the defaults): mu_rate, and
        theta_rate / nu_rate < 0 for the level's default, nu law coefficient and pressure */

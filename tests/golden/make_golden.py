@@ -152,6 +152,10 @@ CASES = {
                                           {}),
     "bubble_theta32_3steps": (lambda: dict(_bubble(32), relax=1, theta_rate=1e3, mu_rate=1e-4), "steps", 3,
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # modified Newton (JREUSE :83, Newton_Solver :826-830, :887)
+    "tube_jreuse_N1000_20steps": (lambda: dict(_tube(1000), jreuse=1), "steps", 20, {}),
+    "bubble_jreuse48_4steps": (lambda: dict(_bubble(48), jreuse=1), "steps", 4, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "lowmach_jreuse32_3steps": (lambda: dict(_lowmach(32), jreuse=1), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)
     "case13_N200_20steps": (lambda: cases.reference_case(13, 200), "steps", 20, {}),
     "lowmach_rus0_32_stage": (lambda: dict(_lowmach(32), rus_local=0), "stage", 0,
