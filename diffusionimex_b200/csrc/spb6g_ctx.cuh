@@ -69,6 +69,7 @@ inline void phys_from_config(const spb6g_config* cfg, Phys& P) {
     P.unify_proj = cfg->unify_proj;
     P.nu_law = cfg->nu_law;
     P.mech = isinf(cfg->mu_rate) ? CL_P : CL_MU;
+    P.order = cfg->order == 1 ? 1 : 2;
     P.rates = (!isinf(cfg->mu_rate) || cfg->unify == 1) ? 1 : 0;
 }
 

@@ -265,11 +265,16 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
     auto lterms = [&](int ly, int lx) -> const R* { return MIXED ? LS + (ly * NLX + lx) * 4 : nullptr; };
     __syncthreads();
 
-    // 2. reconstruction of cells -1..TX (x) and -1..TY (y)
+    // 2. reconstruction of cells -1..TX (x) and -1..TY (y); at first order none, phi = 0 (:372-375)
+    const bool first_order = c.phy.order == 1;
     for (int t = tid; t < NRX * TY; t += nth) {
         const int rx = t % NRX, ry = t / NRX;  // cell i0 - 1 + rx, row j0 + ry
         const int gi = i0 - 1 + rx, gj = j0 + ry;
         if (gi > g.nx || gj >= g.ny) continue;
+        if (first_order) {
+            if (!SPEED && ((gi >= i0 && gi < i0 + TX) || gi == -1 || gi == g.nx)) c.phis_x[rxi(g, gi, gj)] = 0.0;
+            continue;
+        }
         const int lx = rx + 1, ly = ry + HY;
         R Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
@@ -290,6 +295,10 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
             const int rx = t % TX, ry = t / TX;  // cell i0 + rx, row j0 - 1 + ry
             const int gi = i0 + rx, gj = j0 - 1 + ry;
             if (gi >= g.nx || gj > g.ny) continue;
+            if (first_order) {
+                if (!SPEED && ((gj >= j0 && gj < j0 + TY) || gj == -1 || gj == g.ny)) c.phis_y[ryi(g, gi, gj)] = 0.0;
+                continue;
+            }
             const int lx = rx + 2, ly = ry + 1;
             R Ua[NV], Uc[NV], Ub[NV];
 #pragma unroll
@@ -321,16 +330,21 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
         if (gl > g.nx - 1 || gj >= g.ny) continue;
         const int ly = ry + HY, la = f + 1;   // local column of the left cell
         R Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
-        // right face value of the left cell
+        if (first_order) {  // the cells' own values on the face
 #pragma unroll
-        for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, la - 1); Uc[k] = Q(k, ly, la); Ub[k] = Q(k, ly, la + 1); }
-        face_value(Ua, Uc, Ub, VU[ly * NLX + la], VV[ly * NLX + la], RX[(0 * TY + ry) * NRX + f],
-                   RX[(1 * TY + ry) * NRX + f], RX[(2 * TY + ry) * NRX + f], true, wR);
-        // left face value of the right cell
+            for (int k = 0; k < NV; k++) { wR[k] = Q(k, ly, la); wL[k] = Q(k, ly, la + 1); }
+        } else {
+            // right face value of the left cell
 #pragma unroll
-        for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, ly, la + 2); }
-        face_value(Ua, Uc, Ub, VU[ly * NLX + la + 1], VV[ly * NLX + la + 1], RX[(0 * TY + ry) * NRX + f + 1],
-                   RX[(1 * TY + ry) * NRX + f + 1], RX[(2 * TY + ry) * NRX + f + 1], false, wL);
+            for (int k = 0; k < NV; k++) { Ua[k] = Q(k, ly, la - 1); Uc[k] = Q(k, ly, la); Ub[k] = Q(k, ly, la + 1); }
+            face_value(Ua, Uc, Ub, VU[ly * NLX + la], VV[ly * NLX + la], RX[(0 * TY + ry) * NRX + f],
+                       RX[(1 * TY + ry) * NRX + f], RX[(2 * TY + ry) * NRX + f], true, wR);
+            // left face value of the right cell
+#pragma unroll
+            for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, ly, la + 2); }
+            face_value(Ua, Uc, Ub, VU[ly * NLX + la + 1], VV[ly * NLX + la + 1], RX[(0 * TY + ry) * NRX + f + 1],
+                       RX[(1 * TY + ry) * NRX + f + 1], RX[(2 * TY + ry) * NRX + f + 1], false, wL);
+        }
         R uL, uR;
         rusanov_flux<R>(wR, wL, 0, ax, fl, uL, uR);
         if (SPEED) {
@@ -359,14 +373,19 @@ __device__ void flux_tile(const Ctx& c, int bx, int by, unsigned char* smem_byte
             if (gi >= g.nx || gl > g.ny - 1) continue;
             const int lx = rx + 2, la = f + 1;
             R Ua[NV], Uc[NV], Ub[NV], wR[NV], wL[NV], fl[NV];
+            if (first_order) {
 #pragma unroll
-            for (int k = 0; k < NV; k++) { Ua[k] = Q(k, la - 1, lx); Uc[k] = Q(k, la, lx); Ub[k] = Q(k, la + 1, lx); }
-            face_value(Ua, Uc, Ub, VU[la * NLX + lx], VV[la * NLX + lx], RY[(0 * NRY + f) * TX + rx],
-                       RY[(1 * NRY + f) * TX + rx], RY[(2 * NRY + f) * TX + rx], true, wR);
+                for (int k = 0; k < NV; k++) { wR[k] = Q(k, la, lx); wL[k] = Q(k, la + 1, lx); }
+            } else {
 #pragma unroll
-            for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, la + 2, lx); }
-            face_value(Ua, Uc, Ub, VU[(la + 1) * NLX + lx], VV[(la + 1) * NLX + lx], RY[(0 * NRY + f + 1) * TX + rx],
-                       RY[(1 * NRY + f + 1) * TX + rx], RY[(2 * NRY + f + 1) * TX + rx], false, wL);
+                for (int k = 0; k < NV; k++) { Ua[k] = Q(k, la - 1, lx); Uc[k] = Q(k, la, lx); Ub[k] = Q(k, la + 1, lx); }
+                face_value(Ua, Uc, Ub, VU[la * NLX + lx], VV[la * NLX + lx], RY[(0 * NRY + f) * TX + rx],
+                           RY[(1 * NRY + f) * TX + rx], RY[(2 * NRY + f) * TX + rx], true, wR);
+#pragma unroll
+                for (int k = 0; k < NV; k++) { Ua[k] = Uc[k]; Uc[k] = Ub[k]; Ub[k] = Q(k, la + 2, lx); }
+                face_value(Ua, Uc, Ub, VU[(la + 1) * NLX + lx], VV[(la + 1) * NLX + lx], RY[(0 * NRY + f + 1) * TX + rx],
+                           RY[(1 * NRY + f + 1) * TX + rx], RY[(2 * NRY + f + 1) * TX + rx], false, wL);
+            }
             R vL, vR;
             rusanov_flux<R>(wR, wL, 1, ay, fl, vL, vR);
             if (SPEED) {

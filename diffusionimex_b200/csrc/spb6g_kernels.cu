@@ -128,8 +128,10 @@ SPB6G_DEV void set_face(const Ctx& c, int iL, int jL, int ydir, double& ubs, dou
     // the reference's range test (im >= 0 && ... jp < NYT) holds for every face the residual reads
     const double phis = ydir ? SMIN(c.phis_y[ryi(g, iL, jL)], c.phis_y[ryi(g, iR, jR)])
                              : SMIN(c.phis_x[rxi(g, iL, jL)], c.phis_x[rxi(g, iR, jR)]);
-    const double psiP = 1.0 - (1.0 - psi_face(c.phy.limiter, pold_at(c, im, jm), pold_at(c, iL, jL), pold_at(c, iR, jR), pold_at(c, ip, jp))) * phis;
-    const double psiU = psi_face(c.phy.limiter, N[pad_index(g, im, jm)], uL, uR, N[pad_index(g, ip, jp)]);
+    // first order: psi_face is 1 (:979) and phi_x, phi_y are 0 (:373)
+    const bool o1 = c.phy.order == 1;
+    const double psiP = o1 ? 1.0 : 1.0 - (1.0 - psi_face(c.phy.limiter, pold_at(c, im, jm), pold_at(c, iL, jL), pold_at(c, iR, jR), pold_at(c, ip, jp))) * phis;
+    const double psiU = o1 ? 1.0 : psi_face(c.phy.limiter, N[pad_index(g, im, jm)], uL, uR, N[pad_index(g, ip, jp)]);
     double D;
     if (!ydir) {
         const double d = uR - uL;

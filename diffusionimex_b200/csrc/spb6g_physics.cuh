@@ -57,6 +57,7 @@ struct Phys {
     double mu_rate, theta_rate, nu_rate, nu_cr, nu_pc;
     int relax_form, unify, unify_proj, nu_law;
     int mech;  // the mechanical closure type: CL_P (mu = inf) or CL_MU
+    int order; // SpaceOrder (:73): 2 MUSCL, 1 cell values on the faces (no reconstruction)
     int rates; // a finite mu or unify = 1: closure kernels take the extended build even at relax 0
 };
 // Closure types (ClosureType :228): p, finite mu, pT, finite theta, finite nu, pTg.  CL_PND is

@@ -560,6 +560,7 @@ void spb6g_default_config(spb6g_config* cfg) {
     cfg->unify = 0;
     cfg->unify_proj = 1;
     cfg->nu_law = 0;
+    cfg->order = 2;
     cfg->rk = 2; cfg->cfl = 0.2; cfg->cfl_ac = 0.4; cfg->ramp = 1; cfg->rus_local = 1; cfg->limiter = 1;
     cfg->newton_tol = 1e-13; cfg->newton_iter = 60; cfg->bicg_tol = 1e-13; cfg->bicg_iter = 4000;
     cfg->tend = 240e-6;
@@ -576,6 +577,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if ((cfg->bc[2] == SPB6G_BC_PERIODIC) != (cfg->bc[3] == SPB6G_BC_PERIODIC)) return SPB6G_BAD_ARG;
     if (cfg->rus_local != 0 && cfg->rus_local != 1) return SPB6G_BAD_ARG;
     if (cfg->jreuse != 0 && cfg->jreuse != 1) return SPB6G_BAD_ARG;
+    if (cfg->order != 0 && cfg->order != 1 && cfg->order != 2) return SPB6G_BAD_ARG;
     for (int k = 0; k < 2; k++) {
         if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
         if (cfg->kind[k] && !(cfg->mg_G[k] > 0 && cfg->mg_rr[k] > 0)) return SPB6G_BAD_ARG;
@@ -898,12 +900,11 @@ int spb6g_stats_line(spb6g_solver* s, int case_id, double wall_s, char* buf, siz
     if (r != SPB6G_OK) return r;
     const spb6g_stats& q = s->stats;
     const double* M0 = s->M0;
-    // st_cl_fail is never incremented by the reference's IMEX program, so its column is always 0;
-    // the reconstruction is always MUSCL (SpaceOrder 2)
+    // st_cl_fail is never incremented by the reference's IMEX program, so its column is always 0
     std::snprintf(buf, len,
                   "case %d mode 1 order %d rk %d N %d CFL %g | steps %ld (rk1 %ld) rejects %ld floor %ld | stages %ld newton it %ld "
                   "(%.2f/stage) maxres %.2e Tmax %.4g %.4g | closure fails %ld | dM1/M %.2e dM2/M %.2e dE/E %.2e | wall %.2f s",
-                  case_id, 2, s->cfg.rk, s->cfg.nx, s->cfg.cfl, (long)q.steps, (long)q.rk1, (long)q.rejects, (long)q.floor_count,
+                  case_id, s->P.order, s->cfg.rk, s->cfg.nx, s->cfg.cfl, (long)q.steps, (long)q.rk1, (long)q.rejects, (long)q.floor_count,
                   (long)q.stages, (long)q.newton_it, q.stages ? (double)q.newton_it / q.stages : 0.0, q.maxres, q.tmax[0], q.tmax[1],
                   0L, (M1[0] - M0[0]) / M0[0], (M1[1] - M0[1]) / M0[1], (M1[2] - M0[2]) / M0[2], wall_s);
     return SPB6G_OK;
@@ -1142,7 +1143,7 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
         if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
             cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0 ||
             cfgs[i].rus_local != 1 || !std::isinf(cfgs[i].mu_rate) || cfgs[i].unify == 1 ||
-            cfgs[i].jreuse != 0)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov
+            cfgs[i].jreuse != 0 || cfgs[i].order == 1)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov
                                   // speed, a fresh Jacobian every Newton iteration
             return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();

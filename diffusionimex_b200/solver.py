@@ -48,7 +48,8 @@ class Config(ctypes.Structure):
         ("newton_tol", ctypes.c_double), ("newton_iter", ctypes.c_int32), ("bicg_tol", ctypes.c_double),
         ("bicg_iter", ctypes.c_int32), ("share_mode", ctypes.c_int32), ("tend", ctypes.c_double),
         ("device", ctypes.c_int32), ("precision", ctypes.c_int32), ("kind", ctypes.c_int32 * 2),
-        ("relax", ctypes.c_int32), ("jreuse", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
+        ("relax", ctypes.c_int32), ("jreuse", ctypes.c_int32), ("order", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
         ("mg_G", ctypes.c_double * 2), ("mg_rr", ctypes.c_double * 2), ("mg_c1", ctypes.c_double * 2),
         ("mg_c2", ctypes.c_double * 2), ("mg_e1", ctypes.c_double * 2), ("mg_e2", ctypes.c_double * 2),
         ("mg_e0", ctypes.c_double * 2), ("eps_i", ctypes.c_double),
@@ -167,6 +168,7 @@ def make_config(case: dict, device: int = 0) -> Config:
     c.precision = int(case.get("precision", 0))
     c.relax = int(case.get("relax", 0))
     c.jreuse = int(case.get("jreuse", 0))
+    c.order = int(case.get("order", 2))
     c.eps_i = float(case.get("eps_i", 1e-4))
     for k in RATE_KEYS:  # absent keys keep spb6g_default_config's values
         if k in case:

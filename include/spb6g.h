@@ -86,7 +86,9 @@ typedef struct {
     int32_t jreuse;                 /* JREUSE (:83): 1 modified Newton -- the FD Jacobian of the stage's first
                                        iteration is kept while each step is undamped and contracts the
                                        residual 4x (batched form: 0 only) */
-    int32_t reserved[2];
+    int32_t order;                  /* spatial order (order=, :1210): 2 MUSCL reconstruction (the default;
+                                       0 reads as 2), 1 the cell values on the faces (NoRecon, :372-375) */
+    int32_t reserved[1];
     double mg_G[2], mg_rr[2], mg_c1[2], mg_c2[2], mg_e1[2], mg_e2[2], mg_e0[2];
     double eps_i;                   /* EPS_I (physics :40): interface zone eps_I <= alpha1 <= 1 - eps_I (1e-4) */
     /* Relaxation rates (physics :34-46; mu=, theta=, nu=, relaxform=, unify=, unifyproj=, nulaw=,

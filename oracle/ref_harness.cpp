@@ -123,8 +123,8 @@ void setup(Harness& H, const spb6_case& c, const double* U0) {
     GMRESiter = c.bicg_iter;
     RUS_LOCAL = c.rus_local;
     LIMITER = c.limiter;
-    recon = Minmod;
-    SpaceOrder = 2;
+    recon = c.order == 1 ? NoRecon : Minmod;  // order= (:1210, :1222)
+    SpaceOrder = recon == NoRecon ? 1 : 2;
     caltimestep = c.acdt ? Fullydt : IMEXdt;
     x_0 = c.x0; x_1 = c.x1; y_0 = c.y0; y_1 = c.y1;
     time_stop = c.tend;

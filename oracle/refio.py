@@ -26,7 +26,7 @@ CASE_DT = np.dtype([
     ("magic", "<u4"), ("version", "<i4"), ("nx", "<i4"), ("ny", "<i4"), ("bc", "<i4", 4),
     ("rk", "<i4"), ("ramp", "<i4"), ("rus_local", "<i4"), ("limiter", "<i4"), ("acdt", "<i4"),
     ("newton_iter", "<i4"), ("bicg_iter", "<i4"), ("share_mode", "<i4"), ("mode", "<i4"), ("nsteps", "<i4"),
-    ("threads", "<i4"), ("pad", "<i4"),
+    ("threads", "<i4"), ("order", "<i4"),
     ("x0", "<f8"), ("x1", "<f8"), ("y0", "<f8"), ("y1", "<f8"), ("bcu", "<f8", 4), ("bcp", "<f8", 4),
     ("g", "<f8", 2), ("pinf", "<f8", 2), ("q", "<f8", 2), ("qp", "<f8", 2), ("cv", "<f8", 2), ("b", "<f8", 2),
     ("cfl", "<f8"), ("cfl_ac", "<f8"), ("dtfix", "<f8"), ("newton_tol", "<f8"), ("bicg_tol", "<f8"), ("tend", "<f8"),
@@ -68,6 +68,7 @@ def case_record(cfg: dict, mode: int = MODE_STEPS, nsteps: int = 1, threads: int
         r["mg_" + f] = [float(cfg["phases"][k].get(f, 0.0)) for k in range(2)]
     r["relax"] = int(cfg.get("relax", 0))
     r["jreuse"] = int(cfg.get("jreuse", 0))
+    r["order"] = int(cfg.get("order", 2))
     r["eps_i"] = float(cfg.get("eps_i", 1e-4))
     for k, v in RATE_DEFAULTS.items():
         r[k] = type(v)(cfg.get(k, v))

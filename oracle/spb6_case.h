@@ -32,7 +32,8 @@ typedef struct {
     int32_t bc[4]; /* left, right, bottom, top */
     int32_t rk, ramp, rus_local, limiter, acdt, newton_iter, bicg_iter, share_mode;
     int32_t mode, nsteps;
-    int32_t threads, pad;
+    int32_t threads;
+    int32_t order;     /* spatial order: 1 no reconstruction, else MUSCL (reference harness only) */
     double x0, x1, y0, y1;
     double bcu[4], bcp[4];
     double g[2], pinf[2], q[2], qp[2], cv[2], b[2];

@@ -1308,6 +1308,7 @@ int spb6_oracle_run(const spb6_case* c, const double* U0, void* out, size_t cap)
     if (c->kind[0] != 0 || c->kind[1] != 0) return -3;  /* Mie-Grueneisen phases: not restated here */
     if (c->relax != 0) return -3;                        /* thermal relaxation: not restated here */
     if (c->jreuse != 0) return -3;                       /* modified Newton: not restated here */
+    if (c->order == 1) return -3;                        /* first order: not restated here */
     if (!isinf(c->mu_rate) || c->unify != 0 || c->nu_law != 0) return -3;  /* finite rates: not restated */
     const int nx = c->nx, ny = c->ny, n = nx * ny;
     const size_t nstage = (size_t)n * 8 + n + (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1) + 2 * (size_t)n +

@@ -152,6 +152,11 @@ CASES = {
                                           {}),
     "bubble_theta32_3steps": (lambda: dict(_bubble(32), relax=1, theta_rate=1e3, mu_rate=1e-4), "steps", 3,
                               {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # first order: no reconstruction (order=1, TVDReconstruction :372-375, psi_face :979)
+    "tube_order1_N200_20steps": (lambda: dict(_tube(200), order=1), "steps", 20, {}),
+    "bubble_order1_32_3steps": (lambda: dict(_bubble(32), order=1), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "bubble_order1_32_stage": (lambda: dict(_lowmach(32), order=1), "stage", 0,
+                               {"dtfix": 2e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # modified Newton (JREUSE :83, Newton_Solver :826-830, :887)
     "tube_jreuse_N1000_20steps": (lambda: dict(_tube(1000), jreuse=1), "steps", 20, {}),
     "bubble_jreuse48_4steps": (lambda: dict(_bubble(48), jreuse=1), "steps", 4, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
@@ -171,6 +176,7 @@ MAIN_RUNS = {
     "case87_N200": (87, 200, ["snap=1e-4", "probe=0.5,0.5"]),
     "case60_N100": (60, 100, ["snap=3e-5", "probe=0.6,0.5"]),  # Mie-Grueneisen (Cochran-Chan) phases
     "case5_relax_N100": (5, 100, ["relax=1", "snap=1.2e-4", "probe=0.75,0.5"]),  # p-pT relaxation
+    "case5_order1_N100": (5, 100, ["order=1", "snap=1.2e-4", "probe=0.75,0.5"]),  # first order
 }
 
 

@@ -57,7 +57,7 @@ def report(a, b):
     return {f: f"{v:.2e}" for f, v in zip(FIELDS, fieldwise_maxrel(a, b))}
 
 
-@pytest.mark.parametrize("name", ["tube_N200_stage", "bubble48_stage"])
+@pytest.mark.parametrize("name", ["tube_N200_stage", "bubble48_stage", "bubble_order1_32_stage"])
 def test_stage_explicit_and_implicit(name):
     g = load_golden(name)
     c, mode, _ = golden_case(name)
@@ -111,7 +111,8 @@ def test_1d_tube_one_step_bitwise():
 @pytest.mark.parametrize("name", ["case87_N200_tend", "case5_N100_tend", "tube_N1000_tend", "nasg256_20steps",
                                   "tube_walls_N200_20steps", "tube_piston_N200_20steps", "tube_outlet_N200_20steps",
                                   "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps",
-                                  "case83_N200_10steps", "case13_N200_20steps", "lowmach_rus0_32_3steps"])
+                                  "case83_N200_10steps", "case13_N200_20steps", "lowmach_rus0_32_3steps",
+                                  "tube_order1_N200_20steps", "bubble_order1_32_3steps"])
 def test_runs_match_reference_in_l1(name):
     """Whole runs in L1: within 1e-6 of the field maximum, or within 10x the reference's own L1
     change under round-off perturbations (one-ulp libm, FD step 1.01e-7) where that is larger --

@@ -26,7 +26,7 @@ from diffusionimex_b200 import cases
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIX = os.path.join(HERE, "golden", "ref_main_outputs.npz")
-RUNS = ["case5_N100", "case87_N200", "case60_N100", "case5_relax_N100"]
+RUNS = ["case5_N100", "case87_N200", "case60_N100", "case5_relax_N100", "case5_order1_N100"]
 
 
 def _run(tag):
@@ -38,12 +38,13 @@ def _run(tag):
     snaps = [float(v) for v in kv["snap"].split(",")] if "snap" in kv else []
     probe = tuple(float(v) for v in kv["probe"].split(",")) if "probe" in kv else None
     return dict(case=case, n=n, files=files, stdout=bytes(z[f"{tag}/stdout"]).decode(), U=z[f"{tag}/U"], snaps=snaps,
-                probe=probe, relax=int(kv.get("relax", 0)))
+                probe=probe, relax=int(kv.get("relax", 0)), order=int(kv.get("order", 2)))
 
 
 def _case(r):
     c = cases.reference_case(r["case"], r["n"])
     c["relax"] = r["relax"]
+    c["order"] = r["order"]
     return c
 
 
@@ -64,7 +65,7 @@ def test_fixture_has_every_file():
         r = _run(tag)
         assert "run.dat" in r["files"] and "run.dat.probe" in r["files"]
         assert sum(name.startswith("run_s") for name in r["files"]) == len(r["snaps"])
-        assert r["stdout"].startswith(f"case {r['case']} mode 1 order 2 rk 2 N {r['n']} ")
+        assert r["stdout"].startswith(f"case {r['case']} mode 1 order {r['order']} rk 2 N {r['n']} ")
 
 
 @pytest.mark.gpu
