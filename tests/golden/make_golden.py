@@ -155,7 +155,7 @@ CASES = {
     # first order: no reconstruction (order=1, TVDReconstruction :372-375, psi_face :979)
     "tube_order1_N200_20steps": (lambda: dict(_tube(200), order=1), "steps", 20, {}),
     "bubble_order1_32_3steps": (lambda: dict(_bubble(32), order=1), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
-    "bubble_order1_32_stage": (lambda: dict(_lowmach(32), order=1), "stage", 0,
+    "lowmach_order1_32_stage": (lambda: dict(_lowmach(32), order=1), "stage", 0,
                                {"dtfix": 2e-6, "newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # modified Newton (JREUSE :83, Newton_Solver :826-830, :887)
     "tube_jreuse_N1000_20steps": (lambda: dict(_tube(1000), jreuse=1), "steps", 20, {}),

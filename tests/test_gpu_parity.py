@@ -57,7 +57,7 @@ def report(a, b):
     return {f: f"{v:.2e}" for f, v in zip(FIELDS, fieldwise_maxrel(a, b))}
 
 
-@pytest.mark.parametrize("name", ["tube_N200_stage", "bubble48_stage", "bubble_order1_32_stage"])
+@pytest.mark.parametrize("name", ["tube_N200_stage", "bubble48_stage", "lowmach_order1_32_stage"])
 def test_stage_explicit_and_implicit(name):
     g = load_golden(name)
     c, mode, _ = golden_case(name)
