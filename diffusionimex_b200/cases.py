@@ -401,6 +401,69 @@ def riemann_batch(count: int = 512, seed: int = 0, nmin: int = 256, nmax: int = 
     return out
 
 
+def subcell_average(c: dict, state, sub: int = 4) -> np.ndarray:
+    """Cell averages of state(x, y) -> conservative values over sub x sub points per cell, summed
+    in the reference's order (u_initialization :482-487: a over x outer, b over y inner, each
+    term divided by sub^2)."""
+    x, y, dx, dy = cell_centres(c)
+    X, Y = np.meshgrid(x, y)
+    U = np.zeros((c["ny"], c["nx"], NUM_VARS))
+    for a in range(sub):
+        for b in range(sub):
+            U = U + state(X + ((a + 0.5) / sub - 0.5) * dx, Y + ((b + 0.5) / sub - 0.5) * dy) / (sub * sub)
+    return U
+
+
+def he_bubble(nx: int = 600, ny: int = 160) -> dict:
+    """The reference's case 70 (SPB 2009 4.6, physics :1055-1056, :1099-1104): a Mach-1.5 shock in
+    air (ideal-gas Rankine-Hugoniot post-shock state for x > 0.221 m, moving left) reaching a
+    helium bubble (radius 0.02 m at (0.2, 0.04) m) on [0, 0.3] x [0, 0.08] m; transmissive in x,
+    walls in y; 4 x 4 sub-cell averages."""
+    c = default_settings()
+    c.update(nx=nx, ny=ny, x0=0.0, x1=0.3, y0=0.0, y1=0.08, tend=600e-6,
+             phases=[dict(AIR_SG), dict(AIR_SG, g=1.67)], bc=[BC_TRANS, BC_TRANS, BC_WALL, BC_WALL], case=70)
+    ph = c["phases"]
+    g, Ms, p0, r0 = 1.4, 1.5, 101325.0, 1.29
+    c0 = math.sqrt(g * p0 / r0)
+    p1 = p0 * (1 + 2 * g / (g + 1) * (Ms * Ms - 1))
+    r1 = r0 * (g + 1) * Ms * Ms / ((g - 1) * Ms * Ms + 2)
+    u1 = -Ms * c0 * (1 - r0 / r1)
+
+    def state(x, y):
+        inside = (x - 0.2) * (x - 0.2) + (y - 0.04) * (y - 0.04) < 0.02 * 0.02
+        post = x > 0.221
+        a1 = np.where(post, 1 - 1e-6, np.where(inside, 1e-6, 1 - 1e-6))
+        r = np.where(post, r1, r0)
+        u = np.where(post, u1, 0.0)
+        p = np.where(post, p1, p0)
+        return prim2cell(ph, a1, r, 0.167, u, 0.0, p, p)
+
+    c["U"] = subcell_average(c, state)
+    c["workload"] = f"shock on a helium bubble 2D, {nx}x{ny} cells"
+    return c
+
+
+def richtmyer_meshkov(nx: int = 300, ny: int = 100) -> dict:
+    """The reference's case 71 (SPB 2009 4.7, physics :1057-1060, :1105-1107): water left of the arc
+    x = 1.2 + sqrt(0.36 - (y - 0.5)^2) against gas (gamma 1.8), everything at -200 m/s and 1 atm,
+    on [0, 3] x [0, 1] m; a wall on the left (the flow hits it), transmissive on the right, walls
+    in y; the grid-wide Rusanov speed; 4 x 4 sub-cell averages."""
+    c = default_settings()
+    c.update(nx=nx, ny=ny, x0=0.0, x1=3.0, y0=0.0, y1=1.0, tend=8.6e-3, rus_local=0,
+             phases=[dict(WATER_SG), dict(AIR_SG, g=1.8)], bc=[BC_WALL, BC_TRANS, BC_WALL, BC_WALL], case=71)
+    ph = c["phases"]
+
+    def state(x, y):
+        d = y - 0.5
+        xi = 1.2 + np.sqrt(np.maximum(0.0, 0.36 - d * d))
+        W = x < xi
+        return prim2cell(ph, np.where(W, 1 - 1e-6, 1e-6), 1000.0, 100.0, -200.0, 0.0, 101325.0, 101325.0)
+
+    c["U"] = subcell_average(c, state)
+    c["workload"] = f"cavitating Richtmyer-Meshkov 2D, {nx}x{ny} cells"
+    return c
+
+
 def bubble_compression(nx: int = 200, ny: int = 200) -> dict:
     """The reference's case 72 (P-S 2014 5.4, src/spb6_physics_omp.h:1062-1064, :1115-1117): a
     dodecane vapour bubble (radius 0.2 m, centred) in liquid dodecane at 1e5 Pa and 600 K on the
@@ -410,19 +473,14 @@ def bubble_compression(nx: int = 200, ny: int = 200) -> dict:
     c = default_settings()
     c.update(nx=nx, ny=ny, tend=1.2e-3, phases=[dict(DODECANE_LIQ_SG), dict(DODECANE_VAP_SG)],
              bc=[BC_WALL] * 4, bcu=[100.0, 0.0, 0.0, 0.0], relax=2, rus_local=0, case=72)
-    x, y, dx, dy = cell_centres(c)
-    X, Y = np.meshgrid(x, y)
     ph = c["phases"]
     r1, r2 = rho_pT(ph[0], 1e5, 600.0), rho_pT(ph[1], 1e5, 600.0)
-    sub = 4
-    U = np.zeros((ny, nx, NUM_VARS))
-    for a in range(sub):
-        for b in range(sub):
-            xs = X + ((a + 0.5) / sub - 0.5) * dx
-            ys = Y + ((b + 0.5) / sub - 0.5) * dy
-            inside = (xs - 0.5) * (xs - 0.5) + (ys - 0.5) * (ys - 0.5) < 0.04
-            U = U + prim2cell(ph, np.where(inside, 1e-6, 1 - 1e-6), r1, r2, 0.0, 0.0, 1e5, 1e5) / (sub * sub)
-    c["U"] = U
+
+    def state(x, y):
+        inside = (x - 0.5) * (x - 0.5) + (y - 0.5) * (y - 0.5) < 0.04
+        return prim2cell(ph, np.where(inside, 1e-6, 1 - 1e-6), r1, r2, 0.0, 0.0, 1e5, 1e5)
+
+    c["U"] = subcell_average(c, state)
     c["workload"] = f"piston-compressed dodecane vapour bubble 2D, {nx}x{ny} cells, relax 2"
     return c
 
@@ -430,15 +488,18 @@ def bubble_compression(nx: int = 200, ny: int = 200) -> dict:
 def underwater_explosion(nx: int = 361, ny: int = 200) -> dict:
     """The reference's case 73 geometry (Pelanti 8.1.2, src/spb6_physics_omp.h:1067-1069, :1112-1113):
     a JWL detonation-gas bubble (radius 0.05 m, centre (0, -0.32) m, 4.6406e10 Pa) in NASG water at
-    1e5 Pa on [-1.35, 1.35] x [-1.5, 0] m, a wall at y = 0, transmissive elsewhere; cell-centre
-    values (the reference averages 4 x 4 sub-points per cell)."""
+    1e5 Pa on [-1.35, 1.35] x [-1.5, 0] m, a wall at y = 0, transmissive elsewhere; 4 x 4 sub-cell
+    averages as the reference's u_initialization."""
     c = default_settings()
     c.update(nx=nx, ny=ny, x0=-1.35, x1=1.35, y0=-1.5, y1=0.0, tend=0.4e-3,
              phases=[dict(DETONATION_JWL), dict(WATER_NASG)], bc=[BC_TRANS, BC_TRANS, BC_TRANS, BC_WALL], case=73)
-    x, y, _, _ = cell_centres(c)
-    X, Y = np.meshgrid(x, y)
-    inside = X * X + (Y + 0.32) * (Y + 0.32) < 0.05 * 0.05
-    p = np.where(inside, 4.6406e10, 1e5)
-    c["U"] = prim2cell(c["phases"], np.where(inside, 1 - 1e-6, 1e-6), 2000.0, 1044.0, 0.0, 0.0, p, p)
+    ph = c["phases"]
+
+    def state(x, y):
+        inside = x * x + (y + 0.32) * (y + 0.32) < 0.05 * 0.05
+        p = np.where(inside, 4.6406e10, 1e5)
+        return prim2cell(ph, np.where(inside, 1 - 1e-6, 1e-6), 2000.0, 1044.0, 0.0, 0.0, p, p)
+
+    c["U"] = subcell_average(c, state)
     c["workload"] = f"underwater explosion (JWL gas bubble in NASG water) 2D, {nx}x{ny} cells"
     return c

@@ -161,6 +161,10 @@ CASES = {
     "tube_jreuse_N1000_20steps": (lambda: dict(_tube(1000), jreuse=1), "steps", 20, {}),
     "bubble_jreuse48_4steps": (lambda: dict(_bubble(48), jreuse=1), "steps", 4, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "lowmach_jreuse32_3steps": (lambda: dict(_lowmach(32), jreuse=1), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # the reference's own 2D cases 70 (helium bubble) and 71 (cavitating Richtmyer-Meshkov), 4 x 4
+    # sub-cell averaged initial states
+    "hebubble75x20_3steps": (lambda: cases.he_bubble(75, 20), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "rm60x20_3steps": (lambda: cases.richtmyer_meshkov(60, 20), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)
     "case13_N200_20steps": (lambda: cases.reference_case(13, 200), "steps", 20, {}),
     "lowmach_rus0_32_stage": (lambda: dict(_lowmach(32), rus_local=0), "stage", 0,
