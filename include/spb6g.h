@@ -82,7 +82,7 @@ typedef struct {
                                        1 p-pT (instantaneous thermal relaxation), 2 p-pT-pTg and 3 p-pTg
                                        (instantaneous chemical relaxation above the saturation temperature);
                                        SG / NASG phases only (SPB6G_UNSUPPORTED with a Mie-Grueneisen phase);
-                                       the rates are infinite (finite rates are not built) */
+                                       the rates are mu_rate, theta_rate, nu_rate below */
     int32_t jreuse;                 /* JREUSE (:83): 1 modified Newton -- the FD Jacobian of the stage's first
                                        iteration is kept while each step is undamped and contracts the
                                        residual 4x (batched form: 0 only) */
