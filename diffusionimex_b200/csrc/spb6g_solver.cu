@@ -586,9 +586,9 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     if (!(cfg->mu_rate >= 0) || !(cfg->nu_cr >= 0) || !(cfg->nu_pc > 0) || cfg->relax_form < 0 || cfg->relax_form > 1 ||
         cfg->unify < 0 || cfg->unify > 2 || cfg->unify_proj < 0 || cfg->unify_proj > 1 || cfg->nu_law < 0 || cfg->nu_law > 1)
         return SPB6G_BAD_ARG;
-    // Mie-Grueneisen phases relax mechanically and instantaneously only (closure :846)
-    if ((cfg->relax || !std::isinf(cfg->mu_rate) || cfg->unify == 1) && (cfg->kind[0] || cfg->kind[1]))
-        return SPB6G_UNSUPPORTED;
+    // Mie-Grueneisen phases relax mechanically and instantaneously only (closure :846); unify does
+    // not apply to them (:848), as the closure dispatch leaves it
+    if ((cfg->relax || !std::isinf(cfg->mu_rate)) && (cfg->kind[0] || cfg->kind[1])) return SPB6G_UNSUPPORTED;
     if (cfg->relax && !(cfg->eps_i >= 0 && cfg->eps_i < 0.5)) return SPB6G_BAD_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) return SPB6G_NO_DEVICE;

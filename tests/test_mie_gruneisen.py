@@ -64,3 +64,19 @@ def test_mie_gruneisen_runs_match_reference(name):
     assert np.isfinite(U).all()
     d = fieldwise_l1(U, g["U"])
     assert np.all(d <= 1e-6), {f: f"{v:.2e}" for f, v in zip(FIELDS, d)}
+
+
+@pytest.mark.gpu
+def test_unify_leaves_mie_gruneisen_phases_alone():
+    """unify = 1 applies to stiffened-gas / NASG phases only (closure :848): with Mie-Grueneisen
+    phases the run is the plain one, bit for bit."""
+    from diffusionimex_b200 import Solver
+
+    c, _, _ = golden_case("nm_N200_20steps")
+    out = []
+    for unify in (0, 1):
+        s = Solver(dict(c, unify=unify))
+        s.advance(5)
+        out.append(s.state())
+        s.close()
+    assert np.array_equal(out[0], out[1])
