@@ -414,6 +414,57 @@ def subcell_average(c: dict, state, sub: int = 4) -> np.ndarray:
     return U
 
 
+_exp, _pow = np.vectorize(math.exp), np.vectorize(math.pow)
+_sin, _cos = np.vectorize(math.sin), np.vectorize(math.cos)  # the C library's, point by point
+
+
+def vortex_bb(n: int = 40, p0: float = 1.0) -> dict:
+    """The reference's case 56 (Battisti-Boscheri 4.1, physics :1041-1043, :1148-1155): a Hu-Shu
+    isentropic vortex (eps 5) in two ideal gases (gamma 1.35 and 1.4) at one density and pressure,
+    alpha2 a passive smooth bump, translated by (2, 2) across the periodic [-5, 5]^2 (t_end 5 is one
+    period, so the exact solution is the initial state); background pressure p0 (p0=); 4 x 4 sub-cell
+    averages."""
+    c = default_settings()
+    c.update(nx=n, ny=n, x0=-5.0, x1=5.0, y0=-5.0, y1=5.0, tend=5.0,
+             phases=[dict(AIR_SG, g=1.35), dict(AIR_SG)], bc=[BC_PERIODIC] * 4, case=56)
+    ph = c["phases"]
+    g, eps = 1.4, 5.0
+
+    def state(x, y):
+        r2 = x * x + y * y
+        du = eps / (2 * math.pi) * _exp(0.5 * (1 - r2))
+        dT = -(g - 1) * eps * eps / (8 * g * math.pi * math.pi) * _exp(1 - r2)
+        T = p0 + dT
+        rho = _pow(T / p0, 1.0 / (g - 1))
+        p = rho * T
+        a2 = 0.5 + 0.25 * _exp(0.5 * (1 - r2))
+        return prim2cell(ph, 1 - a2, rho, rho, 2.0 - du * y, 2.0 + du * x, p, p)
+
+    c["U"] = subcell_average(c, state)
+    c["workload"] = f"two-phase isentropic vortex 2D, {n}x{n} cells, p0 {p0}"
+    return c
+
+
+def taylor_green(n: int = 50, two_phase: bool = False, p0: float = 1.0) -> dict:
+    """The reference's cases 57 / 58 (Battisti-Boscheri 4.4, physics :1044-1046, :1144-1147): the
+    low-Mach Taylor-Green vortex u = sin x cos y, v = -cos x sin y, p = p0 + (cos 2x + cos 2y) / 4
+    in two ideal gases of gamma 1.4 and density 1 on the periodic [0, 2 pi]^2 to t = 0.2; alpha2 0.5
+    (57) or 0.5 + 0.1 (cos 2x + cos 2y) (58); 4 x 4 sub-cell averages."""
+    c = default_settings()
+    c.update(nx=n, ny=n, x0=0.0, x1=2 * math.pi, y0=0.0, y1=2 * math.pi, tend=0.2,
+             phases=[dict(AIR_SG), dict(AIR_SG)], bc=[BC_PERIODIC] * 4, case=58 if two_phase else 57)
+    ph = c["phases"]
+
+    def state(x, y):
+        p = p0 + 0.25 * (_cos(2 * x) + _cos(2 * y))
+        a2 = 0.5 + 0.1 * (_cos(2 * x) + _cos(2 * y)) if two_phase else np.full_like(x, 0.5)
+        return prim2cell(ph, 1 - a2, 1.0, 1.0, _sin(x) * _cos(y), -_cos(x) * _sin(y), p, p)
+
+    c["U"] = subcell_average(c, state)
+    c["workload"] = f"Taylor-Green vortex 2D, {n}x{n} cells, {'two phases' if two_phase else 'one phase'}"
+    return c
+
+
 def he_bubble(nx: int = 600, ny: int = 160) -> dict:
     """The reference's case 70 (SPB 2009 4.6, physics :1055-1056, :1099-1104): a Mach-1.5 shock in
     air (ideal-gas Rankine-Hugoniot post-shock state for x > 0.221 m, moving left) reaching a

@@ -165,6 +165,9 @@ CASES = {
     # sub-cell averaged initial states
     "hebubble75x20_3steps": (lambda: cases.he_bubble(75, 20), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     "rm60x20_3steps": (lambda: cases.richtmyer_meshkov(60, 20), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    # cases 56 (two-phase vortex) and 58 (two-phase Taylor-Green), periodic in both directions
+    "vortex24_3steps": (lambda: cases.vortex_bb(24), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
+    "taylorgreen24_3steps": (lambda: cases.taylor_green(24, True), "steps", 3, {"newton_tol": 1e-13, "bicg_tol": 1e-13}),
     # grid-wide Rusanov dissipation speed (RUS_LOCAL = 0; RusanovC_x/y :237-259, Update :266-298)
     "case13_N200_20steps": (lambda: cases.reference_case(13, 200), "steps", 20, {}),
     "lowmach_rus0_32_stage": (lambda: dict(_lowmach(32), rus_local=0), "stage", 0,

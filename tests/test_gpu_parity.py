@@ -113,7 +113,7 @@ def test_1d_tube_one_step_bitwise():
                                   "tube_periodic_N200_10steps", "bubble_walls32_3steps", "bubble_outlet32_3steps",
                                   "case83_N200_10steps", "case13_N200_20steps", "lowmach_rus0_32_3steps",
                                   "tube_order1_N200_20steps", "bubble_order1_32_3steps", "hebubble75x20_3steps",
-                                  "rm60x20_3steps"])
+                                  "rm60x20_3steps", "vortex24_3steps", "taylorgreen24_3steps"])
 def test_runs_match_reference_in_l1(name):
     """Whole runs in L1: within 1e-6 of the field maximum, or within 10x the reference's own L1
     change under round-off perturbations (one-ulp libm, FD step 1.01e-7) where that is larger --

@@ -114,11 +114,14 @@ def test_fixture_builders_keep_their_settings():
 
 
 def test_reference_2d_initial_states():
-    """Cases 70, 71, 72, 73 as the reference's own u_initialization builds them, 4 x 4 sub-cell
-    averages included, where the compiled reference exists."""
+    """Cases 56, 57, 58, 70, 71, 72, 73 as the reference's own u_initialization builds them, 4 x 4
+    sub-cell averages included, where the compiled reference exists."""
     if not refio.ref_available():
         pytest.skip("compiled reference not available")
-    for case, build, nx, ny in ((70, cases.he_bubble, 60, 16), (71, cases.richtmyer_meshkov, 60, 20),
+    for case, build, nx, ny in ((56, lambda nx, ny: cases.vortex_bb(nx), 40, 40),
+                                (57, lambda nx, ny: cases.taylor_green(nx), 50, 50),
+                                (58, lambda nx, ny: cases.taylor_green(nx, True), 50, 50),
+                                (70, cases.he_bubble, 60, 16), (71, cases.richtmyer_meshkov, 60, 20),
                                 (72, cases.bubble_compression, 32, 32), (73, cases.underwater_explosion, 60, 40)):
         r = refio.run_ref_main_files([f"case={case}", f"N={nx}", f"ny={ny}", "init=1"], nx=nx, ny=ny)
         c = build(nx, ny)
