@@ -129,7 +129,7 @@ def cell_centres(cfg: dict):
 # --------------------------------------------------------------------------------------------
 # Reference cases (test_setup / test_state, src/spb6_physics_omp.h:1017-1157)
 # --------------------------------------------------------------------------------------------
-def reference_case(case: int, nx: int | None = None) -> dict:
+def reference_case(case: int, nx: int | None = None, ny: int | None = None) -> dict:
     """A subset of the reference's 1D cases: 4 (interface advection), 5 (SPB 4.3.1 water-air),
     12 and 13 (SPB 5.1 / 5.2 epoxy-spinel mixture; 13 takes the grid-wide Rusanov speed,
     rus_local = 0), the liquid-vapour cases of phase transition -- 1, 2 (P-S 2014 5.1 water
@@ -138,8 +138,16 @@ def reference_case(case: int, nx: int | None = None) -> dict:
     depressurisation: pressure outlet left, wall right, relax 2), 40, 41 (uniform non-equilibrium
     states, periodic) -- 80-88 (Schropff 2026 Riemann problems), and the Mie-Grueneisen shock tubes
     60 (SPB 4.2 nitromethane, Cochran-Chan) and 61 (Pelanti 8.1.1, JWL detonation gas against NASG
-    water).  The relaxation level is the case's own (32: 2; the others 0); set "relax" to run one
-    with thermal or chemical relaxation."""
+    water); 0 (SPB 4.4 water cavitation), 6 (SPB 4.3.2 water-air at 1 TPa), 20 and 21 (smooth
+    gas and smooth water advection).  The relaxation level is the case's own (32: 2; the others 0);
+    set "relax" to run one with thermal or chemical relaxation.  The 2D cases 56-58 and 70-73 come
+    from their builders (nx, ny their grid, each builder's own by default)."""
+    builders_2d = {56: lambda a, b: vortex_bb(a), 57: lambda a, b: taylor_green(a), 58: lambda a, b: taylor_green(a, True),
+                   70: he_bubble, 71: richtmyer_meshkov, 72: bubble_compression, 73: underwater_explosion}
+    if case in builders_2d:
+        defaults = {56: (40, 40), 57: (50, 50), 58: (50, 50), 70: (600, 160), 71: (300, 100), 72: (200, 200),
+                    73: (361, 200)}[case]
+        return builders_2d[case](nx or defaults[0], ny or defaults[1])
     c = default_settings()
     air, water = dict(AIR_SG), dict(WATER_SG)
     if case == 4:
@@ -169,6 +177,11 @@ def reference_case(case: int, nx: int | None = None) -> dict:
                  relax=2, bc=[BC_PRES, BC_WALL, BC_TRANS, BC_TRANS], bcp=[1e5, 0.0, 0.0, 0.0])
     elif case in (40, 41):  # :1040
         c.update(phases=[dict(WATER_LIQ_SG), dict(WATER_VAP_SG)], tend=1e-4, bc=[BC_PERIODIC, BC_PERIODIC, BC_TRANS, BC_TRANS])
+    elif case in (0, 6):  # :1019, :1028
+        c.update(phases=[dict(WATER_SG), dict(AIR_SG)], nx=1000, tend=1.85e-3 if case == 0 else 8.3e-6)
+    elif case in (20, 21):  # :1033-1034
+        c.update(phases=[dict(AIR_SG), dict(AIR_SG)] if case == 20 else [dict(WATER_SG), dict(AIR_SG)],
+                 tend=5e-4 if case == 20 else 1e-4)
     elif case in (12, 13):  # test_setup physics :1029-1032
         c.update(phases=[dict(WATER_SG, g=2.43, pinf=5.3e9), dict(AIR_SG, g=1.62, pinf=141e9)], nx=500,
                  tend=80e-6 if case == 12 else 34e-6)
@@ -213,6 +226,18 @@ def reference_case(case: int, nx: int | None = None) -> dict:
         L = x < (0.25 if adv else 0.7)
         p = np.full_like(x, 1e5) if adv else np.where(L, 1e9, 1e5)
         U = prim2cell(ph, np.where(L, 1 - 1e-7, 1e-7), 1000.0, 0.01 if adv else 50.0, 1.0 if adv else 0.0, 0.0, p, p)
+    elif case == 0:  # test_state :1089
+        u = np.where(x < 0.5, -100.0, 100.0)
+        U = prim2cell(ph, np.full_like(x, 1 - 1e-2), 1000.0, 1.0, u, 0.0, 1e5, 1e5)
+    elif case == 6:  # :1132-1134
+        L = x < 0.6
+        p = np.where(L, 1e12, 1e5)
+        U = prim2cell(ph, np.where(L, 1 - 1e-6, 1e-6), 1000.0, 10.0, 0.0, 0.0, p, p)
+    elif case in (20, 21):  # :1157-1159, exp and sin of the C library point by point
+        gs = np.array([math.exp(-(xv - 0.5) * (xv - 0.5) / 0.01) for xv in x])
+        a1 = 0.5 + 0.2 * np.array([math.sin(2 * math.pi * xv) for xv in x])
+        p = 1e5 * (1 + 0.2 * gs)
+        U = prim2cell(ph, a1, 2.0 if case == 20 else 1000.0, 1.0, 50.0 * gs, 0.0, p, p)
     elif case in (1, 2, 30):  # test_state :1090-1092, :1141
         T0 = 353.0 if case == 30 else 354.728
         U0 = 500.0 if case == 2 else 2.0

@@ -126,3 +126,16 @@ def test_reference_2d_initial_states():
         r = refio.run_ref_main_files([f"case={case}", f"N={nx}", f"ny={ny}", "init=1"], nx=nx, ny=ny)
         c = build(nx, ny)
         assert np.array_equal(r["U"].reshape(c["U"].shape), c["U"]), case
+
+
+def test_reference_1d_initial_states():
+    """Every 1D case reference_case restates (0-6, 12, 13, 20, 21, 30-32, 40, 41, 60, 61, 80-88) as
+    the reference's own u_initialization builds it, where the compiled reference exists; the 2D
+    ids go to their builders."""
+    if not refio.ref_available():
+        pytest.skip("compiled reference not available")
+    for case in (0, 1, 2, 3, 4, 5, 6, 12, 13, 20, 21, 30, 31, 32, 40, 41, 60, 61, 80, 81, 82, 83, 84, 85, 86, 87, 88):
+        r = refio.run_ref_main_files([f"case={case}", "N=64", "init=1"], nx=64)
+        assert np.array_equal(r["U"], cases.reference_case(case, 64)["U"]), case
+    c = cases.reference_case(73, 60, 40)
+    assert (c["nx"], c["ny"], c["case"]) == (60, 40, 73)
