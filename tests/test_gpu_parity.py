@@ -4,7 +4,7 @@ own outputs (golden fixtures) and the C restatement.
 Tolerances (field-max-normalised, per conservative variable):
   * explicit predictor (reconstruction + Rusanov update): no reductions are
     involved, so X*, alpha2*, face velocities and limiters must agree to 1e-15;
-  * one stage / one step: 1e-12 (north_star's one-step bar).  In 1D the linear
+  * one stage / one step: 1e-12 (the one-step bar for FP64 parity).  In 1D the linear
     solve is the same sequential Thomas sweep as the reference and the result is
     typically bit-identical; in 2D BiCGStab's dot products are summed in a
     different (deterministic, tree) order, so the converged pressure differs at
