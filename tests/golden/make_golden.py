@@ -11,6 +11,8 @@ where the reference tree does not exist.
 Fixtures:
   ref_<name>.npz      U0 (initial state), U, P, p_ref and run counters of the
                       compiled reference on the case built by CASES[name]
+  ref_main_profile2d.npz
+                      the final profile of the reference main()'s 2D case 70 (30 x 8) and its state
   ref_sat_tables.npz  the reference's saturation tables (SAT after build_sat) of the
                       liquid / vapour pairs in SAT_CASES
   ref_main_outputs.npz
@@ -205,6 +207,18 @@ def main_outputs():
     np.savez_compressed(os.path.join(HERE, "ref_main_outputs.npz"), **out)
 
 
+def main_profile_2d():
+    """The final profile the reference's main() writes for its 2D case 70 on 30 x 8 cells (t_end cut
+    to 2e-5 s), with the captured state: the 2D layout of write_profile (:1083-1094)."""
+    import refio
+
+    args = ["case=70", "N=30", "ny=8", "tend=2e-5"]
+    r = refio.run_ref_main_files(args, out_name="run.dat", nx=30, ny=8)
+    np.savez_compressed(os.path.join(HERE, "ref_main_profile2d.npz"), profile=np.frombuffer(r["files"]["run.dat"], np.uint8),
+                        U=r["U"], args=np.frombuffer(json.dumps(args).encode(), np.uint8))
+    print("profile2d", len(r["files"]["run.dat"]), r["stdout"].strip()[:80])
+
+
 # liquid / vapour pairs whose saturation tables (build_sat, physics :127-153) are pinned
 SAT_CASES = (1, 3, 30, 31, 32)
 
@@ -254,6 +268,9 @@ def main():
     if only == ["sat"]:
         sat_tables()
         return
+    if only == ["profile2d"]:
+        main_profile_2d()
+        return
     for name in (only or CASES):
         c, mode, nsteps = build_case(name)
         r = refio.run_ref(c, mode=modes[mode], nsteps=nsteps)
@@ -276,6 +293,7 @@ def main():
     if only:
         return
     main_outputs()
+    main_profile_2d()
     sat_tables()
     for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
                       ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):

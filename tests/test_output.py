@@ -139,3 +139,15 @@ def _counters(line):
     head = line.split(" | wall")[0]
     ints = re.findall(r"(?:case|order|rk|N|steps|rk1|rejects|floor|stages|it|fails) \(?(-?\d+)\b", head)
     return [int(v) for v in ints]
+
+
+def test_2d_profile_of_the_reference_state_is_byte_identical(tmp_path):
+    """Host formatter only: the state the reference's main() reached on its 2D case 70 (30 x 8 cells)
+    prints as the run.dat it wrote -- rows j outer, i inner, with the y column (:1083-1094)."""
+    from diffusionimex_b200.solver import format_profile
+
+    z = np.load(os.path.join(HERE, "golden", "ref_main_profile2d.npz"))
+    path = str(tmp_path / "p2d.dat")
+    format_profile(cases.reference_case(70, 30, 8), z["U"].reshape(8, 30, 8), path)
+    with open(path, "rb") as f:
+        assert f.read() == bytes(z["profile"])
