@@ -151,3 +151,31 @@ def test_2d_profile_of_the_reference_state_is_byte_identical(tmp_path):
     format_profile(cases.reference_case(70, 30, 8), z["U"].reshape(8, 30, 8), path)
     with open(path, "rb") as f:
         assert f.read() == bytes(z["profile"])
+
+
+@pytest.mark.gpu
+def test_2d_run_writes_the_reference_profile(tmp_path):
+    """The whole 2D run (case 70, 30 x 8 cells, to t = 2e-5 s) on the GPU writes the reference's
+    run.dat: same header, coordinate text and line count; columns within the whole-run bars."""
+    from diffusionimex_b200 import Solver
+
+    z = np.load(os.path.join(HERE, "golden", "ref_main_profile2d.npz"))
+    c = cases.reference_case(70, 30, 8)
+    c["tend"] = 2e-5
+    out = str(tmp_path / "run.dat")
+    s = Solver(c)
+    s.set_output(out)
+    s.advance(0)
+    s.close()
+    with open(out, "rb") as f:
+        mine = f.read().decode().splitlines()
+    ref = bytes(z["profile"]).decode().splitlines()
+    assert len(mine) == len(ref) and mine[0] == ref[0]
+    assert [ln.split()[:2] for ln in mine[1:]] == [ln.split()[:2] for ln in ref[1:]]
+    a, b = _cols(mine[1:]), _cols(ref[1:])
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    a, b = np.nan_to_num(a, nan=0.0), np.nan_to_num(b, nan=0.0)
+    l1 = np.abs(a - b).mean(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)
+    bar = np.full(a.shape[1], L1_BAR)
+    bar[list(TRACE_COLS_DAT)] = L1_BAR_TRACE
+    assert np.all(l1 <= bar), [f"{v:.3g}" for v in l1]
