@@ -80,3 +80,19 @@ def test_no_device_reported_on_cpu_host():
     lib.spb6g_default_config(ctypes.byref(c))
     h = ctypes.c_void_p()
     assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 9  # SPB6G_NO_DEVICE
+
+
+def test_saturation_table_errors():
+    """The host saturation table: the length query, a buffer too small (SPB6G_TOO_LARGE), and a
+    Mie-Grueneisen pair, which has no SG / NASG saturation line (SPB6G_UNSUPPORTED)."""
+    from diffusionimex_b200 import cases
+
+    lib = solver.library()
+    c = solver.make_config(cases.reference_case(3, 16))
+    n = ctypes.c_int()
+    assert lib.spb6g_saturation_table(ctypes.byref(c), None, 0, ctypes.byref(n)) == 0 and n.value > 4
+    buf = (ctypes.c_double * 4)()
+    assert lib.spb6g_saturation_table(ctypes.byref(c), buf, 4, ctypes.byref(n)) == 10  # SPB6G_TOO_LARGE
+    mg = solver.make_config(cases.reference_case(60, 16))
+    assert lib.spb6g_saturation_table(ctypes.byref(mg), None, 0, ctypes.byref(n)) == 8  # SPB6G_UNSUPPORTED
+    assert lib.spb6g_saturation_table(None, None, 0, ctypes.byref(n)) == 7  # SPB6G_BAD_ARG
