@@ -96,3 +96,21 @@ def test_saturation_table_errors():
     mg = solver.make_config(cases.reference_case(60, 16))
     assert lib.spb6g_saturation_table(ctypes.byref(mg), None, 0, ctypes.byref(n)) == 8  # SPB6G_UNSUPPORTED
     assert lib.spb6g_saturation_table(None, None, 0, ctypes.byref(n)) == 7  # SPB6G_BAD_ARG
+
+
+def test_new_settings_validated_before_device_use():
+    """Out-of-range order, jreuse, relaxation rates and forms are SPB6G_BAD_ARG, and relaxation or a
+    finite mu with a Mie-Grueneisen phase is SPB6G_UNSUPPORTED, before any device is touched."""
+    from diffusionimex_b200 import cases
+
+    lib = solver.library()
+    h = ctypes.c_void_p()
+    base = cases.reference_case(5, 16)
+    for bad in (dict(order=3), dict(jreuse=2), dict(relax_form=2), dict(unify=3), dict(unify_proj=2),
+                dict(nu_law=2), dict(mu_rate=-1.0), dict(nu_pc=0.0), dict(relax=4), dict(rus_local=2)):
+        c = solver.make_config(dict(base, **bad))
+        assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 7, bad  # SPB6G_BAD_ARG
+    mg = cases.reference_case(60, 16)
+    for unsup in (dict(relax=1), dict(mu_rate=1e-3)):
+        c = solver.make_config(dict(mg, **unsup))
+        assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 8, unsup  # SPB6G_UNSUPPORTED
