@@ -68,6 +68,11 @@ def test_batched_form_takes_the_per_face_rusanov_speed_only():
     c.rus_local = 0
     b = ctypes.c_void_p()
     assert lib.spb6g_batch_create(ctypes.byref(c), 1, ctypes.byref(b)) == 8  # SPB6G_UNSUPPORTED
+    # nor modified Newton, first order, relaxation, finite or unified rates
+    for field, value in (("jreuse", 1), ("order", 1), ("relax", 1), ("mu_rate", 1e-3), ("unify", 1)):
+        lib.spb6g_default_config(ctypes.byref(c))
+        setattr(c, field, value)
+        assert lib.spb6g_batch_create(ctypes.byref(c), 1, ctypes.byref(b)) == 8, field
 
 
 def test_no_device_reported_on_cpu_host():
