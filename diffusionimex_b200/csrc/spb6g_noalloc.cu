@@ -13,9 +13,15 @@
 //   * at most SPB6G_NOALLOC_MAX_CELLS interior cells (one cell per thread,
 //     one partial per 256-thread block); larger grids are rejected with
 //     SPB6G_TOO_LARGE before any device work;
+//   * it runs on cfg->device (made current for the call, the caller's current
+//     device restored on return); every U_dev[k] must be device (or managed)
+//     memory of that device, checked with cudaPointerGetAttributes before any
+//     launch (SPB6G_BAD_ARG otherwise), and `stream` must belong to it;
 //   * the first call on a device looks up the device addresses of the scratch
-//     arrays (cudaGetSymbolAddress, with that device current) -- make that
-//     first call before any stream capture;
+//     arrays (cudaGetSymbolAddress, with that device current);
+//   * every call is blocking: it copies the result to the host and waits for
+//     `stream`, so no call -- the first or any later one -- may be made while a
+//     stream is being captured into a CUDA graph;
 //   * every call shares the scratch: the block counter is cleared at the start
 //     of each call, and two calls whose work overlaps on the GPU (different
 //     streams, or host threads, at the same time) race on it.
@@ -71,11 +77,38 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_caldt_noalloc(Phys P, int n
     }
 }
 
+// Makes `dev` current for the call and puts the caller's device back on every return.
+struct DeviceScope {
+    int prev = -1;
+    bool set(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) return false;
+        return prev == dev || cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// True when p is device (or managed) memory of device `dev`.
+bool on_device(const void* p, int dev) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
+
 }  // namespace
 
 extern "C" int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
                                    double* inv_rate) {
     if (!cfg || !U_dev || !inv_rate || cfg->nx < 1 || cfg->ny < 1) return SPB6G_BAD_ARG;
+    // the geometry checks of spb6g_create: a degenerate domain has no finite rate
+    if (!(cfg->x1 > cfg->x0) || !(cfg->y1 > cfg->y0) || cfg->device < 0) return SPB6G_BAD_ARG;
+    for (int k = 0; k < 2; k++)
+        if (cfg->kind[k] < 0 || cfg->kind[k] > 2) return SPB6G_BAD_ARG;
     if (cfg->kind[0] != 0 || cfg->kind[1] != 0) return SPB6G_UNSUPPORTED;  // stiffened gas / NASG phases only
     for (int k = 0; k < NV; k++)
         if (!U_dev[k]) return SPB6G_BAD_ARG;
@@ -85,8 +118,16 @@ extern "C" int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const*
                 (int)SPB6G_NOALLOC_MAX_CELLS);
         return SPB6G_TOO_LARGE;
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SPB6G_NO_DEVICE;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device >= ndev || cfg->device >= 64) {
+        cudaGetLastError();
+        return SPB6G_NO_DEVICE;
+    }
+    const int dev = cfg->device;
+    DeviceScope scope;
+    if (!scope.set(dev)) return SPB6G_NO_DEVICE;
+    for (int k = 0; k < NV; k++)
+        if (!on_device(U_dev[k], dev)) return SPB6G_BAD_ARG;
     {
         std::lock_guard<std::mutex> lock(g_syms_mutex);
         NoallocSymbols& sy = g_syms[dev];

@@ -226,11 +226,17 @@ int64_t spb6g_kernel_launches(spb6g_solver* s);
  * (SoA, cell (i, j) at i + j*nx); cfg supplies the grid and phases.  The only
  * scratch is a file-scope device array sized for SPB6G_NOALLOC_MAX_CELLS cells,
  * held by every GPU that loads the library until the process exits; larger
- * grids return SPB6G_TOO_LARGE.  The first call on a device looks up the
- * scratch's device address, so make it before any stream capture.  All calls
- * share the scratch (its counter is cleared at the start of each call): calls
- * whose GPU work overlaps race.  stream: a cudaStream_t, or NULL for the
- * default stream; the call returns after the result has reached *inv_rate. */
+ * grids return SPB6G_TOO_LARGE.  The call runs on cfg->device (made current
+ * for the call; the caller's current device is restored on return), every
+ * U_dev[k] must be device or managed memory of that device (SPB6G_BAD_ARG
+ * otherwise, found before any launch) and stream must belong to it.  The first
+ * call on a device looks up the scratch's device address.  Every call is
+ * blocking -- it copies the result to *inv_rate and waits for stream -- so no
+ * call, first or later, may be made while a stream is being captured.  All
+ * calls share the scratch (its counter is cleared at the start of each call):
+ * calls whose GPU work overlaps race.  stream: a cudaStream_t, or NULL for the
+ * default stream.  A degenerate domain (x1 <= x0 or y1 <= y0) or a phase kind
+ * outside 0..2 is SPB6G_BAD_ARG; a Mie-Grueneisen phase SPB6G_UNSUPPORTED. */
 #define SPB6G_NOALLOC_MAX_CELLS (4 * 1024 * 1024)
 int spb6g_caldt_noalloc(const spb6g_config* cfg, const double* const* U_dev, int acoustic, void* stream,
                         double* inv_rate);

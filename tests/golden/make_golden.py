@@ -41,7 +41,7 @@ sys.path.insert(0, os.path.dirname(HERE))  # tests/helpers.py
 
 from diffusionimex_b200 import cases  # noqa: E402
 
-REF_TREE = "/root/reference"
+REF_TREE = os.environ.get("SPB6_REFERENCE", "/root/reference")  # the reference source tree
 
 
 def _tube(n):

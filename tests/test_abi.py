@@ -119,3 +119,39 @@ def test_new_settings_validated_before_device_use():
     for unsup in (dict(relax=1), dict(mu_rate=1e-3)):
         c = solver.make_config(dict(mg, **unsup))
         assert lib.spb6g_create(ctypes.byref(c), ctypes.byref(h)) == 8, unsup  # SPB6G_UNSUPPORTED
+
+
+def test_noalloc_caldt_arguments_rejected_before_device_use():
+    """spb6g_caldt_noalloc checks the domain, the phase kinds and the device ordinal before it
+    touches a device: a degenerate domain, a kind outside 0..2 and a negative device are
+    SPB6G_BAD_ARG, a Mie-Grueneisen phase SPB6G_UNSUPPORTED (the pointers are never read)."""
+    from diffusionimex_b200 import cases
+
+    lib = solver.library()
+    ptrs = (ctypes.c_void_p * 8)(*([16] * 8))  # never dereferenced: every case stops before a launch
+    out = ctypes.c_double(0.0)
+    base = solver.make_config(cases.water_air_tube(64))
+    for field, value in (("x1", 0.0), ("y1", 0.0), ("device", -1)):
+        c = solver.make_config(cases.water_air_tube(64))
+        setattr(c, field, value)
+        assert lib.spb6g_caldt_noalloc(ctypes.byref(c), ptrs, 0, None, ctypes.byref(out)) == 7, field
+    c = solver.make_config(cases.water_air_tube(64))
+    c.kind[0] = 5
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(c), ptrs, 0, None, ctypes.byref(out)) == 7
+    c.kind[0] = 1
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(c), ptrs, 0, None, ctypes.byref(out)) == 8
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(base), None, 0, None, ctypes.byref(out)) == 7
+
+
+def test_noalloc_caldt_without_a_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from diffusionimex_b200 import cases
+
+    lib = solver.library()
+    ptrs = (ctypes.c_void_p * 8)(*([16] * 8))
+    out = ctypes.c_double(0.0)
+    c = solver.make_config(cases.water_air_tube(64))
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(c), ptrs, 0, None, ctypes.byref(out)) == 9  # SPB6G_NO_DEVICE

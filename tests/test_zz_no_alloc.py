@@ -58,3 +58,23 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     out = ctypes.c_double(0.0)
     assert lib.spb6g_caldt_noalloc(ctypes.byref(cfg), ptrs, 0, None, ctypes.byref(out)) == 10
     del keep
+
+
+def test_noalloc_checks_the_device_of_its_pointers():
+    """The call runs on cfg->device and refuses, before any launch, pointers that are not memory
+    of that device (here host memory) and a device ordinal beyond the count; the caller's current
+    device is unchanged afterwards."""
+    import torch
+
+    lib = library()
+    c = cases.water_air_tube(300)
+    cfg = make_config(c)
+    host = np.ascontiguousarray(np.moveaxis(c["U"], -1, 0)).reshape(8, -1)
+    hptrs = (ctypes.c_void_p * 8)(*[host[k].ctypes.data for k in range(8)])
+    out = ctypes.c_double(-1.0)
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(cfg), hptrs, 0, None, ctypes.byref(out)) == 7  # SPB6G_BAD_ARG
+    cfg.device = torch.cuda.device_count()
+    keep, ptrs = device_state(c["U"])
+    assert lib.spb6g_caldt_noalloc(ctypes.byref(cfg), ptrs, 0, None, ctypes.byref(out)) == 9  # SPB6G_NO_DEVICE
+    assert torch.cuda.current_device() == 0
+    del keep
