@@ -14,7 +14,8 @@ namespace spb6g {
 struct BicgScalars {
     double rho, alpha, omega, bn, Einv, cb, r0A1, cc, cs, rr, r0r, ts, tt, ss;
     double tol;
-    int maxit, iters, status, pad;
+    int maxit, iters, status;
+    int x0_learned;  // 1: the solve started from the learned first iterate
 };
 enum { BICG_RUNNING = 0, BICG_CONV = 1, BICG_FAIL = 2, BICG_CONV_HALF = 3, BICG_TIMEOUT = 4 };
 
@@ -24,6 +25,7 @@ struct GridBarrier {
     int err, pad;
 };
 constexpr int PB_THREADS = 512;  // threads (and rows per chunk) of a persistent BiCGStab block
+constexpr int PB_SLOT_Q = 8;     // partial sums per block in one grid-barrier record
 
 // Reduction results read back by the host after a Newton decision point.
 struct NewtonScalars {
@@ -109,6 +111,10 @@ struct Ctx {
     float *fC, *fW, *fE, *fS, *fN;  // precision form: FP32 diagonals for the SpMV
     double *br, *br0, *bp, *bv, *bq, *bs, *bu, *bt;
     double *tcp, *tdp;
+    // learned warm start (no counterpart in the reference)
+    double* Prate;     // pressure rate (P_converged - P_start) / sdt of the last converged stage, or null
+    const double* x0l; // learned first BiCGStab iterate of this solve, or null (the plain start M^-1 b)
+    double sdt;        // time span of the stage: (c_s - c_{s-1}) dt, c the implicit tableau's row sums
     // final state
     State Ust;
     double* H;  // 8*n, this stage's derivative (U_s - Qs)/adt
@@ -118,7 +124,7 @@ struct Ctx {
     NewtonScalars* ns;
     BicgScalars* bs_;
     GridBarrier* gbar;  // persistent BiCGStab: barrier state (zero at start)
-    double* gpart;      // persistent BiCGStab: 2 slots x G blocks x 4 partial sums
+    double* gpart;      // persistent BiCGStab: 2 slots x G blocks x PB_SLOT_Q partial sums
     long long* nlaunch;  // host-side count of kernel launches (never dereferenced on the device)
 };
 
@@ -129,8 +135,9 @@ SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(
 
 // Normalisation of the warm-start features (mean / 1/std of the centre values,
 // 1/std of the neighbour differences, per field) and the target scale.
+constexpr int NFIELD = 7;  // rho, rho u, rho v, alpha1, E*, P, the previous stage's pressure rate
 struct FeatureNorm {
-    double mean[6], istd[6], idstd[6];
+    double mean[NFIELD], istd[NFIELD], idstd[NFIELD];
     double tscale;
 };
 
@@ -187,10 +194,11 @@ void launch_thomas(const Ctx& c, cudaStream_t st);
 // flux tiles of width tw (128 or 256); one persistent launch
 int launch_batch(BatchInst* insts, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st);
 int batch_max_blocks(int threads, int tw, int device);
-// learned warm start: BF16 feature rows (n x 64), dP = y * tscale, training targets
+// learned warm start: BF16 feature rows (n x 64), dP = sdt (Prate + y tscale), and after a converged
+// stage the training target (if t) and the new pressure rate
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
 void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale);
-void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
+void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);
 void launch_floor(const Ctx& c, cudaStream_t st, double tol);

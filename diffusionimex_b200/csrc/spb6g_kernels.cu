@@ -867,13 +867,14 @@ SPB6G_DEV bool barrier_arrive_wait(GridBarrier* gb, unsigned target) {
     return true;
 }
 
-// Publishes this block's NQ partial sums (records of 4), waits for every block,
-// and folds all G records in block order in warp 0; `tot` is then the same in
-// every thread of every block.  `epoch` counts the barriers of the launch.
+// Publishes this block's NQ partial sums (records of PB_SLOT_Q), waits for every
+// block, and folds all G records in block order in warp 0; `tot` is then the same
+// in every thread of every block.  `epoch` counts the barriers of the launch.
 template <int NQ>
 SPB6G_DEV bool sync_fold(double (&acc)[NQ], double* slot, unsigned G, GridBarrier* gb, unsigned& epoch, double (&tot)[NQ]) {
-    __shared__ double sh[4 * 32];
-    __shared__ double bc[4];
+    static_assert(NQ <= PB_SLOT_Q, "a barrier record holds PB_SLOT_Q sums");
+    __shared__ double sh[NQ * 32];
+    __shared__ double bc[NQ];
     __shared__ int s_ok;
     block_fold<RedSum, NQ>(acc, sh);
     epoch += 1;
@@ -881,7 +882,7 @@ SPB6G_DEV bool sync_fold(double (&acc)[NQ], double* slot, unsigned G, GridBarrie
         int ok = 1;
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int q = 0; q < NQ; q++) slot[4 * blockIdx.x + q] = acc[q];
+            for (int q = 0; q < NQ; q++) slot[PB_SLOT_Q * blockIdx.x + q] = acc[q];
             ok = barrier_arrive_wait(gb, epoch * G) ? 1 : 0;
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -892,7 +893,7 @@ SPB6G_DEV bool sync_fold(double (&acc)[NQ], double* slot, unsigned G, GridBarrie
             for (int q = 0; q < NQ; q++) f[q] = 0.0;
             for (unsigned b = threadIdx.x; b < G; b += 32) {
 #pragma unroll
-                for (int q = 0; q < NQ; q++) f[q] += __ldcg(slot + 4 * b + q);
+                for (int q = 0; q < NQ; q++) f[q] += __ldcg(slot + PB_SLOT_Q * b + q);
             }
 #pragma unroll
             for (int q = 0; q < NQ; q++) f[q] = warp_fold<RedSum>(f[q]);
@@ -1097,7 +1098,7 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     const bool two_d = c.g.ny > 1;
     GridBarrier* gb = c.gbar;
     unsigned epoch = 0;
-    double* slots = c.gpart;  // G records of 4 per barrier, two barriers apart
+    double* slots = c.gpart;  // G records of PB_SLOT_Q per barrier, two barriers apart
     const double* __restrict__ dinv = c.dinv;
     const double* __restrict__ A1 = c.A1;
     double* __restrict__ br = c.br;
@@ -1106,21 +1107,69 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     double* __restrict__ bs = c.bs;
     double* __restrict__ bt = c.bt;
     double* __restrict__ dP = c.dP;
-    auto slot = [&](int k) { return slots + (size_t)(k & 1) * 4 * G; };
+    auto slot = [&](int k) { return slots + (size_t)(k & 1) * PB_SLOT_Q * G; };
     const MT* const mat[5] = {diag<MT>(c, 0), diag<MT>(c, 1), diag<MT>(c, 2), diag<MT>(c, 3), diag<MT>(c, 4)};
 
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
     const double cb = ns.sumb * Einv;
-    // set-up: x = M^-1 b, r = r0 = b - A x, p = v = 0 (plain row loop, once per solve)
+    const double* __restrict__ x0l = c.x0l;
+    int bar = 0;
+    // Learned first iterate (no counterpart in the reference): the start is x0 = a M^-1 b + c xl,
+    // (a, c) minimising ||b - A x0||_2 over that plane, used only when its residual is below
+    // 0.99 of the plain start's ||b - A M^-1 b||; otherwise the plain start x0 = M^-1 b stands.
+    // A pass forms u = A M^-1 b and w = A xl (kept in br and bq) and the five inner products.
+    bool use_l = false;
+    double la = 1.0, lc = 0.0;
+    if (x0l) {
+        double a5[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, t5[5];
+        for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
+            const int j = x / nx, i = x - j * nx;
+            const Nbr nb = neighbours(c.g, i, j, x);
+            const double u = spmv_row(c, nb, x, [&](int q) { return dinv[q] * (-c.G[q]) + cb; });
+            const double w = spmv_row(c, nb, x, [&](int q) { return x0l[q]; });
+            const double b = -c.G[x];
+            br[x] = u;
+            bq[x] = w;
+            a5[0] += b * u;
+            a5[1] += u * u;
+            a5[2] += b * w;
+            a5[3] += u * w;
+            a5[4] += w * w;
+        }
+        if (!sync_fold<5>(a5, slot(bar++), G, gb, epoch, t5)) goto timeout;
+        const double bu = t5[0], uu = t5[1], bw = t5[2], uw = t5[3], ww = t5[4];
+        const double det = uu * ww - uw * uw;
+        if (isfinite(det) && det > 1e-12 * uu * ww) {
+            const double a = (bu * ww - bw * uw) / det, cl = (bw * uu - bu * uw) / det;
+            // squared residuals: the plane's minimum and the plain start's
+            const double r_l = ns.bb - (a * bu + cl * bw), r_p = ns.bb - 2.0 * bu + uu;
+            if (isfinite(a) && isfinite(cl) && r_l < 0.99 * r_p) {
+                use_l = true;
+                la = a;
+                lc = cl;
+            }
+        }
+    }
+    {
+    // set-up: x = x0, r = r0 = b - A x, p = v = 0 (plain row loop, once per solve)
     double a4[4] = {0.0, 0.0, 0.0, 0.0}, t4[4];
     for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
         const int j = x / nx, i = x - j * nx;
-        const Nbr nb = neighbours(c.g, i, j, x);
         auto xv = [&](int q) { return dinv[q] * (-c.G[q]) + cb; };
-        const double Ax = spmv_row(c, nb, x, xv);
-        const double r = -c.G[x] - Ax;
-        dP[x] = xv(x);
+        double r;
+        if (!x0l) {
+            const Nbr nb = neighbours(c.g, i, j, x);
+            const double Ax = spmv_row(c, nb, x, xv);
+            r = -c.G[x] - Ax;
+            dP[x] = xv(x);
+        } else if (!use_l) {
+            r = -c.G[x] - br[x];
+            dP[x] = xv(x);
+        } else {
+            r = -c.G[x] - la * br[x] - lc * bq[x];
+            dP[x] = la * xv(x) + lc * x0l[x];
+        }
         br[x] = r;
         c.br0[x] = r;
         c.bp[x] = 0.0;
@@ -1130,14 +1179,14 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
         a4[2] += r;
         a4[3] += A1[x];
     }
-    if (!sync_fold<4>(a4, slot(0), G, gb, epoch, t4)) goto timeout;
+    if (!sync_fold<4>(a4, slot(bar++), G, gb, epoch, t4)) goto timeout;
     {
         double rho = 1.0, alpha = 1.0, omega = 1.0, cc = 0.0, cs = 0.0, ss = 0.0, ts = 0.0, tt = 0.0;
         const double bn = sqrt(ns.bb) + 1e-300;
         double rr = t4[0], r0r = t4[0], sr = t4[2];
         const double r0A1 = t4[1], sA1 = t4[3];
         int status = ns.fail ? BICG_FAIL : (sqrt(rr) <= tol * bn ? BICG_CONV : (r0r == 0 ? BICG_FAIL : BICG_RUNNING));
-        int iters = 0, parity = 0, bar = 1;
+        int iters = 0, parity = 0;
         double a3[3], t3[3];
         while (status == BICG_RUNNING) {
             const double* p_old = parity ? c.tcp : c.bp;
@@ -1260,9 +1309,10 @@ __global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
             BicgScalars& B = *c.bs_;
             B.rho = rho; B.alpha = alpha; B.omega = omega; B.bn = bn; B.Einv = Einv; B.cb = cb;
             B.r0A1 = r0A1; B.cc = cc; B.cs = cs; B.rr = rr; B.r0r = r0r; B.ts = ts; B.tt = tt; B.ss = ss;
-            B.tol = tol; B.maxit = maxit; B.iters = iters; B.status = status;
+            B.tol = tol; B.maxit = maxit; B.iters = iters; B.status = status; B.x0_learned = use_l ? 1 : 0;
         }
         return;
+    }
     }
 timeout:
     if (threadIdx.x == 0) c.bs_->status = BICG_TIMEOUT;
@@ -1296,38 +1346,49 @@ int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int 
 }
 
 // ============================================================ learned warm start (no counterpart in the reference)
-// Feature row of cell (i, j): for each field f of (rho, rho u, rho v, alpha1, E*, P)
-// taken from the explicit predictor X* (boundary-mapped like every stencil read)
-// and the stage's starting pressure (through M_P): the centre value normalised as
-// (v - mean_f) / std_f, then the 8 neighbours (rows below, same row, above; west
-// to east) as differences to the centre over dstd_f.  54 values, padded to 64, BF16.
+// Feature row of cell (i, j): for each field f of (rho, rho u, rho v, alpha1, E*, P, R)
+// -- the first five from the explicit predictor X* (boundary-mapped like every
+// stencil read), P the stage's starting pressure and R the pressure rate of the
+// last converged stage (both through M_P; R = 0 before the first) -- the centre
+// value normalised as (v - mean_f) / std_f, then the 8 neighbours (rows below,
+// same row, above; west to east) as differences to the centre over dstd_f.
+// 63 values, padded to 64, BF16.
+constexpr double FEAT_CLAMP = 1024.0;
 __global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X) {
     const Geom& g = c.g;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const int i = x % g.nx, j = x / g.nx;
-        double v[9][6];
+        double v[9][NFIELD];
         int k = 0;
         for (int dj = -1; dj <= 1; dj++)
             for (int di = -1; di <= 1; di++) {
                 double q[NV];
                 xs_at(c, i + di, j + dj, q);
                 double* f = v[(dj == 0 && di == 0) ? 0 : ++k];
+                const int m = mp_index(g, i + di, j + dj);
                 f[0] = q[IM1] + q[IM2];
                 f[1] = q[IMU];
                 f[2] = q[IMV];
                 f[3] = q[IA1];
                 f[4] = q[IEN];
-                f[5] = c.P[mp_index(g, i + di, j + dj)];
+                f[5] = c.P[m];
+                f[6] = c.Prate ? c.Prate[m] : 0.0;
             }
+        // normalised values are clamped to +-FEAT_CLAMP (a field that was constant in the pilot
+        // run has a tiny scale), and a non-finite value reads as 0
+        auto fb = [](double z) {
+            z = z == z ? fmin(fmax(z, -FEAT_CLAMP), FEAT_CLAMP) : 0.0;
+            return __float2bfloat16_rn((float)z);
+        };
         __align__(16) __nv_bfloat16 row[64];
 #pragma unroll
-        for (int f = 0; f < 6; f++) {
-            row[f * 9] = __float2bfloat16_rn((float)((v[0][f] - nm.mean[f]) * nm.istd[f]));
+        for (int f = 0; f < NFIELD; f++) {
+            row[f * 9] = fb((v[0][f] - nm.mean[f]) * nm.istd[f]);
 #pragma unroll
-            for (int m = 1; m < 9; m++) row[f * 9 + m] = __float2bfloat16_rn((float)((v[m][f] - v[0][f]) * nm.idstd[f]));
+            for (int m = 1; m < 9; m++) row[f * 9 + m] = fb((v[m][f] - v[0][f]) * nm.idstd[f]);
         }
 #pragma unroll
-        for (int m = 54; m < 64; m++) row[m] = __float2bfloat16_rn(0.0f);
+        for (int m = 9 * NFIELD; m < 64; m++) row[m] = __float2bfloat16_rn(0.0f);
         uint4* dst = (uint4*)(X + (size_t)x * 64);
 #pragma unroll
         for (int q = 0; q < 8; q++) dst[q] = ((const uint4*)row)[q];
@@ -1338,24 +1399,31 @@ void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void*
     k_features<<<blocks_for(c.n), TPB, 0, st>>>(c, nm, (__nv_bfloat16*)X);
     count(c, 1);
 }
-// Step towards the learned guess: the network predicts the stage's pressure rate
-// (P_converged - P_start) / tau in units of tscale, so dP = y * tscale * tau.
+// Step towards the learned guess: the network predicts how far the stage's pressure
+// rate departs from the last stage's, in units of tscale, so the guess extrapolates
+// P_start + sdt (R + y tscale): dP = sdt (R + y tscale).
 __global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale) {
-    const double f = tscale * c.adt;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) c.dP[x] = (double)y[x] * f;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+        const double r = c.Prate ? c.Prate[x] : 0.0;
+        c.dP[x] = c.sdt * (r + (double)y[x] * tscale);
+    }
 }
 void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale) {
     k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale);
     count(c, 1);
 }
-// Training target of the stage: (P_converged - P_start) / (tau * tscale).
-__global__ void k_target(Ctx c, const double* __restrict__ P0, double itscale, float* __restrict__ t) {
-    const double f = itscale / c.adt;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x)
-        t[x] = (float)((c.P[x] - P0[x]) * f);
+// After a converged stage: the new rate R' = (P_converged - P_start) / sdt, the training
+// target (R' - R) / tscale (when t is not null), and R = R'.
+__global__ void k_rate(Ctx c, const double* __restrict__ P0, double itscale, float* __restrict__ t) {
+    const double idt = 1.0 / c.sdt;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+        const double r = (c.P[x] - P0[x]) * idt;
+        if (t) t[x] = (float)((r - c.Prate[x]) * itscale);
+        c.Prate[x] = r;
+    }
 }
-void launch_target(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t) {
-    k_target<<<blocks_for(c.n), TPB, 0, st>>>(c, P0, itscale, t);
+void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t) {
+    k_rate<<<blocks_for(c.n), TPB, 0, st>>>(c, P0, itscale, t);
     count(c, 1);
 }
 

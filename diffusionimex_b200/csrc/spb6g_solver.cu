@@ -7,6 +7,7 @@
 // criterion, BiCGStab status), through one pinned record per sync point.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -70,7 +71,12 @@ struct spb6g_solver {
     FeatureNorm norm{};                 // feature normalisation and target scale
     void* featbuf = nullptr;            // n x 64 BF16 feature rows of the current stage
     float* ybuf = nullptr;              // network output per cell
-    double* Pstart = nullptr;           // stage's starting pressure (training targets)
+    double* Pstart = nullptr;           // stage's starting pressure (pressure rate, training targets)
+    double* Prate = nullptr;            // pressure rate of the last converged stage (a feature and the extrapolation)
+    double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
+    int warm_mode = 3;                  // 1: learned Newton start, 2: learned first BiCGStab iterate, 3: both
+    double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
+    int attempt_stage = -1;             // stage-level API: the last stage of the attempt that converged (-1: none)
     void* rows_cur = nullptr;           // where this stage's feature rows were written
     void* dumpX = nullptr;              // caller's buffers for (feature row, target) pairs
     float* dumpT = nullptr;
@@ -85,6 +91,7 @@ struct spb6g_solver {
     int prec = 16;
     double M0[3] = {0, 0, 0};           // conserved totals at the start of the run (:1251)
     std::vector<double> host_U;         // AoS staging of the state for the writers
+    int verbose = 0;                    // SPB6G_VERBOSE >= 3: one line per Newton iteration (VERBOSE, :810)
 };
 
 namespace {
@@ -282,24 +289,37 @@ int newton(spb6g_solver* s, double& resfinal) {
     if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
     if (s->pin->ns.fail & 1) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
     double res = s->pin->ns.res;
+    // learned prediction dP = sdt (R + MLP(features) tscale) of the stage's pressure change
+    bool have_pred = false, chosen = false;
     if (s->warm) {
-        // learned guess P + dP, dP = MLP(features) * tscale; it replaces the plain guess only
-        // when its residual norm is smaller (and every closure of it succeeded)
         tbegin(s, TG_WARM);
         if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
         launch_guess(c, s->st, s->ybuf, s->norm.tscale);
-        launch_residual(c, s->st, 1, 1.0);
-        tend_(s, TG_WARM);
-        if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
-        if (!s->pin->ns.fail && s->pin->ns.res < res) {
-            std::swap(c.P, c.Pn);
-            std::swap(c.G, c.Gn);
-            std::swap(c.sc, c.scn);
-            res = s->pin->ns.res;
-            s->stats.learned++;
+        have_pred = true;
+        if (s->warm_mode & 1) {
+            // Newton starts from P + dP only when its residual norm is below the plain guess's (and
+            // every closure of it succeeded)
+            launch_residual(c, s->st, 1, 1.0);
+            tend_(s, TG_WARM);
+            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+            if (s->verbose >= 3) fprintf(stderr, "    learned guess res %.3e, plain guess res %.3e\n", s->pin->ns.res, res);
+            if (!s->pin->ns.fail && s->pin->ns.res < res) {
+                std::swap(c.P, c.Pn);
+                std::swap(c.G, c.Gn);
+                std::swap(c.sc, c.scn);
+                res = s->pin->ns.res;
+                s->stats.learned++;
+                chosen = true;
+            }
+            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+        } else {
+            tend_(s, TG_WARM);
         }
-        if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+        // from the plain start, the prediction is the first BiCGStab iterate's candidate
+        if (!chosen && (s->warm_mode & 2) && !tri && s->bicg_G > 0)
+            CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
     }
+    const bool x0_pending = have_pred && !chosen && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
     // jreuse (modified Newton, :826-830, :887): the Jacobian is rebuilt at the first iteration, after
     // a damped step or a contraction above 0.25 (fresh_ok :797), and when the kept one lets the
     // line search fail; the step criterion meanwhile uses the scales of the last build
@@ -308,6 +328,7 @@ int newton(spb6g_solver* s, double& resfinal) {
     bool fresh = false;
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
+        if (s->verbose >= 3) fprintf(stderr, "    newton it %d res %.3e\n", it, res);
         if (res < tol) return SPB6G_OK;
         const bool build = !jreuse || it == 0 || !(lamprev == 1.0 && ratio <= 0.25);
         tbegin(s, TG_JACOBIAN);
@@ -334,8 +355,11 @@ int newton(spb6g_solver* s, double& resfinal) {
             if (s->pin->ns.fail) { tend_(s, TG_LINEAR); return SPB6G_NEWTON_FAIL; }
             if (s->bicg_G > 0) {  // the whole solve in one persistent launch
                 CK(cudaMemsetAsync(c.gbar, 0, sizeof(GridBarrier), s->st));
-                if (launch_bicg_solve(c, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter, s->bicg_G) != 0) return SPB6G_CUDA_ERROR;
+                Ctx cl = c;
+                cl.x0l = (x0_pending && it == 0) ? s->x0buf : nullptr;
+                if (launch_bicg_solve(cl, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter, s->bicg_G) != 0) return SPB6G_CUDA_ERROR;
                 if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
+                if (cl.x0l && s->pin->bs.x0_learned) s->stats.learned_x0++;
                 if (s->pin->bs.status == BICG_TIMEOUT) {  // a grid barrier gave up (blocks not co-resident)
                     fprintf(stderr, "spb6g: BiCGStab grid barrier timed out\n");
                     tend_(s, TG_LINEAR);
@@ -373,6 +397,9 @@ int newton(spb6g_solver* s, double& resfinal) {
         launch_residual(c, s->st, 1, 1.0);
         tend_(s, TG_RESIDUAL);
         if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
+        if (s->verbose >= 3)
+            fprintf(stderr, "      linear its %d  step %.3e  trial res %.3e%s\n", tri ? 0 : s->pin->bs.iters, s->pin->ns.sn,
+                    s->pin->ns.res, s->pin->ns.fail ? " (closure failed)" : "");
         if (s->pin->ns.sn < tol) {
             launch_apply_step(c, s->st);
             s->stats.newton_it++;
@@ -409,6 +436,7 @@ int newton(spb6g_solver* s, double& resfinal) {
         }
         ratio = res / res0;
         lamprev = lam;
+        if (s->verbose >= 3) fprintf(stderr, "      line search lam %.4g res %.3e%s\n", lam, res, acc ? "" : " (not accepted)");
         if (!acc) {  // round-off floor acceptance (:890-899)
             resfinal = res;
             if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -428,18 +456,27 @@ int newton(spb6g_solver* s, double& resfinal) {
 }
 
 // One stage: combination, explicit predictor, stage data, Newton, final state and H_s.
-int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double dt) {
+// Ae_row[r], Ai_row[r] (r < rks) combine the earlier stages; Ai_row[rks] * dt is the stage's
+// implicit step adt (main :1341-1350).
+int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_row, double dt) {
     Ctx& c = s->c;
     tbegin(s, TG_EXPLICIT);
     for (int k = 0; k < NV; k++) c.Un.v[k] = s->U[k];
     c.Hprev = s->Hs;
     c.nH = rks;
     for (int r = 0; r < 2; r++) {  // Ae[s][r] * dt and Ai[s][r] * dt, as main forms them (:1346-1347)
-        c.ce[r] = r < rks ? Ae[rks][r] * dt : 0.0;
-        c.ci[r] = r < rks ? Ai[rks][r] * dt : 0.0;
+        c.ce[r] = r < rks ? Ae_row[r] * dt : 0.0;
+        c.ci[r] = r < rks ? Ai_row[r] * dt : 0.0;
     }
-    c.adt = Ai[rks][rks] * dt;
+    c.adt = Ai_row[rks] * dt;
     c.tau = c.adt;
+    {  // time span of the stage, from the implicit tableau's row sums (the stage times c_s)
+        double cs = 0;
+        for (int r = 0; r <= rks; r++) cs += Ai_row[r];
+        const double cp = rks > 0 ? s->stage_c : 0.0;
+        c.sdt = (cs - cp) * dt > 0.05 * c.adt ? (cs - cp) * dt : c.adt;
+        s->stage_c = cs;
+    }
     c.rx = c.tau / s->g.dx;
     c.ry = c.tau / s->g.dy;
     c.H = s->Hs + (size_t)rks * NV * s->n;
@@ -449,20 +486,25 @@ int run_stage(spb6g_solver* s, int rks, double Ae[3][3], double Ai[3][3], double
     // warm-start features of the stage (X* and the starting pressure), into the caller's
     // dump buffer when one has room, else into the solver's own rows
     s->dump_stage = s->dumpX && s->dump_count + s->n <= s->dump_cap;
+    // the pressure rate is tracked once a feature normalisation has been set (a feature, and the
+    // extrapolation), so that it stays current on steps without a dump
+    const bool track = s->Prate != nullptr;
+    c.Prate = track ? s->Prate : nullptr;
+    c.x0l = nullptr;
     if (s->warm || s->dump_stage) {
         tbegin(s, TG_WARM);
         s->rows_cur = s->dump_stage ? (void*)((char*)s->dumpX + (size_t)s->dump_count * 128) : s->featbuf;
         launch_features(c, s->st, s->norm, s->rows_cur);
-        if (s->dump_stage) CK(cudaMemcpyAsync(s->Pstart, c.P, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
         tend_(s, TG_WARM);
     }
+    if (track) CK(cudaMemcpyAsync(s->Pstart, c.P, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
     prep_and_shock(s);
     double res = 0;
     const int rc = newton(s, res);
     if (rc != SPB6G_OK) return rc;
-    if (s->dump_stage) {  // training pair: (features, (P_converged - P_start) / tscale)
-        launch_target(c, s->st, s->Pstart, 1.0 / s->norm.tscale, s->dumpT + s->dump_count);
-        s->dump_count += s->n;
+    if (track) {  // the new pressure rate, and the training pair (features, (R' - R) / tscale)
+        launch_rate(c, s->st, s->Pstart, 1.0 / s->norm.tscale, s->dump_stage ? s->dumpT + s->dump_count : nullptr);
+        if (s->dump_stage) s->dump_count += s->n;
     }
     if (res > s->stats.maxres) s->stats.maxres = res;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -516,7 +558,7 @@ int do_step(spb6g_solver* s) {
         if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
         bool ok = true;
         for (int rks = 0; rks < rk && ok; rks++) {
-            rc = run_stage(s, rks, Ae, Ai, s->dt);
+            rc = run_stage(s, rks, Ae[rks], Ai[rks], s->dt);
             if (rc == SPB6G_CUDA_ERROR) return rc;
             ok = rc == SPB6G_OK;
         }
@@ -596,6 +638,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     spb6g_solver* s = new (std::nothrow) spb6g_solver();
     if (!s) return SPB6G_BAD_ARG;
     s->cfg = *cfg;
+    if (const char* v = getenv("SPB6G_VERBOSE")) s->verbose = atoi(v);
     phys_from_config(cfg, s->P);
     s->g.nx = cfg->nx; s->g.ny = cfg->ny;
     for (int q = 0; q < 4; q++) { s->g.bcs[q] = cfg->bc[q]; s->g.bcu[q] = cfg->bcu[q]; s->g.bcp[q] = cfg->bcp[q]; }
@@ -678,7 +721,7 @@ int spb6g_create(const spb6g_config* cfg, spb6g_solver** out) {
     c.bs_ = (BicgScalars*)A(sizeof(BicgScalars) / sizeof(double) + 1);
     c.gbar = (GridBarrier*)A(sizeof(GridBarrier) / sizeof(double) + 1);
     if (!(ny == 1 && cfg->bc[0] != SPB6G_BC_PERIODIC)) s->bicg_G = bicg_solve_blocks(cfg->device, (int)n);
-    c.gpart = A(8 * (size_t)(s->bicg_G > 0 ? s->bicg_G : 1));
+    c.gpart = A(2 * PB_SLOT_Q * (size_t)(s->bicg_G > 0 ? s->bicg_G : 1));
     if (ok && cudaMallocHost((void**)&s->pin, sizeof(Pinned)) != cudaSuccess) ok = false;
     if (ok)
         for (int e = 0; e < 2; e++)
@@ -924,6 +967,9 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     c.nH = 0;
     c.ce[0] = c.ce[1] = c.ci[0] = c.ci[1] = 0.0;
     c.adt = Ai[0][0] * dt; c.tau = c.adt; c.rx = c.tau / s->g.dx; c.ry = c.tau / s->g.dy;
+    c.sdt = c.adt;
+    c.x0l = nullptr;
+    c.Prate = nullptr;  // the dumped stage runs from the plain guess
     c.H = s->Hs;
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
     launch_flux(c, s->st);
@@ -949,7 +995,10 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     }
     prep_and_shock(s);
     double res;
+    spb6g_mlp* warm = s->warm;
+    s->warm = nullptr;
     int rc = newton(s, res);
+    s->warm = warm;
     if (rc != SPB6G_OK) return rc;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
     launch_final(c, s->st);
@@ -959,6 +1008,44 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     c.Ust = State{};
     for (int k = 0; k < NV; k++) c.Ust.v[k] = s->Ust[k];
     s->Pmain = c.P;
+    return SPB6G_OK;
+}
+int spb6g_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_row, double dt, spb6g_stats* st) {
+    if (!s || rks < 0 || rks > 2 || !Ai_row || (rks > 0 && !Ae_row) || !(dt > 0) || !std::isfinite(dt) ||
+        !(Ai_row[rks] > 0) || !std::isfinite(Ai_row[rks]))
+        return SPB6G_BAD_ARG;
+    for (int r = 0; r < rks; r++)
+        if (!std::isfinite(Ae_row[r]) || !std::isfinite(Ai_row[r])) return SPB6G_BAD_ARG;
+    // a later stage needs the earlier stages of the same attempt
+    if (rks > 0 && s->attempt_stage != rks - 1) return SPB6G_BAD_ARG;
+    CK(cudaSetDevice(s->cfg.device));
+    s->dt = dt;
+    if (rks == 0) {  // a new attempt: RelaxationActivation (:1333) and Pst = P (:1335)
+        s->attempt_stage = -1;
+        if (s->cfg.relax) {
+            State u;
+            for (int k = 0; k < NV; k++) u.v[k] = s->U[k];
+            launch_relax_activate(s->c, s->st, u);
+        }
+        if (begin_attempt_pressure(s)) return SPB6G_CUDA_ERROR;
+    }
+    const int rc = run_stage(s, rks, Ae_row, Ai_row, dt);
+    s->attempt_stage = rc == SPB6G_OK ? rks : -1;
+    if (st) *st = s->stats;
+    return rc;
+}
+int spb6g_stage_accept(spb6g_solver* s, double dt) {
+    if (!s || !(dt > 0) || !std::isfinite(dt)) return SPB6G_BAD_ARG;
+    if (s->attempt_stage < 0) return SPB6G_BAD_ARG;  // no converged stage to accept
+    for (int k = 0; k < NV; k++) {  // u_con = Ust, P = Pst (:1374); t += dt (:1379)
+        std::swap(s->U[k], s->Ust[k]);
+        s->c.Ust.v[k] = s->Ust[k];
+    }
+    s->Pmain = s->c.P;
+    s->attempt_stage = -1;
+    s->t = s->t + dt;
+    s->dtprev = dt;
+    s->stats.steps++;
     return SPB6G_OK;
 }
 int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double* qph) {
@@ -985,17 +1072,23 @@ int spb6g_stage_data(spb6g_solver* s, double* fx, double* fy, double* kw, double
     return SPB6G_OK;
 }
 
+static int ensure_warm_buffers(spb6g_solver* s);
 int spb6g_set_feature_norm(spb6g_solver* s, const double* norm) {
     if (!s || !norm) return SPB6G_BAD_ARG;
-    for (int f = 0; f < 6; f++) {
-        if (!(norm[6 + f] > 0) || !(norm[12 + f] > 0)) return SPB6G_BAD_ARG;
-        s->norm.mean[f] = norm[f];
-        s->norm.istd[f] = 1.0 / norm[6 + f];
-        s->norm.idstd[f] = 1.0 / norm[12 + f];
+    FeatureNorm nm{};
+    for (int f = 0; f < NFIELD; f++) {
+        if (!std::isfinite(norm[f]) || !(norm[NFIELD + f] > 0) || !(norm[2 * NFIELD + f] > 0)) return SPB6G_BAD_ARG;
+        nm.mean[f] = norm[f];
+        nm.istd[f] = 1.0 / norm[NFIELD + f];
+        nm.idstd[f] = 1.0 / norm[2 * NFIELD + f];
     }
-    if (!(norm[18] > 0)) return SPB6G_BAD_ARG;
-    s->norm.tscale = norm[18];
-    return SPB6G_OK;
+    if (!(norm[3 * NFIELD] > 0) || !std::isfinite(norm[3 * NFIELD])) return SPB6G_BAD_ARG;
+    nm.tscale = norm[3 * NFIELD];
+    s->norm = nm;
+    // the feature rows and the pressure-rate tracking start here, so that R is current at the
+    // first stage that is dumped or warm-started
+    cudaSetDevice(s->cfg.device);
+    return ensure_warm_buffers(s);
 }
 static int ensure_warm_buffers(spb6g_solver* s) {
     if (!s->featbuf) {
@@ -1006,9 +1099,13 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc((void**)&s->ybuf, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(s->ybuf);
     }
-    if (!s->Pstart) {
-        if (cudaMalloc((void**)&s->Pstart, (size_t)s->n * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
-        s->allocs.push_back(s->Pstart);
+    for (double** b : {&s->Pstart, &s->Prate, &s->x0buf}) {
+        if (*b) continue;
+        if (cudaMalloc((void**)b, (size_t)s->n * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(*b);
+        // no rate before the first converged stage
+        if (b == &s->Prate && cudaMemsetAsync(s->Prate, 0, (size_t)s->n * sizeof(double), s->st) != cudaSuccess)
+            return SPB6G_CUDA_ERROR;
     }
     return SPB6G_OK;
 }
@@ -1021,6 +1118,11 @@ int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
         if (rc) return rc;
     }
     s->warm = m;
+    return SPB6G_OK;
+}
+int spb6g_set_warmstart_mode(spb6g_solver* s, int mode) {
+    if (!s || mode < 1 || mode > 3) return SPB6G_BAD_ARG;
+    s->warm_mode = mode;
     return SPB6G_OK;
 }
 int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity) {

@@ -65,7 +65,7 @@ class Stats(ctypes.Structure):
         ("steps", ctypes.c_int64), ("rejects", ctypes.c_int64), ("rk1", ctypes.c_int64), ("stages", ctypes.c_int64),
         ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
         ("learned", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
-        ("p_ref", ctypes.c_double), ("tmax", ctypes.c_double * 2),
+        ("p_ref", ctypes.c_double), ("tmax", ctypes.c_double * 2), ("learned_x0", ctypes.c_int64),
     ]
 
 
@@ -117,6 +117,8 @@ def library() -> ctypes.CDLL:
         "spb6g_region_end": (I, [P, P]),
         "spb6g_kernel_launches": (ctypes.c_int64, [P]),
         "spb6g_stage_data": (I, [P, P, P, P, P]),
+        "spb6g_stage": (I, [P, I, P, P, D, P]),
+        "spb6g_stage_accept": (I, [P, D]),
         "spb6g_caldt_noalloc": (I, [P, P, I, P, P]),
         "spb6g_saturation_table": (I, [P, P, I, P]),
         "spb6g_batch_create": (I, [P, I, P]),
@@ -128,6 +130,7 @@ def library() -> ctypes.CDLL:
         "spb6g_batch_autotune": (I, [P, I, P, P, P]),
         "spb6g_set_feature_norm": (I, [P, P]),
         "spb6g_set_warmstart": (I, [P, P]),
+        "spb6g_set_warmstart_mode": (I, [P, I]),
         "spb6g_set_dump": (I, [P, P, P, ctypes.c_int64]),
         "spb6g_dump_count": (I, [P, P]),
         "spb6g_mlp_create": (I, [I, P]),
@@ -326,6 +329,23 @@ class Solver:
                     "stage_dump")
         return out
 
+    def stage(self, rks: int, Ae_row, Ai_row, dt: float) -> int:
+        """Stage rks of the current attempt (spb6g_stage: TVDReconstruction + Update +
+        PressureSubsystem with Qe, Qs combined from Ae_row, Ai_row and adt = Ai_row[rks] dt).
+        Returns 0 when the stage converged, else the failure status (1 inadmissible, 2 Newton,
+        3 BiCGStab), after which the caller halves dt and starts again at rks = 0, as main()
+        does (:1366-1376); bad arguments and CUDA errors raise."""
+        ae = np.ascontiguousarray(list(Ae_row[:rks]) + [0.0], dtype=np.float64)
+        ai = np.ascontiguousarray(list(Ai_row[:rks + 1]), dtype=np.float64)
+        rc = self.lib.spb6g_stage(self.h, int(rks), _ptr(ae), _ptr(ai), float(dt), None)
+        if rc not in (0, 1, 2, 3):
+            raise SolverError(rc, "spb6g_stage")
+        return rc
+
+    def stage_accept(self, dt: float):
+        """Accept the attempt: the state and the pressure of its last stage become U^n and P (:1374)."""
+        self._check(self.lib.spb6g_stage_accept(self.h, float(dt)), "spb6g_stage_accept")
+
     def stage_data(self) -> dict:
         """Face coefficients, residual scale and shock budget of the last stage."""
         nx, ny, n = self.nx, self.ny, self.nx * self.ny
@@ -384,15 +404,24 @@ class Solver:
         return ms.value
 
     # ---- learned warm start (no counterpart in the reference)
+    NORM_LEN = 22
+
     def set_feature_norm(self, norm):
-        """19 values: mean[6], std[6] of the centre values, std[6] of the neighbour differences of
-        (rho, rho u, rho v, alpha1, E*, P - P_REF), then the target scale."""
-        a = (ctypes.c_double * 19)(*[float(v) for v in norm])
+        """22 values: mean[7], std[7] of the centre values, std[7] of the neighbour differences of
+        (rho, rho u, rho v, alpha1, E*, P - P_REF, R), R the last converged stage's pressure rate,
+        then the target scale.  Setting it starts the tracking of R."""
+        if len(norm) != self.NORM_LEN:
+            raise ValueError(f"feature normalisation has {self.NORM_LEN} values, got {len(norm)}")
+        a = (ctypes.c_double * self.NORM_LEN)(*[float(v) for v in norm])
         self._check(self.lib.spb6g_set_feature_norm(self.h, a), "spb6g_set_feature_norm")
 
-    def set_warmstart(self, mlp):
+    def set_warmstart(self, mlp, mode: int = 3):
+        """mode 1: learned Newton start (when its residual is below the plain guess's); 2: learned
+        first BiCGStab iterate from the plain start; 3: both."""
         self._warm = mlp
         self._check(self.lib.spb6g_set_warmstart(self.h, mlp.handle if mlp is not None else None), "spb6g_set_warmstart")
+        if mlp is not None:
+            self._check(self.lib.spb6g_set_warmstart_mode(self.h, int(mode)), "spb6g_set_warmstart_mode")
 
     def set_dump(self, X=None, t=None):
         """X: (cap, 64) torch.bfloat16, t: (cap,) torch.float32 on the device, or None to stop."""

@@ -1,7 +1,7 @@
 """Learned warm start for the implicit-pressure Newton (no counterpart in the reference).
 
 `MLP` wraps the tensor-core network of libspb6g (spb6g_mlp_*): 64 BF16 inputs
-per row (54 features used), three hidden layers of 64 with SiLU, one output;
+per row (the solver's features use 63), three hidden layers of 64 with SiLU, one output;
 FP32 master weights trained with Adam on the device.
 """
 from __future__ import annotations

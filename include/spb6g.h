@@ -111,6 +111,7 @@ typedef struct {
     int64_t learned;                /* stages whose Newton started from the learned guess */
     double t, dt, maxres, p_ref;
     double tmax[2];                 /* max phase temperatures of the stages' final states (st_Tmax :96, :1070) */
+    int64_t learned_x0;             /* BiCGStab solves that started from the learned first iterate */
 } spb6g_stats;
 
 typedef struct spb6g_solver spb6g_solver;
@@ -156,6 +157,20 @@ int spb6g_advance(spb6g_solver* s, int nsteps);
  * ube_y (nx*(ny+1)), phi_x, phi_y (nx*ny). */
 int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double* ube_x, double* ube_y,
                      double* phi_x, double* phi_y);
+
+/* One stage of any tableau on the device state, the three calls of main()'s stage loop
+ * (:1341-1366): Qe = U^n + sum_{r<rks} Ae_row[r] dt H_r, Qs = U^n + sum_{r<rks} Ai_row[r] dt H_r,
+ * TVDReconstruction + Update (:369, :264) and PressureSubsystem (:908) with adt = Ai_row[rks] dt,
+ * then H_rks = (U_s - Qs) / adt (:1360).  U^n is the handle's state, which stages do not change.
+ * rks = 0 begins an attempt: RelaxationActivation (:1333, relax > 0) and Pst = P (:1335); stage
+ * rks > 0 needs stage rks - 1 of the same attempt to have converged (else SPB6G_BAD_ARG).
+ * Ae_row needs rks entries, Ai_row rks + 1.  A failed stage returns its status (the caller halves
+ * dt and starts a new attempt at rks = 0); *st (if not NULL) receives the handle's statistics. */
+int spb6g_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_row, double dt, spb6g_stats* st);
+/* Accepts the attempt whose last stage converged: u_con = U_s, P = Pst (:1374), and advances the
+ * handle's time by dt (t, the last accepted step, the step count; :1379).  SPB6G_BAD_ARG when no
+ * stage of the current attempt has converged. */
+int spb6g_stage_accept(spb6g_solver* s, double dt);
 
 /* Stage data of the last stage (StageData, :591-608): x-face coefficients ubs, kp, wL, pv
  * (4 blocks of (nx+1)*ny, faces i-1/2 .. nx-1/2), y-face coefficients (4 blocks of nx*(ny+1)),
@@ -270,16 +285,26 @@ int spb6g_mlp_train_async(spb6g_mlp* m, const void* X_dev, const float* target_d
  * tensor-core wait of any earlier call as an error). */
 int spb6g_mlp_last_loss(spb6g_mlp* m, void* stream, float* loss_sum);
 
-/* Warm start on the solver (no counterpart in the reference).  norm: 19 doubles:
- * mean[6], std[6] of the centre values and std[6] of the neighbour differences of
- * the fields (rho, rho u, rho v, alpha1, E*, P - P_REF), then the target scale. */
+/* Warm start on the solver (no counterpart in the reference).  The features of a cell are
+ * the 3x3 stencils of 7 fields: rho, rho u, rho v, alpha1, E* of the explicit predictor, the
+ * stage's starting pressure P - P_REF, and R, the pressure rate (P_converged - P_start) / dts
+ * of the last converged stage (dts = the stage's time span, (c_s - c_{s-1}) dt from the
+ * implicit tableau's row sums; R = 0 before the first stage) -- 63 of the 64 columns.
+ * norm: 22 doubles: mean[7], std[7] of the centre values and std[7] of the neighbour
+ * differences of the 7 fields, then the target scale.  Setting it also starts tracking R. */
 int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
-/* m != NULL: every stage also evaluates the residual at P + tau * MLP(features) * scale
- * (tau = the stage's implicit step) and starts Newton from it when its residual norm is
- * below the plain guess's; NULL: off. */
+/* m != NULL: every stage predicts its pressure change dP = dts (R + MLP(features) scale).
+ * Mode bit 1 (spb6g_set_warmstart_mode; 3 by default): Newton starts from P + dP when the
+ * residual norm there is below the plain guess's (the previous stage's pressure), else from
+ * the plain guess.  Mode bit 2: from the plain guess, the first BiCGStab solve of the stage
+ * starts from x0 = a M^-1 b + c dP, (a, c) minimising ||b - A x0||, when that residual is
+ * below 0.99 of the plain start's (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.
+ * Newton and BiCGStab keep their tolerances.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
+int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
 /* Training data: each stage appends n feature rows (64 BF16 each) to X_dev and n
- * targets (P_converged - P_start) / (tau * scale) to target_dev while capacity allows. */
+ * targets (R' - R) / scale to target_dev while capacity allows (R' the stage's converged
+ * pressure rate, R the last stage's). */
 int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity);
 int spb6g_dump_count(spb6g_solver* s, int64_t* count);
 
