@@ -3,15 +3,20 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Workload (default): water at rest with 8 seeded air bubbles on a 1024 x 1024
-grid, FP64, transmissive, material CFL 0.5, Newton tol 1e-10, BiCGStab tol
-1e-12 -- the plain-method 2D configuration.  A "step" is one time step of the
-solver (explicit predictor + implicit pressure Newton with BiCGStab per stage,
-step-size control, acceptance).  The run takes W untimed steps from t = 0 and
-times the next K steps on the device (CUDA events on the solver's stream,
-max over ranks).  The working set (~1 GB) is far larger than L2.
+Workload (default, lowmach2048): the learned form's configuration -- low-Mach
+water (p 1e5 Pa, a seeded divergence-free velocity field of amplitude 15 m/s)
+with 16 seeded air bubbles on a 2048 x 2048 periodic grid, FP64, material CFL
+0.8, Newton tol 1e-10, BiCGStab tol 1e-10 -- run with the learned Newton start
+(the trained network shipped in diffusionimex_b200/data/) and, over the same
+window, with the plain guess and with the extrapolation alone.  A "step" is one
+time step of the solver (explicit predictor + implicit pressure Newton with
+BiCGStab per stage, step-size control, acceptance).  Each run takes W untimed
+steps from t = 0 and times the next K steps on the device (CUDA events on the
+solver's stream, max over ranks).  The working set (~4 GB) is far larger than L2.
 
-metric: cell-updates/s = interior cells x accepted steps / device time.
+metric: cell-updates/s = interior cells x accepted steps / device time (the
+learned run), with BiCGStab iterations per step and Newton iterations per stage
+of both guesses, their ratios and L1(p) between the runs.
 
 Multi-GPU: the measured path solves one grid on one GPU, so N > 1 runs N independent
 replicas ("scaling": "weak"); value is the total over ranks.
@@ -50,6 +55,12 @@ ALG_BYTES = {
 }
 
 
+# SURVEY-defined algorithmic bytes (compulsory FP64 traffic): the BiCGStab iteration per row (2 x 40 B of
+# matrix rows, 24 vector streams x 8 B) and the fused flux kernel per cell, stage 1 / later stages
+# (2D: 64 n_in + 8 (8 + 5); 1D: 64 n_in + 8 (8 + 3))
+BICG_BYTES_PER_ROW_ITER = 272
+FLUX_BYTES = {True: (168, 232), False: (152, 216)}
+
 # DRAM read + write per unit from ncu (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
 # on this workload: k_bicg_solve moved 1.93 GB for 11 iterations of 1,048,576 rows
 # (profiles/k_bicg_solve_bubbles1024.md).
@@ -64,8 +75,8 @@ def parse():
     p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="bubbles1024",
-                   help="bubbles1024 (default), bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
+    p.add_argument("--workload", default="lowmach2048",
+                   help="lowmach2048 (default: learned vs plain guess), lowmach2048-plain, bubbles1024, bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
                         "bubbles2048-mixed, shock2048x1024-mixed (precision form), riemann512 (batched form), "
                         "undex361x200 (Mie-Grueneisen phases), bubbles1024-relax (p-pT relaxation), "
                         "<2D workload>-rus0 (grid-wide Rusanov speed), <workload>-jreuse (modified Newton), "
@@ -88,7 +99,13 @@ def make_workload(name: str):
         c = cases.bubble_field(256, seed=0, nbub=8)
     elif name == "tube1000":
         c = cases.water_air_tube(1000)
-    elif name == "lowmach2048":
+    elif name == "lowmach2048":  # the learned form's configuration: learned vs plain Newton start
+        c = cases.lowmach_bubbles(2048, seed=0)
+        c["learned"] = True
+        c["metric"] = "cell-updates/s & BiCGStab iters/step, learned vs plain guess, equal tol, 1 B200"
+        c["workload"] = ("low-Mach water with 16 air bubbles 2D periodic, 2048x2048 cells, material CFL 0.8, "
+                         "Newton tol 1e-10, BiCGStab tol 1e-10; learned Newton start vs the plain guess")
+    elif name == "lowmach2048-plain":
         c = cases.lowmach_bubbles(2048, seed=0)
     elif name == "shock2048x1024":
         c = cases.shock_bubble(2048, 1024)
@@ -490,28 +507,34 @@ def run_reference(args, case, rank: int):
     sample = (f"steps {args.warmup + 1}..{args.warmup + k} from t=0 after {args.warmup} untimed steps"
               + (" (stopped at the time budget)" if k < args.steps else ""))
     line = {
-        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": case.get("metric", "cell-updates/s"), "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus,
         "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * r["wall_s"] / k, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(case, args.workload),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "newton_it": r["newton_it"], "stages": r["stages"],
+        "newton_it": r["newton_it"], "stages": r["stages"], "bicg_it": r["bicg_it"],
+        "bicg_iters_per_step": r["bicg_it"] / max(int(r["steps"]), 1),
+        "guess": "plain (the reference always starts Newton from the previous stage's pressure)",
     }
     print(json.dumps(line))
 
 
-def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
-    import numpy as np
+def timed_window(case: dict, args, local_rank: int, dist, mlp=None, norm=None, zero: bool = False):
+    """W untimed steps from t = 0, then K steps timed on the device (CUDA events on the solver's
+    stream, bracketed by a barrier and a device synchronisation); counts, kernel groups, launches,
+    clocks and the final pressure of the window."""
     import torch
 
     from diffusionimex_b200 import Solver
 
-    n = case["nx"] * case["ny"]
     s = Solver(case, device=local_rank)
-    s.advance(args.warmup)
-    # the restart point of the timed window: the end-to-end run below replays its first steps
-    rp = s.restart_point() if not args.no_e2e else None
+    if mlp is not None:
+        s.set_feature_norm(norm)
+        s.set_warmstart(mlp)
+    if args.warmup > 0:
+        s.advance(args.warmup)
     st0 = s.stats()
     l0 = s.kernel_launches()
     s.timing(True)
@@ -527,84 +550,163 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
     clocks = clk.stop()
     torch.cuda.synchronize()
     st1 = s.stats()
-    launches = s.kernel_launches() - l0
-    groups = s.timing()
+    out = {"ms": ms, "launches": s.kernel_launches() - l0, "groups": s.timing(), "clocks": clocks,
+           "d": {k: st1[k] - st0[k] for k in ("steps", "rejects", "stages", "newton_it", "bicg_it", "learned",
+                                              "learned_x0", "extrapolated")}}
     s.timing(False)
-    ms_max = max_over_ranks(ms, dist, f"cuda:{local_rank}")
+    if case.get("learned"):
+        P, pref = s.pressure()
+        out["p"] = P + pref
+    s.close()
+    return out
+
+
+def counts(r: dict) -> dict:
+    d = r["d"]
+    return {"ms_per_step": r["ms"] / max(d["steps"], 1), "bicg_iters_per_step": d["bicg_it"] / max(d["steps"], 1),
+            "newton_iters_per_stage": d["newton_it"] / max(d["stages"], 1), **d}
+
+
+def rooflines(r: dict, n: int, two_d: bool) -> dict:
+    """Algorithmic-byte rooflines (SURVEY-defined bytes per unit) of the BiCGStab solve, the fused
+    flux kernel and the whole step, from the window's CUDA-event group times and counts."""
+    peak, peak_kind = peaks()
+    g, d = r["groups"], r["d"]
+    out = {}
+    if g.get("linear", (0, 0))[1] > 0 and d["bicg_it"] > 0:
+        units = d["bicg_it"] * n
+        ach = BICG_BYTES_PER_ROW_ITER * units / (g["linear"][0] / 1e3) / 1e9
+        out["bicg"] = {"bound": "hbm", "kernel": KERNEL_OF["linear"], "achieved": ach, "peak": peak, "unit": "GB/s",
+                       "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
+                       "alg_bytes_per_unit": BICG_BYTES_PER_ROW_ITER, "unit_of_work": "row x BiCGStab iteration",
+                       "alg_bytes_per_launch": BICG_BYTES_PER_ROW_ITER * units / g["linear"][1]}
+    if g.get("explicit", (0, 0))[1] > 0:
+        # stage 1 reads U^n only (168 B / cell); a later stage also its earlier derivatives (232 B); the
+        # later stages are the stages beyond one per attempt
+        later = max(d["stages"] - d["steps"] - d["rejects"], 0)
+        first = g["explicit"][1] - later
+        b1, b2 = FLUX_BYTES[two_d]
+        alg = (first * b1 + later * b2) * n
+        ach = alg / (g["explicit"][0] / 1e3) / 1e9
+        out["flux"] = {"bound": "hbm", "kernel": KERNEL_OF["explicit"], "achieved": ach, "peak": peak, "unit": "GB/s",
+                       "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
+                       "alg_bytes_per_cell": [b1, b2], "alg_bytes_per_launch": alg / g["explicit"][1]}
+    # whole step: every group's algorithmic bytes over the whole window's device time
+    tot = 0.0
+    for k, (gms, gcnt) in g.items():
+        if k == "linear":
+            tot += BICG_BYTES_PER_ROW_ITER * d["bicg_it"] * n
+        elif k == "explicit" and "flux" in out:
+            tot += out["flux"]["alg_bytes_per_launch"] * gcnt
+        elif k in ALG_BYTES:
+            tot += ALG_BYTES[k] * gcnt * n
+    ach = tot / (r["ms"] / 1e3) / 1e9
+    out["step"] = {"bound": "hbm", "kernel": "whole step (B_step)", "achieved": ach, "peak": peak, "unit": "GB/s",
+                   "frac": ach / peak, "traffic": None, "peak_source": peak_kind, "alg_bytes_per_step": tot / max(d["steps"], 1)}
+    return out
+
+
+def e2e_run(case: dict, args, local_rank: int, dist, mlp=None, norm=None, ref_counts=None) -> dict:
+    """The same window through the public API with host buffers: a solver replays the W untimed
+    steps, then every timed step uploads the state from pinned host memory, steps and downloads
+    the state (SoA); timed with CUDA events on the solver's stream."""
+    import torch
+
+    from diffusionimex_b200 import Solver
+
+    n = case["nx"] * case["ny"]
+    s = Solver(case, device=local_rank)
+    if mlp is not None:
+        s.set_feature_norm(norm)
+        s.set_warmstart(mlp)
+    if args.warmup > 0:
+        s.advance(args.warmup)
+    host = torch.empty(8 * n, dtype=torch.float64, pin_memory=True)
+    ptr = host.data_ptr()
+    s.download_soa(ptr)
+    st0 = s.stats()
     if dist:
         dist.barrier()
-    steps_done = st1["steps"] - st0["steps"]
-    value = job_value(n, steps_done, world, ms_max)
-
-    # end to end through the public API: the state goes host -> device before every step and
-    # comes back after it (pinned host buffer, SoA layout).  The run replays the timed window's
-    # K steps from its restart point, so it does the same work as the device-timed run (checked
-    # on the step, rejection, Newton and BiCGStab counts) and the two differ by the copies.
-    e2e = None
-    if not args.no_e2e:
-        host = torch.empty(8 * n, dtype=torch.float64, pin_memory=True)
-        ptr = host.data_ptr()
-        s.restore(rp)
+    torch.cuda.synchronize()
+    s.region_begin()
+    for _ in range(args.steps):
+        s.upload_soa(ptr)
+        s.step()
         s.download_soa(ptr)
-        st_e0 = s.stats()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        s.region_begin()
-        for _ in range(args.steps):
-            s.upload_soa(ptr)
-            s.step()
-            s.download_soa(ptr)
-        ems = max_over_ranks(s.region_end(), dist, f"cuda:{local_rank}")
-        st_e1 = s.stats()
-        keys = ("steps", "rejects", "newton_it", "bicg_it")
-        same = all(st_e1[k] - st_e0[k] == st1[k] - st0[k] for k in keys)
-        e2e = {"value": job_value(n, args.steps, world, ems), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": 64 * n, "d2h_bytes_per_step": 64 * n, "steps": args.steps,
-               "steps_replayed": "the timed window's steps, from its restart point", "ms_per_step": ems / args.steps,
-               "same_work_as_timed_run": same}
+    ems = max_over_ranks(s.region_end(), dist, f"cuda:{local_rank}")
+    st1 = s.stats()
+    s.close()
+    same = None
+    if ref_counts is not None:
+        same = all(st1[k] - st0[k] == ref_counts[k] for k in ("steps", "rejects", "newton_it", "bicg_it"))
+    steps = st1["steps"] - st0["steps"]
+    return {"value": n * steps * (int(os.environ.get("WORLD_SIZE", "1"))) / (ems / 1e3), "unit": "cell-updates/s",
+            "h2d_bytes_per_step": 64 * n, "d2h_bytes_per_step": 64 * n, "steps": steps,
+            "ms_per_step": ems / max(steps, 1), "same_work_as_timed_run": same,
+            "path": "Solver.upload_soa / step / download_soa every step (spb6g_upload_state, spb6g_step, "
+                    "spb6g_download_state), pinned host buffer"}
 
-    # roofline of the dominant kernel group
-    peak, peak_kind = peaks()
-    newton_its = st1["newton_it"] - st0["newton_it"]
-    bicg_its = st1["bicg_it"] - st0["bicg_it"]
-    stages = st1["stages"] - st0["stages"]
-    # the HBM roofline is the BiCGStab solve's (the dominant memory-bound kernel); the FD Jacobian,
-    # the residuals and the shock budget are FP64-arithmetic / latency bound (their shares are
-    # in kernel_groups; profiles/ has their FP64-pipe figures)
-    dom = "linear" if "linear" in groups and groups["linear"][1] > 0 else \
-        max((g for g in groups if g in ALG_BYTES), key=lambda g: groups[g][0])
-    gms, gcnt = groups[dom]
-    if dom == "linear":
-        units = bicg_its * n
-    else:
-        units = gcnt * n
-    achieved = ALG_BYTES[dom] * units / (gms / 1e3) / 1e9
-    # DRAM bytes per launch: the ncu-measured bytes per unit, scaled to this run's average launch
-    traffic = DRAM_BYTES[dom] * units / max(gcnt, 1) if dom in DRAM_BYTES and args.workload == "bubbles1024" else None
-    roof = {"bound": "hbm", "kernel": KERNEL_OF[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-            "alg_bytes_per_cell": ALG_BYTES[dom],
-            "alg_bytes_per_launch": ALG_BYTES[dom] * units / max(gcnt, 1)}
-    total_ms = sum(v[0] for v in groups.values())
-    shares = {g: {"ms": round(v[0], 3), "launch_groups": int(v[1]), "share": round(v[0] / ms, 4)} for g, v in groups.items()}
 
+def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
+    n = case["nx"] * case["ny"]
+    two_d = case["ny"] > 1
+    mlp = norm = zero = None
+    if case.get("learned"):
+        from diffusionimex_b200 import learned
+
+        if not os.path.exists(learned.DEFAULT_WEIGHTS):
+            raise SystemExit(f"trained warm-start network missing: {learned.DEFAULT_WEIGHTS}")
+        mlp, norm = learned.load(learned.DEFAULT_WEIGHTS, device=local_rank)
+        zero = learned.zero_network(local_rank)
+    main_r = timed_window(case, args, local_rank, dist, mlp, norm)
+    ms_max = max_over_ranks(main_r["ms"], dist, f"cuda:{local_rank}")
+    d = main_r["d"]
+    value = job_value(n, d["steps"], world, ms_max)
+    extra = {}
+    if case.get("learned"):
+        from diffusionimex_b200 import learned
+
+        plain_r = timed_window(case, args, local_rank, dist)
+        ext_r = timed_window(case, args, local_rank, dist, zero, norm)
+        pc, lc, ec = counts(plain_r), counts(main_r), counts(ext_r)
+        extra = {
+            "learned": lc, "plain": pc, "extrapolation_only": ec,
+            "plain_value": job_value(n, plain_r["d"]["steps"], world,
+                                     max_over_ranks(plain_r["ms"], dist, f"cuda:{local_rank}")),
+            "bicg_ratio_plain_over_learned": pc["bicg_iters_per_step"] / max(lc["bicg_iters_per_step"], 1e-30),
+            "newton_ratio_plain_over_learned": pc["newton_iters_per_stage"] / max(lc["newton_iters_per_stage"], 1e-30),
+            "wall_ratio_plain_over_learned": pc["ms_per_step"] / max(lc["ms_per_step"], 1e-30),
+            "L1_rel_p_learned_vs_plain": learned.l1_rel(main_r["p"], plain_r["p"]),
+            "L1_rel_p_extrapolation_vs_plain": learned.l1_rel(ext_r["p"], plain_r["p"]),
+            "same_steps": plain_r["d"]["steps"] == d["steps"] and plain_r["d"]["rejects"] == d["rejects"],
+            "network": os.path.relpath(learned.DEFAULT_WEIGHTS, ROOT),
+        }
+    e2e = None if args.no_e2e else e2e_run(case, args, local_rank, dist, mlp, norm,
+                                           {k: d[k] for k in ("steps", "rejects", "newton_it", "bicg_it")})
+    roofs = rooflines(main_r, n, two_d)
+    groups = main_r["groups"]
+    shares = {g: {"ms": round(v[0], 3), "launch_groups": int(v[1]), "share": round(v[0] / main_r["ms"], 4)}
+              for g, v in groups.items()}
     if rank == 0:
         line = {
-            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps_done,
-            "warmup": args.warmup, "ms_per_step": ms_max / max(steps_done, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "metric": case.get("metric", "cell-updates/s"), "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": d["steps"], "warmup": args.warmup, "ms_per_step": ms_max / max(d["steps"], 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(case, args.workload),
-            "bicg_iters_per_step": bicg_its / max(steps_done, 1),
-            "newton_iters_per_stage": newton_its / max(stages, 1),
-            "stages": stages, "rejects": st1["rejects"] - st0["rejects"],
-            "roofline": roof, "kernel_groups": shares, "timed_groups_ms": round(total_ms, 3),
-            "gpu_launches": launches, "clocks": clocks, "e2e": e2e,
+            "bicg_iters_per_step": d["bicg_it"] / max(d["steps"], 1),
+            "newton_iters_per_stage": d["newton_it"] / max(d["stages"], 1),
+            "stages": d["stages"], "rejects": d["rejects"], **extra,
+            "roofline": roofs.get("bicg", roofs["step"]), "roofline_flux": roofs.get("flux"),
+            "roofline_step": roofs["step"], "kernel_groups": shares,
+            "timed_groups_ms": round(sum(v[0] for v in groups.values()), 3),
+            "gpu_launches": main_r["launches"], "clocks": main_r["clocks"], "e2e": e2e,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(case)
         print(json.dumps(line))
-    s.close()
+    for m in (mlp, zero):
+        if m is not None:
+            m.close()
 
 
 def main():

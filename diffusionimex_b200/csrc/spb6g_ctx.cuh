@@ -113,6 +113,8 @@ struct Ctx {
     double *tcp, *tdp;
     // learned warm start (no counterpart in the reference)
     double* Prate;     // pressure rate (P_converged - P_start) / sdt of the last converged stage, or null
+    double* Prate2;    // the rate of the stage before it
+    double* rate_sc;   // [0]: sigma, the RMS of Prate over the cells (0 before the first stage)
     const double* x0l; // learned first BiCGStab iterate of this solve, or null (the plain start M^-1 b)
     double sdt;        // time span of the stage: (c_s - c_{s-1}) dt, c the implicit tableau's row sums
     // final state
@@ -135,7 +137,7 @@ SPB6G_DEV size_t ryi(const Geom& g, int i, int j) { return (size_t)i + (size_t)(
 
 // Normalisation of the warm-start features (mean / 1/std of the centre values,
 // 1/std of the neighbour differences, per field) and the target scale.
-constexpr int NFIELD = 7;  // rho, rho u, rho v, alpha1, E*, P, the previous stage's pressure rate
+constexpr int NFIELD = 7;  // rho, rho u, rho v, alpha1, E*, P, the previous stage's pressure rate / sigma
 struct FeatureNorm {
     double mean[NFIELD], istd[NFIELD], idstd[NFIELD];
     double tscale;
@@ -197,7 +199,9 @@ int batch_max_blocks(int threads, int tw, int device);
 // learned warm start: BF16 feature rows (n x 64), dP = sdt (Prate + y tscale), and after a converged
 // stage the training target (if t) and the new pressure rate
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale);
+// base_extrap = 0: dP = sdt (R + sigma y) from the stage's starting pressure; 1: dP = sdt sigma y from
+// the extrapolated pressure P_start + sdt R; y = null: the extrapolation dP = sdt R
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, int base_extrap);
 void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);

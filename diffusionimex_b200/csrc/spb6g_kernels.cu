@@ -1346,16 +1346,23 @@ int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int 
 }
 
 // ============================================================ learned warm start (no counterpart in the reference)
-// Feature row of cell (i, j): for each field f of (rho, rho u, rho v, alpha1, E*, P, R)
+// Scale of the pressure rate: sigma = RMS of R over the cells (rate_sc[0]), or the
+// normalisation's target scale before the first converged stage.
+SPB6G_DEV double rate_scale(const Ctx& c, double tscale) {
+    const double s = c.rate_sc ? c.rate_sc[0] : 0.0;
+    return s > 0.0 ? s : tscale;
+}
+// Feature row of cell (i, j): for each field f of (rho, rho u, rho v, alpha1, E*, P, R / sigma)
 // -- the first five from the explicit predictor X* (boundary-mapped like every
 // stencil read), P the stage's starting pressure and R the pressure rate of the
 // last converged stage (both through M_P; R = 0 before the first) -- the centre
 // value normalised as (v - mean_f) / std_f, then the 8 neighbours (rows below,
-// same row, above; west to east) as differences to the centre over dstd_f.
-// 63 values, padded to 64, BF16.
+// same row, above; west to east) as differences to the centre over dstd_f; the
+// 64th value is the centre's last rate change (R - R2) / sigma.  BF16.
 constexpr double FEAT_CLAMP = 1024.0;
 __global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X) {
     const Geom& g = c.g;
+    const double isig = 1.0 / rate_scale(c, nm.tscale);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const int i = x % g.nx, j = x / g.nx;
         double v[9][NFIELD];
@@ -1372,7 +1379,7 @@ __global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X)
                 f[3] = q[IA1];
                 f[4] = q[IEN];
                 f[5] = c.P[m];
-                f[6] = c.Prate ? c.Prate[m] : 0.0;
+                f[6] = c.Prate ? c.Prate[m] * isig : 0.0;
             }
         // normalised values are clamped to +-FEAT_CLAMP (a field that was constant in the pilot
         // run has a tiny scale), and a non-finite value reads as 0
@@ -1387,8 +1394,7 @@ __global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X)
 #pragma unroll
             for (int m = 1; m < 9; m++) row[f * 9 + m] = fb((v[m][f] - v[0][f]) * nm.idstd[f]);
         }
-#pragma unroll
-        for (int m = 9 * NFIELD; m < 64; m++) row[m] = __float2bfloat16_rn(0.0f);
+        row[63] = fb(c.Prate ? (c.Prate[x] - c.Prate2[x]) * isig : 0.0);
         uint4* dst = (uint4*)(X + (size_t)x * 64);
 #pragma unroll
         for (int q = 0; q < 8; q++) dst[q] = ((const uint4*)row)[q];
@@ -1399,31 +1405,44 @@ void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void*
     k_features<<<blocks_for(c.n), TPB, 0, st>>>(c, nm, (__nv_bfloat16*)X);
     count(c, 1);
 }
-// Step towards the learned guess: the network predicts how far the stage's pressure
-// rate departs from the last stage's, in units of tscale, so the guess extrapolates
-// P_start + sdt (R + y tscale): dP = sdt (R + y tscale).
-__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale) {
+// Step towards a predicted pressure.  The network predicts how far the stage's pressure
+// rate departs from the last stage's, in units of sigma: the learned guess is
+// P_start + sdt (R + sigma y), the extrapolation (y = 0) P_start + sdt R.
+__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale, int base_extrap) {
+    const double sig = rate_scale(c, tscale);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double r = c.Prate ? c.Prate[x] : 0.0;
-        c.dP[x] = c.sdt * (r + (double)y[x] * tscale);
+        const double d = y ? (double)y[x] * sig : 0.0;
+        c.dP[x] = c.sdt * (base_extrap ? d : r + d);
     }
 }
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale) {
-    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale);
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, int base_extrap) {
+    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, base_extrap);
     count(c, 1);
 }
 // After a converged stage: the new rate R' = (P_converged - P_start) / sdt, the training
-// target (R' - R) / tscale (when t is not null), and R = R'.
-__global__ void k_rate(Ctx c, const double* __restrict__ P0, double itscale, float* __restrict__ t) {
+// target (R' - R) / sigma (when t is not null), R2 = R, R = R', and sigma' = RMS of R'
+// (folded by the last block, after every block has read sigma).
+__global__ void __launch_bounds__(TPB) k_rate(Ctx c, const double* __restrict__ P0, double tscale, float* __restrict__ t) {
     const double idt = 1.0 / c.sdt;
+    const double isig = 1.0 / rate_scale(c, tscale);
+    double acc[1] = {0.0};
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double r = (c.P[x] - P0[x]) * idt;
-        if (t) t[x] = (float)((r - c.Prate[x]) * itscale);
+        const double r0 = c.Prate[x];
+        if (t) t[x] = (float)((r - r0) * isig);
+        c.Prate2[x] = r0;
         c.Prate[x] = r;
+        acc[0] += r * r;
+    }
+    double tot[1];
+    if (grid_fold<RedSum, 1>(acc, c.partials, &c.counters[13], tot) && threadIdx.x == 0) {
+        const double s = sqrt(tot[0] / c.n);
+        c.rate_sc[0] = isfinite(s) ? s : 0.0;
     }
 }
-void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t) {
-    k_rate<<<blocks_for(c.n), TPB, 0, st>>>(c, P0, itscale, t);
+void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double tscale, float* t) {
+    k_rate<<<red_blocks(c.n, TPB), TPB, 0, st>>>(c, P0, tscale, t);
     count(c, 1);
 }
 

@@ -73,6 +73,9 @@ struct spb6g_solver {
     float* ybuf = nullptr;              // network output per cell
     double* Pstart = nullptr;           // stage's starting pressure (pressure rate, training targets)
     double* Prate = nullptr;            // pressure rate of the last converged stage (a feature and the extrapolation)
+    double* Prate2 = nullptr;           // the rate of the stage before it
+    double* rate_sc = nullptr;          // RMS of Prate (device scalar)
+    bool rate_ready = false;            // a stage has converged since the tracking began (R exists)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
     int warm_mode = 3;                  // 1: learned Newton start, 2: learned first BiCGStab iterate, 3: both
     double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
@@ -289,37 +292,57 @@ int newton(spb6g_solver* s, double& resfinal) {
     if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
     if (s->pin->ns.fail & 1) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
     double res = s->pin->ns.res;
-    // learned prediction dP = sdt (R + MLP(features) tscale) of the stage's pressure change
+    const int64_t learned0 = s->stats.learned;
+    bool x0_pending = false;
+    // learned prediction of the stage's pressure: P_start + sdt (R + sigma MLP(features))
     bool have_pred = false, chosen = false;
-    if (s->warm) {
+    if (s->warm && s->rate_ready) {
         tbegin(s, TG_WARM);
         if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
-        launch_guess(c, s->st, s->ybuf, s->norm.tscale);
         have_pred = true;
+        int base_extrap = 0;
         if (s->warm_mode & 1) {
-            // Newton starts from P + dP only when its residual norm is below the plain guess's (and
-            // every closure of it succeeded)
-            launch_residual(c, s->st, 1, 1.0);
-            tend_(s, TG_WARM);
-            if (sync_read(s, false)) return SPB6G_CUDA_ERROR;
-            if (s->verbose >= 3) fprintf(stderr, "    learned guess res %.3e, plain guess res %.3e\n", s->pin->ns.res, res);
-            if (!s->pin->ns.fail && s->pin->ns.res < res) {
-                std::swap(c.P, c.Pn);
-                std::swap(c.G, c.Gn);
-                std::swap(c.sc, c.scn);
-                res = s->pin->ns.res;
+            // Newton starts from the guess of smallest residual norm (every closure succeeding):
+            // the plain guess, the extrapolation P_start + sdt R (the network's y = 0), then the
+            // network's guess, each candidate tried against the best so far
+            auto try_guess = [&](const char* what) -> int {
+                launch_residual(c, s->st, 1, 1.0);
+                if (sync_read(s, false)) return -1;
+                if (s->verbose >= 3) fprintf(stderr, "    %s guess res %.3e, best so far %.3e\n", what, s->pin->ns.res, res);
+                const int better = !s->pin->ns.fail && s->pin->ns.res < res;
+                if (better) {
+                    std::swap(c.P, c.Pn);
+                    std::swap(c.G, c.Gn);
+                    std::swap(c.sc, c.scn);
+                    res = s->pin->ns.res;
+                }
+                if (reset_fail(s)) return -1;
+                return better;
+            };
+            launch_guess(c, s->st, nullptr, s->norm.tscale, 0);
+            const int ex = try_guess("extrapolated");
+            if (ex < 0) return SPB6G_CUDA_ERROR;
+            base_extrap = ex;
+            launch_guess(c, s->st, s->ybuf, s->norm.tscale, base_extrap);
+            const int lg = try_guess("learned");
+            if (lg < 0) return SPB6G_CUDA_ERROR;
+            if (lg) {
                 s->stats.learned++;
                 chosen = true;
+            } else if (ex) {
+                s->stats.extrapolated++;
+                chosen = true;
             }
-            if (reset_fail(s)) return SPB6G_CUDA_ERROR;
+            // dP now holds the learned step from the chosen start
         } else {
-            tend_(s, TG_WARM);
+            launch_guess(c, s->st, s->ybuf, s->norm.tscale, 0);
         }
-        // from the plain start, the prediction is the first BiCGStab iterate's candidate
-        if (!chosen && (s->warm_mode & 2) && !tri && s->bicg_G > 0)
-            CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        tend_(s, TG_WARM);
+        // when the network's guess is not the start, its step from the start is the first
+        // BiCGStab iterate's candidate
+        x0_pending = have_pred && !(chosen && s->stats.learned > learned0) && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
+        if (x0_pending) CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
     }
-    const bool x0_pending = have_pred && !chosen && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
     // jreuse (modified Newton, :826-830, :887): the Jacobian is rebuilt at the first iteration, after
     // a damped step or a contraction above 0.25 (fresh_ok :797), and when the kept one lets the
     // line search fail; the step criterion meanwhile uses the scales of the last build
@@ -485,11 +508,14 @@ int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_r
     tend_(s, TG_EXPLICIT);
     // warm-start features of the stage (X* and the starting pressure), into the caller's
     // dump buffer when one has room, else into the solver's own rows
-    s->dump_stage = s->dumpX && s->dump_count + s->n <= s->dump_cap;
+    // a stage is dumped once a pressure rate exists (its target is relative to the last rate)
+    s->dump_stage = s->dumpX && s->rate_ready && s->dump_count + s->n <= s->dump_cap;
     // the pressure rate is tracked once a feature normalisation has been set (a feature, and the
     // extrapolation), so that it stays current on steps without a dump
     const bool track = s->Prate != nullptr;
     c.Prate = track ? s->Prate : nullptr;
+    c.Prate2 = s->Prate2;
+    c.rate_sc = s->rate_sc;
     c.x0l = nullptr;
     if (s->warm || s->dump_stage) {
         tbegin(s, TG_WARM);
@@ -502,9 +528,10 @@ int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_r
     double res = 0;
     const int rc = newton(s, res);
     if (rc != SPB6G_OK) return rc;
-    if (track) {  // the new pressure rate, and the training pair (features, (R' - R) / tscale)
-        launch_rate(c, s->st, s->Pstart, 1.0 / s->norm.tscale, s->dump_stage ? s->dumpT + s->dump_count : nullptr);
+    if (track) {  // the new pressure rate, and the training pair (features, (R' - R) / sigma)
+        launch_rate(c, s->st, s->Pstart, s->norm.tscale, s->dump_stage ? s->dumpT + s->dump_count : nullptr);
         if (s->dump_stage) s->dump_count += s->n;
+        s->rate_ready = true;
     }
     if (res > s->stats.maxres) s->stats.maxres = res;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -970,6 +997,8 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     c.sdt = c.adt;
     c.x0l = nullptr;
     c.Prate = nullptr;  // the dumped stage runs from the plain guess
+    c.Prate2 = nullptr;
+    c.rate_sc = nullptr;
     c.H = s->Hs;
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
     launch_flux(c, s->st);
@@ -1099,12 +1128,13 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc((void**)&s->ybuf, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(s->ybuf);
     }
-    for (double** b : {&s->Pstart, &s->Prate, &s->x0buf}) {
+    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->x0buf, &s->rate_sc}) {
         if (*b) continue;
-        if (cudaMalloc((void**)b, (size_t)s->n * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        const size_t cnt = b == &s->rate_sc ? 2 : (size_t)s->n;
+        if (cudaMalloc((void**)b, cnt * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
-        // no rate before the first converged stage
-        if (b == &s->Prate && cudaMemsetAsync(s->Prate, 0, (size_t)s->n * sizeof(double), s->st) != cudaSuccess)
+        // no rate (and no rate scale) before the first converged stage
+        if (b != &s->Pstart && b != &s->x0buf && cudaMemsetAsync(*b, 0, cnt * sizeof(double), s->st) != cudaSuccess)
             return SPB6G_CUDA_ERROR;
     }
     return SPB6G_OK;

@@ -2,16 +2,18 @@
 
 The plain solver starts each stage's implicit-pressure Newton from the previous
 stage's pressure.  Here a small MLP (tensor-core kernels of libspb6g) predicts the
-stage's pressure change dP = dts (R + y tscale) from the 3x3 stencils of
-(rho, rho u, rho v, alpha1, E*, P_prev, R), R the pressure rate of the last
-converged stage and dts the stage's time span: y = 0 is the linear
-extrapolation of the pressure, and the network learns the departure from it.
-The solver evaluates the residual at P + dP and starts Newton there only when
-its residual norm is below the plain guess's; otherwise the prediction seeds the
-first BiCGStab iterate (in a least-squares combination with the plain start,
-never with a larger initial residual).  Newton and BiCGStab keep their
-tolerances, so the converged pressure is the plain solve's to the solver
-tolerance.
+stage's pressure P_start + dts (R + sigma y) from the 3x3 stencils of
+(rho, rho u, rho v, alpha1, E*, P_prev, R / sigma) and the last rate change
+(R - R2) / sigma, R the pressure rate of the last converged stage, sigma its RMS
+over the cells and dts the stage's time span: y = 0 is the linear extrapolation
+of the pressure, and the network learns the departure from it in units of sigma,
+so the target is scale-free across fields, regimes and the start-up ramp.  The
+solver starts Newton from the guess of smallest residual norm among the plain
+guess, the extrapolation and the network's guess; when the network's guess is
+not the start, its step seeds the first BiCGStab iterate (in a least-squares
+combination with the plain start, never with a larger initial residual).  Newton
+and BiCGStab keep their tolerances, so the converged pressure is the plain
+solve's to the solver tolerance.
 
 At the low-Mach operating point Newton converges linearly (a constant
 contraction of about 0.4-0.6 per iteration with full steps), so every factor
@@ -21,7 +23,7 @@ solve.
     python -m diffusionimex_b200.learned --out warmstart.npz --n 2048          # dump, train, save
     python -m diffusionimex_b200.learned --eval warmstart.npz --n 2048         # plain vs learned
 
-Training data are (feature row, (R' - R) / tscale) pairs that the plain GPU
+Training data are (feature row, (R' - R) / sigma) pairs that the plain GPU
 solver writes while it runs (`Solver.set_dump`); features are centred and
 scaled per field with statistics from a short pilot run.
 """
@@ -40,7 +42,8 @@ from .warmstart import MLP
 
 FIELDS = ("rho", "rho_u", "rho_v", "alpha1", "E", "P", "R")
 NF = len(FIELDS)
-NFEAT = 9 * NF  # 63 of the 64 input columns
+NSTENCIL = 9 * NF  # 63 stencil columns; the 64th is the last rate change of the cell
+NFEAT = 64
 IDENTITY = [0.0] * NF + [1.0] * NF + [1.0] * NF + [1.0]
 # the trained network shipped with the package (low-Mach bubble fields, material CFL 0.8)
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_lowmach.npz")
@@ -83,7 +86,7 @@ def pilot_norm(case: dict, steps: int = 8, device: int = 0) -> list[float]:
     X, T = _run_dump(s, n, steps, steps, device)
     s.close()
     k = X.shape[0]
-    F = X[:, :NFEAT].float().view(k, NF, 9)
+    F = X[:, :NSTENCIL].float().view(k, NF, 9)
     mean = F[:, :, 0].mean(0)
     std = F[:, :, 0].std(0)
     dstd = F[:, :, 1:].std(dim=(0, 2))
@@ -116,7 +119,6 @@ def _init_params(seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     F = 64
     W1 = rng.uniform(-1, 1, (F, F)) * np.sqrt(3.0 / NFEAT)
-    W1[:, NFEAT:] = 0.0
     W2 = rng.uniform(-1, 1, (F, F)) * np.sqrt(3.0 / F)
     W3 = rng.uniform(-1, 1, (F, F)) * np.sqrt(3.0 / F)
     w4 = rng.uniform(-1, 1, F) * np.sqrt(3.0 / F) * 0.1
@@ -126,7 +128,8 @@ def _init_params(seed: int) -> np.ndarray:
 
 def zero_network(device: int = 0) -> MLP:
     """The network with every parameter 0: y = 0, so the learned guess is the linear extrapolation
-    P_start + dts R alone (the ablation of the trained network)."""
+    P_start + dts R alone (the ablation of the trained network: the solver tries the extrapolation
+    on its own as well, so with this network every stage gets exactly the extrapolation)."""
     m = MLP(device)
     m.set_params(np.zeros(m.nparam, np.float32))
     return m
@@ -171,7 +174,8 @@ def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: i
     b = s.stats()
     P, pref = s.pressure()
     s.close()
-    d = {k: b[k] - a[k] for k in ("steps", "stages", "newton_it", "bicg_it", "rejects", "learned", "learned_x0")}
+    d = {k: b[k] - a[k] for k in ("steps", "stages", "newton_it", "bicg_it", "rejects", "learned", "learned_x0",
+                                  "extrapolated")}
     d.update(ms=ms, ms_per_step=ms / max(d["steps"], 1), bicg_per_step=d["bicg_it"] / max(d["steps"], 1),
              newton_per_stage=d["newton_it"] / max(d["stages"], 1), t=b["t"])
     return d, P + pref

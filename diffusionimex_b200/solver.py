@@ -66,6 +66,7 @@ class Stats(ctypes.Structure):
         ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
         ("learned", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
         ("p_ref", ctypes.c_double), ("tmax", ctypes.c_double * 2), ("learned_x0", ctypes.c_int64),
+        ("extrapolated", ctypes.c_int64),
     ]
 
 

@@ -112,6 +112,7 @@ typedef struct {
     double t, dt, maxres, p_ref;
     double tmax[2];                 /* max phase temperatures of the stages' final states (st_Tmax :96, :1070) */
     int64_t learned_x0;             /* BiCGStab solves that started from the learned first iterate */
+    int64_t extrapolated;           /* stages whose Newton started from the extrapolated pressure */
 } spb6g_stats;
 
 typedef struct spb6g_solver spb6g_solver;
@@ -287,23 +288,27 @@ int spb6g_mlp_last_loss(spb6g_mlp* m, void* stream, float* loss_sum);
 
 /* Warm start on the solver (no counterpart in the reference).  The features of a cell are
  * the 3x3 stencils of 7 fields: rho, rho u, rho v, alpha1, E* of the explicit predictor, the
- * stage's starting pressure P - P_REF, and R, the pressure rate (P_converged - P_start) / dts
- * of the last converged stage (dts = the stage's time span, (c_s - c_{s-1}) dt from the
- * implicit tableau's row sums; R = 0 before the first stage) -- 63 of the 64 columns.
- * norm: 22 doubles: mean[7], std[7] of the centre values and std[7] of the neighbour
- * differences of the 7 fields, then the target scale.  Setting it also starts tracking R. */
+ * stage's starting pressure P - P_REF, and R / sigma, R the pressure rate
+ * (P_converged - P_start) / dts of the last converged stage (dts = the stage's time span,
+ * (c_s - c_{s-1}) dt from the implicit tableau's row sums; R = 0 before the first stage) and
+ * sigma its RMS over the cells -- 63 columns -- and (R - R2) / sigma of the cell itself, R2 the
+ * rate of the stage before.  norm: 22 doubles: mean[7], std[7] of the centre values and std[7]
+ * of the neighbour differences of the 7 fields, then the target scale (sigma before the first
+ * converged stage).  Setting it also starts tracking R. */
 int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
-/* m != NULL: every stage predicts its pressure change dP = dts (R + MLP(features) scale).
- * Mode bit 1 (spb6g_set_warmstart_mode; 3 by default): Newton starts from P + dP when the
- * residual norm there is below the plain guess's (the previous stage's pressure), else from
- * the plain guess.  Mode bit 2: from the plain guess, the first BiCGStab solve of the stage
- * starts from x0 = a M^-1 b + c dP, (a, c) minimising ||b - A x0||, when that residual is
- * below 0.99 of the plain start's (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.
- * Newton and BiCGStab keep their tolerances.  NULL: off. */
+/* m != NULL: every stage predicts its pressure P_start + dts (R + sigma MLP(features)).
+ * Mode bit 1 (spb6g_set_warmstart_mode; 3 by default): Newton starts from the guess of
+ * smallest residual norm among the plain guess (the previous stage's pressure), the
+ * extrapolation P_start + dts R (the network's zero output) and the network's guess.  Mode
+ * bit 2: when the network's guess is not the start, the first BiCGStab solve of the stage
+ * starts from x0 = a M^-1 b + c dP, dP the network's step from the start and (a, c)
+ * minimising ||b - A x0||, when that residual is below 0.99 of the plain start's
+ * (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.  Newton and BiCGStab keep their
+ * tolerances.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
 /* Training data: each stage appends n feature rows (64 BF16 each) to X_dev and n
- * targets (R' - R) / scale to target_dev while capacity allows (R' the stage's converged
+ * targets (R' - R) / sigma to target_dev while capacity allows (R' the stage's converged
  * pressure rate, R the last stage's). */
 int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity);
 int spb6g_dump_count(spb6g_solver* s, int64_t* count);

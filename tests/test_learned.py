@@ -1,11 +1,11 @@
 """Learned warm start inside the solver (no counterpart in the reference).
 
-The network predicts each stage's pressure change dP = dts (R + y tscale), R the pressure
-rate of the last converged stage.  The solver evaluates the residual at P + dP and starts
-Newton from it only when its residual norm is below the plain guess's; from the plain
-start the prediction may seed the first BiCGStab iterate, in a least-squares combination
-that never has the larger initial residual.  Newton and BiCGStab keep their tolerances,
-so every run must reach the plain run's solution: L1(p) against the plain FP64 solve at
+The network predicts each stage's pressure P_start + dts (R + sigma y), R the pressure rate
+of the last converged stage and sigma its RMS.  The solver starts Newton from the guess of
+smallest residual norm among the plain guess, the extrapolation (y = 0) and the network's
+guess; when the network's guess is not the start, its step may seed the first BiCGStab
+iterate, in a least-squares combination that never has the larger initial residual.
+Newton and BiCGStab keep their tolerances, so every run must reach the plain run's solution: L1(p) against the plain FP64 solve at
 most 1e-8 relative (the learned form's bar).  The last test trains a network on other
 seeds of the low-Mach field and records what it gains over the plain guess on seed 0."""
 from __future__ import annotations
@@ -24,6 +24,13 @@ N = 256
 L1_BAR = 1e-8  # relative L1(p) of a learned run against the plain FP64 run
 
 
+def lowmach(seed: int) -> dict:
+    """The low-Mach bubble field on N^2 with 4 bubbles, Newton and BiCGStab at 1e-12: runs from
+    different starts then agree far inside the L1(p) bar, whatever iterate each one stops at (at
+    the configuration's 1e-10 the stopping point alone moves L1(p) by about 1e-8 on this grid)."""
+    return dict(cases.lowmach_bubbles(N, seed=seed, nbub=4), newton_tol=1e-12, bicg_tol=1e-12)
+
+
 def _run(case, steps, warmup, mlp=None, norm=None, mode=3):
     from diffusionimex_b200 import learned
 
@@ -35,7 +42,7 @@ def test_dump_pairs_and_feature_rows():
 
     from diffusionimex_b200 import learned
 
-    c = cases.lowmach_bubbles(N, seed=1, nbub=4)
+    c = lowmach(1)
     norm = learned.pilot_norm(c, steps=4)
     assert len(norm) == 22 and all(np.isfinite(norm)) and norm[21] > 0
     X, T = learned.dump_pairs([(c, 6, 2)], norm)
@@ -43,23 +50,22 @@ def test_dump_pairs_and_feature_rows():
     assert T.shape == (X.shape[0],)
     Xf = X.float()
     assert torch.isfinite(Xf).all() and torch.isfinite(T).all()
-    assert (Xf[:, 63:] == 0).all()  # padding column
     assert float(Xf.abs().max()) <= 1024.0  # normalised features stay within the clamp
     # centre features are standardised with the pilot's statistics
     assert abs(float(Xf[:, 0].mean())) < 1.0 and 0.1 < float(Xf[:, 0].std()) < 10.0
-    # the pressure-rate stencil (field 7) is tracked between the dumped steps
-    assert float(Xf[:, 54].abs().max()) > 0
+    # the pressure-rate stencil (field 7) and the rate change (column 64) are tracked between the
+    # dumped steps
+    assert float(Xf[:, 54].abs().max()) > 0 and float(Xf[:, 63].abs().max()) > 0
 
 
-def test_bad_guess_is_never_chosen_and_changes_nothing():
-    """A network whose prediction is 50 target standard deviations off everywhere has the larger
-    residual every stage, so with the learned Newton start alone (mode 1) the plain guess stands
-    everywhere and the run is bitwise the plain run."""
+def test_bad_guess_is_never_chosen():
+    """A network whose prediction is 50 sigma off everywhere has the larger residual every stage, so
+    its guess never starts Newton (mode 1), and the run reaches the plain run's solution."""
     from diffusionimex_b200 import learned
     from diffusionimex_b200.warmstart import MLP
 
-    c = cases.lowmach_bubbles(N, seed=0, nbub=4)
-    norm = learned.pilot_norm(cases.lowmach_bubbles(N, seed=1, nbub=4), steps=4)
+    c = lowmach(0)
+    norm = learned.pilot_norm(lowmach(1), steps=4)
     m = MLP()
     p = np.zeros(m.nparam, np.float32)
     p[-1] = 50.0  # output bias: y = 50 for every cell
@@ -67,8 +73,8 @@ def test_bad_guess_is_never_chosen_and_changes_nothing():
     plain, Pp = _run(c, 6, 3)
     warm, Pw = _run(c, 6, 3, mlp=m, norm=norm, mode=1)
     assert warm["learned"] == 0 and warm["learned_x0"] == 0
-    assert np.array_equal(Pp, Pw)
-    assert warm["newton_it"] == plain["newton_it"] and warm["bicg_it"] == plain["bicg_it"]
+    assert warm["steps"] == plain["steps"] and warm["newton_it"] <= plain["newton_it"]
+    assert learned.l1_rel(Pw, Pp) <= L1_BAR
     m.close()
 
 
@@ -77,8 +83,8 @@ def test_learned_first_iterate_keeps_the_solution():
     to its tolerance: the run reaches the plain solution (L1(p) bar) with the same steps."""
     from diffusionimex_b200 import learned
 
-    c = cases.lowmach_bubbles(N, seed=0, nbub=4)
-    norm = learned.pilot_norm(cases.lowmach_bubbles(N, seed=1, nbub=4), steps=4)
+    c = lowmach(0)
+    norm = learned.pilot_norm(lowmach(1), steps=4)
     z = learned.zero_network()
     plain, Pp = _run(c, 10, 3)
     warm, Pw = _run(c, 10, 3, mlp=z, norm=norm, mode=2)
@@ -93,8 +99,8 @@ def test_extrapolation_guess_reaches_the_plain_solution():
     taken wherever its residual is smaller, and the run keeps the plain run's steps and solution."""
     from diffusionimex_b200 import learned
 
-    c = cases.lowmach_bubbles(N, seed=0, nbub=4)
-    norm = learned.pilot_norm(cases.lowmach_bubbles(N, seed=1, nbub=4), steps=4)
+    c = lowmach(0)
+    norm = learned.pilot_norm(lowmach(1), steps=4)
     z = learned.zero_network()
     plain, Pp = _run(c, 12, 3)
     warm, Pw = _run(c, 12, 3, mlp=z, norm=norm, mode=1)
@@ -108,13 +114,13 @@ def test_trained_warm_start_reaches_the_plain_solution_and_records_its_gain():
 
     from diffusionimex_b200 import learned
 
-    norm = learned.pilot_norm(cases.lowmach_bubbles(N, seed=1, nbub=4), steps=6)
-    X, T = learned.dump_pairs([(cases.lowmach_bubbles(N, seed=s, nbub=4), 30, 1) for s in (1, 2)], norm)
+    norm = learned.pilot_norm(lowmach(1), steps=6)
+    X, T = learned.dump_pairs([(lowmach(s), 30, 1) for s in (1, 2)], norm)
     m, hist = learned.train_mlp(X, T, steps=400, batch=1 << 18, lr=2e-3, log_every=100)
     assert np.isfinite(hist[-1][1]) and hist[-1][1] < hist[0][1]
     del X, T
     torch.cuda.empty_cache()
-    r = learned.compare(cases.lowmach_bubbles(N, seed=0, nbub=4), m, norm, steps=20, warmup=5)
+    r = learned.compare(lowmach(0), m, norm, steps=20, warmup=5)
     assert r["L1_rel_p"] <= L1_BAR and r["extrapolation_L1_rel_p"] <= L1_BAR
     assert r["same_steps"]
     out = os.environ.get("SPB6G_LEARNED_REPORT")
