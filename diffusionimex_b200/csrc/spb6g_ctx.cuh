@@ -203,6 +203,8 @@ void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void*
 // the extrapolated pressure P_start + sdt R; y = null: the extrapolation dP = sdt R
 void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, int base_extrap);
 void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
+// separable box average of radius r (0 < r <= nx, ny) of y, in place (tmp: n floats)
+void launch_smooth(const Ctx& c, cudaStream_t st, float* y, float* tmp, int r);
 void launch_stepnorm(const Ctx& c, cudaStream_t st);
 void launch_apply_step(const Ctx& c, cudaStream_t st);
 void launch_floor(const Ctx& c, cudaStream_t st, double tol);

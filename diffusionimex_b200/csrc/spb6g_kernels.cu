@@ -1420,6 +1420,29 @@ void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, 
     k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, base_extrap);
     count(c, 1);
 }
+// Box average of radius r along x (dir 0) or y (dir 1) of a per-cell field, boundary-mapped like
+// every stencil read (periodic wrap, else the edge cell): the separable smoothing of the network's
+// output, so that its step carries only the smooth part of the prediction.
+__global__ void k_smooth(Ctx c, const float* __restrict__ in, float* __restrict__ out, int r, int dir) {
+    const Geom& g = c.g;
+    const float w = 1.0f / (2 * r + 1);
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
+        const int i = x % g.nx, j = x / g.nx;
+        float s = 0.0f;
+        for (int d = -r; d <= r; d++) s += in[dir == 0 ? mp_index(g, i + d, j) : mp_index(g, i, j + d)];
+        out[x] = s * w;
+    }
+}
+void launch_smooth(const Ctx& c, cudaStream_t st, float* y, float* tmp, int r) {
+    k_smooth<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tmp, r, 0);
+    if (c.g.ny > 1) {
+        k_smooth<<<blocks_for(c.n), TPB, 0, st>>>(c, tmp, y, r, 1);
+        count(c, 2);
+    } else {
+        cudaMemcpyAsync(y, tmp, (size_t)c.n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        count(c, 1);
+    }
+}
 // After a converged stage: the new rate R' = (P_converged - P_start) / sdt, the training
 // target (R' - R) / sigma (when t is not null), R2 = R, R = R', and sigma' = RMS of R'
 // (folded by the last block, after every block has read sigma).

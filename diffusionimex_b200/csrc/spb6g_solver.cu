@@ -78,6 +78,8 @@ struct spb6g_solver {
     bool rate_ready = false;            // a stage has converged since the tracking began (R exists)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
     int warm_mode = 3;                  // 1: learned Newton start, 2: learned first BiCGStab iterate, 3: both
+    int warm_smooth = 0;                // radius of the box average of the network's output (0: none)
+    float* ytmp = nullptr;              // scratch of the smoothing
     double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
     int attempt_stage = -1;             // stage-level API: the last stage of the attempt that converged (-1: none)
     void* rows_cur = nullptr;           // where this stage's feature rows were written
@@ -299,6 +301,7 @@ int newton(spb6g_solver* s, double& resfinal) {
     if (s->warm && s->rate_ready) {
         tbegin(s, TG_WARM);
         if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
+        if (s->warm_smooth > 0) launch_smooth(c, s->st, s->ybuf, s->ytmp, s->warm_smooth);
         have_pred = true;
         int base_extrap = 0;
         if (s->warm_mode & 1) {
@@ -1124,9 +1127,10 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc(&s->featbuf, (size_t)s->n * 128) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(s->featbuf);
     }
-    if (!s->ybuf) {
-        if (cudaMalloc((void**)&s->ybuf, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
-        s->allocs.push_back(s->ybuf);
+    for (float** b : {&s->ybuf, &s->ytmp}) {
+        if (*b) continue;
+        if (cudaMalloc((void**)b, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(*b);
     }
     for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->x0buf, &s->rate_sc}) {
         if (*b) continue;
@@ -1153,6 +1157,11 @@ int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode) {
     if (!s || mode < 1 || mode > 3) return SPB6G_BAD_ARG;
     s->warm_mode = mode;
+    return SPB6G_OK;
+}
+int spb6g_set_warmstart_smoothing(spb6g_solver* s, int radius) {
+    if (!s || radius < 0 || radius > 64 || radius >= s->g.nx || (s->g.ny > 1 && radius >= s->g.ny)) return SPB6G_BAD_ARG;
+    s->warm_smooth = radius;
     return SPB6G_OK;
 }
 int spb6g_set_dump(spb6g_solver* s, void* X_dev, float* target_dev, int64_t capacity) {

@@ -77,19 +77,41 @@ def _run_dump(s: Solver, n: int, steps: int, every: int, device: int, first: int
     return X, T
 
 
+def rough_norm(case: dict) -> list[float]:
+    """A first normalisation from the initial state alone (per-field mean and spread of rho, rho u,
+    rho v, alpha1, E and their x-differences; fixed scales for P - P_REF and R / sigma), enough to
+    keep the pilot's feature rows inside the feature kernel's clamp."""
+    U = np.asarray(case["U"], dtype=np.float64).reshape(case["ny"], case["nx"], 8)
+    fields = [U[..., 1] + U[..., 2], U[..., 3], U[..., 4], U[..., 0], U[..., 7]]
+    mean = [float(f.mean()) for f in fields] + [0.0, 0.0]
+    std = [max(float(f.std()), 1e-3 * abs(float(f.mean())), 1e-30) for f in fields] + [1e5, 1.0]
+    dstd = [max(float(np.abs(np.diff(f, axis=1)).mean()) if case["nx"] > 1 else 0.0, 1e-3 * sd, 1e-30)
+            for f, sd in zip(fields, std)] + [1e4, 1.0]
+    return mean + std + dstd + [1.0]
+
+
 def pilot_norm(case: dict, steps: int = 8, device: int = 0) -> list[float]:
     """Per-field mean / std of the centre values, std of the neighbour differences and the std
-    of the target, from the stages of the last step of a plain run of `steps` steps."""
+    of the target, from the stages of the last step of a plain run of `steps` steps: the rows are
+    written with the rough normalisation of the initial state and mapped back before the
+    statistics are taken."""
+    torch = _torch()
     n = case["nx"] * case["ny"]
+    rough = rough_norm(case)
     s = Solver(case, device=device)
-    s.set_feature_norm(IDENTITY)
+    s.set_feature_norm(rough)
     X, T = _run_dump(s, n, steps, steps, device)
     s.close()
     k = X.shape[0]
-    F = X[:, :NSTENCIL].float().view(k, NF, 9)
-    mean = F[:, :, 0].mean(0)
-    std = F[:, :, 0].std(0)
-    dstd = F[:, :, 1:].std(dim=(0, 2))
+    F = X[:, :NSTENCIL].float().view(k, NF, 9).double()
+    m0 = torch.tensor(rough[:NF], dtype=torch.float64, device=F.device)
+    s0 = torch.tensor(rough[NF:2 * NF], dtype=torch.float64, device=F.device)
+    d0 = torch.tensor(rough[2 * NF:3 * NF], dtype=torch.float64, device=F.device)
+    centre = F[:, :, 0] * s0 + m0
+    diffs = F[:, :, 1:] * d0[None, :, None]
+    mean = centre.mean(0)
+    std = centre.std(0)
+    dstd = diffs.std(dim=(0, 2))
     tscale = T.std()
     fl = lambda v, lo: [max(float(a), lo * (abs(float(m)) + 1e-30), 1e-30) for a, m in zip(v, mean)]
     return [float(m) for m in mean] + fl(std, 1e-6) + fl(dstd, 1e-9) + [max(float(tscale), 1e-30)]
@@ -157,13 +179,14 @@ def train_mlp(X, T, steps: int = 3000, batch: int = 1 << 20, lr: float = 1e-3, s
     return m, hist
 
 
-def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 3) -> tuple:
+def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 3,
+             smooth: int = 0) -> tuple:
     """Advance `warmup` untimed steps, then `steps` timed ones; counts and device time."""
     torch = _torch()
     s = Solver(case, device=device)
     if mlp is not None:
         s.set_feature_norm(norm)
-        s.set_warmstart(mlp, mode)
+        s.set_warmstart(mlp, mode, smooth)
     if warmup > 0:  # advance(0) would run to t_end
         s.advance(warmup)
     a = s.stats()

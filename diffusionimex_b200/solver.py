@@ -132,6 +132,7 @@ def library() -> ctypes.CDLL:
         "spb6g_set_feature_norm": (I, [P, P]),
         "spb6g_set_warmstart": (I, [P, P]),
         "spb6g_set_warmstart_mode": (I, [P, I]),
+        "spb6g_set_warmstart_smoothing": (I, [P, I]),
         "spb6g_set_dump": (I, [P, P, P, ctypes.c_int64]),
         "spb6g_dump_count": (I, [P, P]),
         "spb6g_mlp_create": (I, [I, P]),
@@ -416,13 +417,15 @@ class Solver:
         a = (ctypes.c_double * self.NORM_LEN)(*[float(v) for v in norm])
         self._check(self.lib.spb6g_set_feature_norm(self.h, a), "spb6g_set_feature_norm")
 
-    def set_warmstart(self, mlp, mode: int = 3):
-        """mode 1: learned Newton start (when its residual is below the plain guess's); 2: learned
-        first BiCGStab iterate from the plain start; 3: both."""
+    def set_warmstart(self, mlp, mode: int = 3, smooth: int = 0):
+        """mode 1: learned Newton start (the guess of smallest residual among the plain guess, the
+        extrapolation and the network's); 2: learned first BiCGStab iterate; 3: both.  smooth: radius
+        of the box average of the network's output (0: none)."""
         self._warm = mlp
         self._check(self.lib.spb6g_set_warmstart(self.h, mlp.handle if mlp is not None else None), "spb6g_set_warmstart")
         if mlp is not None:
             self._check(self.lib.spb6g_set_warmstart_mode(self.h, int(mode)), "spb6g_set_warmstart_mode")
+            self._check(self.lib.spb6g_set_warmstart_smoothing(self.h, int(smooth)), "spb6g_set_warmstart_smoothing")
 
     def set_dump(self, X=None, t=None):
         """X: (cap, 64) torch.bfloat16, t: (cap,) torch.float32 on the device, or None to stop."""

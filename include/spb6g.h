@@ -307,6 +307,11 @@ int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
  * tolerances.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
+/* Radius r (0: none, the default; at most 64 and below nx, ny) of a separable box average of the
+ * network's output before it forms a guess: the implicit pressure operator amplifies a cell-to-
+ * cell error of the guess by about (c tau / h)^2, so only the smooth part of a per-cell prediction
+ * can improve a start whose own error is smooth. */
+int spb6g_set_warmstart_smoothing(spb6g_solver* s, int radius);
 /* Training data: each stage appends n feature rows (64 BF16 each) to X_dev and n
  * targets (R' - R) / sigma to target_dev while capacity allows (R' the stage's converged
  * pressure rate, R the last stage's). */

@@ -1,0 +1,87 @@
+"""Parity at the workload sizes, against the reference run live on the host cores.
+
+The golden fixtures of the other parity tests are small grids (up to 120 x 80).  Here the
+compiled reference (oracle/_ref, built from the reference's own sources) runs the same
+initial data at full size beside the GPU path:
+
+  * one full step (stages, Newton, BiCGStab, acceptance) of the 8-bubble water field on
+    1024^2, of the Mach-1.5 shock on a light-gas bubble on 2048 x 1024 and of the low-Mach
+    bubble field on 2048^2 (material CFL 0.8, periodic): every conservative field within
+    1e-12 of its maximum, or -- where strong shocks put glibc's and CUDA's exp / log / pow
+    into the shock-profile shooting -- within 10x the reference's own change when those
+    calls move by one ulp (the reference's acceptance rule for round-off,
+    docs/code/openmp_optimisation.md:81-82);
+  * the 8-bubble field over its 200 steps, in L1 against the reference's final state.
+
+A reference step at 2048^2 takes a few seconds on the host cores; the 200-step run a few
+minutes."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import refio
+from diffusionimex_b200 import Solver, cases
+from helpers import FIELDS, fieldwise_l1, fieldwise_maxrel
+
+pytestmark = pytest.mark.gpu
+
+CORES = os.cpu_count() or 1
+
+
+def _need_ref():
+    if not refio.ref_available():
+        pytest.fail("oracle/_ref/spb6_ref is missing: the reference must be built (make -C oracle ref)")
+
+
+def _gpu(c, nsteps):
+    s = Solver(c)
+    s.advance(nsteps)
+    out = {"U": s.state(), "stats": s.stats()}
+    out["P"], out["p_ref"] = s.pressure()
+    s.close()
+    return out
+
+
+def _report(d):
+    return {f: f"{v:.2e}" for f, v in zip(FIELDS, d)}
+
+
+@pytest.mark.parametrize("name,make,shocks", [
+    ("bubbles1024", lambda: cases.bubble_field(1024, seed=0, nbub=8), False),
+    ("shock2048x1024", lambda: cases.shock_bubble(2048, 1024), True),
+    ("lowmach2048", lambda: cases.lowmach_bubbles(2048, seed=0), False),
+])
+def test_one_step_at_workload_size(name, make, shocks):
+    _need_ref()
+    c = make()
+    r = refio.run_ref(c, mode=refio.MODE_STEPS, nsteps=1, threads=CORES)
+    g = _gpu(c, 1)
+    assert g["stats"]["steps"] == r["steps"] == 1
+    assert (g["stats"]["rejects"], g["stats"]["newton_it"]) == (r["rejects"], r["newton_it"]), (g["stats"], r)
+    d = fieldwise_maxrel(g["U"], r["U"])
+    bar = np.full(8, 1e-12)
+    if shocks and d.max() > 1e-12:
+        ru = refio.run_ref(c, mode=refio.MODE_STEPS, nsteps=1, threads=CORES, variant="ulp")
+        bar = np.maximum(10 * fieldwise_maxrel(ru["U"], r["U"]), 1e-12)
+    assert np.all(d <= bar), {"gpu": _report(d), "bar": _report(bar)}
+    pscale = np.abs(r["P"]).max() + abs(r["p_ref"])
+    assert np.abs(g["P"] - r["P"]).max() / pscale <= (1e-12 if not shocks else max(1e-12, float(bar.max())))
+
+
+def test_bubble_field_200_steps_in_l1():
+    """The 8-bubble field on 1024^2 over its 200 steps: the same step and rejection counts, and every
+    field within 1e-6 of its maximum in L1 (the whole-run bar of the small fixtures), or within 10x
+    the reference's own L1 change under one-ulp libm where that is larger."""
+    _need_ref()
+    c = cases.bubble_field(1024, seed=0, nbub=8)
+    r = refio.run_ref(c, mode=refio.MODE_STEPS, nsteps=200, threads=CORES)
+    g = _gpu(c, 200)
+    assert (g["stats"]["steps"], g["stats"]["rejects"]) == (r["steps"], r["rejects"])
+    d = fieldwise_l1(g["U"], r["U"])
+    if d.max() > 1e-6:
+        ru = refio.run_ref(c, mode=refio.MODE_STEPS, nsteps=200, threads=CORES, variant="ulp")
+        noise = fieldwise_l1(ru["U"], r["U"])
+        assert np.all(d <= np.maximum(10 * noise, 1e-6)), {"gpu": _report(d), "noise": _report(noise)}
