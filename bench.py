@@ -515,7 +515,7 @@ def run_reference(args, case, rank: int):
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "newton_it": r["newton_it"], "stages": r["stages"], "bicg_it": r["bicg_it"],
-        "bicg_iters_per_step": r["bicg_it"] / max(int(r["steps"]), 1),
+        "bicg_iters_per_step": (r["bicg_it"] / max(int(r["steps"]), 1)) if r["bicg_it"] else None,
         "guess": "plain (the reference always starts Newton from the previous stage's pressure)",
     }
     print(json.dumps(line))

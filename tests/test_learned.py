@@ -120,11 +120,36 @@ def test_trained_warm_start_reaches_the_plain_solution_and_records_its_gain():
     assert np.isfinite(hist[-1][1]) and hist[-1][1] < hist[0][1]
     del X, T
     torch.cuda.empty_cache()
-    r = learned.compare(lowmach(0), m, norm, steps=20, warmup=5)
+    r = learned.compare(lowmach(0), m, norm, steps=12, warmup=5)
+    # the L1 bar compares the same steps: a run whose rejections differ is on another time grid
+    assert r["same_steps"], (r["plain"], r["learned"])
     assert r["L1_rel_p"] <= L1_BAR and r["extrapolation_L1_rel_p"] <= L1_BAR
-    assert r["same_steps"]
     out = os.environ.get("SPB6G_LEARNED_REPORT")
     if out:
         with open(out, "w") as f:
             json.dump(r, f)
     m.close()
+
+
+def test_shipped_network_on_the_learned_configuration():
+    """The learned form's configuration -- the low-Mach field on 2048^2, material CFL 0.8, Newton
+    and BiCGStab at 1e-10 -- over steps 6-25 with the network shipped in the package, against the
+    plain guess over the same steps: the same steps, L1(p) within the bar, and fewer BiCGStab
+    iterations per step.  The measured ratios are written to SPB6G_LEARNED_REPORT if set."""
+    from diffusionimex_b200 import learned
+
+    m, norm = learned.load()
+    c = cases.lowmach_bubbles(2048, seed=0)
+    r = learned.compare(c, m, norm, steps=20, warmup=5)
+    m.close()
+    assert r["same_steps"], (r["plain"], r["learned"])
+    assert r["L1_rel_p"] <= L1_BAR, r["L1_rel_p"]
+    assert r["learned"]["bicg_it"] < r["plain"]["bicg_it"] and r["learned"]["newton_it"] < r["plain"]["newton_it"]
+    print(f"learned form 2048^2, steps 6-25: BiCGStab {r['bicg_ratio']:.2f}x fewer, Newton {r['newton_ratio']:.2f}x "
+          f"fewer, wall {r['time_ratio']:.2f}x faster, L1(p) {r['L1_rel_p']:.2e}; network guess taken in "
+          f"{r['learned']['learned']} stages, extrapolation in {r['learned']['extrapolated']}, learned first "
+          f"iterate in {r['learned']['learned_x0']} solves")
+    out = os.environ.get("SPB6G_LEARNED_REPORT")
+    if out:
+        with open(out + ".config5.json", "w") as f:
+            json.dump(r, f)
