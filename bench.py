@@ -72,8 +72,8 @@ KERNEL_OF = {"linear": "k_bicg_solve (BiCGStab solve, one launch per Newton iter
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="lowmach2048",
                    help="lowmach2048 (default: learned vs plain guess), lowmach2048-plain, bubbles1024, bubbles2048, bubbles256, tube1000, lowmach2048, shock2048x1024, "
