@@ -910,18 +910,20 @@ SPB6G_DEV bool sync_fold(double (&acc)[NQ], double* slot, unsigned G, GridBarrie
     return s_ok != 0;
 }
 
-// Work unit of the persistent passes: a strip of SW = 30 columns x J rows owned by one
-// warp for the whole solve.  Lane l holds column i0 - 1 + l: lanes 1..30 are the
-// strip's own columns, lanes 0 and 31 the columns just outside it, so west / east
-// neighbours of every own column come from the neighbouring lanes by warp shuffle.
-// The warp walks the rows upward with everything in registers: the stencil values of
-// the rows below, at and above the current row roll through three registers, and the
-// operands of the row two ahead and of the next own row are loaded while the current
-// row is used, so every warp keeps two rows of every operand in flight.  No shared-
-// memory staging.
-constexpr int RB_THREADS = 384;  // threads of a block of the persistent solve
-constexpr int RB_WARPS = RB_THREADS / 32;
-constexpr int SW = 30;           // own columns of a strip
+// Work unit of the persistent passes: a strip of 32 columns x J rows owned by one
+// warp for the whole solve.  Lane l holds column i0 + l and walks the rows
+// upward; west / east neighbours come from the row's values in shared memory,
+// south / north ones from the rows below and above, which the walk loads anyway.
+// Rows arrive through a PS_D-deep cp.async pipeline (loads for row t + PS_D - 1
+// are in flight while row t is used), so each warp keeps several rows of every
+// operand in flight instead of one.
+constexpr int PB_WARPS = PB_THREADS / 32;
+constexpr int PS_D = 4;                           // rows in flight per warp
+constexpr int PS_HV = 4;                          // operands needed at the neighbours (34 columns)
+constexpr int PS_RV = 6;                          // operands needed at the row itself (32 columns)
+constexpr int PS_STAGE = PS_HV * 34 + PS_RV * 32;  // doubles per row stage
+constexpr int PS_WARP = PS_D * PS_STAGE + 3 * 34;  // + three rows of scaled stencil values
+constexpr size_t PB_SMEM = (size_t)PB_WARPS * PS_WARP * sizeof(double);
 
 struct Strip {
     int i0, j0, J;
@@ -929,18 +931,18 @@ struct Strip {
 struct StripGrid {
     int ncols, J, nstrips;
 };
-// J rows per strip, so that the strips of the grid number at most `warps` (one strip per warp)
 SPB6G_DEV StripGrid strip_grid(const Geom& g, int warps) {
     StripGrid s;
-    s.ncols = (g.nx + SW - 1) / SW;
-    const int per_col = warps / s.ncols > 1 ? warps / s.ncols : 1;
-    s.J = (g.ny + per_col - 1) / per_col;
+    s.ncols = (g.nx + 31) / 32;
+    const long cells = (long)g.ny * s.ncols;
+    s.J = (int)((cells + warps - 1) / warps);
+    if (s.J < 1) s.J = 1;
     s.nstrips = s.ncols * ((g.ny + s.J - 1) / s.J);
     return s;
 }
 SPB6G_DEV Strip strip_at(const Geom& g, const StripGrid& sg, int s) {
     Strip st;
-    st.i0 = (s % sg.ncols) * SW;
+    st.i0 = (s % sg.ncols) * 32;
     st.j0 = (s / sg.ncols) * sg.J;
     st.J = min(sg.J, g.ny - st.j0);
     return st;
@@ -960,51 +962,106 @@ SPB6G_DEV int map_row(const Geom& g, int j) {
     if (j > g.ny - 1) return yp ? j - g.ny : g.ny - 1;
     return j;
 }
+SPB6G_DEV void cp_async8(double* s, const double* gp) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)), "l"(gp) : "memory");
+}
+SPB6G_DEV void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+SPB6G_DEV void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Five-point pass over one strip.  OP supplies, for the pass:
-//   Raw                      operands needed at the neighbours (and at the row itself);
-//   Own                      operands needed at the row itself only;
-//   load(idx, Raw&)          the neighbour operands of cell idx (boundary-mapped index);
-//   own(x, Own&)             the row operands of own cell x;
-//   cen(Raw, Cen&)           the row's values from its neighbour operands; returns its stencil value;
-//   out(x, Cen, Own, phS, phW, phC, phE, phN)   consumes an own cell.
-template <class OP>
-SPB6G_DEV void reg_strip(const Geom& g, const Strip& st, OP& op) {
-    using Raw = typename OP::Raw;
-    using Own = typename OP::Own;
-    using Cen = typename OP::Cen;
-    const unsigned full = 0xffffffffu;
+// Five-point pass over one strip.  hv: the PS_HV operands of the scaled stencil
+// value ph(k) (rows j0-1 .. j0+J, columns i0-1 .. i0+32, boundary-mapped);
+// mat: the five matrix diagonals (self, W, E, S, N) at the row itself, of type MT
+// (FP64, or FP32 in the precision form); ex: NEX FP64 operands at the row itself.
+// phf(stage, col) gives ph from a row stage; out(a, e, stage, col, phS, phW, phC,
+// phE, phN, x) consumes a row, a[m * 32] being diagonal m and e[v * 32] operand v.
+constexpr int PS_HV_BYTES = PS_HV * 34 * 8;
+template <class MT>
+SPB6G_DEV void cp_async_el(MT* s, const MT* gp) {
+    if constexpr (sizeof(MT) == 8) cp_async8((double*)s, (const double*)gp);
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)), "l"(gp) : "memory");
+}
+template <class MT, int NEX, class PH, class OUT>
+SPB6G_DEV void stencil_strip(const Geom& g, const Strip& st, double* ws, const double* const (&hv)[PS_HV],
+                             const MT* const (&mat)[5], const double* const* ex, PH phf, OUT out) {
     const int lane = threadIdx.x & 31;
-    const int col = st.i0 - 1 + lane;
-    const int ic = map_col(g, col);
-    const bool own = lane >= 1 && lane <= SW && col < g.nx;
-    auto base = [&](int t) { return (size_t)map_row(g, st.j0 - 1 + t) * g.nx; };  // t = 0 .. J + 1
-    Raw a, b;
-    Own oc, on;
-    Cen cc, cn;
-    // rows 0 (south of the first own row) and 1 (the first own row)
-    op.load(base(0) + ic, a);
-    double phS = op.cen(a, cn);
-    op.load(base(1) + ic, a);
-    double phC = op.cen(a, cc);
-    const size_t xrow0 = (size_t)st.j0 * g.nx + col;
-    if (own) op.own(xrow0, oc);
-    // row 2 in flight
-    op.load(base(2) + ic, a);
-    for (int t = 1; t <= st.J; t++) {
-        // issue: row t + 2 and the row operands of row t + 1
-        if (t + 2 <= st.J + 1) op.load(base(t + 2) + ic, b);
-        if (own && t + 1 <= st.J) op.own(xrow0 + (size_t)t * g.nx, on);
-        // the north row (t + 1) arrived in the last iteration's loads
-        const double phN = op.cen(a, cn);
-        const double phW = __shfl_up_sync(full, phC, 1), phE = __shfl_down_sync(full, phC, 1);
-        if (own) op.out(xrow0 + (size_t)(t - 1) * g.nx, cc, oc, phS, phW, phC, phE, phN);
-        phS = phC;
-        phC = phN;
-        cc = cn;
-        oc = on;
-        a = b;
+    const int nload = st.J + 2;
+    double* stages = ws;
+    double* phr = ws + PS_D * PS_STAGE;
+    const int ic_own = map_col(g, st.i0 + lane);
+    const int ic_halo = lane == 0 ? map_col(g, st.i0 - 1) : map_col(g, st.i0 + 32);
+    const bool own = st.i0 + lane < g.nx;
+    auto matp = [&](double* sp) { return (MT*)((char*)sp + PS_HV_BYTES); };
+    auto exp_ = [&](double* sp) { return (double*)((char*)sp + PS_HV_BYTES + 5 * 32 * sizeof(MT)); };
+    auto issue = [&](int t) {
+        if (t < nload) {
+            double* sp = stages + (t % PS_D) * PS_STAGE;
+            const size_t rb = (size_t)map_row(g, st.j0 - 1 + t) * g.nx;
+#pragma unroll
+            for (int v = 0; v < PS_HV; v++) cp_async8(sp + v * 34 + lane + 1, hv[v] + rb + ic_own);
+            if (lane < 2) {
+#pragma unroll
+                for (int v = 0; v < PS_HV; v++) cp_async8(sp + v * 34 + (lane ? 33 : 0), hv[v] + rb + ic_halo);
+            }
+            if (own && t >= 1 && t <= st.J) {
+                MT* mp = matp(sp);
+#pragma unroll
+                for (int m = 0; m < 5; m++) cp_async_el<MT>(mp + m * 32 + lane, mat[m] + rb + ic_own);
+                double* ep = exp_(sp);
+#pragma unroll
+                for (int v = 0; v < NEX; v++) cp_async8(ep + v * 32 + lane, ex[v] + rb + ic_own);
+            }
+        }
+        cp_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < PS_D - 1; t++) issue(t);
+    for (int t = 0; t < nload; t++) {
+        cp_wait<PS_D - 2>();
+        __syncwarp();
+        const double* sp = stages + (t % PS_D) * PS_STAGE;
+        double* pr = phr + (t % 3) * 34;
+        pr[lane + 1] = phf(sp, lane + 1);
+        if (lane < 2) pr[lane ? 33 : 0] = phf(sp, lane ? 33 : 0);
+        __syncwarp();
+        if (t >= 2 && own) {
+            double* so = stages + ((t - 1) % PS_D) * PS_STAGE;
+            const double* pS = phr + ((t - 2) % 3) * 34;
+            const double* pC = phr + ((t - 1) % 3) * 34;
+            out((const MT*)matp(so) + lane, (const double*)exp_(so) + lane, (const double*)so, lane + 1, pS[lane + 1],
+                pC[lane], pC[lane + 1], pC[lane + 2], pr[lane + 1], (st.j0 + t - 2) * g.nx + st.i0 + lane);
+        }
+        __syncwarp();
+        issue(t + PS_D - 1);
     }
+    cp_wait<0>();
+    __syncwarp();
+}
+// Row-local pass over one strip: NRV operands of each own cell through the same pipeline.
+template <int NRV, class OUT>
+SPB6G_DEV void row_strip(const Geom& g, const Strip& st, double* ws, const double* const (&rv)[NRV], OUT out) {
+    const int lane = threadIdx.x & 31;
+    const bool own = st.i0 + lane < g.nx;
+    auto issue = [&](int t) {
+        if (t < st.J && own) {
+            double* sp = ws + (t % PS_D) * PS_STAGE;
+            const size_t x = (size_t)(st.j0 + t) * g.nx + st.i0 + lane;
+#pragma unroll
+            for (int v = 0; v < NRV; v++) cp_async8(sp + v * 32 + lane, rv[v] + x);
+        }
+        cp_commit();
+    };
+#pragma unroll
+    for (int t = 0; t < PS_D - 1; t++) issue(t);
+    for (int t = 0; t < st.J; t++) {
+        cp_wait<PS_D - 2>();
+        __syncwarp();
+        if (own) out(ws + (t % PS_D) * PS_STAGE, lane, (st.j0 + t) * g.nx + st.i0 + lane);
+        __syncwarp();
+        issue(t + PS_D - 1);
+    }
+    cp_wait<0>();
+    __syncwarp();
 }
 
 // The five diagonals in the SpMV's precision.
@@ -1018,117 +1075,25 @@ template <>
 SPB6G_DEV const float* diag<float>(const Ctx& c, int m) {
     return m == 0 ? c.fC : m == 1 ? c.fW : m == 2 ? c.fE : m == 3 ? c.fS : c.fN;
 }
-// One SpMV row in the reference's entry order (self, W, E, S, N), accumulated in MT.
-template <class MT>
-SPB6G_DEV double spmv5(const MT (&a)[5], bool two_d, double phS, double phW, double phC, double phE, double phN) {
-    MT q = 0;
-    q += a[0] * (MT)phC;
-    q += a[1] * (MT)phW;
-    q += a[2] * (MT)phE;
-    if (two_d) {
-        q += a[3] * (MT)phS;
-        q += a[4] * (MT)phN;
-    }
-    return (double)q;
-}
 
-// Pass A of iteration k (k >= 1 fuses the end of iteration k - 1, the reference's
-// x += alpha ph + omega sh and r = s - omega t, with the start of iteration k):
-// r = s - wx t; x += ax (D^-1 p_old + cx) + wx (D^-1 s + sx); p = r + beta (p_old - om v);
-// q = A (D^-1 p); sums 1^T p, r0^T q, 1^T q, 1^T r.
-template <class MT>
-struct PassA {
-    struct Raw { double s, t, p, v, d; };
-    struct Own { MT a[5]; double r0, x; };
-    struct Cen { double r, pn, xi; };
-    const Ctx* c;
-    const double *s, *t, *p, *v, *dinv, *r0;
-    const MT* mat[5];
-    double *x, *rout, *pout, *qout;
-    double wx, ax, cx, sx, beta, om;
-    bool two_d;
-    double acc[4];
-    SPB6G_DEV void load(size_t i, Raw& o) const { o.s = s[i]; o.t = t[i]; o.p = p[i]; o.v = v[i]; o.d = dinv[i]; }
-    SPB6G_DEV void own(size_t i, Own& o) const {
-#pragma unroll
-        for (int m = 0; m < 5; m++) o.a[m] = mat[m][i];
-        o.r0 = r0[i];
-        o.x = x[i];
-    }
-    SPB6G_DEV double pn(const Raw& o) const { return (o.s - wx * o.t) + beta * (o.p - om * o.v); }
-    SPB6G_DEV double ph(const Raw& o) const { return o.d * pn(o); }
-    SPB6G_DEV double cen(const Raw& o, Cen& e) const {
-        e.r = o.s - wx * o.t;
-        e.pn = e.r + beta * (o.p - om * o.v);
-        e.xi = ax * (o.d * o.p + cx) + wx * (o.d * o.s + sx);
-        return o.d * e.pn;
-    }
-    SPB6G_DEV void out(size_t i, const Cen& e, const Own& o, double phS, double phW, double phC, double phE, double phN) {
-        const double q = spmv5<MT>(o.a, two_d, phS, phW, phC, phE, phN);
-        rout[i] = e.r;
-        pout[i] = e.pn;
-        qout[i] = q;
-        x[i] = o.x + e.xi;
-        acc[0] += e.pn;
-        acc[1] += o.r0 * q;
-        acc[2] += q;
-        acc[3] += e.r;
-    }
-};
-// Pass B: v = q + cc A1; s = r - alpha v; t = A (D^-1 s) + cs A1;
-// sums s^T s, t^T s, t^T t, r0^T s, r0^T t.
-template <class MT>
-struct PassB {
-    struct Raw { double r, q, a1, d; };
-    struct Own { MT a[5]; double r0; };
-    struct Cen { double v, s, a1; };
-    const Ctx* c;
-    const double *r, *q, *A1, *dinv, *r0;
-    const MT* mat[5];
-    double *vout, *sout, *tout;
-    double al, cc, cs;
-    bool two_d;
-    double acc[5];
-    SPB6G_DEV void load(size_t i, Raw& o) const { o.r = r[i]; o.q = q[i]; o.a1 = A1[i]; o.d = dinv[i]; }
-    SPB6G_DEV void own(size_t i, Own& o) const {
-#pragma unroll
-        for (int m = 0; m < 5; m++) o.a[m] = mat[m][i];
-        o.r0 = r0[i];
-    }
-    SPB6G_DEV double ph(const Raw& o) const { return o.d * (o.r - al * (o.q + cc * o.a1)); }
-    SPB6G_DEV double cen(const Raw& o, Cen& e) const {
-        e.v = o.q + cc * o.a1;
-        e.s = o.r - al * e.v;
-        e.a1 = o.a1;
-        return o.d * e.s;
-    }
-    SPB6G_DEV void out(size_t i, const Cen& e, const Own& o, double phS, double phW, double phC, double phE, double phN) {
-        const double u = spmv5<MT>(o.a, two_d, phS, phW, phC, phE, phN);
-        const double tv = u + cs * e.a1;
-        vout[i] = e.v;
-        sout[i] = e.s;
-        tout[i] = tv;
-        acc[0] += e.s * e.s;
-        acc[1] += tv * e.s;
-        acc[2] += tv * tv;
-        acc[3] += o.r0 * e.s;
-        acc[4] += o.r0 * tv;
-    }
-};
+#define PB_STRIPS_BEGIN                                                         \
+    for (int s_ = wid; s_ < sg.nstrips; s_ += nwarps) {                         \
+        const Strip st = strip_at(c.g, sg, s_);
+#define PB_STRIPS_END }
 
-// The whole BiCGStab solve (GMRES_Solver :752-794) in one persistent cooperative launch,
-// two passes per iteration.  Besides the A 1 identity of the four-pass kernels
-// (A M^-1 r = A (D^-1 r) + (1^T r / E) A 1), the quantities the reference forms from r
-// at the top of an iteration come from pass B's sums through exact identities,
-// r = s - omega t:  r0^T r = r0^T s - omega r0^T t and r^T r = s^T s - omega t^T s
-// (omega = t^T s / t^T t), so the x and r updates move into the next iteration's pass A
-// (the reference's dot products, summed in another order: the rounding of these scalars
-// differs).  Every sum is folded in a fixed order, so a solve is bitwise reproducible.
+// Three passes per iteration.  Besides the A 1 trick of the four-pass kernels
+// (A M^-1 r = A (D^-1 r) + (1^T r / E) A 1), the coarse coefficient of s is
+// formed from sums the first barrier already carries: 1^T s = 1^T r - alpha 1^T v
+// with 1^T v = 1^T q + cc 1^T A1, so t = A M^-1 s and its two inner products are
+// finished in the same pass as s (the reference sums s itself; the identity is
+// exact, the rounding of this one scalar differs).
 template <class MT>
-__global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol, int maxit) {
+__global__ void __launch_bounds__(PB_THREADS, 1) k_bicg_solve(Ctx c, double tol, int maxit) {
+    extern __shared__ double pb_smem[];
     const int n = c.n, nx = c.g.nx;
     const unsigned G = gridDim.x;
-    const int nwarps = G * RB_WARPS, wid = blockIdx.x * RB_WARPS + (threadIdx.x >> 5);
+    const int nwarps = G * PB_WARPS, wid = blockIdx.x * PB_WARPS + (threadIdx.x >> 5);
+    double* ws = pb_smem + (threadIdx.x >> 5) * PS_WARP;
     const StripGrid sg = strip_grid(c.g, nwarps);
     const bool two_d = c.g.ny > 1;
     GridBarrier* gb = c.gbar;
@@ -1143,7 +1108,7 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     double* __restrict__ bt = c.bt;
     double* __restrict__ dP = c.dP;
     auto slot = [&](int k) { return slots + (size_t)(k & 1) * PB_SLOT_Q * G; };
-    const int gtid = blockIdx.x * RB_THREADS + threadIdx.x, gstride = G * RB_THREADS;
+    const MT* const mat[5] = {diag<MT>(c, 0), diag<MT>(c, 1), diag<MT>(c, 2), diag<MT>(c, 3), diag<MT>(c, 4)};
 
     const NewtonScalars ns = *c.ns;
     const double Einv = (ns.E != 0.0 && isfinite(ns.E)) ? 1.0 / ns.E : 0.0;
@@ -1158,7 +1123,7 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     double la = 1.0, lc = 0.0;
     if (x0l) {
         double a5[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, t5[5];
-        for (int x = gtid; x < n; x += gstride) {
+        for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
             const int j = x / nx, i = x - j * nx;
             const Nbr nb = neighbours(c.g, i, j, x);
             const double u = spmv_row(c, nb, x, [&](int q) { return dinv[q] * (-c.G[q]) + cb; });
@@ -1187,9 +1152,9 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
         }
     }
     {
-    // set-up: x = x0, r = r0 = b - A x, p = v = 0; s = r and t = 0 for the first pass A (plain row loop)
+    // set-up: x = x0, r = r0 = b - A x, p = v = 0 (plain row loop, once per solve)
     double a4[4] = {0.0, 0.0, 0.0, 0.0}, t4[4];
-    for (int x = gtid; x < n; x += gstride) {
+    for (int x = blockIdx.x * PB_THREADS + threadIdx.x; x < n; x += G * PB_THREADS) {
         const int j = x / nx, i = x - j * nx;
         auto xv = [&](int q) { return dinv[q] * (-c.G[q]) + cb; };
         double r;
@@ -1207,8 +1172,6 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
         }
         br[x] = r;
         c.br0[x] = r;
-        bs[x] = r;
-        bt[x] = 0.0;
         c.bp[x] = 0.0;
         bv[x] = 0.0;
         a4[0] += r * r;
@@ -1218,83 +1181,129 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
     }
     if (!sync_fold<4>(a4, slot(bar++), G, gb, epoch, t4)) goto timeout;
     {
-        // reference scalars (rho, alpha, omega start at 1); those of the deferred x update start at 0
         double rho = 1.0, alpha = 1.0, omega = 1.0, cc = 0.0, cs = 0.0, ss = 0.0, ts = 0.0, tt = 0.0;
-        double ax = 0.0, wx = 0.0, cx = 0.0, sx = 0.0;
         const double bn = sqrt(ns.bb) + 1e-300;
-        double rr = t4[0], r0r = t4[0];
+        double rr = t4[0], r0r = t4[0], sr = t4[2];
         const double r0A1 = t4[1], sA1 = t4[3];
         int status = ns.fail ? BICG_FAIL : (sqrt(rr) <= tol * bn ? BICG_CONV : (r0r == 0 ? BICG_FAIL : BICG_RUNNING));
         int iters = 0, parity = 0;
-        bool half = false;
-        const MT* const mat[5] = {diag<MT>(c, 0), diag<MT>(c, 1), diag<MT>(c, 2), diag<MT>(c, 3), diag<MT>(c, 4)};
+        double a3[3], t3[3];
         while (status == BICG_RUNNING) {
             const double* p_old = parity ? c.tcp : c.bp;
             double* p_new = parity ? c.bp : c.tcp;
-            // pass A: the deferred x and r updates, p, q = A D^-1 p; sums 1^T p, r0^T q, 1^T q, 1^T r
-            double tA[4];
+            // pass 1: p = r + beta (p - omega v); q = A D^-1 p; sums 1^T p, r0^T q, 1^T q
             {
-                PassA<MT> op;
-                op.c = &c;
-                op.s = bs; op.t = bt; op.p = p_old; op.v = bv; op.dinv = dinv; op.r0 = c.br0;
-                for (int m = 0; m < 5; m++) op.mat[m] = mat[m];
-                op.x = dP; op.rout = br; op.pout = p_new; op.qout = bq;
-                op.wx = wx; op.ax = ax; op.cx = cx; op.sx = sx;
-                op.beta = (r0r / rho) * (alpha / omega);
-                op.om = omega;
-                op.two_d = two_d;
-                op.acc[0] = op.acc[1] = op.acc[2] = op.acc[3] = 0.0;
-                for (int s_ = wid; s_ < sg.nstrips; s_ += nwarps) reg_strip(c.g, strip_at(c.g, sg, s_), op);
-                if (!sync_fold<4>(op.acc, slot(bar++), G, gb, epoch, tA)) goto timeout;
+                const double beta = (r0r / rho) * (alpha / omega), om = omega;
+                const double* const hv[PS_HV] = {br, p_old, bv, dinv};
+                const double* const ex[1] = {c.br0};
+                auto pn = [&](const double* sp, int k) { return sp[k] + beta * (sp[34 + k] - om * sp[68 + k]); };
+                auto phf = [&](const double* sp, int k) { return sp[102 + k] * pn(sp, k); };
+                a3[0] = a3[1] = a3[2] = 0.0;
+                PB_STRIPS_BEGIN
+                    stencil_strip<MT, 1>(c.g, st, ws, hv, mat, ex, phf,
+                        [&](const MT* a, const double* e, const double* so, int k, double phS, double phW, double phC,
+                            double phE, double phN, int x) {
+                            const double p = pn(so, k);
+                            MT qm = 0;  // the SpMV row in the matrix precision
+                            qm += a[0] * (MT)phC;
+                            qm += a[32] * (MT)phW;
+                            qm += a[64] * (MT)phE;
+                            if (two_d) {
+                                qm += a[96] * (MT)phS;
+                                qm += a[128] * (MT)phN;
+                            }
+                            const double q = (double)qm;
+                            p_new[x] = p;
+                            bq[x] = q;
+                            a3[0] += p;
+                            a3[1] += e[0] * q;
+                            a3[2] += q;
+                        });
+                PB_STRIPS_END
             }
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
             rho = r0r;
-            cc = tA[0] * Einv;
-            alpha = rho / (tA[1] + cc * r0A1);
-            cs = (tA[3] - alpha * (tA[2] + cc * sA1)) * Einv;
-            // pass B: v, s, t = A D^-1 s + cs A1; sums s^T s, t^T s, t^T t, r0^T s, r0^T t
-            double tB[5];
+            cc = t3[0] * Einv;
+            alpha = rho / (t3[1] + cc * r0A1);
+            cs = (sr - alpha * (t3[2] + cc * sA1)) * Einv;
+            // pass 2: v = q + cc A1; s = r - alpha v; t = A D^-1 s + cs A1; sums s^T s, t^T s, t^T t
             {
-                PassB<MT> op;
-                op.c = &c;
-                op.r = br; op.q = bq; op.A1 = A1; op.dinv = dinv; op.r0 = c.br0;
-                for (int m = 0; m < 5; m++) op.mat[m] = mat[m];
-                op.vout = bv; op.sout = bs; op.tout = bt;
-                op.al = alpha; op.cc = cc; op.cs = cs;
-                op.two_d = two_d;
-                op.acc[0] = op.acc[1] = op.acc[2] = op.acc[3] = op.acc[4] = 0.0;
-                for (int s_ = wid; s_ < sg.nstrips; s_ += nwarps) reg_strip(c.g, strip_at(c.g, sg, s_), op);
-                if (!sync_fold<5>(op.acc, slot(bar++), G, gb, epoch, tB)) goto timeout;
+                const double al = alpha, ccv = cc, csv = cs;
+                const double* const hv[PS_HV] = {br, bq, A1, dinv};
+                auto sv = [&](const double* sp, int k) { return sp[k] - al * (sp[34 + k] + ccv * sp[68 + k]); };
+                auto phf = [&](const double* sp, int k) { return sp[102 + k] * sv(sp, k); };
+                a3[0] = a3[1] = a3[2] = 0.0;
+                PB_STRIPS_BEGIN
+                    stencil_strip<MT, 0>(c.g, st, ws, hv, mat, nullptr, phf,
+                        [&](const MT* a, const double*, const double* so, int k, double phS, double phW, double phC,
+                            double phE, double phN, int x) {
+                            const double v = so[34 + k] + ccv * so[68 + k];
+                            const double s = so[k] - al * v;
+                            MT um = 0;
+                            um += a[0] * (MT)phC;
+                            um += a[32] * (MT)phW;
+                            um += a[64] * (MT)phE;
+                            if (two_d) {
+                                um += a[96] * (MT)phS;
+                                um += a[128] * (MT)phN;
+                            }
+                            const double u = (double)um;
+                            const double tv = u + csv * so[68 + k];
+                            bv[x] = v;
+                            bs[x] = s;
+                            bt[x] = tv;
+                            a3[0] += s * s;
+                            a3[1] += tv * s;
+                            a3[2] += tv * tv;
+                        });
+                PB_STRIPS_END
+            }
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
+            ss = t3[0];
+            const bool half = sqrt(ss) <= tol * bn;
+            if (!half) {
+                ts = t3[1];
+                tt = t3[2];
+                omega = ts / tt;
+            }
+            // pass 3: x += alpha ph + omega sh; r = s - omega t; sums r^T r, r0^T r, 1^T r
+            a3[0] = a3[1] = a3[2] = 0.0;
+            if (half) {
+                const double al = alpha, ccv = cc;
+                const double* const rv[3] = {dinv, p_new, dP};
+                PB_STRIPS_BEGIN
+                    row_strip<3>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
+                        const double ph = sp[k] * sp[32 + k] + ccv;
+                        dP[x] = sp[64 + k] + al * ph;
+                    });
+                PB_STRIPS_END
+            } else {
+                const double al = alpha, om = omega, ccv = cc, csv = cs;
+                const double* const rv[6] = {dinv, p_new, bs, bt, dP, c.br0};
+                PB_STRIPS_BEGIN
+                    row_strip<6>(c.g, st, ws, rv, [&](const double* sp, int k, int x) {
+                        const double ph = sp[k] * sp[32 + k] + ccv;
+                        const double sh = sp[k] * sp[64 + k] + csv;
+                        dP[x] = sp[128 + k] + (al * ph + om * sh);
+                        const double r = sp[64 + k] - om * sp[96 + k];
+                        br[x] = r;
+                        a3[0] += r * r;
+                        a3[1] += sp[160 + k] * r;
+                        a3[2] += r;
+                    });
+                PB_STRIPS_END
             }
             iters += 1;
-            ss = tB[0];
-            if (sqrt(ss) <= tol * bn) {  // x += alpha ph (:777-780)
-                half = true;
-                status = BICG_CONV;
-                break;
-            }
-            ts = tB[1];
-            tt = tB[2];
-            omega = ts / tt;
-            // r = s - omega t: its inner products through the identities
-            const double rr_ = ss - omega * ts;
-            rr = rr_ > 0.0 ? rr_ : 0.0;
-            r0r = tB[3] - omega * tB[4];
-            ax = alpha; wx = omega; cx = cc; sx = cs;
-            if (!isfinite(ss) || !isfinite(ts) || !isfinite(tt) || !isfinite(rr_)) status = BICG_FAIL;
-            else if (sqrt(rr) <= tol * bn) status = BICG_CONV;
+            if (half) { status = BICG_CONV; break; }
+            if (!sync_fold<3>(a3, slot(bar++), G, gb, epoch, t3)) goto timeout;
+            rr = t3[0];
+            r0r = t3[1];
+            sr = t3[2];
+            if (sqrt(rr) <= tol * bn) status = BICG_CONV;
             else if (iters >= maxit) status = sqrt(rr) <= 1e3 * tol * bn ? BICG_CONV : BICG_FAIL;
             else if (r0r == 0) status = BICG_FAIL;
+            else if (!isfinite(rr)) status = BICG_FAIL;  // NaN never converges; the reference loops to GMRESiter and fails
             parity ^= 1;
-        }
-        // the last update of x: alpha ph (half step) or alpha ph + omega sh, p the last p
-        if (iters > 0) {
-            const double* pl = parity ? c.tcp : c.bp;  // parity flipped after the last full iteration
-            const double* pp = half ? (parity ? c.bp : c.tcp) : pl;
-            for (int x = gtid; x < n; x += gstride) {
-                const double ph = dinv[x] * pp[x] + (half ? cc : cx);
-                if (half) dP[x] = dP[x] + alpha * ph;
-                else dP[x] = dP[x] + (ax * ph + wx * (dinv[x] * bs[x] + sx));
-            }
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             BicgScalars& B = *c.bs_;
@@ -1308,18 +1317,23 @@ __global__ void __launch_bounds__(RB_THREADS, 1) k_bicg_solve(Ctx c, double tol,
 timeout:
     if (threadIdx.x == 0) c.bs_->status = BICG_TIMEOUT;
 }
+#undef PB_STRIPS_BEGIN
+#undef PB_STRIPS_END
 
 int bicg_solve_blocks(int device, int n) {
     int per_sm = 0, sms = 0, coop = 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_bicg_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(k_bicg_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM) != cudaSuccess)
+        return 0;
     int per_sm_f = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicg_solve<double>, RB_THREADS, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_bicg_solve<float>, RB_THREADS, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicg_solve<double>, PB_THREADS, PB_SMEM) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_bicg_solve<float>, PB_THREADS, PB_SMEM) != cudaSuccess)
         return 0;
     if (per_sm_f < per_sm) per_sm = per_sm_f;
     // about four rows per thread at least: small grids use fewer blocks (cheaper barriers)
-    const long want = ((long)n + 4L * RB_THREADS - 1) / (4L * RB_THREADS);
+    const long want = ((long)n + 4L * PB_THREADS - 1) / (4L * PB_THREADS);
     long G = (long)per_sm * sms;
     if (G > want) G = want;
     return G > 0 ? (int)G : 0;
@@ -1328,7 +1342,7 @@ int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int 
     void* args[] = {(void*)&c, (void*)&tol, (void*)&maxit};
     count(c, 1);
     const void* fn = c.prec ? (const void*)k_bicg_solve<float> : (const void*)k_bicg_solve<double>;
-    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(RB_THREADS), args, 0, st) == cudaSuccess ? 0 : -1;
+    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(PB_THREADS), args, PB_SMEM, st) == cudaSuccess ? 0 : -1;
 }
 
 // ============================================================ learned warm start (no counterpart in the reference)
