@@ -223,6 +223,27 @@ def main_profile_2d():
 SAT_CASES = (1, 3, 30, 31, 32)
 
 
+def schropff_profiles():
+    """The reference's archived runs of its cases 80-88 (data/Schropff2026_Riemann_problems/c<case>_<N>.dat,
+    the density column) and the relative L1 density errors it publishes for them (L1_table.md there),
+    to pin the exact Riemann solvers of oracle/exact_riemann.py: they must reproduce the table."""
+    import re
+
+    base = "data/Schropff2026_Riemann_problems"
+    out = {}
+    for f in sorted(os.listdir(os.path.join(REF_TREE, base))):
+        m = re.fullmatch(r"c(\d+)_(\d+)\.dat", f)
+        if m:
+            d = np.loadtxt(os.path.join(REF_TREE, base, f))
+            out[f"rho_c{m.group(1)}_{m.group(2)}"] = d[:, 5]
+    for line in open(os.path.join(REF_TREE, base, "L1_table.md")):
+        m = re.match(r"\|\s*(\d+)\s*\|[^|]*\|\s*(\d+)\s*\|\s*([0-9.eE+-]+)\s*\|", line)
+        if m:
+            out[f"pub_c{m.group(1)}_{m.group(2)}"] = np.float64(m.group(3))
+    np.savez_compressed(os.path.join(HERE, "ref_schropff_profiles.npz"), source=base, **out)
+    print("schropff profiles", len(out))
+
+
 def sat_tables():
     """The reference's own saturation table (its global SAT after build_sat) for the phase pairs of
     SAT_CASES, one archive: n, pcrit, vcrit, pmin, ln p[n], Tsat[n] per case."""
@@ -268,6 +289,9 @@ def main():
     if only == ["sat"]:
         sat_tables()
         return
+    if only == ["schropff"]:
+        schropff_profiles()
+        return
     if only == ["profile2d"]:
         main_profile_2d()
         return
@@ -295,6 +319,7 @@ def main():
     main_outputs()
     main_profile_2d()
     sat_tables()
+    schropff_profiles()
     for tag, path in (("archived_case5_N100", "data/SPB2009_4.3.1_water_air/water_air_N100_t240us.dat"),
                       ("archived_case87_N200", "data/Schropff2026_Riemann_problems/c87_200.dat")):
         d = np.loadtxt(os.path.join(REF_TREE, path))
