@@ -35,6 +35,17 @@ NVCC_FLAGS = [
 
 
 MG_VARIANT_SOURCES = ("spb6g_kernels.cu", "spb6g_flux.cu")
+# SPB6G_CONTRACT=1: compile the implicit-stage kernels (residual, FD Jacobian, final state, BiCGStab;
+# spb6g_kernels.cu) with FP multiply-add contraction -- a measured variant, not the default: with it
+# the device no longer rounds like the reference's x86-64 build (the one-step 1D test is no longer
+# bitwise); the explicit predictor (spb6g_flux.cu) keeps -fmad=false either way.
+CONTRACT_SOURCES = ("spb6g_kernels.cu",)
+
+
+def _flags(src: str) -> list[str]:
+    if os.environ.get("SPB6G_CONTRACT") == "1" and os.path.basename(src) in CONTRACT_SOURCES:
+        return [f for f in NVCC_FLAGS if f != "-fmad=false"] + ["-fmad=true"]
+    return NVCC_FLAGS
 
 
 def _nvcc() -> str:
@@ -67,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     jobs += [(src, os.path.join(objdir, os.path.basename(src) + ".mg.o"), ["-DSPB6G_MG=1", "-Dspb6g=spb6g_mg"])
              for src in sources() if os.path.basename(src) in MG_VARIANT_SOURCES]
     for src, obj, defs in jobs:
-        cmd = [_nvcc(), *NVCC_FLAGS, *defs, "-I", INCLUDE, "-dc", "-c", src, "-o", obj]
+        cmd = [_nvcc(), *_flags(src), *defs, "-I", INCLUDE, "-dc", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
