@@ -65,6 +65,13 @@ FLUX_BYTES = {True: (168, 232), False: (152, 216)}
 # on this workload: k_bicg_solve moved 1.93 GB for 11 iterations of 1,048,576 rows
 # (profiles/k_bicg_solve_bubbles1024.md).
 DRAM_BYTES = {"linear": 1.934e9 / (11 * 1048576)}
+# The same from the --set full captures on the low-Mach field 2048^2 (profiles/k_bicg_solve_lowmach2048.md,
+# profiles/k_flux_lowmach2048.md): the BiCGStab solve moved 39.09 GB in 36 iterations of 4,194,304 rows,
+# the fused flux kernel 1.412 GB for 4,194,304 cells.
+DRAM_BYTES_BY_WORKLOAD = {
+    "lowmach2048": {"linear": 39.091e9 / (36 * 4194304), "explicit": 1.412e9 / 4194304},
+    "bubbles1024": {"linear": 1.934e9 / (11 * 1048576)},
+}
 KERNEL_OF = {"linear": "k_bicg_solve (BiCGStab solve, one launch per Newton iteration)",
              "jacobian": "k_jac_entries", "residual": "k_residual", "explicit": "k_flux"}
 
@@ -567,17 +574,20 @@ def counts(r: dict) -> dict:
             "newton_iters_per_stage": d["newton_it"] / max(d["stages"], 1), **d}
 
 
-def rooflines(r: dict, n: int, two_d: bool) -> dict:
+def rooflines(r: dict, n: int, two_d: bool, workload: str = "") -> dict:
     """Algorithmic-byte rooflines (SURVEY-defined bytes per unit) of the BiCGStab solve, the fused
     flux kernel and the whole step, from the window's CUDA-event group times and counts."""
     peak, peak_kind = peaks()
     g, d = r["groups"], r["d"]
+    dram = DRAM_BYTES_BY_WORKLOAD.get(workload, {})
     out = {}
     if g.get("linear", (0, 0))[1] > 0 and d["bicg_it"] > 0:
         units = d["bicg_it"] * n
         ach = BICG_BYTES_PER_ROW_ITER * units / (g["linear"][0] / 1e3) / 1e9
         out["bicg"] = {"bound": "hbm", "kernel": KERNEL_OF["linear"], "achieved": ach, "peak": peak, "unit": "GB/s",
-                       "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
+                       "frac": ach / peak,
+                       "traffic": dram["linear"] * units / g["linear"][1] if "linear" in dram else None,
+                       "peak_source": peak_kind,
                        "alg_bytes_per_unit": BICG_BYTES_PER_ROW_ITER, "unit_of_work": "row x BiCGStab iteration",
                        "alg_bytes_per_launch": BICG_BYTES_PER_ROW_ITER * units / g["linear"][1]}
     if g.get("explicit", (0, 0))[1] > 0:
@@ -589,7 +599,8 @@ def rooflines(r: dict, n: int, two_d: bool) -> dict:
         alg = (first * b1 + later * b2) * n
         ach = alg / (g["explicit"][0] / 1e3) / 1e9
         out["flux"] = {"bound": "hbm", "kernel": KERNEL_OF["explicit"], "achieved": ach, "peak": peak, "unit": "GB/s",
-                       "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
+                       "frac": ach / peak, "traffic": dram["explicit"] * n if "explicit" in dram else None,
+                       "peak_source": peak_kind,
                        "alg_bytes_per_cell": [b1, b2], "alg_bytes_per_launch": alg / g["explicit"][1]}
     # whole step: every group's algorithmic bytes over the whole window's device time
     tot = 0.0
@@ -683,7 +694,7 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
         }
     e2e = None if args.no_e2e else e2e_run(case, args, local_rank, dist, mlp, norm,
                                            {k: d[k] for k in ("steps", "rejects", "newton_it", "bicg_it")})
-    roofs = rooflines(main_r, n, two_d)
+    roofs = rooflines(main_r, n, two_d, args.workload)
     groups = main_r["groups"]
     shares = {g: {"ms": round(v[0], 3), "launch_groups": int(v[1]), "share": round(v[0] / main_r["ms"], 4)}
               for g, v in groups.items()}
