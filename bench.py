@@ -186,17 +186,18 @@ def run_reference_batch(args, case, rank: int):
 
 
 def run_batch(args, case, rank: int, world: int, local_rank: int, dist):
-    """Batched form: every grid advances `steps` steps in one persistent launch (after `warmup`
-    untimed steps in another); value = sum of cells x accepted steps / device time."""
+    """Batched form: every grid advances `steps` steps in one replay of the persistent launches (one
+    per block size, concurrent; after `warmup` untimed steps in another); value = sum of cells x
+    accepted steps / device time."""
     import torch
 
     from diffusionimex_b200 import BatchSolver
 
     cs = case["batch"]
     b = BatchSolver(cs, device=local_rank)
-    threads, tile, _ = b.autotune(2)
     if args.warmup:
         b.advance(args.warmup)
+    threads, tile, _ = b.autotune(5)  # from the warmed-up state, restored after every trial
     s0 = [b.instance(i).stats() for i in range(len(cs))]
     torch.cuda.synchronize()
     if dist:
@@ -233,10 +234,10 @@ def run_batch(args, case, rank: int, world: int, local_rank: int, dist):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / max(args.steps, 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": case["workload"], "instances": len(cs), "cells": cells, "seed": 0,
-                           "launch": {"threads_per_grid": threads, "flux_tile": tile}},
+                           "launch": {"threads_largest_grid": threads, "flux_tile": tile}},
                 "rejects": sum(q["rejects"] - p["rejects"] for p, q in zip(s0, s1)),
                 "newton_iters": sum(q["newton_it"] - p["newton_it"] for p, q in zip(s0, s1)),
-                "gpu_launches": 1, "clocks": clocks, "e2e": e2e}
+                "gpu_launches": b.launches(), "clocks": clocks, "e2e": e2e}
         print(json.dumps(line))
     b.close()
 

@@ -194,7 +194,7 @@ int launch_bicg_solve(const Ctx& c, cudaStream_t st, double tol, int maxit, int 
 void launch_thomas(const Ctx& c, cudaStream_t st);
 // batched form: `count` instances, `nsteps` time steps each, one block of `threads` per instance,
 // flux tiles of width tw (128 or 256); one persistent launch
-int launch_batch(BatchInst* insts, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st);
+int launch_batch(BatchInst* insts, const int* list, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st);
 int batch_max_blocks(int threads, int tw, int device);
 // learned warm start: BF16 feature rows (n x 64), dP = sdt (Prate + y tscale), and after a converged
 // stage the training target (if t) and the new pressure rate

@@ -2087,12 +2087,13 @@ SPB6G_DEV int b_step(BatchShared& s, BatchInst& B, unsigned char* fsm) {  // mai
     __syncthreads();
     return SPB6G_OK;
 }
+// Blocks take the grids list[0..count) (all of insts when list is NULL) in order.
 template <int TW>
-__global__ void __launch_bounds__(256) k_batch(BatchInst* insts, int count, int nsteps) {
+__global__ void __launch_bounds__(256) k_batch(BatchInst* insts, const int* list, int count, int nsteps) {
     extern __shared__ __align__(16) unsigned char batch_smem[];
     __shared__ BatchShared s;
-    for (int b = blockIdx.x; b < count; b += gridDim.x) {
-        BatchInst& B = insts[b];
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        BatchInst& B = insts[list ? list[k] : k];
         __syncthreads();
         if (threadIdx.x == 0) s.c = B.c;
         __syncthreads();
@@ -2122,10 +2123,10 @@ int batch_max_blocks(int threads, int tw, int device) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
     return per_sm * sms;
 }
-int launch_batch(BatchInst* insts, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st) {
+int launch_batch(BatchInst* insts, const int* list, int count, int nsteps, int threads, int tw, int grid, cudaStream_t st) {
     const size_t smem = flux_tile_bytes_1d(tw);
-    if (tw == 128) k_batch<128><<<grid, threads, smem, st>>>(insts, count, nsteps);
-    else k_batch<256><<<grid, threads, smem, st>>>(insts, count, nsteps);
+    if (tw == 128) k_batch<128><<<grid, threads, smem, st>>>(insts, list, count, nsteps);
+    else k_batch<256><<<grid, threads, smem, st>>>(insts, list, count, nsteps);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

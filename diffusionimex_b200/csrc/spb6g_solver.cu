@@ -5,6 +5,7 @@
 // (:799-904) decision for decision.  All field data stays on the device; the
 // host reads back only the scalars a decision needs (residual norm, step
 // criterion, BiCGStab status), through one pinned record per sync point.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1198,8 +1199,15 @@ struct spb6g_batch {
     BatchInst* dev = nullptr;
     cudaStream_t st = nullptr;
     int threads = 128, tw = 256;
-    cudaGraphExec_t graph = nullptr;  // the persistent launch for (graph_steps, graph_threads, graph_tw)
+    cudaGraphExec_t graph = nullptr;  // the persistent launches for (graph_steps, graph_threads, graph_tw)
     int graph_steps = -1, graph_threads = 0, graph_tw = 0;
+    // block-size plan for graph_threads: grids grouped by block size (class c: block size
+    // cls[c], grids order[off[c] .. off[c+1]), longest first); one launch per class
+    std::vector<int> cls, off, order;
+    int* dorder = nullptr;
+    std::vector<cudaStream_t> side;  // one stream per class after the first
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
 };
 
 namespace {
@@ -1237,23 +1245,83 @@ void batch_unpack(spb6g_batch* b) {
         b->status[i] = B.status;
     }
 }
-int batch_grid(spb6g_batch* b, int threads, int tw) {
-    int g = batch_max_blocks(threads, tw, b->device);
-    if (g <= 0) return 0;
-    return g < (int)b->inst.size() ? g : (int)b->inst.size();
+// Block size of every grid: threads in proportion to its cells (a multiple of 32, at least
+// 32, at most `threads`), so that every block has about the same cells per thread -- the
+// launch lasts as long as its slowest grid.  The cells per thread are the fewest for which
+// all blocks are resident at once (their threads within 15/16 of the device's thread slots
+// at the kernel's register count), and at least the largest grid's cells over `threads`.
+// Grids are grouped by block size, each group longest first; the groups run as concurrent
+// launches.
+int batch_plan(spb6g_batch* b, int threads, int tw) {
+    const int count = (int)b->inst.size();
+    long nmax = 1;
+    for (spb6g_solver* s : b->inst) nmax = std::max(nmax, (long)s->n);
+    auto block_of = [&](long n, long per_thread) {
+        const long t = (n + 32L * per_thread - 1) / (32L * per_thread) * 32L;
+        return (int)std::min<long>(std::max<long>(t, 32L), threads);
+    };
+    const long slots = (long)batch_max_blocks(256, tw, b->device) * 256L * 15L / 16L;
+    long per_thread = (nmax + threads - 1) / threads;
+    for (; per_thread < nmax; per_thread++) {
+        long total = 0;
+        for (spb6g_solver* s : b->inst) total += block_of(s->n, per_thread);
+        if (total <= slots) break;
+    }
+    std::vector<int> bs(count);
+    for (int i = 0; i < count; i++) bs[i] = block_of(b->inst[i]->n, per_thread);
+    b->order.resize(count);
+    for (int i = 0; i < count; i++) b->order[i] = i;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+        return bs[x] != bs[y] ? bs[x] > bs[y] : b->inst[x]->n > b->inst[y]->n;
+    });
+    b->cls.clear();
+    b->off.clear();
+    for (int k = 0; k < count; k++)
+        if (k == 0 || bs[b->order[k]] != bs[b->order[k - 1]]) {
+            b->cls.push_back(bs[b->order[k]]);
+            b->off.push_back(k);
+        }
+    b->off.push_back(count);
+    for (int bsz : b->cls)
+        if (batch_max_blocks(bsz, tw, b->device) <= 0) return SPB6G_UNSUPPORTED;
+    while (b->side.size() + 1 < b->cls.size()) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t e = nullptr;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        b->side.push_back(st);
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->join.push_back(e);
+    }
+    if (!b->fork) CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    CK(cudaMemcpy(b->dorder, b->order.data(), (size_t)count * sizeof(int), cudaMemcpyHostToDevice));
+    return SPB6G_OK;
 }
 // One persistent launch of nsteps steps per instance (a captured CUDA graph, rebuilt when the
 // step count or the launch shape changes), device time in *ms if not NULL.
 int batch_run(spb6g_batch* b, int nsteps, int threads, int tw, float* ms) {
-    const int grid = batch_grid(b, threads, tw);
-    if (grid <= 0) return SPB6G_UNSUPPORTED;
-    batch_pack(b);
-    CK(cudaMemcpyAsync(b->dev, b->host.data(), b->host.size() * sizeof(BatchInst), cudaMemcpyHostToDevice, b->st));
     if (!b->graph || b->graph_steps != nsteps || b->graph_threads != threads || b->graph_tw != tw) {
         if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+        b->graph_steps = -1;
+        const int prc = batch_plan(b, threads, tw);
+        if (prc != SPB6G_OK) return prc;
+    }
+    batch_pack(b);
+    CK(cudaMemcpyAsync(b->dev, b->host.data(), b->host.size() * sizeof(BatchInst), cudaMemcpyHostToDevice, b->st));
+    if (!b->graph) {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-        const int lrc = launch_batch(b->dev, (int)b->inst.size(), nsteps, threads, tw, grid, b->st);
+        int lrc = 0;
+        const int ncls = (int)b->cls.size();
+        if (ncls > 1) lrc |= cudaEventRecord(b->fork, b->st) != cudaSuccess;
+        for (int c = 1; c < ncls; c++) lrc |= cudaStreamWaitEvent(b->side[c - 1], b->fork, 0) != cudaSuccess;
+        for (int c = 0; c < ncls; c++) {
+            const int n_c = b->off[c + 1] - b->off[c];
+            lrc |= launch_batch(b->dev, b->dorder + b->off[c], n_c, nsteps, b->cls[c], tw, n_c, c ? b->side[c - 1] : b->st) != 0;
+        }
+        for (int c = 1; c < ncls; c++) {
+            lrc |= cudaEventRecord(b->join[c - 1], b->side[c - 1]) != cudaSuccess;
+            lrc |= cudaStreamWaitEvent(b->st, b->join[c - 1], 0) != cudaSuccess;
+        }
         CK(cudaStreamEndCapture(b->st, &g));
         if (lrc) { cudaGraphDestroy(g); return SPB6G_CUDA_ERROR; }
         CK(cudaGraphInstantiate(&b->graph, g, 0));
@@ -1299,7 +1367,8 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     b->host.resize(count);
     b->status.assign(count, SPB6G_OK);
     if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc((void**)&b->dev, (size_t)count * sizeof(BatchInst)) != cudaSuccess) {
+        cudaMalloc((void**)&b->dev, (size_t)count * sizeof(BatchInst)) != cudaSuccess ||
+        cudaMalloc((void**)&b->dorder, (size_t)count * sizeof(int)) != cudaSuccess) {
         spb6g_batch_destroy(b);
         return SPB6G_CUDA_ERROR;
     }
@@ -1311,6 +1380,10 @@ void spb6g_batch_destroy(spb6g_batch* b) {
     cudaSetDevice(b->device);
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->dev) cudaFree(b->dev);
+    if (b->dorder) cudaFree(b->dorder);
+    for (cudaStream_t st : b->side) cudaStreamDestroy(st);
+    for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->st) cudaStreamDestroy(b->st);
     for (spb6g_solver* s : b->inst) spb6g_destroy(s);
     delete b;
@@ -1323,8 +1396,12 @@ int spb6g_batch_status(spb6g_batch* b, int i) {
     if (!b || i < 0 || i >= (int)b->inst.size()) return SPB6G_BAD_ARG;
     return b->status[i];
 }
+int spb6g_batch_launches(spb6g_batch* b) {
+    if (!b) return SPB6G_BAD_ARG;
+    return b->graph && b->graph_threads == b->threads && b->graph_tw == b->tw ? (int)b->cls.size() : 0;
+}
 int spb6g_batch_set_shape(spb6g_batch* b, int threads, int tile) {
-    if (!b || (threads != 64 && threads != 128 && threads != 256) || (tile != 128 && tile != 256)) return SPB6G_BAD_ARG;
+    if (!b || threads < 32 || threads > 256 || threads % 32 != 0 || (tile != 128 && tile != 256)) return SPB6G_BAD_ARG;
     b->threads = threads;
     b->tw = tile;
     return SPB6G_OK;
@@ -1358,7 +1435,7 @@ int spb6g_batch_autotune(spb6g_batch* b, int nsteps, int* threads_out, int* tile
     }
     int bt = b->threads, bw = b->tw;
     float bms = INFINITY;
-    for (int threads : {64, 128, 256})
+    for (int threads : {64, 96, 128, 256})
         for (int tw : {128, 256}) {
             float ms = 0;
             const int rc = batch_run(b, nsteps, threads, tw, &ms);

@@ -129,6 +129,7 @@ def library() -> ctypes.CDLL:
         "spb6g_batch_set_shape": (I, [P, I, I]),
         "spb6g_batch_advance": (I, [P, I, P]),
         "spb6g_batch_autotune": (I, [P, I, P, P, P]),
+        "spb6g_batch_launches": (I, [P]),
         "spb6g_set_feature_norm": (I, [P, P]),
         "spb6g_set_warmstart": (I, [P, P]),
         "spb6g_set_warmstart_mode": (I, [P, I]),
@@ -510,6 +511,10 @@ class BatchSolver:
 
     def status(self, i: int) -> int:
         return self.lib.spb6g_batch_status(self.h, i)
+
+    def launches(self) -> int:
+        """Kernel launches of one advance under the current shape (one per block size)."""
+        return self.lib.spb6g_batch_launches(self.h)
 
     def close(self):
         if getattr(self, "h", None):

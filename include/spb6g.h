@@ -320,9 +320,9 @@ int spb6g_dump_count(spb6g_solver* s, int64_t* count);
 
 /* ---------------------------------------------------------------------------
  * Batched form (no counterpart in the reference): independent 1D grids (ny = 1,
- * non-periodic, so the Thomas path) advanced together in one persistent launch --
- * one thread block per grid runs that grid's whole time loop -- replayed from a
- * captured CUDA graph.  Each grid is an ordinary solver handle
+ * non-periodic, so the Thomas path) advanced together by persistent launches -- one
+ * thread block per grid runs that grid's whole time loop, one launch per block size,
+ * the launches concurrent -- replayed from a captured CUDA graph.  Each grid is an ordinary solver handle
  * (spb6g_batch_instance) for upload, initial pressure, download and statistics. */
 typedef struct spb6g_batch spb6g_batch;
 int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out);
@@ -330,13 +330,19 @@ void spb6g_batch_destroy(spb6g_batch* b);
 spb6g_solver* spb6g_batch_instance(spb6g_batch* b, int i);
 /* Status of grid i after the last advance (SPB6G_OK, or the error that stopped it). */
 int spb6g_batch_status(spb6g_batch* b, int i);
-/* Launch shape: threads per grid (64, 128, 256) and flux tile width (128, 256). */
+/* Launch shape: block size of the largest grid (a multiple of 32 from 32 to 256) and flux
+ * tile width (128, 256).  Every other grid gets a block size in proportion to its cells
+ * (rounded up to a multiple of 32, at least 32); grids of one block size form one launch,
+ * longest first, and the launches run concurrently. */
 int spb6g_batch_set_shape(spb6g_batch* b, int threads, int tile);
 /* nsteps time steps of every grid (fewer for a grid that reaches its t_end); device time
  * of the launch in *ms if not NULL.  Returns the first grid's error, if any. */
 int spb6g_batch_advance(spb6g_batch* b, int nsteps, float* ms);
-/* Times nsteps steps with every launch shape from the current state (restored after each
- * trial) and keeps the fastest. */
+/* Kernel launches of one advance under the current shape (one per block size); 0 before the
+ * first advance under it, or a negative status. */
+int spb6g_batch_launches(spb6g_batch* b);
+/* Times nsteps steps with every launch shape (largest block 64, 96, 128, 256 x tile 128, 256)
+ * from the current state (restored after each trial) and keeps the fastest. */
 int spb6g_batch_autotune(spb6g_batch* b, int nsteps, int* threads, int* tile, float* best_ms);
 
 /* Human-readable status name. */

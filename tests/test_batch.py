@@ -22,12 +22,16 @@ def _single(c, steps):
     return U, P, pref, st
 
 
-def test_batch_matches_single_grid_runs():
+@pytest.mark.parametrize("threads,tile", [(128, 256), (96, 128), (32, 128)])
+def test_batch_matches_single_grid_runs(threads, tile):
+    """`threads` is the block size of the largest grid; the others get block sizes in proportion
+    to their cells (multiples of 32), one concurrent launch per block size -- here 1 to 4 of them."""
     cs = cases.riemann_batch(count=10, seed=3, nmin=64, nmax=600)
     b = BatchSolver(cs)
-    b.set_shape(128, 256)
+    b.set_shape(threads, tile)
     b.advance(6)
     b.advance(4)  # a second launch continues from the first
+    assert 1 <= b.launches() <= threads // 32
     for i, c in enumerate(cs):
         assert b.status(i) == 0
         v = b.instance(i)
@@ -45,7 +49,7 @@ def test_autotune_restores_the_state_and_keeps_a_shape():
     cs = cases.riemann_batch(count=6, seed=4, nmin=64, nmax=300)
     b = BatchSolver(cs)
     threads, tile, ms = b.autotune(2)
-    assert threads in (64, 128, 256) and tile in (128, 256) and ms > 0
+    assert threads in (64, 96, 128, 256) and tile in (128, 256) and ms > 0
     b.advance(5)
     for i, c in enumerate(cs):
         U, P, _, st = _single(c, 5)
