@@ -78,7 +78,8 @@ struct spb6g_solver {
     double* rate_sc = nullptr;          // RMS of Prate (device scalar)
     bool rate_ready = false;            // a stage has converged since the tracking began (R exists)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
-    int warm_mode = 3;                  // 1: learned Newton start, 2: learned first BiCGStab iterate, 3: both
+    int warm_mode = 7;                  // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
+                                        // 4 the last Newton correction as the next solve's first iterate
     int warm_smooth = 0;                // radius of the box average of the network's output (0: none)
     float* ytmp = nullptr;              // scratch of the smoothing
     double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
@@ -353,6 +354,9 @@ int newton(spb6g_solver* s, double& resfinal) {
     const bool jreuse = s->cfg.jreuse != 0;
     double ratio = 1.0, lamprev = 1.0;
     bool fresh = false;
+    // mode bit 4: from the second solve of the stage on, the last Newton correction dP (the last
+    // solve's solution, still in dP) is the first iterate's candidate, combined with M^-1 b the same way
+    const bool hist_x0 = s->warm && (s->warm_mode & 4) && !tri && s->bicg_G > 0;
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
         if (s->verbose >= 3) fprintf(stderr, "    newton it %d res %.3e\n", it, res);
@@ -384,6 +388,10 @@ int newton(spb6g_solver* s, double& resfinal) {
                 CK(cudaMemsetAsync(c.gbar, 0, sizeof(GridBarrier), s->st));
                 Ctx cl = c;
                 cl.x0l = (x0_pending && it == 0) ? s->x0buf : nullptr;
+                if (hist_x0 && it > 0) {
+                    CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+                    cl.x0l = s->x0buf;
+                }
                 if (launch_bicg_solve(cl, s->st, s->cfg.bicg_tol, s->cfg.bicg_iter, s->bicg_G) != 0) return SPB6G_CUDA_ERROR;
                 if (sync_read(s, true)) return SPB6G_CUDA_ERROR;
                 if (cl.x0l && s->pin->bs.x0_learned) s->stats.learned_x0++;
@@ -1156,7 +1164,7 @@ int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
     return SPB6G_OK;
 }
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode) {
-    if (!s || mode < 1 || mode > 3) return SPB6G_BAD_ARG;
+    if (!s || mode < 1 || mode > 7) return SPB6G_BAD_ARG;
     s->warm_mode = mode;
     return SPB6G_OK;
 }

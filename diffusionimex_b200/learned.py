@@ -179,7 +179,7 @@ def train_mlp(X, T, steps: int = 3000, batch: int = 1 << 20, lr: float = 1e-3, s
     return m, hist
 
 
-def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 3,
+def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 7,
              smooth: int = 0) -> tuple:
     """Advance `warmup` untimed steps, then `steps` timed ones; counts and device time."""
     torch = _torch()

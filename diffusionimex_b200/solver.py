@@ -418,10 +418,11 @@ class Solver:
         a = (ctypes.c_double * self.NORM_LEN)(*[float(v) for v in norm])
         self._check(self.lib.spb6g_set_feature_norm(self.h, a), "spb6g_set_feature_norm")
 
-    def set_warmstart(self, mlp, mode: int = 3, smooth: int = 0):
-        """mode 1: learned Newton start (the guess of smallest residual among the plain guess, the
-        extrapolation and the network's); 2: learned first BiCGStab iterate; 3: both.  smooth: radius
-        of the box average of the network's output (0: none)."""
+    def set_warmstart(self, mlp, mode: int = 7, smooth: int = 0):
+        """mode bits -- 1: learned Newton start (the guess of smallest residual among the plain guess,
+        the extrapolation and the network's); 2: learned first BiCGStab iterate; 4: the last Newton
+        correction as the first iterate's candidate of the stage's later solves.  smooth: radius of
+        the box average of the network's output (0: none)."""
         self._warm = mlp
         self._check(self.lib.spb6g_set_warmstart(self.h, mlp.handle if mlp is not None else None), "spb6g_set_warmstart")
         if mlp is not None:

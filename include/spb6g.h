@@ -297,14 +297,15 @@ int spb6g_mlp_last_loss(spb6g_mlp* m, void* stream, float* loss_sum);
  * converged stage).  Setting it also starts tracking R. */
 int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
 /* m != NULL: every stage predicts its pressure P_start + dts (R + sigma MLP(features)).
- * Mode bit 1 (spb6g_set_warmstart_mode; 3 by default): Newton starts from the guess of
+ * Mode bit 1 (spb6g_set_warmstart_mode; 7, every bit, by default): Newton starts from the guess of
  * smallest residual norm among the plain guess (the previous stage's pressure), the
  * extrapolation P_start + dts R (the network's zero output) and the network's guess.  Mode
  * bit 2: when the network's guess is not the start, the first BiCGStab solve of the stage
  * starts from x0 = a M^-1 b + c dP, dP the network's step from the start and (a, c)
  * minimising ||b - A x0||, when that residual is below 0.99 of the plain start's
- * (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.  Newton and BiCGStab keep their
- * tolerances.  NULL: off. */
+ * (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.  Mode bit 4: every later solve of the
+ * stage takes the last Newton correction as that candidate dP.  Newton and BiCGStab keep
+ * their tolerances.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
 /* Radius r (0: none, the default; at most 64 and below nx, ny) of a separable box average of the

@@ -4,7 +4,8 @@ The network predicts each stage's pressure P_start + dts (R + sigma y), R the pr
 of the last converged stage and sigma its RMS.  The solver starts Newton from the guess of
 smallest residual norm among the plain guess, the extrapolation (y = 0) and the network's
 guess; when the network's guess is not the start, its step may seed the first BiCGStab
-iterate, in a least-squares combination that never has the larger initial residual.
+iterate, and the last Newton correction the stage's later ones, in a least-squares combination
+that never has the larger initial residual.
 Newton and BiCGStab keep their tolerances, so every run must reach the plain run's solution: L1(p) against the plain FP64 solve at
 most 1e-8 relative (the learned form's bar).  The last test trains a network on other
 seeds of the low-Mach field and records what it gains over the plain guess on seed 0."""
@@ -31,7 +32,7 @@ def lowmach(seed: int) -> dict:
     return dict(cases.lowmach_bubbles(N, seed=seed, nbub=4), newton_tol=1e-12, bicg_tol=1e-12)
 
 
-def _run(case, steps, warmup, mlp=None, norm=None, mode=3):
+def _run(case, steps, warmup, mlp=None, norm=None, mode=7):
     from diffusionimex_b200 import learned
 
     return learned.run_case(case, steps, warmup, mlp=mlp, norm=norm, mode=mode)
