@@ -560,7 +560,7 @@ def timed_window(case: dict, args, local_rank: int, dist, mlp=None, norm=None, z
     st1 = s.stats()
     out = {"ms": ms, "launches": s.kernel_launches() - l0, "groups": s.timing(), "clocks": clocks,
            "d": {k: st1[k] - st0[k] for k in ("steps", "rejects", "stages", "newton_it", "bicg_it", "learned",
-                                              "learned_x0", "extrapolated")}}
+                                              "learned_x0", "extrapolated", "extrapolated2", "combined", "refined")}}
     s.timing(False)
     if case.get("learned"):
         P, pref = s.pressure()

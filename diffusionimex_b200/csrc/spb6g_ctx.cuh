@@ -201,7 +201,16 @@ int batch_max_blocks(int threads, int tw, int device);
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
 // base_extrap = 0: dP = sdt (R + sigma y) from the stage's starting pressure; 1: dP = sdt sigma y from
 // the extrapolated pressure P_start + sdt R; y = null: the extrapolation dP = sdt R
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, int base_extrap);
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_y);
+// residual vectors of the residual-minimising start (g[0] at the plain start, g[j] at candidate j)
+constexpr int GRAM_Q = 9;
+struct GramIn {
+    const double* g[4];
+    int base[4];
+    int K;
+};
+int launch_gram(const Ctx& c, cudaStream_t st, const GramIn& in, double* part, double* out);
+void launch_jacobi_dir(const Ctx& c, cudaStream_t st, double coef);
 void launch_rate(const Ctx& c, cudaStream_t st, const double* P0, double itscale, float* t);
 // separable box average of radius r (0 < r <= nx, ny) of y, in place (tmp: n floats)
 void launch_smooth(const Ctx& c, cudaStream_t st, float* y, float* tmp, int r);

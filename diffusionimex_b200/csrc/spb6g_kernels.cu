@@ -1408,18 +1408,83 @@ void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void*
 // Step towards a predicted pressure.  The network predicts how far the stage's pressure
 // rate departs from the last stage's, in units of sigma: the learned guess is
 // P_start + sdt (R + sigma y), the extrapolation (y = 0) P_start + sdt R.
-__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale, int base_extrap) {
+// Step from the current start to a candidate: dP = sdt (a_r R + a_q (R - R2) + a_y sigma y), R the
+// pressure rate of the last converged stage and R2 that of the one before.
+__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale, double a_r, double a_q, double a_y) {
     const double sig = rate_scale(c, tscale);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double r = c.Prate ? c.Prate[x] : 0.0;
-        const double d = y ? (double)y[x] * sig : 0.0;
-        c.dP[x] = c.sdt * (base_extrap ? d : r + d);
+        const double r2 = c.Prate2 ? c.Prate2[x] : r;
+        const double d = y ? a_y * (double)y[x] * sig : 0.0;
+        c.dP[x] = c.sdt * (a_r * r + a_q * (r - r2) + d);
     }
 }
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, int base_extrap) {
-    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, base_extrap);
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_y) {
+    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, a_r, a_q, a_y);
     count(c, 1);
 }
+// Jacobi step on the nonlinear residual with the diagonal of the last Jacobian built:
+// dP = coef D^-1 (-G).
+__global__ void k_jacobi_dir(Ctx c, double coef) {
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x)
+        c.dP[x] = coef * (c.dinv[x] * (-c.G[x]));
+}
+void launch_jacobi_dir(const Ctx& c, cudaStream_t st, double coef) {
+    k_jacobi_dir<<<blocks_for(c.n), TPB, 0, st>>>(c, coef);
+    count(c, 1);
+}
+// Inner products of the residual-minimising start: with g[0] the residual at the plain start and
+// w_j = g[j] - g[base_j] (j = 1..K, K <= 3) the residual changes along the candidate directions,
+// the Gram matrix <w_j, w_k> (j <= k, row by row) and <w_j, g[0]>; per-block partials, folded by
+// k_gram_fold in block order.
+__global__ void __launch_bounds__(RED_THREADS) k_gram(int n, GramIn in, double* __restrict__ part) {
+    __shared__ double sh[GRAM_Q * 32];
+    double acc[GRAM_Q];
+#pragma unroll
+    for (int q = 0; q < GRAM_Q; q++) acc[q] = 0.0;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+        double w[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < in.K; j++) w[j] = in.g[j + 1][x] - in.g[in.base[j + 1]][x];
+        const double g0 = in.g[0][x];
+        acc[0] += w[0] * w[0];
+        acc[1] += w[0] * w[1];
+        acc[2] += w[0] * w[2];
+        acc[3] += w[1] * w[1];
+        acc[4] += w[1] * w[2];
+        acc[5] += w[2] * w[2];
+        acc[6] += w[0] * g0;
+        acc[7] += w[1] * g0;
+        acc[8] += w[2] * g0;
+    }
+    block_fold<RedSum, GRAM_Q>(acc, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < GRAM_Q; q++) part[(size_t)blockIdx.x * GRAM_Q + q] = acc[q];
+    }
+}
+__global__ void k_gram_fold(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    double f[GRAM_Q];
+#pragma unroll
+    for (int q = 0; q < GRAM_Q; q++) f[q] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) {
+#pragma unroll
+        for (int q = 0; q < GRAM_Q; q++) f[q] += part[(size_t)b * GRAM_Q + q];
+    }
+#pragma unroll
+    for (int q = 0; q < GRAM_Q; q++) f[q] = warp_fold<RedSum>(f[q]);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < GRAM_Q; q++) out[q] = f[q];
+    }
+}
+int launch_gram(const Ctx& c, cudaStream_t st, const GramIn& in, double* part, double* out) {
+    const int nb = red_blocks(c.n, RED_THREADS);
+    k_gram<<<nb, RED_THREADS, 0, st>>>(c.n, in, part);
+    k_gram_fold<<<1, 32, 0, st>>>(part, nb, out);
+    count(c, 2);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 // Box average of radius r along x (dir 0) or y (dir 1) of a per-cell field, boundary-mapped like
 // every stencil read (periodic wrap, else the edge cell): the separable smoothing of the network's
 // output, so that its step carries only the smooth part of the prediction.

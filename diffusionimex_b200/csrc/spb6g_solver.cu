@@ -77,9 +77,15 @@ struct spb6g_solver {
     double* Prate2 = nullptr;           // the rate of the stage before it
     double* rate_sc = nullptr;          // RMS of Prate (device scalar)
     bool rate_ready = false;            // a stage has converged since the tracking began (R exists)
+    double span1 = 0.0, span2 = 0.0;    // time spans of the stages behind Prate and Prate2 (0: none yet)
+    bool jac_ready = false;             // a Jacobian has been built (its diagonal's inverse is in dinv)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
-    int warm_mode = 7;                  // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
-                                        // 4 the last Newton correction as the next solve's first iterate
+    double* gstore = nullptr;           // 4 x n residuals of the residual-minimising start
+    double* gram_part = nullptr;        // its per-block inner products
+    double* gram = nullptr;             // and their totals
+    int warm_mode = 15;                 // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
+                                        // 4 the last Newton correction as the next solve's first iterate,
+                                        // 8 residual-minimising combination, 16 Jacobi sweeps of the start
     int warm_smooth = 0;                // radius of the box average of the network's output (0: none)
     float* ytmp = nullptr;              // scratch of the smoothing
     double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
@@ -266,6 +272,70 @@ int caldt(spb6g_solver* s, bool acoustic, double& inv) {
     return SPB6G_OK;
 }
 
+// Coefficients x minimising ||g0 + sum_j x_j w_j||_2 from the Gram sums m (k_gram's layout):
+// the normal equations by Cholesky, with a relative ridge of 1e-12 on the diagonal, over the
+// directions whose ||w_j||^2 is above 1e-24 of the largest (the others get 0: a zero network
+// output adds no direction).  False when nothing is left or the system is not finite.
+static bool solve_gram(const double* m, int K, double* x) {
+    const int idx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    double dmax = 0.0;
+    for (int i = 0; i < K; i++) dmax = std::max(dmax, m[idx[i][i]]);
+    if (!(dmax > 0.0) || !std::isfinite(dmax)) return false;
+    int act[3], na = 0;
+    for (int i = 0; i < K; i++) {
+        x[i] = 0.0;
+        if (m[idx[i][i]] > 1e-24 * dmax) act[na++] = i;
+    }
+    double L[3][3] = {}, y[3], z[3];
+    for (int i = 0; i < na; i++) {
+        for (int j = 0; j <= i; j++) {
+            double v = m[idx[act[i]][act[j]]] * (i == j ? 1.0 + 1e-12 : 1.0);
+            for (int k = 0; k < j; k++) v -= L[i][k] * L[j][k];
+            if (i == j) {
+                if (!(v > 0.0) || !std::isfinite(v)) return false;
+                L[i][i] = std::sqrt(v);
+            } else {
+                L[i][j] = v / L[j][j];
+            }
+        }
+    }
+    for (int i = 0; i < na; i++) {
+        double v = -m[6 + act[i]];
+        for (int k = 0; k < i; k++) v -= L[i][k] * y[k];
+        y[i] = v / L[i][i];
+    }
+    for (int i = na - 1; i >= 0; i--) {
+        double v = y[i];
+        for (int k = i + 1; k < na; k++) v -= L[k][i] * z[k];
+        z[i] = v / L[i][i];
+    }
+    for (int i = 0; i < na; i++) {
+        if (!std::isfinite(z[i])) return false;
+        x[act[i]] = z[i];
+    }
+    return true;
+}
+
+// Evaluates the residual at P + dP (into Pn, Gn, scn), copying Gn to `keep` if given; r is the
+// max-norm, or infinity where a closure failed.
+static int eval_warm(spb6g_solver* s, Ctx& c, const char* what, double* keep, double best, double& r) {
+    launch_residual(c, s->st, 1, 1.0);
+    if (keep && cudaMemcpyAsync(keep, c.Gn, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st) != cudaSuccess)
+        return -1;
+    if (sync_read(s, false)) return -1;
+    r = s->pin->ns.fail ? INFINITY : s->pin->ns.res;
+    if (s->verbose >= 3) fprintf(stderr, "    %s guess res %.3e, best so far %.3e\n", what, r, best);
+    if (reset_fail(s)) return -1;
+    return 0;
+}
+// The evaluated guess (Pn, Gn, scn) becomes the start.
+static void take_warm(Ctx& c, double& res, double r) {
+    std::swap(c.P, c.Pn);
+    std::swap(c.G, c.Gn);
+    std::swap(c.sc, c.scn);
+    res = r;
+}
+
 // Newton_Solver (:799-904), jreuse = 0.  P lives in s->c.P (the stage pressure).
 int newton(spb6g_solver* s, double& resfinal) {
     Ctx& c = s->c;
@@ -296,57 +366,167 @@ int newton(spb6g_solver* s, double& resfinal) {
     if (s->pin->ns.err) return SPB6G_INADMISSIBLE;  // Update / prep admissibility (:272, :929)
     if (s->pin->ns.fail & 1) { resfinal = INFINITY; return SPB6G_NEWTON_FAIL; }
     double res = s->pin->ns.res;
-    const int64_t learned0 = s->stats.learned;
     bool x0_pending = false;
     // learned prediction of the stage's pressure: P_start + sdt (R + sigma MLP(features))
-    bool have_pred = false, chosen = false;
+    bool have_pred = false;
     if (s->warm && s->rate_ready) {
         tbegin(s, TG_WARM);
         if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
         if (s->warm_smooth > 0) launch_smooth(c, s->st, s->ybuf, s->ytmp, s->warm_smooth);
         have_pred = true;
-        int base_extrap = 0;
+        // the start on the rate model: P = P_start + sdt (b_r R + b_q (R - R2) + b_y sigma y)
+        double b_r = 0.0, b_q = 0.0, b_y = 0.0;
         if (s->warm_mode & 1) {
-            // Newton starts from the guess of smallest residual norm (every closure succeeding):
-            // the plain guess, the extrapolation P_start + sdt R (the network's y = 0), then the
-            // network's guess, each candidate tried against the best so far
-            auto try_guess = [&](const char* what) -> int {
-                launch_residual(c, s->st, 1, 1.0);
-                if (sync_read(s, false)) return -1;
-                if (s->verbose >= 3) fprintf(stderr, "    %s guess res %.3e, best so far %.3e\n", what, s->pin->ns.res, res);
-                const int better = !s->pin->ns.fail && s->pin->ns.res < res;
-                if (better) {
-                    std::swap(c.P, c.Pn);
-                    std::swap(c.G, c.Gn);
-                    std::swap(c.sc, c.scn);
-                    res = s->pin->ns.res;
+            auto eval_guess = [&](const char* what, double* keep, double& r) { return eval_warm(s, c, what, keep, res, r); };
+            auto take = [&](double r) { take_warm(c, res, r); };
+            const double kq = s->span2 > 0.0 ? (s->span1 + c.sdt) / (s->span2 + s->span1) : 0.0;
+            if (s->warm_mode & 8) {
+                // Residual-minimising start: from the plain start P0 the candidates -- the
+                // extrapolation, the second-order extrapolation and the network's guess -- give
+                // the residual's change along the directions sdt R, sdt kq (R - R2) and sdt sigma y;
+                // the start combining them that minimises ||G||_2 of the residual taken linear in
+                // P is evaluated too, and the candidate of smallest max-norm starts Newton.
+                double* const gst = s->gstore;
+                CK(cudaMemcpyAsync(gst, c.G, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+                const double coef[3][3] = {{1.0, 0.0, 0.0}, {1.0, kq, 0.0}, {1.0, 0.0, 1.0}};
+                const char* names[3] = {"extrapolated", "second-order extrapolated", "learned"};
+                double cres[3] = {INFINITY, INFINITY, INFINITY};
+                for (int k = 0; k < 3; k++) {
+                    if (k == 1 && !(kq > 0.0)) continue;
+                    launch_guess(c, s->st, k == 2 ? s->ybuf : nullptr, s->norm.tscale, coef[k][0], coef[k][1], coef[k][2]);
+                    if (eval_guess(names[k], gst + (size_t)(k + 1) * s->n, cres[k]) < 0) return SPB6G_CUDA_ERROR;
                 }
-                if (reset_fail(s)) return -1;
-                return better;
-            };
-            launch_guess(c, s->st, nullptr, s->norm.tscale, 0);
-            const int ex = try_guess("extrapolated");
-            if (ex < 0) return SPB6G_CUDA_ERROR;
-            base_extrap = ex;
-            launch_guess(c, s->st, s->ybuf, s->norm.tscale, base_extrap);
-            const int lg = try_guess("learned");
-            if (lg < 0) return SPB6G_CUDA_ERROR;
-            if (lg) {
-                s->stats.learned++;
-                chosen = true;
-            } else if (ex) {
-                s->stats.extrapolated++;
-                chosen = true;
+                // directions: the extrapolation from P0, the second-order term and the network's
+                // term from the extrapolation (candidates whose closures failed are left out)
+                // (g[0] the residual at P0, g[1] at the extrapolation; w_j = g[j] - g[base_j])
+                GramIn gi{};
+                double dir[3][3];
+                int K = 0;
+                gi.g[0] = gst;
+                if (std::isfinite(cres[0])) {
+                    for (int k = 0; k < 3; k++) {
+                        if (!std::isfinite(cres[k])) continue;
+                        gi.g[K + 1] = gst + (size_t)(k + 1) * s->n;
+                        gi.base[K + 1] = k == 0 ? 0 : 1;
+                        for (int q = 0; q < 3; q++) dir[K][q] = coef[k][q] - (k == 0 ? 0.0 : coef[0][q]);
+                        K++;
+                    }
+                }
+                gi.K = K;
+                double cc[3] = {0.0, 0.0, 0.0}, cres_ls = INFINITY;
+                if (K >= 1) {
+                    if (launch_gram(c, s->st, gi, s->gram_part, s->gram) != 0) return SPB6G_CUDA_ERROR;
+                    double m[GRAM_Q];
+                    CK(cudaMemcpyAsync(m, s->gram, sizeof m, cudaMemcpyDeviceToHost, s->st));
+                    CK(cudaStreamSynchronize(s->st));
+                    double x[3];
+                    if (solve_gram(m, K, x)) {
+                        for (int j = 0; j < K; j++)
+                            for (int q = 0; q < 3; q++) cc[q] += x[j] * dir[j][q];
+                        launch_guess(c, s->st, s->ybuf, s->norm.tscale, cc[0], cc[1], cc[2]);
+                        if (eval_guess("combined", nullptr, cres_ls) < 0) return SPB6G_CUDA_ERROR;
+                    }
+                }
+                // the smallest max-norm among the plain start, the candidates and the combination
+                int best = -1;
+                double rb = res;
+                for (int k = 0; k < 3; k++)
+                    if (cres[k] < rb) { rb = cres[k]; best = k; }
+                if (cres_ls < rb) {
+                    take(cres_ls);
+                    b_r = cc[0]; b_q = cc[1]; b_y = cc[2];
+                    s->stats.combined++;
+                } else if (best >= 0) {
+                    double r = 0;
+                    launch_guess(c, s->st, best == 2 ? s->ybuf : nullptr, s->norm.tscale, coef[best][0], coef[best][1], coef[best][2]);
+                    if (eval_guess(names[best], nullptr, r) < 0) return SPB6G_CUDA_ERROR;
+                    take(r);
+                    b_r = coef[best][0]; b_q = coef[best][1]; b_y = coef[best][2];
+                    if (best == 2) s->stats.learned++;
+                    else if (best == 1) s->stats.extrapolated2++;
+                    else s->stats.extrapolated++;
+                }
+            } else {
+                // the candidates in sequence, each tried against the best so far: the extrapolation
+                // P_start + sdt R (the network's y = 0), the second-order extrapolation, then the
+                // network's guess
+                double r = 0;
+                launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0, 0.0, 0.0);
+                if (eval_guess("extrapolated", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
+                const bool ex = r < res;
+                if (ex) { take(r); b_r = 1.0; }
+                // second order: the rate taken linear in time through the midpoints of the last two
+                // stages (R at the last one's, R2 at the one before), averaged over this stage
+                bool eq = false;
+                if (kq > 0.0) {
+                    launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0 - b_r, kq, 0.0);
+                    if (eval_guess("second-order extrapolated", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
+                    eq = r < res;
+                    if (eq) { take(r); b_r = 1.0; b_q = kq; }
+                }
+                // the network's guess P_start + sdt (R + sigma y), from the chosen start
+                launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, 1.0);
+                if (eval_guess("learned", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
+                if (r < res) {
+                    take(r);
+                    b_r = 1.0; b_q = 0.0; b_y = 1.0;
+                    s->stats.learned++;
+                } else if (eq) {
+                    s->stats.extrapolated2++;
+                } else if (ex) {
+                    s->stats.extrapolated++;
+                }
             }
-            // dP now holds the learned step from the chosen start
-        } else {
-            launch_guess(c, s->st, s->ybuf, s->norm.tscale, 0);
+        }
+        // mode bit 16: up to two Jacobi sweeps on the nonlinear residual from the chosen start, with
+        // the diagonal of the last Jacobian built (the previous stage's) and the step length that
+        // minimises ||G||_2 of the residual taken linear along the step; a sweep stands when it
+        // lowers the max-norm.  Only for a start within 30 tolerances: a sweep cuts the max-norm
+        // by 4-10x, which can spare the stage its Newton iterations there, and not elsewhere.
+        bool refined = false;
+        if ((s->warm_mode & 16) && s->jac_ready && !tri && res < 30.0 * tol) {
+            double* const gst = s->gstore;
+            for (int sweep = 0; sweep < 2 && res >= tol; sweep++) {
+                double r1 = INFINITY, r2 = INFINITY, x = 0.0;
+                CK(cudaMemcpyAsync(gst, c.G, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+                launch_jacobi_dir(c, s->st, 1.0);
+                if (eval_warm(s, c, "jacobi", gst + s->n, res, r1) < 0) return SPB6G_CUDA_ERROR;
+                if (std::isfinite(r1)) {
+                    GramIn gi{};
+                    gi.g[0] = gst;
+                    gi.g[1] = gst + s->n;
+                    gi.K = 1;
+                    if (launch_gram(c, s->st, gi, s->gram_part, s->gram) != 0) return SPB6G_CUDA_ERROR;
+                    double m[GRAM_Q];
+                    CK(cudaMemcpyAsync(m, s->gram, sizeof m, cudaMemcpyDeviceToHost, s->st));
+                    CK(cudaStreamSynchronize(s->st));
+                    if (solve_gram(m, 1, &x) && x != 1.0) {
+                        launch_jacobi_dir(c, s->st, x);
+                        if (eval_warm(s, c, "jacobi, step length", nullptr, res, r2) < 0) return SPB6G_CUDA_ERROR;
+                    }
+                }
+                if (r2 < res && r2 <= r1) {
+                    take_warm(c, res, r2);
+                } else if (r1 < res) {
+                    launch_jacobi_dir(c, s->st, 1.0);
+                    if (eval_warm(s, c, "jacobi", nullptr, res, r1) < 0) return SPB6G_CUDA_ERROR;
+                    take_warm(c, res, r1);
+                } else {
+                    break;
+                }
+                refined = true;
+            }
+            if (refined) s->stats.refined++;
         }
         tend_(s, TG_WARM);
-        // when the network's guess is not the start, its step from the start is the first
-        // BiCGStab iterate's candidate
-        x0_pending = have_pred && !(chosen && s->stats.learned > learned0) && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
-        if (x0_pending) CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        // the network's step from the chosen start is the first BiCGStab iterate's candidate,
+        // unless the start is the network's guess itself or Jacobi sweeps moved it
+        const bool is_net = b_r == 1.0 && b_q == 0.0 && b_y == 1.0;
+        x0_pending = have_pred && !is_net && !refined && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
+        if (x0_pending) {
+            launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, 1.0 - b_y);
+            CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        }
     }
     // jreuse (modified Newton, :826-830, :887): the Jacobian is rebuilt at the first iteration, after
     // a damped step or a contraction above 0.25 (fresh_ok :797), and when the kept one lets the
@@ -374,6 +554,7 @@ int newton(spb6g_solver* s, double& resfinal) {
             launch_jacobian(c, s->st);
         }
         if (jreuse && build) CK(cudaMemcpyAsync(s->sc_build, c.sc, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+        s->jac_ready = true;
         fresh = build;
         tend_(s, TG_JACOBIAN);
         tbegin(s, TG_LINEAR);
@@ -544,6 +725,8 @@ int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_r
         launch_rate(c, s->st, s->Pstart, s->norm.tscale, s->dump_stage ? s->dumpT + s->dump_count : nullptr);
         if (s->dump_stage) s->dump_count += s->n;
         s->rate_ready = true;
+        s->span2 = s->span1;
+        s->span1 = c.sdt;
     }
     if (res > s->stats.maxres) s->stats.maxres = res;
     if (reset_fail(s)) return SPB6G_CUDA_ERROR;
@@ -1141,13 +1324,17 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc((void**)b, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
     }
-    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->x0buf, &s->rate_sc}) {
+    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->x0buf, &s->rate_sc, &s->gstore, &s->gram_part, &s->gram}) {
         if (*b) continue;
-        const size_t cnt = b == &s->rate_sc ? 2 : (size_t)s->n;
+        const size_t cnt = b == &s->rate_sc ? 2
+                           : b == &s->gstore ? 4 * (size_t)s->n
+                           : b == &s->gram_part ? (size_t)red_blocks(s->n, RED_THREADS) * GRAM_Q
+                           : b == &s->gram ? (size_t)GRAM_Q
+                                                 : (size_t)s->n;
         if (cudaMalloc((void**)b, cnt * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
         // no rate (and no rate scale) before the first converged stage
-        if (b != &s->Pstart && b != &s->x0buf && cudaMemsetAsync(*b, 0, cnt * sizeof(double), s->st) != cudaSuccess)
+        if ((b == &s->Prate || b == &s->Prate2 || b == &s->rate_sc) && cudaMemsetAsync(*b, 0, cnt * sizeof(double), s->st) != cudaSuccess)
             return SPB6G_CUDA_ERROR;
     }
     return SPB6G_OK;
@@ -1164,7 +1351,7 @@ int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
     return SPB6G_OK;
 }
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode) {
-    if (!s || mode < 1 || mode > 7) return SPB6G_BAD_ARG;
+    if (!s || mode < 1 || mode > 31) return SPB6G_BAD_ARG;
     s->warm_mode = mode;
     return SPB6G_OK;
 }

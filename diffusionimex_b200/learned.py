@@ -179,7 +179,7 @@ def train_mlp(X, T, steps: int = 3000, batch: int = 1 << 20, lr: float = 1e-3, s
     return m, hist
 
 
-def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 7,
+def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: int = 0, mode: int = 15,
              smooth: int = 0) -> tuple:
     """Advance `warmup` untimed steps, then `steps` timed ones; counts and device time."""
     torch = _torch()
@@ -198,7 +198,7 @@ def run_case(case: dict, steps: int, warmup: int, mlp=None, norm=None, device: i
     P, pref = s.pressure()
     s.close()
     d = {k: b[k] - a[k] for k in ("steps", "stages", "newton_it", "bicg_it", "rejects", "learned", "learned_x0",
-                                  "extrapolated")}
+                                  "extrapolated", "extrapolated2", "combined", "refined")}
     d.update(ms=ms, ms_per_step=ms / max(d["steps"], 1), bicg_per_step=d["bicg_it"] / max(d["steps"], 1),
              newton_per_stage=d["newton_it"] / max(d["stages"], 1), t=b["t"])
     return d, P + pref

@@ -66,7 +66,8 @@ class Stats(ctypes.Structure):
         ("newton_it", ctypes.c_int64), ("floor_count", ctypes.c_int64), ("bicg_it", ctypes.c_int64),
         ("learned", ctypes.c_int64), ("t", ctypes.c_double), ("dt", ctypes.c_double), ("maxres", ctypes.c_double),
         ("p_ref", ctypes.c_double), ("tmax", ctypes.c_double * 2), ("learned_x0", ctypes.c_int64),
-        ("extrapolated", ctypes.c_int64),
+        ("extrapolated", ctypes.c_int64), ("extrapolated2", ctypes.c_int64), ("combined", ctypes.c_int64),
+        ("refined", ctypes.c_int64),
     ]
 
 
@@ -418,7 +419,7 @@ class Solver:
         a = (ctypes.c_double * self.NORM_LEN)(*[float(v) for v in norm])
         self._check(self.lib.spb6g_set_feature_norm(self.h, a), "spb6g_set_feature_norm")
 
-    def set_warmstart(self, mlp, mode: int = 7, smooth: int = 0):
+    def set_warmstart(self, mlp, mode: int = 15, smooth: int = 0):
         """mode bits -- 1: learned Newton start (the guess of smallest residual among the plain guess,
         the extrapolation and the network's); 2: learned first BiCGStab iterate; 4: the last Newton
         correction as the first iterate's candidate of the stage's later solves.  smooth: radius of

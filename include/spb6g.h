@@ -111,8 +111,11 @@ typedef struct {
     int64_t learned;                /* stages whose Newton started from the learned guess */
     double t, dt, maxres, p_ref;
     double tmax[2];                 /* max phase temperatures of the stages' final states (st_Tmax :96, :1070) */
-    int64_t learned_x0;             /* BiCGStab solves that started from the learned first iterate */
+    int64_t learned_x0;             /* BiCGStab solves that started from a learned first iterate */
     int64_t extrapolated;           /* stages whose Newton started from the extrapolated pressure */
+    int64_t extrapolated2;          /* ... from the second-order extrapolation */
+    int64_t combined;               /* ... from the residual-minimising combination (mode bit 8) */
+    int64_t refined;                /* stages whose start Jacobi sweeps improved (mode bit 16) */
 } spb6g_stats;
 
 typedef struct spb6g_solver spb6g_solver;
@@ -297,15 +300,21 @@ int spb6g_mlp_last_loss(spb6g_mlp* m, void* stream, float* loss_sum);
  * converged stage).  Setting it also starts tracking R. */
 int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
 /* m != NULL: every stage predicts its pressure P_start + dts (R + sigma MLP(features)).
- * Mode bit 1 (spb6g_set_warmstart_mode; 7, every bit, by default): Newton starts from the guess of
- * smallest residual norm among the plain guess (the previous stage's pressure), the
- * extrapolation P_start + dts R (the network's zero output) and the network's guess.  Mode
- * bit 2: when the network's guess is not the start, the first BiCGStab solve of the stage
- * starts from x0 = a M^-1 b + c dP, dP the network's step from the start and (a, c)
- * minimising ||b - A x0||, when that residual is below 0.99 of the plain start's
- * (x0 = M^-1 b, GMRES_Solver :769), else from M^-1 b.  Mode bit 4: every later solve of the
- * stage takes the last Newton correction as that candidate dP.  Newton and BiCGStab keep
- * their tolerances.  NULL: off. */
+ * Mode bits (spb6g_set_warmstart_mode; 15 by default):
+ *  1: Newton starts from the guess of smallest residual max-norm among the plain guess (the
+ *     previous stage's pressure), the extrapolation P_start + dts R (the network's zero output),
+ *     the second-order extrapolation P_start + dts (R + k (R - R2)) (R2 the rate of the stage
+ *     before, k from the stages' time spans) and the network's guess;
+ *  2: when the network's guess is not the start, the first BiCGStab solve of the stage starts
+ *     from x0 = a M^-1 b + c dP, dP the network's step from the start and (a, c) minimising
+ *     ||b - A x0||, when that residual is below 0.99 of the plain start's (x0 = M^-1 b,
+ *     GMRES_Solver :769), else from M^-1 b;
+ *  4: every later solve of the stage takes the last Newton correction as that candidate dP;
+ *  8: with bit 1, the start combining the candidates' steps that minimises ||G||_2 of the
+ *     residual taken linear in P (from the candidates' residuals) is a candidate too;
+ *  16: up to two Jacobi sweeps of the start (the last Jacobian's diagonal, step length by the
+ *     same minimisation) when its residual is within 30 tolerances.
+ * Newton and BiCGStab keep their tolerances.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
 /* Radius r (0: none, the default; at most 64 and below nx, ny) of a separable box average of the

@@ -32,7 +32,7 @@ def lowmach(seed: int) -> dict:
     return dict(cases.lowmach_bubbles(N, seed=seed, nbub=4), newton_tol=1e-12, bicg_tol=1e-12)
 
 
-def _run(case, steps, warmup, mlp=None, norm=None, mode=7):
+def _run(case, steps, warmup, mlp=None, norm=None, mode=15):
     from diffusionimex_b200 import learned
 
     return learned.run_case(case, steps, warmup, mlp=mlp, norm=norm, mode=mode)
@@ -108,6 +108,27 @@ def test_extrapolation_guess_reaches_the_plain_solution():
     z.close()
     assert warm["steps"] == plain["steps"]
     assert learned.l1_rel(Pw, Pp) <= L1_BAR
+
+
+@pytest.mark.parametrize("mode", [5, 13, 29])
+def test_extrapolation_combination_and_sweeps_keep_the_plain_solution(mode):
+    """With the zero network: the second-order extrapolation and the last-correction first iterates
+    (mode 5), the residual-minimising combination of the candidates (bit 8) and the Jacobi sweeps of
+    the start (bit 16) change only where Newton starts and where BiCGStab starts; the run keeps the
+    plain run's steps and reaches its solution (L1(p) bar), with no more Newton iterations."""
+    from diffusionimex_b200 import learned
+
+    c = lowmach(0)
+    norm = learned.pilot_norm(lowmach(1), steps=4)
+    z = learned.zero_network()
+    plain, Pp = _run(c, 12, 3)
+    warm, Pw = _run(c, 12, 3, mlp=z, norm=norm, mode=mode)
+    z.close()
+    assert warm["steps"] == plain["steps"] and warm["rejects"] == plain["rejects"]
+    assert warm["newton_it"] <= plain["newton_it"]
+    assert learned.l1_rel(Pw, Pp) <= L1_BAR
+    if mode & 8:
+        assert warm["combined"] + warm["extrapolated2"] + warm["extrapolated"] > 0
 
 
 def test_trained_warm_start_reaches_the_plain_solution_and_records_its_gain():
