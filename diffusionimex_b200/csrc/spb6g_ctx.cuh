@@ -114,6 +114,7 @@ struct Ctx {
     // learned warm start (no counterpart in the reference)
     double* Prate;     // pressure rate (P_converged - P_start) / sdt of the last converged stage, or null
     double* Prate2;    // the rate of the stage before it
+    double* Prate3;    // and the one before that (NULL: not tracked)
     double* rate_sc;   // [0]: sigma, the RMS of Prate over the cells (0 before the first stage)
     const double* x0l; // learned first BiCGStab iterate of this solve, or null (the plain start M^-1 b)
     double sdt;        // time span of the stage: (c_s - c_{s-1}) dt, c the implicit tableau's row sums
@@ -201,12 +202,15 @@ int batch_max_blocks(int threads, int tw, int device);
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X);
 // base_extrap = 0: dP = sdt (R + sigma y) from the stage's starting pressure; 1: dP = sdt sigma y from
 // the extrapolated pressure P_start + sdt R; y = null: the extrapolation dP = sdt R
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_y);
-// residual vectors of the residual-minimising start (g[0] at the plain start, g[j] at candidate j)
-constexpr int GRAM_Q = 9;
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_c,
+                  double a_y);
+// residual vectors of the residual-minimising start (g[0] at the plain start, g[j] at candidate j):
+// the Gram matrix of up to GRAM_K directions (upper triangle, row by row), then the right-hand side
+constexpr int GRAM_K = 4;
+constexpr int GRAM_Q = GRAM_K * (GRAM_K + 1) / 2 + GRAM_K;
 struct GramIn {
-    const double* g[4];
-    int base[4];
+    const double* g[GRAM_K + 1];
+    int base[GRAM_K + 1];
     int K;
 };
 int launch_gram(const Ctx& c, cudaStream_t st, const GramIn& in, double* part, double* out);

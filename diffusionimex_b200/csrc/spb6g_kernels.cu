@@ -1408,19 +1408,21 @@ void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void*
 // Step towards a predicted pressure.  The network predicts how far the stage's pressure
 // rate departs from the last stage's, in units of sigma: the learned guess is
 // P_start + sdt (R + sigma y), the extrapolation (y = 0) P_start + sdt R.
-// Step from the current start to a candidate: dP = sdt (a_r R + a_q (R - R2) + a_y sigma y), R the
-// pressure rate of the last converged stage and R2 that of the one before.
-__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale, double a_r, double a_q, double a_y) {
+// Step from the current start to a candidate: dP = sdt (a_r R + a_q (R - R2) + a_c (R2 - R3) +
+// a_y sigma y), R the pressure rate of the last converged stage, R2 and R3 those of the two before.
+__global__ void k_guess(Ctx c, const float* __restrict__ y, double tscale, double a_r, double a_q, double a_c, double a_y) {
     const double sig = rate_scale(c, tscale);
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
         const double r = c.Prate ? c.Prate[x] : 0.0;
         const double r2 = c.Prate2 ? c.Prate2[x] : r;
+        const double r3 = c.Prate3 ? c.Prate3[x] : r2;
         const double d = y ? a_y * (double)y[x] * sig : 0.0;
-        c.dP[x] = c.sdt * (a_r * r + a_q * (r - r2) + d);
+        c.dP[x] = c.sdt * (a_r * r + a_q * (r - r2) + a_c * (r2 - r3) + d);
     }
 }
-void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_y) {
-    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, a_r, a_q, a_y);
+void launch_guess(const Ctx& c, cudaStream_t st, const float* y, double tscale, double a_r, double a_q, double a_c,
+                  double a_y) {
+    k_guess<<<blocks_for(c.n), TPB, 0, st>>>(c, y, tscale, a_r, a_q, a_c, a_y);
     count(c, 1);
 }
 // Jacobi step on the nonlinear residual with the diagonal of the last Jacobian built:
@@ -1434,27 +1436,26 @@ void launch_jacobi_dir(const Ctx& c, cudaStream_t st, double coef) {
     count(c, 1);
 }
 // Inner products of the residual-minimising start: with g[0] the residual at the plain start and
-// w_j = g[j] - g[base_j] (j = 1..K, K <= 3) the residual changes along the candidate directions,
-// the Gram matrix <w_j, w_k> (j <= k, row by row) and <w_j, g[0]>; per-block partials, folded by
-// k_gram_fold in block order.
+// w_j = g[j] - g[base_j] (j = 1..K, K <= GRAM_K) the residual changes along the candidate
+// directions, the Gram matrix <w_j, w_k> (j <= k, row by row) and <w_j, g[0]>; per-block partials,
+// folded by k_gram_fold in block order.
 __global__ void __launch_bounds__(RED_THREADS) k_gram(int n, GramIn in, double* __restrict__ part) {
     __shared__ double sh[GRAM_Q * 32];
     double acc[GRAM_Q];
 #pragma unroll
     for (int q = 0; q < GRAM_Q; q++) acc[q] = 0.0;
     for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
-        double w[3] = {0.0, 0.0, 0.0};
-        for (int j = 0; j < in.K; j++) w[j] = in.g[j + 1][x] - in.g[in.base[j + 1]][x];
+        double w[GRAM_K];
+#pragma unroll
+        for (int j = 0; j < GRAM_K; j++) w[j] = j < in.K ? in.g[j + 1][x] - in.g[in.base[j + 1]][x] : 0.0;
         const double g0 = in.g[0][x];
-        acc[0] += w[0] * w[0];
-        acc[1] += w[0] * w[1];
-        acc[2] += w[0] * w[2];
-        acc[3] += w[1] * w[1];
-        acc[4] += w[1] * w[2];
-        acc[5] += w[2] * w[2];
-        acc[6] += w[0] * g0;
-        acc[7] += w[1] * g0;
-        acc[8] += w[2] * g0;
+        int q = 0;
+#pragma unroll
+        for (int j = 0; j < GRAM_K; j++)
+#pragma unroll
+            for (int k = j; k < GRAM_K; k++) acc[q++] += w[j] * w[k];
+#pragma unroll
+        for (int j = 0; j < GRAM_K; j++) acc[q++] += w[j] * g0;
     }
     block_fold<RedSum, GRAM_Q>(acc, sh);
     if (threadIdx.x == 0) {
@@ -1519,6 +1520,7 @@ __global__ void __launch_bounds__(TPB) k_rate(Ctx c, const double* __restrict__ 
         const double r = (c.P[x] - P0[x]) * idt;
         const double r0 = c.Prate[x];
         if (t) t[x] = (float)((r - r0) * isig);
+        if (c.Prate3) c.Prate3[x] = c.Prate2[x];
         c.Prate2[x] = r0;
         c.Prate[x] = r;
         acc[0] += r * r;

@@ -75,17 +75,20 @@ struct spb6g_solver {
     double* Pstart = nullptr;           // stage's starting pressure (pressure rate, training targets)
     double* Prate = nullptr;            // pressure rate of the last converged stage (a feature and the extrapolation)
     double* Prate2 = nullptr;           // the rate of the stage before it
+    double* Prate3 = nullptr;           // and the one before that
     double* rate_sc = nullptr;          // RMS of Prate (device scalar)
     bool rate_ready = false;            // a stage has converged since the tracking began (R exists)
     double span1 = 0.0, span2 = 0.0;    // time spans of the stages behind Prate and Prate2 (0: none yet)
+    double span3 = 0.0;                 // and behind Prate3
     bool jac_ready = false;             // a Jacobian has been built (its diagonal's inverse is in dinv)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
-    double* gstore = nullptr;           // 4 x n residuals of the residual-minimising start
+    double* gstore = nullptr;           // (GRAM_K + 1) x n residuals of the residual-minimising start
     double* gram_part = nullptr;        // its per-block inner products
     double* gram = nullptr;             // and their totals
     int warm_mode = 15;                 // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
                                         // 4 the last Newton correction as the next solve's first iterate,
-                                        // 8 residual-minimising combination, 16 Jacobi sweeps of the start
+                                        // 8 residual-minimising combination, 16 Jacobi sweeps of the start,
+                                        // 32 the older rate change as a fourth direction
     int warm_smooth = 0;                // radius of the box average of the network's output (0: none)
     float* ytmp = nullptr;              // scratch of the smoothing
     double stage_c = 0;                 // implicit stage time c_s of the last stage run (for the next stage's span)
@@ -277,16 +280,19 @@ int caldt(spb6g_solver* s, bool acoustic, double& inv) {
 // directions whose ||w_j||^2 is above 1e-24 of the largest (the others get 0: a zero network
 // output adds no direction).  False when nothing is left or the system is not finite.
 static bool solve_gram(const double* m, int K, double* x) {
-    const int idx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    int idx[GRAM_K][GRAM_K];
+    for (int j = 0, q = 0; j < GRAM_K; j++)
+        for (int k = j; k < GRAM_K; k++, q++) idx[j][k] = idx[k][j] = q;
+    const double* rhs = m + GRAM_K * (GRAM_K + 1) / 2;
     double dmax = 0.0;
     for (int i = 0; i < K; i++) dmax = std::max(dmax, m[idx[i][i]]);
     if (!(dmax > 0.0) || !std::isfinite(dmax)) return false;
-    int act[3], na = 0;
+    int act[GRAM_K], na = 0;
     for (int i = 0; i < K; i++) {
         x[i] = 0.0;
         if (m[idx[i][i]] > 1e-24 * dmax) act[na++] = i;
     }
-    double L[3][3] = {}, y[3], z[3];
+    double L[GRAM_K][GRAM_K] = {}, y[GRAM_K], z[GRAM_K];
     for (int i = 0; i < na; i++) {
         for (int j = 0; j <= i; j++) {
             double v = m[idx[act[i]][act[j]]] * (i == j ? 1.0 + 1e-12 : 1.0);
@@ -300,7 +306,7 @@ static bool solve_gram(const double* m, int K, double* x) {
         }
     }
     for (int i = 0; i < na; i++) {
-        double v = -m[6 + act[i]];
+        double v = -rhs[act[i]];
         for (int k = 0; k < i; k++) v -= L[i][k] * y[k];
         y[i] = v / L[i][i];
     }
@@ -368,90 +374,100 @@ int newton(spb6g_solver* s, double& resfinal) {
     double res = s->pin->ns.res;
     bool x0_pending = false;
     // learned prediction of the stage's pressure: P_start + sdt (R + sigma MLP(features))
-    bool have_pred = false;
+    bool have_pred = false, warm_start = false;
     if (s->warm && s->rate_ready) {
         tbegin(s, TG_WARM);
         if (spb6g_mlp_forward(s->warm, s->rows_cur, s->n, s->ybuf, s->st) != SPB6G_OK) return SPB6G_CUDA_ERROR;
         if (s->warm_smooth > 0) launch_smooth(c, s->st, s->ybuf, s->ytmp, s->warm_smooth);
         have_pred = true;
-        // the start on the rate model: P = P_start + sdt (b_r R + b_q (R - R2) + b_y sigma y)
-        double b_r = 0.0, b_q = 0.0, b_y = 0.0;
+        // the start on the rate model: P = P_start + sdt (b_r R + b_q (R - R2) + b_c (R2 - R3) + b_y sigma y)
+        double b_r = 0.0, b_q = 0.0, b_c = 0.0, b_y = 0.0;
+        warm_start = (s->warm_mode & 1) != 0;
         if (s->warm_mode & 1) {
             auto eval_guess = [&](const char* what, double* keep, double& r) { return eval_warm(s, c, what, keep, res, r); };
             auto take = [&](double r) { take_warm(c, res, r); };
             const double kq = s->span2 > 0.0 ? (s->span1 + c.sdt) / (s->span2 + s->span1) : 0.0;
             if (s->warm_mode & 8) {
                 // Residual-minimising start: from the plain start P0 the candidates -- the
-                // extrapolation, the second-order extrapolation and the network's guess -- give
-                // the residual's change along the directions sdt R, sdt kq (R - R2) and sdt sigma y;
-                // the start combining them that minimises ||G||_2 of the residual taken linear in
-                // P is evaluated too, and the candidate of smallest max-norm starts Newton.
+                // extrapolation, the second-order extrapolation, with bit 32 the extrapolation plus
+                // the older rate change, and the network's guess -- give the residual's change along
+                // the directions sdt R, sdt kq (R - R2), sdt (R2 - R3) and sdt sigma y; the start
+                // combining them that minimises ||G||_2 of the residual taken linear in P is
+                // evaluated too, and the candidate of smallest max-norm starts Newton.
+                constexpr int NC = 4;
                 double* const gst = s->gstore;
                 CK(cudaMemcpyAsync(gst, c.G, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
-                const double coef[3][3] = {{1.0, 0.0, 0.0}, {1.0, kq, 0.0}, {1.0, 0.0, 1.0}};
-                const char* names[3] = {"extrapolated", "second-order extrapolated", "learned"};
-                double cres[3] = {INFINITY, INFINITY, INFINITY};
-                for (int k = 0; k < 3; k++) {
-                    if (k == 1 && !(kq > 0.0)) continue;
-                    launch_guess(c, s->st, k == 2 ? s->ybuf : nullptr, s->norm.tscale, coef[k][0], coef[k][1], coef[k][2]);
+                const double coef[NC][4] = {{1.0, 0.0, 0.0, 0.0}, {1.0, kq, 0.0, 0.0}, {1.0, 0.0, 1.0, 0.0}, {1.0, 0.0, 0.0, 1.0}};
+                const bool avail[NC] = {true, kq > 0.0, (s->warm_mode & 32) && s->span3 > 0.0, true};
+                const char* names[NC] = {"extrapolated", "second-order extrapolated", "older rate change", "learned"};
+                auto guess = [&](const double* k) {
+                    launch_guess(c, s->st, k[3] != 0.0 ? s->ybuf : nullptr, s->norm.tscale, k[0], k[1], k[2], k[3]);
+                };
+                double cres[NC];
+                for (int k = 0; k < NC; k++) {
+                    cres[k] = INFINITY;
+                    if (!avail[k]) continue;
+                    guess(coef[k]);
                     if (eval_guess(names[k], gst + (size_t)(k + 1) * s->n, cres[k]) < 0) return SPB6G_CUDA_ERROR;
                 }
-                // directions: the extrapolation from P0, the second-order term and the network's
-                // term from the extrapolation (candidates whose closures failed are left out)
-                // (g[0] the residual at P0, g[1] at the extrapolation; w_j = g[j] - g[base_j])
+                // directions: the extrapolation from P0, the other terms from the extrapolation
+                // (candidates whose closures failed are left out); g[0] the residual at P0, g[1]
+                // at the extrapolation, w_j = g[j] - g[base_j]
                 GramIn gi{};
-                double dir[3][3];
+                double dir[NC][4];
                 int K = 0;
                 gi.g[0] = gst;
                 if (std::isfinite(cres[0])) {
-                    for (int k = 0; k < 3; k++) {
+                    for (int k = 0; k < NC; k++) {
                         if (!std::isfinite(cres[k])) continue;
                         gi.g[K + 1] = gst + (size_t)(k + 1) * s->n;
                         gi.base[K + 1] = k == 0 ? 0 : 1;
-                        for (int q = 0; q < 3; q++) dir[K][q] = coef[k][q] - (k == 0 ? 0.0 : coef[0][q]);
+                        for (int q = 0; q < 4; q++) dir[K][q] = coef[k][q] - (k == 0 ? 0.0 : coef[0][q]);
                         K++;
                     }
                 }
                 gi.K = K;
-                double cc[3] = {0.0, 0.0, 0.0}, cres_ls = INFINITY;
+                double cc[4] = {0.0, 0.0, 0.0, 0.0}, cres_ls = INFINITY;
                 if (K >= 1) {
                     if (launch_gram(c, s->st, gi, s->gram_part, s->gram) != 0) return SPB6G_CUDA_ERROR;
                     double m[GRAM_Q];
                     CK(cudaMemcpyAsync(m, s->gram, sizeof m, cudaMemcpyDeviceToHost, s->st));
                     CK(cudaStreamSynchronize(s->st));
-                    double x[3];
+                    double x[GRAM_K];
                     if (solve_gram(m, K, x)) {
                         for (int j = 0; j < K; j++)
-                            for (int q = 0; q < 3; q++) cc[q] += x[j] * dir[j][q];
-                        launch_guess(c, s->st, s->ybuf, s->norm.tscale, cc[0], cc[1], cc[2]);
+                            for (int q = 0; q < 4; q++) cc[q] += x[j] * dir[j][q];
+                        guess(cc);
                         if (eval_guess("combined", nullptr, cres_ls) < 0) return SPB6G_CUDA_ERROR;
                     }
                 }
                 // the smallest max-norm among the plain start, the candidates and the combination
                 int best = -1;
                 double rb = res;
-                for (int k = 0; k < 3; k++)
+                for (int k = 0; k < NC; k++)
                     if (cres[k] < rb) { rb = cres[k]; best = k; }
+                const double* pick = nullptr;
                 if (cres_ls < rb) {
                     take(cres_ls);
-                    b_r = cc[0]; b_q = cc[1]; b_y = cc[2];
+                    pick = cc;
                     s->stats.combined++;
                 } else if (best >= 0) {
                     double r = 0;
-                    launch_guess(c, s->st, best == 2 ? s->ybuf : nullptr, s->norm.tscale, coef[best][0], coef[best][1], coef[best][2]);
+                    guess(coef[best]);
                     if (eval_guess(names[best], nullptr, r) < 0) return SPB6G_CUDA_ERROR;
                     take(r);
-                    b_r = coef[best][0]; b_q = coef[best][1]; b_y = coef[best][2];
-                    if (best == 2) s->stats.learned++;
-                    else if (best == 1) s->stats.extrapolated2++;
-                    else s->stats.extrapolated++;
+                    pick = coef[best];
+                    if (best == 3) s->stats.learned++;
+                    else if (best == 0) s->stats.extrapolated++;
+                    else s->stats.extrapolated2++;
                 }
+                if (pick) { b_r = pick[0]; b_q = pick[1]; b_c = pick[2]; b_y = pick[3]; }
             } else {
                 // the candidates in sequence, each tried against the best so far: the extrapolation
                 // P_start + sdt R (the network's y = 0), the second-order extrapolation, then the
                 // network's guess
                 double r = 0;
-                launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0, 0.0, 0.0);
+                launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0, 0.0, 0.0, 0.0);
                 if (eval_guess("extrapolated", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
                 const bool ex = r < res;
                 if (ex) { take(r); b_r = 1.0; }
@@ -459,13 +475,13 @@ int newton(spb6g_solver* s, double& resfinal) {
                 // stages (R at the last one's, R2 at the one before), averaged over this stage
                 bool eq = false;
                 if (kq > 0.0) {
-                    launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0 - b_r, kq, 0.0);
+                    launch_guess(c, s->st, nullptr, s->norm.tscale, 1.0 - b_r, kq, 0.0, 0.0);
                     if (eval_guess("second-order extrapolated", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
                     eq = r < res;
                     if (eq) { take(r); b_r = 1.0; b_q = kq; }
                 }
                 // the network's guess P_start + sdt (R + sigma y), from the chosen start
-                launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, 1.0);
+                launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, 0.0, 1.0);
                 if (eval_guess("learned", nullptr, r) < 0) return SPB6G_CUDA_ERROR;
                 if (r < res) {
                     take(r);
@@ -521,10 +537,10 @@ int newton(spb6g_solver* s, double& resfinal) {
         tend_(s, TG_WARM);
         // the network's step from the chosen start is the first BiCGStab iterate's candidate,
         // unless the start is the network's guess itself or Jacobi sweeps moved it
-        const bool is_net = b_r == 1.0 && b_q == 0.0 && b_y == 1.0;
+        const bool is_net = b_r == 1.0 && b_q == 0.0 && b_c == 0.0 && b_y == 1.0;
         x0_pending = have_pred && !is_net && !refined && (s->warm_mode & 2) && !tri && s->bicg_G > 0;
         if (x0_pending) {
-            launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, 1.0 - b_y);
+            launch_guess(c, s->st, s->ybuf, s->norm.tscale, 1.0 - b_r, -b_q, -b_c, 1.0 - b_y);
             CK(cudaMemcpyAsync(s->x0buf, c.dP, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
         }
     }
@@ -540,7 +556,10 @@ int newton(spb6g_solver* s, double& resfinal) {
     for (int it = 0; it < s->cfg.newton_iter; it++) {
         resfinal = res;
         if (s->verbose >= 3) fprintf(stderr, "    newton it %d res %.3e\n", it, res);
-        if (res < tol) return SPB6G_OK;
+        // a warm start below the tolerance still takes one Newton step: the solve, not the
+        // prediction, ends every stage (a start accepted as it is would stop the stage at the
+        // tolerance's edge, where the plain path's last step lands far inside it)
+        if (res < tol && !(warm_start && it == 0)) return SPB6G_OK;
         const bool build = !jreuse || it == 0 || !(lamprev == 1.0 && ratio <= 0.25);
         tbegin(s, TG_JACOBIAN);
         if (!build) {  // the kept diagonals; the BiCGStab set-up sums of the new right-hand side
@@ -708,6 +727,7 @@ int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_r
     const bool track = s->Prate != nullptr;
     c.Prate = track ? s->Prate : nullptr;
     c.Prate2 = s->Prate2;
+    c.Prate3 = s->Prate3;
     c.rate_sc = s->rate_sc;
     c.x0l = nullptr;
     if (s->warm || s->dump_stage) {
@@ -725,6 +745,7 @@ int run_stage(spb6g_solver* s, int rks, const double* Ae_row, const double* Ai_r
         launch_rate(c, s->st, s->Pstart, s->norm.tscale, s->dump_stage ? s->dumpT + s->dump_count : nullptr);
         if (s->dump_stage) s->dump_count += s->n;
         s->rate_ready = true;
+        s->span3 = s->span2;
         s->span2 = s->span1;
         s->span1 = c.sdt;
     }
@@ -1193,6 +1214,7 @@ int spb6g_stage_dump(spb6g_solver* s, double dt, double* Xs, double* a2s, double
     c.x0l = nullptr;
     c.Prate = nullptr;  // the dumped stage runs from the plain guess
     c.Prate2 = nullptr;
+    c.Prate3 = nullptr;
     c.rate_sc = nullptr;
     c.H = s->Hs;
     if (reset_flags(s)) return SPB6G_CUDA_ERROR;
@@ -1324,17 +1346,17 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc((void**)b, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
     }
-    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->x0buf, &s->rate_sc, &s->gstore, &s->gram_part, &s->gram}) {
+    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->Prate3, &s->x0buf, &s->rate_sc, &s->gstore, &s->gram_part, &s->gram}) {
         if (*b) continue;
         const size_t cnt = b == &s->rate_sc ? 2
-                           : b == &s->gstore ? 4 * (size_t)s->n
+                           : b == &s->gstore ? (size_t)(GRAM_K + 1) * s->n
                            : b == &s->gram_part ? (size_t)red_blocks(s->n, RED_THREADS) * GRAM_Q
                            : b == &s->gram ? (size_t)GRAM_Q
                                                  : (size_t)s->n;
         if (cudaMalloc((void**)b, cnt * sizeof(double)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
         // no rate (and no rate scale) before the first converged stage
-        if ((b == &s->Prate || b == &s->Prate2 || b == &s->rate_sc) && cudaMemsetAsync(*b, 0, cnt * sizeof(double), s->st) != cudaSuccess)
+        if ((b == &s->Prate || b == &s->Prate2 || b == &s->Prate3 || b == &s->rate_sc) && cudaMemsetAsync(*b, 0, cnt * sizeof(double), s->st) != cudaSuccess)
             return SPB6G_CUDA_ERROR;
     }
     return SPB6G_OK;
@@ -1351,7 +1373,7 @@ int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m) {
     return SPB6G_OK;
 }
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode) {
-    if (!s || mode < 1 || mode > 31) return SPB6G_BAD_ARG;
+    if (!s || mode < 1 || mode > 63) return SPB6G_BAD_ARG;
     s->warm_mode = mode;
     return SPB6G_OK;
 }

@@ -313,8 +313,10 @@ int spb6g_set_feature_norm(spb6g_solver* s, const double* norm);
  *  8: with bit 1, the start combining the candidates' steps that minimises ||G||_2 of the
  *     residual taken linear in P (from the candidates' residuals) is a candidate too;
  *  16: up to two Jacobi sweeps of the start (the last Jacobian's diagonal, step length by the
- *     same minimisation) when its residual is within 30 tolerances.
- * Newton and BiCGStab keep their tolerances.  NULL: off. */
+ *     same minimisation) when its residual is within 30 tolerances;
+ *  32: with bit 8, the older rate change dts (R2 - R3) as a fourth direction.
+ * Newton and BiCGStab keep their tolerances, and a warm-started stage always takes at least one
+ * Newton step.  NULL: off. */
 int spb6g_set_warmstart(spb6g_solver* s, spb6g_mlp* m);
 int spb6g_set_warmstart_mode(spb6g_solver* s, int mode);
 /* Radius r (0: none, the default; at most 64 and below nx, ny) of a separable box average of the

@@ -110,11 +110,12 @@ def test_extrapolation_guess_reaches_the_plain_solution():
     assert learned.l1_rel(Pw, Pp) <= L1_BAR
 
 
-@pytest.mark.parametrize("mode", [5, 13, 29])
+@pytest.mark.parametrize("mode", [5, 13, 29, 45])
 def test_extrapolation_combination_and_sweeps_keep_the_plain_solution(mode):
     """With the zero network: the second-order extrapolation and the last-correction first iterates
     (mode 5), the residual-minimising combination of the candidates (bit 8) and the Jacobi sweeps of
-    the start (bit 16) change only where Newton starts and where BiCGStab starts; the run keeps the
+    the start (bit 16) and the older rate change as a fourth direction (bit 32) change only where
+    Newton starts and where BiCGStab starts; the run keeps the
     plain run's steps and reaches its solution (L1(p) bar), with no more Newton iterations."""
     from diffusionimex_b200 import learned
 
