@@ -162,6 +162,7 @@ struct BatchInst {
     // statistics
     long long steps, rejects, rk1, stages, newton_it, floor_count;
     double maxres;
+    double tmax[2];
 };
 
 // ------------------------------------------------------------ launchers (spb6g_kernels.cu)

@@ -1900,7 +1900,7 @@ void launch_pbar_init(const Ctx& c, cudaStream_t st, CState U, double p_ref, dou
 // instance computes exactly what a single-grid solver on it computes.
 struct BatchShared {
     Ctx c;
-    double red[32];
+    double red[64];
     double bc;
 };
 SPB6G_DEV double b_max(double v, BatchShared& s) {
@@ -2079,9 +2079,15 @@ SPB6G_DEV int b_stage(BatchShared& s, BatchInst& B, int rks, double Ae[3][3], do
     if (rc != SPB6G_OK) return rc;
     if (tid == 0 && res > B.maxres) B.maxres = res;
     b_clear(&c.ns->fail, 1);
-    for (int x = tid; x < c.n; x += nth) final_at(c, x);
+    double tm[2] = {0.0, 0.0};  // st_Tmax of the stage's final state (:1064-1070)
+    for (int x = tid; x < c.n; x += nth) final_at(c, x, tm);
+    block_fold<RedMax, 2>(tm, s.red);
     if (b_flag(&c.ns->fail)) return SPB6G_NEWTON_FAIL;
-    if (tid == 0) B.stages++;
+    if (tid == 0) {
+        B.stages++;
+        B.tmax[0] = SMAX(B.tmax[0], tm[0]);
+        B.tmax[1] = SMAX(B.tmax[1], tm[1]);
+    }
     return SPB6G_OK;
 }
 template <int TW>
@@ -2165,7 +2171,7 @@ __global__ void __launch_bounds__(256) k_batch(BatchInst* insts, const int* list
         if (threadIdx.x == 0) s.c = B.c;
         __syncthreads();
         for (int k = 0; k < nsteps; k++) {
-            const bool stop = B.status != SPB6G_OK || !(B.t < B.tend);
+            const bool stop = B.status != SPB6G_OK || !(B.t < B.tend * (1 - 1e-12));  // as spb6g_advance
             __syncthreads();
             if (stop) break;
             const int rc = b_step<TW>(s, B, batch_smem);

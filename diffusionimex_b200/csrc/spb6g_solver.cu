@@ -1428,6 +1428,13 @@ struct spb6g_batch {
 };
 
 namespace {
+// What the batched kernel runs: 1D non-periodic grids, SG / NASG phases, p relaxation
+// (instantaneous), per-face Rusanov speed, a fresh Jacobian every Newton iteration, second order,
+// FP64.
+bool batch_config_ok(const spb6g_config& c) {
+    return c.ny == 1 && c.bc[0] != SPB6G_BC_PERIODIC && c.kind[0] == 0 && c.kind[1] == 0 && c.relax == 0 &&
+           c.rus_local == 1 && std::isinf(c.mu_rate) && c.unify != 1 && c.jreuse == 0 && c.order != 1 && c.precision == 0;
+}
 void batch_pack(spb6g_batch* b) {
     for (size_t i = 0; i < b->inst.size(); i++) {
         spb6g_solver* s = b->inst[i];
@@ -1447,6 +1454,7 @@ void batch_pack(spb6g_batch* b) {
         B.ramp = cf.ramp; B.acdt = cf.acdt; B.rk = cf.rk; B.newton_iter = cf.newton_iter;
         B.steps = s->stats.steps; B.rejects = s->stats.rejects; B.rk1 = s->stats.rk1; B.stages = s->stats.stages;
         B.newton_it = s->stats.newton_it; B.floor_count = s->stats.floor_count; B.maxres = s->stats.maxres;
+        B.tmax[0] = s->stats.tmax[0]; B.tmax[1] = s->stats.tmax[1];
     }
 }
 void batch_unpack(spb6g_batch* b) {
@@ -1459,6 +1467,7 @@ void batch_unpack(spb6g_batch* b) {
         s->t = B.t; s->dt = B.dt; s->dtprev = B.dtprev; s->startup = B.startup != 0;
         s->stats.steps = B.steps; s->stats.rejects = B.rejects; s->stats.rk1 = B.rk1; s->stats.stages = B.stages;
         s->stats.newton_it = B.newton_it; s->stats.floor_count = B.floor_count; s->stats.maxres = B.maxres;
+        s->stats.tmax[0] = B.tmax[0]; s->stats.tmax[1] = B.tmax[1];
         b->status[i] = B.status;
     }
 }
@@ -1553,11 +1562,11 @@ int batch_run(spb6g_batch* b, int nsteps, int threads, int tw, float* ms) {
     CK(cudaStreamSynchronize(b->st));
     if (ms) { cudaEventElapsedTime(ms, e0, e1); cudaEventDestroy(e0); cudaEventDestroy(e1); }
     batch_unpack(b);
-    for (spb6g_solver* s : b->inst) s->nlaunch += 0;
     for (size_t i = 0; i < b->status.size(); i++)
         if (b->status[i] != SPB6G_OK) return b->status[i];
     return SPB6G_OK;
 }
+
 }  // namespace
 
 extern "C" {
@@ -1566,12 +1575,7 @@ int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     if (!cfgs || !out || count < 1) return SPB6G_BAD_ARG;
     *out = nullptr;
     for (int i = 0; i < count; i++)
-        if (cfgs[i].ny != 1 || cfgs[i].bc[0] == SPB6G_BC_PERIODIC || cfgs[i].device != cfgs[0].device ||
-            cfgs[i].kind[0] != 0 || cfgs[i].kind[1] != 0 || cfgs[i].relax != 0 ||
-            cfgs[i].rus_local != 1 || !std::isinf(cfgs[i].mu_rate) || cfgs[i].unify == 1 ||
-            cfgs[i].jreuse != 0 || cfgs[i].order == 1)  // the batched kernel: SG / NASG, p (instantaneous), per-face Rusanov
-                                  // speed, a fresh Jacobian every Newton iteration
-            return SPB6G_UNSUPPORTED;
+        if (!batch_config_ok(cfgs[i]) || cfgs[i].device != cfgs[0].device) return SPB6G_UNSUPPORTED;
     spb6g_batch* b = new spb6g_batch();
     b->device = cfgs[0].device;
     for (int i = 0; i < count; i++) {

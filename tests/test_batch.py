@@ -56,3 +56,28 @@ def test_autotune_restores_the_state_and_keeps_a_shape():
         assert b.instance(i).stats()["steps"] == 5
         assert np.array_equal(b.instance(i).state(), U), i
     b.close()
+
+
+@pytest.mark.parametrize("which", ["tube1000_30steps", "case87_N200_tend", "nasg_instance_50steps"])
+def test_batch_of_one_matches_the_host_loop_to_t_end(which):
+    """One grid in the batched kernel against the host-driven loop: state, pressure, counters, time,
+    step size, largest residual and the phase-temperature maxima (st_Tmax) bitwise -- also over a
+    whole run to t_end, where the kernel stops as spb6g_advance does."""
+    if which == "tube1000_30steps":
+        c, steps = cases.water_air_tube(1000), 30
+    elif which == "case87_N200_tend":
+        c, steps = cases.reference_case(87, 200), 0
+    else:
+        c, steps = next(b for b in cases.riemann_batch(count=512, seed=0) if b["nasg"]), 50
+    Uh, Ph, ph, sh = _single(c, steps)
+    b = BatchSolver([c])
+    b.advance(steps if steps > 0 else 1 << 20)
+    assert b.status(0) == 0
+    v = b.instance(0)
+    sd = v.stats()
+    Pd, pd = v.pressure()
+    assert np.array_equal(v.state(), Uh) and np.array_equal(Pd, Ph) and pd == ph
+    for k in ("steps", "rejects", "rk1", "stages", "newton_it", "floor_count", "t", "dt", "maxres"):
+        assert sd[k] == sh[k], (k, sd[k], sh[k])
+    assert sd["tmax"] == sh["tmax"]
+    b.close()
