@@ -1360,49 +1360,66 @@ SPB6G_DEV double rate_scale(const Ctx& c, double tscale) {
 // same row, above; west to east) as differences to the centre over dstd_f; the
 // 64th value is the centre's last rate change (R - R2) / sigma.  BF16.
 constexpr double FEAT_CLAMP = 1024.0;
-__global__ void k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X) {
+// One block per FT_X x FT_Y tile: the seven fields of the tile and its one-cell ring go to shared
+// memory once (each through the boundary maps, as every stencil read), then every thread forms its
+// cell's row from there.  Neighbour m = 1..8 of the row runs over the rows below, the same row and
+// the rows above, west to east.
+constexpr int FT_X = 32, FT_Y = 8;
+__global__ void __launch_bounds__(FT_X * FT_Y, 3) k_features(Ctx c, FeatureNorm nm, __nv_bfloat16* __restrict__ X) {
+    __shared__ double F[NFIELD][FT_Y + 2][FT_X + 2];
     const Geom& g = c.g;
     const double isig = 1.0 / rate_scale(c, nm.tscale);
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < c.n; x += gridDim.x * blockDim.x) {
-        const int i = x % g.nx, j = x / g.nx;
-        double v[9][NFIELD];
-        int k = 0;
-        for (int dj = -1; dj <= 1; dj++)
-            for (int di = -1; di <= 1; di++) {
-                double q[NV];
-                xs_at(c, i + di, j + dj, q);
-                double* f = v[(dj == 0 && di == 0) ? 0 : ++k];
-                const int m = mp_index(g, i + di, j + dj);
-                f[0] = q[IM1] + q[IM2];
-                f[1] = q[IMU];
-                f[2] = q[IMV];
-                f[3] = q[IA1];
-                f[4] = q[IEN];
-                f[5] = c.P[m];
-                f[6] = c.Prate ? c.Prate[m] * isig : 0.0;
-            }
-        // normalised values are clamped to +-FEAT_CLAMP (a field that was constant in the pilot
-        // run has a tiny scale), and a non-finite value reads as 0
-        auto fb = [](double z) {
-            z = z == z ? fmin(fmax(z, -FEAT_CLAMP), FEAT_CLAMP) : 0.0;
-            return __float2bfloat16_rn((float)z);
-        };
-        __align__(16) __nv_bfloat16 row[64];
+    const int i0 = blockIdx.x * FT_X, j0 = blockIdx.y * FT_Y;
+    for (int t = threadIdx.x; t < (FT_X + 2) * (FT_Y + 2); t += FT_X * FT_Y) {
+        const int lx = t % (FT_X + 2), ly = t / (FT_X + 2);
+        const int i = i0 - 1 + lx, j = j0 - 1 + ly;
+        if (i > g.nx || j > g.ny) continue;  // beyond the ring of the last cells
+        double q[NV];
+        xs_at(c, i, j, q);
+        const int m = mp_index(g, i, j);
+        F[0][ly][lx] = q[IM1] + q[IM2];
+        F[1][ly][lx] = q[IMU];
+        F[2][ly][lx] = q[IMV];
+        F[3][ly][lx] = q[IA1];
+        F[4][ly][lx] = q[IEN];
+        F[5][ly][lx] = c.P[m];
+        F[6][ly][lx] = c.Prate ? c.Prate[m] * isig : 0.0;
+    }
+    __syncthreads();
+    const int li = threadIdx.x % FT_X, lj = threadIdx.x / FT_X;
+    const int i = i0 + li, j = j0 + lj;
+    if (i >= g.nx || j >= g.ny) return;
+    const size_t x = (size_t)j * g.nx + i;
+    // normalised values are clamped to +-FEAT_CLAMP (a field that was constant in the pilot
+    // run has a tiny scale), and a non-finite value reads as 0
+    auto fb = [](double z) {
+        z = z == z ? fmin(fmax(z, -FEAT_CLAMP), FEAT_CLAMP) : 0.0;
+        return __float2bfloat16_rn((float)z);
+    };
+    constexpr int DI[9] = {0, -1, 0, 1, -1, 1, -1, 0, 1}, DJ[9] = {0, -1, -1, -1, 0, 0, 1, 1, 1};
+    auto value = [&](int idx) -> __nv_bfloat16 {
+        if (idx == 63) return fb(c.Prate ? (c.Prate[x] - c.Prate2[x]) * isig : 0.0);
+        const int f = idx / 9, m = idx % 9;
+        const double v0 = F[f][lj + 1][li + 1];
+        if (m == 0) return fb((v0 - nm.mean[f]) * nm.istd[f]);
+        return fb((F[f][lj + 1 + DJ[m]][li + 1 + DI[m]] - v0) * nm.idstd[f]);
+    };
+    uint4* dst = (uint4*)(X + x * 64);
 #pragma unroll
-        for (int f = 0; f < NFIELD; f++) {
-            row[f * 9] = fb((v[0][f] - nm.mean[f]) * nm.istd[f]);
+    for (int q = 0; q < 8; q++) {
+        unsigned w[4];
 #pragma unroll
-            for (int m = 1; m < 9; m++) row[f * 9 + m] = fb((v[m][f] - v[0][f]) * nm.idstd[f]);
+        for (int h = 0; h < 4; h++) {
+            const __nv_bfloat162 p2 = __halves2bfloat162(value(8 * q + 2 * h), value(8 * q + 2 * h + 1));
+            w[h] = *reinterpret_cast<const unsigned*>(&p2);
         }
-        row[63] = fb(c.Prate ? (c.Prate[x] - c.Prate2[x]) * isig : 0.0);
-        uint4* dst = (uint4*)(X + (size_t)x * 64);
-#pragma unroll
-        for (int q = 0; q < 8; q++) dst[q] = ((const uint4*)row)[q];
+        dst[q] = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 void launch_features(const Ctx& c, cudaStream_t st, const FeatureNorm& nm, void* X) {
     SPB6G_MG_FORWARD(launch_features, mg_view(c), st, mg_view(nm), X);
-    k_features<<<blocks_for(c.n), TPB, 0, st>>>(c, nm, (__nv_bfloat16*)X);
+    const dim3 grid((unsigned)((c.g.nx + FT_X - 1) / FT_X), (unsigned)((c.g.ny + FT_Y - 1) / FT_Y));
+    k_features<<<grid, FT_X * FT_Y, 0, st>>>(c, nm, (__nv_bfloat16*)X);
     count(c, 1);
 }
 // Step towards a predicted pressure.  The network predicts how far the stage's pressure

@@ -83,6 +83,7 @@ struct spb6g_solver {
     bool jac_ready = false;             // a Jacobian has been built (its diagonal's inverse is in dinv)
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
     double* gstore = nullptr;           // (GRAM_K + 1) x n residuals of the residual-minimising start
+    double* scstore = nullptr;          // GRAM_K x n row scales of its candidates
     double* gram_part = nullptr;        // its per-block inner products
     double* gram = nullptr;             // and their totals
     int warm_mode = 15;                 // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
@@ -324,9 +325,12 @@ static bool solve_gram(const double* m, int K, double* x) {
 
 // Evaluates the residual at P + dP (into Pn, Gn, scn), copying Gn to `keep` if given; r is the
 // max-norm, or infinity where a closure failed.
-static int eval_warm(spb6g_solver* s, Ctx& c, const char* what, double* keep, double best, double& r) {
+static int eval_warm(spb6g_solver* s, Ctx& c, const char* what, double* keep, double best, double& r,
+                     double* keep_sc = nullptr) {
     launch_residual(c, s->st, 1, 1.0);
     if (keep && cudaMemcpyAsync(keep, c.Gn, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st) != cudaSuccess)
+        return -1;
+    if (keep_sc && cudaMemcpyAsync(keep_sc, c.scn, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st) != cudaSuccess)
         return -1;
     if (sync_read(s, false)) return -1;
     r = s->pin->ns.fail ? INFINITY : s->pin->ns.res;
@@ -408,7 +412,8 @@ int newton(spb6g_solver* s, double& resfinal) {
                     cres[k] = INFINITY;
                     if (!avail[k]) continue;
                     guess(coef[k]);
-                    if (eval_guess(names[k], gst + (size_t)(k + 1) * s->n, cres[k]) < 0) return SPB6G_CUDA_ERROR;
+                    if (eval_warm(s, c, names[k], gst + (size_t)(k + 1) * s->n, res, cres[k], s->scstore + (size_t)k * s->n) < 0)
+                        return SPB6G_CUDA_ERROR;
                 }
                 // directions: the extrapolation from P0, the other terms from the extrapolation
                 // (candidates whose closures failed are left out); g[0] the residual at P0, g[1]
@@ -452,10 +457,17 @@ int newton(spb6g_solver* s, double& resfinal) {
                     pick = cc;
                     s->stats.combined++;
                 } else if (best >= 0) {
-                    double r = 0;
+                    // the candidate's trial state from its kept residual and row scales: Pn = P0 + dP
+                    // (as the residual's trial forms it), Gn, scn
+                    const size_t nb = (size_t)s->n * sizeof(double);
                     guess(coef[best]);
-                    if (eval_guess(names[best], nullptr, r) < 0) return SPB6G_CUDA_ERROR;
-                    take(r);
+                    CK(cudaMemcpyAsync(c.Pn, c.P, nb, cudaMemcpyDeviceToDevice, s->st));
+                    Ctx cp = c;
+                    cp.P = c.Pn;
+                    launch_apply_step(cp, s->st);
+                    CK(cudaMemcpyAsync(c.Gn, gst + (size_t)(best + 1) * s->n, nb, cudaMemcpyDeviceToDevice, s->st));
+                    CK(cudaMemcpyAsync(c.scn, s->scstore + (size_t)best * s->n, nb, cudaMemcpyDeviceToDevice, s->st));
+                    take(cres[best]);
                     pick = coef[best];
                     if (best == 3) s->stats.learned++;
                     else if (best == 0) s->stats.extrapolated++;
@@ -1346,10 +1358,12 @@ static int ensure_warm_buffers(spb6g_solver* s) {
         if (cudaMalloc((void**)b, (size_t)s->n * sizeof(float)) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(*b);
     }
-    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->Prate3, &s->x0buf, &s->rate_sc, &s->gstore, &s->gram_part, &s->gram}) {
+    for (double** b : {&s->Pstart, &s->Prate, &s->Prate2, &s->Prate3, &s->x0buf, &s->rate_sc, &s->gstore, &s->scstore,
+                        &s->gram_part, &s->gram}) {
         if (*b) continue;
         const size_t cnt = b == &s->rate_sc ? 2
                            : b == &s->gstore ? (size_t)(GRAM_K + 1) * s->n
+                           : b == &s->scstore ? (size_t)GRAM_K * s->n
                            : b == &s->gram_part ? (size_t)red_blocks(s->n, RED_THREADS) * GRAM_Q
                            : b == &s->gram ? (size_t)GRAM_Q
                                                  : (size_t)s->n;
