@@ -84,6 +84,7 @@ struct spb6g_solver {
     double* x0buf = nullptr;            // learned first BiCGStab iterate of a stage
     double* gstore = nullptr;           // (GRAM_K + 1) x n residuals of the residual-minimising start
     double* scstore = nullptr;          // GRAM_K x n row scales of its candidates
+    NewtonScalars* cand_ns = nullptr;   // and their norms and failure flags
     double* gram_part = nullptr;        // its per-block inner products
     double* gram = nullptr;             // and their totals
     int warm_mode = 15;                 // bits: 1 learned Newton start, 2 learned first BiCGStab iterate,
@@ -278,20 +279,21 @@ int caldt(spb6g_solver* s, bool acoustic, double& inv) {
 
 // Coefficients x minimising ||g0 + sum_j x_j w_j||_2 from the Gram sums m (k_gram's layout):
 // the normal equations by Cholesky, with a relative ridge of 1e-12 on the diagonal, over the
-// directions whose ||w_j||^2 is above 1e-24 of the largest (the others get 0: a zero network
-// output adds no direction).  False when nothing is left or the system is not finite.
-static bool solve_gram(const double* m, int K, double* x) {
+// directions of `mask` whose ||w_j||^2 is above 1e-24 of the largest (the others get 0: a zero
+// network output adds no direction).  False when nothing is left or the system is not finite.
+static bool solve_gram(const double* m, int K, double* x, unsigned mask = ~0u) {
     int idx[GRAM_K][GRAM_K];
     for (int j = 0, q = 0; j < GRAM_K; j++)
         for (int k = j; k < GRAM_K; k++, q++) idx[j][k] = idx[k][j] = q;
     const double* rhs = m + GRAM_K * (GRAM_K + 1) / 2;
     double dmax = 0.0;
-    for (int i = 0; i < K; i++) dmax = std::max(dmax, m[idx[i][i]]);
+    for (int i = 0; i < K; i++)
+        if ((mask >> i) & 1u) dmax = std::max(dmax, m[idx[i][i]]);
     if (!(dmax > 0.0) || !std::isfinite(dmax)) return false;
     int act[GRAM_K], na = 0;
     for (int i = 0; i < K; i++) {
         x[i] = 0.0;
-        if (m[idx[i][i]] > 1e-24 * dmax) act[na++] = i;
+        if (((mask >> i) & 1u) && m[idx[i][i]] > 1e-24 * dmax) act[na++] = i;
     }
     double L[GRAM_K][GRAM_K] = {}, y[GRAM_K], z[GRAM_K];
     for (int i = 0; i < na; i++) {
@@ -407,44 +409,57 @@ int newton(spb6g_solver* s, double& resfinal) {
                 auto guess = [&](const double* k) {
                     launch_guess(c, s->st, k[3] != 0.0 ? s->ybuf : nullptr, s->norm.tscale, k[0], k[1], k[2], k[3]);
                 };
+                // the candidates' residuals (kept with their row scales and norms), then the Gram
+                // sums over all of them, with one read-back for everything
                 double cres[NC];
                 for (int k = 0; k < NC; k++) {
                     cres[k] = INFINITY;
                     if (!avail[k]) continue;
                     guess(coef[k]);
-                    if (eval_warm(s, c, names[k], gst + (size_t)(k + 1) * s->n, res, cres[k], s->scstore + (size_t)k * s->n) < 0)
-                        return SPB6G_CUDA_ERROR;
+                    launch_residual(c, s->st, 1, 1.0);
+                    CK(cudaMemcpyAsync(gst + (size_t)(k + 1) * s->n, c.Gn, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+                    CK(cudaMemcpyAsync(s->scstore + (size_t)k * s->n, c.scn, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+                    CK(cudaMemcpyAsync(s->cand_ns + k, c.ns, sizeof(NewtonScalars), cudaMemcpyDeviceToDevice, s->st));
+                    if (reset_fail(s)) return SPB6G_CUDA_ERROR;
                 }
-                // directions: the extrapolation from P0, the other terms from the extrapolation
-                // (candidates whose closures failed are left out); g[0] the residual at P0, g[1]
-                // at the extrapolation, w_j = g[j] - g[base_j]
+                // directions: the extrapolation from P0, the other terms from the extrapolation;
+                // g[0] the residual at P0, g[1] at the extrapolation, w_j = g[j] - g[base_j]
                 GramIn gi{};
                 double dir[NC][4];
-                int K = 0;
+                int K = 0, cand_of[NC];
                 gi.g[0] = gst;
-                if (std::isfinite(cres[0])) {
-                    for (int k = 0; k < NC; k++) {
-                        if (!std::isfinite(cres[k])) continue;
-                        gi.g[K + 1] = gst + (size_t)(k + 1) * s->n;
-                        gi.base[K + 1] = k == 0 ? 0 : 1;
-                        for (int q = 0; q < 4; q++) dir[K][q] = coef[k][q] - (k == 0 ? 0.0 : coef[0][q]);
-                        K++;
-                    }
+                for (int k = 0; k < NC; k++) {
+                    if (!avail[k]) continue;
+                    gi.g[K + 1] = gst + (size_t)(k + 1) * s->n;
+                    gi.base[K + 1] = k == 0 ? 0 : 1;
+                    for (int q = 0; q < 4; q++) dir[K][q] = coef[k][q] - (k == 0 ? 0.0 : coef[0][q]);
+                    cand_of[K++] = k;
                 }
                 gi.K = K;
+                if (launch_gram(c, s->st, gi, s->gram_part, s->gram) != 0) return SPB6G_CUDA_ERROR;
+                NewtonScalars cns[NC];
+                double m[GRAM_Q];
+                CK(cudaMemcpyAsync(cns, s->cand_ns, sizeof cns, cudaMemcpyDeviceToHost, s->st));
+                CK(cudaMemcpyAsync(m, s->gram, sizeof m, cudaMemcpyDeviceToHost, s->st));
+                CK(cudaStreamSynchronize(s->st));
+                for (int k = 0; k < NC; k++) {
+                    if (!avail[k]) continue;
+                    cres[k] = cns[k].fail ? INFINITY : cns[k].res;
+                    if (s->verbose >= 3) fprintf(stderr, "    %s guess res %.3e, best so far %.3e\n", names[k], cres[k], res);
+                }
+                // the combination over the directions whose candidates' closures succeeded (each
+                // is taken from the extrapolation, so that one has to)
+                unsigned mask = 0;
+                if (std::isfinite(cres[0]))
+                    for (int j = 0; j < K; j++)
+                        if (std::isfinite(cres[cand_of[j]])) mask |= 1u << j;
                 double cc[4] = {0.0, 0.0, 0.0, 0.0}, cres_ls = INFINITY;
-                if (K >= 1) {
-                    if (launch_gram(c, s->st, gi, s->gram_part, s->gram) != 0) return SPB6G_CUDA_ERROR;
-                    double m[GRAM_Q];
-                    CK(cudaMemcpyAsync(m, s->gram, sizeof m, cudaMemcpyDeviceToHost, s->st));
-                    CK(cudaStreamSynchronize(s->st));
-                    double x[GRAM_K];
-                    if (solve_gram(m, K, x)) {
-                        for (int j = 0; j < K; j++)
-                            for (int q = 0; q < 4; q++) cc[q] += x[j] * dir[j][q];
-                        guess(cc);
-                        if (eval_guess("combined", nullptr, cres_ls) < 0) return SPB6G_CUDA_ERROR;
-                    }
+                double x[GRAM_K];
+                if (mask && solve_gram(m, K, x, mask)) {
+                    for (int j = 0; j < K; j++)
+                        for (int q = 0; q < 4; q++) cc[q] += x[j] * dir[j][q];
+                    guess(cc);
+                    if (eval_guess("combined", nullptr, cres_ls) < 0) return SPB6G_CUDA_ERROR;
                 }
                 // the smallest max-norm among the plain start, the candidates and the combination
                 int best = -1;
@@ -1349,6 +1364,10 @@ int spb6g_set_feature_norm(spb6g_solver* s, const double* norm) {
     return ensure_warm_buffers(s);
 }
 static int ensure_warm_buffers(spb6g_solver* s) {
+    if (!s->cand_ns) {
+        if (cudaMalloc((void**)&s->cand_ns, GRAM_K * sizeof(NewtonScalars)) != cudaSuccess) return SPB6G_CUDA_ERROR;
+        s->allocs.push_back(s->cand_ns);
+    }
     if (!s->featbuf) {
         if (cudaMalloc(&s->featbuf, (size_t)s->n * 128) != cudaSuccess) return SPB6G_CUDA_ERROR;
         s->allocs.push_back(s->featbuf);
