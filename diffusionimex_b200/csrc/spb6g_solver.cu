@@ -1513,21 +1513,11 @@ void batch_unpack(spb6g_batch* b) {
 // launches.
 int batch_plan(spb6g_batch* b, int threads, int tw) {
     const int count = (int)b->inst.size();
-    long nmax = 1;
-    for (spb6g_solver* s : b->inst) nmax = std::max(nmax, (long)s->n);
-    auto block_of = [&](long n, long per_thread) {
-        const long t = (n + 32L * per_thread - 1) / (32L * per_thread) * 32L;
-        return (int)std::min<long>(std::max<long>(t, 32L), threads);
-    };
-    const long slots = (long)batch_max_blocks(256, tw, b->device) * 256L * 15L / 16L;
-    long per_thread = (nmax + threads - 1) / threads;
-    for (; per_thread < nmax; per_thread++) {
-        long total = 0;
-        for (spb6g_solver* s : b->inst) total += block_of(s->n, per_thread);
-        if (total <= slots) break;
-    }
+    std::vector<int64_t> cells(count);
+    for (int i = 0; i < count; i++) cells[i] = b->inst[i]->n;
+    const int64_t slots = (int64_t)batch_max_blocks(256, tw, b->device) * 256 * 15 / 16;
     std::vector<int> bs(count);
-    for (int i = 0; i < count; i++) bs[i] = block_of(b->inst[i]->n, per_thread);
+    if (spb6g_batch_block_sizes(cells.data(), count, threads, slots, bs.data(), nullptr) != SPB6G_OK) return SPB6G_UNSUPPORTED;
     b->order.resize(count);
     for (int i = 0; i < count; i++) b->order[i] = i;
     std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
@@ -1603,6 +1593,31 @@ int batch_run(spb6g_batch* b, int nsteps, int threads, int tw, float* ms) {
 }  // namespace
 
 extern "C" {
+
+int spb6g_batch_block_sizes(const int64_t* cells, int count, int threads, int64_t slots, int* block,
+                            int64_t* per_thread_out) {
+    if (!cells || !block || count < 1 || threads < 32 || threads > 256 || threads % 32 != 0 || slots < 0)
+        return SPB6G_BAD_ARG;
+    int64_t nmax = 1;
+    for (int i = 0; i < count; i++) {
+        if (cells[i] < 1) return SPB6G_BAD_ARG;
+        nmax = std::max(nmax, cells[i]);
+    }
+    auto block_of = [&](int64_t n, int64_t per_thread) {
+        const int64_t t = (n + 32 * per_thread - 1) / (32 * per_thread) * 32;
+        return (int)std::min<int64_t>(std::max<int64_t>(t, 32), threads);
+    };
+    int64_t per_thread = (nmax + threads - 1) / threads;
+    if (slots > 0)
+        for (; per_thread < nmax; per_thread++) {
+            int64_t total = 0;
+            for (int i = 0; i < count; i++) total += block_of(cells[i], per_thread);
+            if (total <= slots) break;
+        }
+    for (int i = 0; i < count; i++) block[i] = block_of(cells[i], per_thread);
+    if (per_thread_out) *per_thread_out = per_thread;
+    return SPB6G_OK;
+}
 
 int spb6g_batch_create(const spb6g_config* cfgs, int count, spb6g_batch** out) {
     if (!cfgs || !out || count < 1) return SPB6G_BAD_ARG;

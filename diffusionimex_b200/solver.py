@@ -131,6 +131,7 @@ def library() -> ctypes.CDLL:
         "spb6g_batch_advance": (I, [P, I, P]),
         "spb6g_batch_autotune": (I, [P, I, P, P, P]),
         "spb6g_batch_launches": (I, [P]),
+        "spb6g_batch_block_sizes": (I, [P, I, I, ctypes.c_int64, P, P]),
         "spb6g_set_feature_norm": (I, [P, P]),
         "spb6g_set_warmstart": (I, [P, P]),
         "spb6g_set_warmstart_mode": (I, [P, I]),
@@ -463,6 +464,20 @@ class Solver:
         ng = ctypes.c_int()
         self._check(self.lib.spb6g_timing_get(self.h, ms, cnt, 16, ctypes.byref(ng)), "timing")
         return {self.lib.spb6g_timing_name(g).decode(): (ms[g], cnt[g]) for g in range(ng.value)}
+
+
+def batch_block_sizes(cells, threads: int, slots: int = 0):
+    """Block size of each grid of a batch (spb6g_batch_block_sizes; host only): threads in proportion
+    to its cells, a multiple of 32 from 32 to `threads`, with the fewest cells per thread for which
+    the blocks' threads fit in `slots` (0: no limit).  Returns (block sizes, cells per thread)."""
+    lib = library()
+    c = np.ascontiguousarray(cells, dtype=np.int64)
+    out = np.zeros(len(c), dtype=np.int32)
+    per = ctypes.c_int64()
+    rc = lib.spb6g_batch_block_sizes(_ptr(c), int(len(c)), int(threads), int(slots), _ptr(out), ctypes.byref(per))
+    if rc != 0:
+        raise SolverError(rc, "spb6g_batch_block_sizes")
+    return out, per.value
 
 
 class BatchSolver:

@@ -350,6 +350,13 @@ int spb6g_batch_set_shape(spb6g_batch* b, int threads, int tile);
 /* nsteps time steps of every grid (fewer for a grid that reaches its t_end); device time
  * of the launch in *ms if not NULL.  Returns the first grid's error, if any. */
 int spb6g_batch_advance(spb6g_batch* b, int nsteps, float* ms);
+/* The block size each grid of a batch gets (host only, no device): threads in proportion to its
+ * cells, a multiple of 32 from 32 to `threads` (the largest grid's cap), with the fewest cells
+ * per thread for which the blocks' threads fit in `slots` (0: no limit; the batch uses 15/16 of
+ * the device's thread slots at the kernel's register count); the cells per thread in
+ * *per_thread if not NULL. */
+int spb6g_batch_block_sizes(const int64_t* cells, int count, int threads, int64_t slots, int* block,
+                            int64_t* per_thread);
 /* Kernel launches of one advance under the current shape (one per block size); 0 before the
  * first advance under it, or a negative status. */
 int spb6g_batch_launches(spb6g_batch* b);
