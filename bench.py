@@ -692,6 +692,7 @@ def run_ours(args, case, rank: int, world: int, local_rank: int, dist):
             "L1_rel_p_extrapolation_vs_plain": learned.l1_rel(ext_r["p"], plain_r["p"]),
             "same_steps": plain_r["d"]["steps"] == d["steps"] and plain_r["d"]["rejects"] == d["rejects"],
             "network": os.path.relpath(learned.DEFAULT_WEIGHTS, ROOT),
+            "warmstart_mode": 15,  # the library default: candidate starts, their combination, first iterates
         }
     e2e = None if args.no_e2e else e2e_run(case, args, local_rank, dist, mlp, norm,
                                            {k: d[k] for k in ("steps", "rejects", "newton_it", "bicg_it")})
