@@ -55,7 +55,7 @@ ALG_BYTES = {
 }
 
 
-# SURVEY-defined algorithmic bytes (compulsory FP64 traffic): the BiCGStab iteration per row (2 x 40 B of
+# Algorithmic bytes (compulsory FP64 traffic): the BiCGStab iteration per row (2 x 40 B of
 # matrix rows, 24 vector streams x 8 B) and the fused flux kernel per cell, stage 1 / later stages
 # (2D: 64 n_in + 8 (8 + 5); 1D: 64 n_in + 8 (8 + 3))
 BICG_BYTES_PER_ROW_ITER = 272
@@ -576,7 +576,7 @@ def counts(r: dict) -> dict:
 
 
 def rooflines(r: dict, n: int, two_d: bool, workload: str = "") -> dict:
-    """Algorithmic-byte rooflines (SURVEY-defined bytes per unit) of the BiCGStab solve, the fused
+    """Algorithmic-byte rooflines (the compulsory bytes per unit above) of the BiCGStab solve, the fused
     flux kernel and the whole step, from the window's CUDA-event group times and counts."""
     peak, peak_kind = peaks()
     g, d = r["groups"], r["d"]
