@@ -8,12 +8,16 @@ stage's pressure P_start + dts (R + sigma y) from the 3x3 stencils of
 over the cells and dts the stage's time span: y = 0 is the linear extrapolation
 of the pressure, and the network learns the departure from it in units of sigma,
 so the target is scale-free across fields, regimes and the start-up ramp.  The
-solver starts Newton from the guess of smallest residual norm among the plain
-guess, the extrapolation and the network's guess; when the network's guess is
-not the start, its step seeds the first BiCGStab iterate (in a least-squares
-combination with the plain start, never with a larger initial residual).  Newton
-and BiCGStab keep their tolerances, so the converged pressure is the plain
-solve's to the solver tolerance.
+solver starts Newton from the guess of smallest residual max-norm among the plain
+guess, the extrapolation, the second-order extrapolation, the network's guess and
+(warm-start mode bit 8, on by default) the combination of their steps that
+minimises the residual's 2-norm with the residual taken linear in P -- the
+network's output is one direction of that combination; when the network's guess
+is not the start, its step seeds the first BiCGStab iterate, and the last Newton
+correction the stage's later ones (in a least-squares combination with the plain
+start, never with a larger initial residual).  Newton and BiCGStab keep their
+tolerances, a warm-started stage always takes one Newton step, and the converged
+pressure is the plain solve's to the solver tolerance.
 
 At the low-Mach operating point Newton converges linearly (a constant
 contraction of about 0.4-0.6 per iteration with full steps), so every factor
